@@ -1,0 +1,284 @@
+"""Benchmark: Gcell-updates/s of the composite-grid time loop on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--small]
+
+Workload (one step = one pass of main.cpp's time loop over the whole composite):
+the three-grid ratio-3 composite 1081x1081x121 @ 5 m / 361x361x161 @ 15 m /
+121x121x101 @ 45 m (163,856,303 points), FP32 fields, free surface, Ricker vz
+source at the surface centre, 1081 vz surface receivers, energy every 100
+steps.  Inputs are seeded synthetic media (no dataset exists for this path).
+N > 1 runs N independent replicas (one per GPU, launched by torchrun): the
+path has no exchange step, so there is no collective on the data path.
+
+The line printed by rank 0 carries the device-timed throughput (`value`), the
+end-to-end throughput through the C ABI with host buffers (`e2e`), the HBM
+roofline of the dominant kernel (`roofline`), the reference's OpenMP CPU path
+timed on this host (`cpu_baseline`), SM clocks sampled during the timed
+region, and the number of kernels launched.
+"""
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BYTES_PER_CELL = {"iso": 132, "ortho9": 148, "gen21": 196}   # compulsory FP32 traffic per cell-update
+STRESS_BYTES = {"iso": 80, "ortho9": 96, "gen21": 144}       # stress kernel: 3v + 6 sigma (rmw) + N_C words
+VEL_BYTES = 52                                               # velocity kernel: 6 sigma + 3 v (rmw) + buoyancy
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            return float(json.load(fh)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampling (200 ms) during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and r[5 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def cpu_reference(steps_sample=None, warm=2):
+    """The reference's own OpenMP time loop (oracle/_ref/libecsg_ref64.so, the
+    unmodified sources compiled with -O3 -fopenmp) on its own experiment
+    tests/test1-cmp-eci-ii/eci (two grids at ratio 2, 13,055,365 points; the
+    reference cannot run ratio 3), check_energy off, all host threads."""
+    from ecsg_b200.workloads import eci_test_case
+    from oracle.ref import RefRun
+    cores = len(os.sched_getaffinity(0))
+    case = eci_test_case(1)
+    r = RefRun(case, energy=False, threads=cores)
+    try:
+        r.run(warm, 0)
+        # size the sample to roughly 10-20 s of CPU work
+        t1 = r.run(2, warm)
+        n = steps_sample or max(2, min(200, int(15.0 / max(t1 / 2, 1e-3))))
+        t = r.run(n, warm + 2)
+    finally:
+        r.close()
+    pts = case.points()
+    return {"value": pts * n / t / 1e9, "unit": "Gcell/s", "cores": cores, "kind": "reference",
+            "sample": "%d steps of the reference experiment test1-cmp-eci-ii/eci (2 grids, ratio 2, %d points, "
+                      "FP64 as shipped, energy off) on %d host threads; wall clock" % (n, pts, cores)}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    try:
+        base = cpu_reference()
+    except Exception as e:  # the reference build did not travel
+        print(json.dumps({"impl": "reference", "unavailable": "reference CPU build not runnable: %s" % e}))
+        return
+    line = {"impl": "reference", "metric": "Gcell-updates/s", "value": base["value"], "unit": "Gcell/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "reference experiment test1-cmp-eci-ii/eci (CPU twin of the three-grid "
+                                   "benchmark: the reference implements ratio 2 and isotropic media only)"},
+            "cpu_baseline": base,
+            "e2e": {"value": base["value"], "unit": "Gcell/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--small", action="store_true", help="1/27-volume case (profiling)")
+    ap.add_argument("--energy-every", type=int, default=100)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import ecsg_b200
+    from ecsg_b200.workloads import three_grid_case, THREE_GRID
+
+    rank, world, local = dist_env()
+    pg = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+        pg = dist
+
+    grids = THREE_GRID
+    if args.small:
+        grids = [((360, 360, 40), 5.0), ((120, 120, 54), 15.0), ((40, 40, 34), 45.0)]
+    case = three_grid_case(seed=0, grids=grids, nsteps=args.steps)
+    medium = "iso"
+    pts = case.points()
+    sim = ecsg_b200.Simulation(case, precision="f32", energy=True, device=local)
+    ev = args.energy_every
+
+    def barrier():
+        if pg is not None:
+            import torch
+            t = torch.zeros(1, device="cuda:%d" % local)
+            pg.all_reduce(t)
+            torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if pg is None:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device="cuda:%d" % local)
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    # warm-up (untimed), then the device-timed region (inputs resident in HBM,
+    # 20 GB of fields and media >> 126 MB L2)
+    sim.run(max(args.warmup, 3), energy_every=ev)
+    barrier()
+    with Clocks(local) as clk:
+        sim.run(args.steps, energy_every=ev)
+        run_ms, launches = sim.last_run()
+    barrier()
+    run_ms = max_over_ranks(run_ms)
+    value = pts * args.steps * world / (run_ms * 1e-3) / 1e9
+
+    # end to end through the C ABI with host buffers: source trace H2D from
+    # pinned memory, all steps, receiver traces D2H into pinned memory
+    import torch
+    trace_host = torch.empty((args.steps, len(sim.rec)), dtype=torch.float32).pin_memory().numpy()
+    src_host = torch.from_numpy(np.ascontiguousarray(case.src["trace"], dtype=np.float32)).pin_memory().numpy()
+    L = ecsg_b200.lib()
+    barrier()
+    sim.timer_start()
+    g, ix, iy, iz = sim.src
+    sim._ck(L.ecsg_set_source(sim.h, g, ix, iy, iz, case.src["comp"], src_host.ctypes.data_as(ecsg_b200.c_fp),
+                              src_host.size, float(case.src["scale"])))
+    sim.run(args.steps, energy_every=ev, traces_out=trace_host)
+    e2e_ms = sim.timer_stop()
+    barrier()
+    e2e_ms = max_over_ranks(e2e_ms)
+    e2e = pts * args.steps * world / (e2e_ms * 1e-3) / 1e9
+    h2d = src_host.nbytes / args.steps
+    d2h = trace_host.nbytes / args.steps
+    ok_traces = bool(np.isfinite(trace_host).all())
+
+    # roofline of the dominant kernel from per-kernel CUDA events
+    kt = sim.time_kernels(3)
+    peak, peak_kind = measured_peak()
+    n0 = case.grids[0]["n"]
+    cells0 = (n0[0] + 1) * (n0[1] + 1) * (n0[2] + 1)
+    st_ms, ve_ms = kt["stress"][0], kt["vel"][0]
+    if st_ms >= ve_ms:
+        dom, dom_ms, dom_bytes = "stress_kernel<float,ISO5> (grid 0)", st_ms, STRESS_BYTES[medium] * cells0
+    else:
+        dom, dom_ms, dom_bytes = "vel_kernel<float> (grid 0)", ve_ms, VEL_BYTES * cells0
+    achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
+    step_ms = run_ms / args.steps
+    step_gbs = BYTES_PER_CELL[medium] * pts / (step_ms * 1e-3) / 1e9
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        try:
+            traffic = json.load(open(tpath)).get(dom.split(" ")[0])
+        except Exception:
+            traffic = None
+
+    base = None
+    if rank == 0 and not args.no_cpu_baseline:
+        try:
+            base = cpu_reference()
+        except Exception as e:
+            base = {"value": None, "unit": "Gcell/s", "cores": 0, "kind": "reference", "sample": "unavailable: %s" % e}
+
+    dev_bytes = sim.device_bytes()
+    sim.close()
+    if rank == 0:
+        line = {
+            "metric": "Gcell-updates/s", "value": value, "unit": "Gcell/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "three-grid ratio-3 composite %s, %d points, free surface, Ricker vz point "
+                                   "force, %d vz receivers, energy every %d steps"
+                                   % (" / ".join("%dx%dx%d@%gm" % (n[0] + 1, n[1] + 1, n[2] + 1, h)
+                                                 for n, h in grids), pts, len(sim.rec), ev),
+                       "medium": "isotropic stiffness from the seeded vp/vs/rho model (5 distinct moduli)",
+                       "points": pts, "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "inputs larger than L2: %.1f GB of fields and media resident" % (dev_bytes / 1e9)},
+            "e2e": {"value": e2e, "unit": "Gcell/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "traces_finite": ok_traces},
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
+                         "algorithmic_bytes_per_launch": dom_bytes,
+                         "step_achieved": step_gbs, "step_frac": step_gbs / peak,
+                         "bytes_per_cell_update": BYTES_PER_CELL[medium]},
+            "kernel_ms_per_step": kt,
+            "cpu_baseline": base,
+            "clocks": clk.summary(),
+            "gpu_launches": launches,
+        }
+        print(json.dumps(line))
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,994 @@
+// api.cu -- the C ABI (include/ecsg_b200.h): device state, set-up, operators
+// and the fused time loop.
+//
+// One ecsg_sim owns one CUDA stream and all device memory of a composite run.
+// There is no host fallback: without a usable device every entry point fails.
+#include "ecsg_device.cuh"
+#include "../../include/ecsg_b200.h"
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace ecsg {
+// stencil.cu
+template <typename T>
+cudaError_t launch_vel(const GridDev<T> &, int, int, int, T *const[3], int, cudaStream_t);
+template <typename T>
+cudaError_t launch_vel_mirror(const GridDev<T> &, int, int, int, cudaStream_t);
+template <typename T>
+cudaError_t launch_stress(const GridDev<T> &, int, int, int, int, cudaStream_t);
+// interface.cu
+template <typename T>
+cudaError_t launch_ghost_vz(const GridDev<T> &, const GridDev<T> &, int, int, cudaStream_t);
+template <typename T>
+cudaError_t launch_ghost_syz(const GridDev<T> &, const GridDev<T> &, int, cudaStream_t);
+template <typename T>
+cudaError_t launch_sxz_matrix(const GridDev<T> &, const GridDev<T> &, int, double *, cudaStream_t);
+template <typename T>
+int sxz_solve_blocks(int, int);
+template <typename T>
+cudaError_t launch_sxz_solve(const GridDev<T> &, const GridDev<T> &, int, const SxzWork &, int, cudaStream_t);
+// diag.cu
+template <typename T>
+cudaError_t launch_energy(const GridDev<T> &, int, T *const[3], double *, int, double, double, double, double *,
+                          const int *, int, int, int *, cudaStream_t);
+template <typename T>
+cudaError_t launch_residue(const GridDev<T> &, const GridDev<T> &, int, double, double *, int, double *, cudaStream_t);
+template <typename T>
+cudaError_t launch_avgabs(const GridDev<T> &, int, const int[3], double *, int, double *, cudaStream_t);
+template <typename T>
+cudaError_t launch_src_rec(const SrcRec &, cudaStream_t);
+template <typename T, typename S>
+cudaError_t launch_pack(T *, const Geo &, const S *, int, int, int, int, cudaStream_t);
+template <typename T>
+cudaError_t launch_unpack(double *, const Geo &, const T *, int, int, int, int, cudaStream_t);
+template <typename T>
+cudaError_t launch_iso_medium(const Geo &, const double *, const double *, double *, T *const[5], cudaStream_t);
+} // namespace ecsg
+
+using namespace ecsg;
+
+static const int kPos[9][3] = {{0, 0, 0}, {1, 1, 0}, {1, 0, 1}, {1, 0, 0}, {1, 0, 0},
+                               {1, 0, 0}, {1, 1, 1}, {0, 0, 1}, {0, 1, 0}};
+static const int kStiffPos[9][3] = {{1, 0, 0}, {1, 0, 0}, {1, 0, 0}, {1, 0, 0}, {1, 0, 0},
+                                    {1, 0, 0}, {1, 1, 1}, {0, 0, 1}, {0, 1, 0}};
+
+struct Iface {
+    int r = 2;
+    double *A = nullptr, *B = nullptr, *X0 = nullptr, *X1 = nullptr, *partial = nullptr;
+    int nblocks = 0;
+    bool A_ready = false;
+};
+
+struct ecsg_sim {
+    int ng = 0, R = 1, imode = 1, top_bc = 0, prec = ECSG_F32, medium = ECSG_MEDIUM_ISO, energy = 0;
+    int jacobi_max_iter = 10000, device = 0, sms = 148;
+    double dt = 0;
+    size_t tsize = 4;
+    Geo geo[kMaxGrids];
+    double h[kMaxGrids][3];
+    void *f[kMaxGrids][9] = {};
+    void *b[kMaxGrids] = {};
+    void *c[kMaxGrids][9] = {};
+    int nc = 5;
+    void *vc[kMaxGrids][3] = {};
+    bool medium_set[kMaxGrids] = {};
+    Iface itf[kMaxGrids];
+    // shared device scalars: [0] status, [1] step clock, [2] last sxz sweeps
+    int *ints = nullptr;
+    long long *iters_total = nullptr;   // per interface
+    double *dscal = nullptr;            // [0] energy, [1] total, [2..] last tol per interface, [16..] residue scratch
+    unsigned *bar = nullptr;            // 2 per interface
+    double *partial = nullptr;          // reductions
+    int red_blocks = 0;
+    // source / receivers
+    int src_grid = -1, src_off = 0, src_comp = 0, src_nt = 0;
+    float src_scale = 1.0f;
+    float *src_trace = nullptr;
+    int nrec = 0, rec_comp = 0;
+    int *rec_grid = nullptr, *rec_off = nullptr;
+    float *traces = nullptr;
+    int trace_cap = 0;
+    double *run_energy = nullptr;
+    int run_energy_cap = 0;
+    double *run_res = nullptr;
+    int run_res_cap = 0;
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};   // [0,1] run loop, [2,3] user timer
+    double last_run_ms = 0;
+    long long launches = 0;        // kernels launched by the last ecsg_run (all steps)
+    long long bytes = 0;
+    std::string err;
+};
+
+static int fail(ecsg_sim *s, int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    if (s) s->err = buf;
+    return code;
+}
+
+#define CK(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess) return fail(s, ECSG_ERR_CUDA, "%s: %s (%s:%d)", #call, cudaGetErrorString(e_), __FILE__, __LINE__); \
+    } while (0)
+
+static int dmalloc(ecsg_sim *s, void **p, size_t bytes)
+{
+    CK(cudaMalloc(p, bytes));
+    CK(cudaMemsetAsync(*p, 0, bytes, s->st));
+    s->bytes += (long long)bytes;
+    return ECSG_OK;
+}
+
+template <typename T>
+static GridDev<T> dev(const ecsg_sim *s, int g)
+{
+    GridDev<T> G;
+    memset(&G, 0, sizeof G);
+    G.g = s->geo[g];
+    for (int k = 0; k < 9; k++) G.f[k] = (T *)s->f[g][k];
+    G.b = (const T *)s->b[g];
+    for (int k = 0; k < s->nc; k++) G.c[k] = (const T *)s->c[g][k];
+    for (int d = 0; d < 3; d++) {
+        // FD coefficient of radius 1: fd[0]*dt/h with fd[0] = 1 (init_del_fdcoeff.cpp:19)
+        const double kd = 1.0 * s->dt / s->h[g][d];
+        G.kd[d] = kd;
+        G.k[d] = (T)kd;
+    }
+    return G;
+}
+
+static int field_len(const ecsg_sim *s, int g, int k, int len[3])
+{
+    const Geo &G = s->geo[g];
+    const int n[3] = {G.nx, G.ny, G.nz};
+    for (int d = 0; d < 3; d++) len[d] = kPos[k][d] ? n[d] + 2 * s->R : n[d] + 1 + 2 * s->R;
+    return 0;
+}
+
+// The entry points below take their C linkage from the declarations in
+// include/ecsg_b200.h (extern "C").
+
+int ecsg_device_count(void)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+    return n;
+}
+
+const char *ecsg_last_error(const ecsg_sim *sim) { return sim ? sim->err.c_str() : "null simulation"; }
+
+long long ecsg_device_bytes(const ecsg_sim *sim) { return sim ? sim->bytes : 0; }
+
+int ecsg_create(const ecsg_grid_desc *grids, const ecsg_config *cfg, ecsg_sim **out)
+{
+    if (!grids || !cfg || !out) return ECSG_ERR_INVALID;
+    *out = nullptr;
+    ecsg_sim *s = new ecsg_sim();
+    auto bail = [&](int code) { ecsg_destroy(s); return code; };
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= 0) {
+        fprintf(stderr, "ecsg_b200: no CUDA device available; this library has no CPU path\n");
+        delete s;
+        return ECSG_ERR_NO_DEVICE;
+    }
+    if (cfg->num_grids < 1 || cfg->num_grids > kMaxGrids) { fail(s, ECSG_ERR_INVALID, "num_grids out of range"); return bail(ECSG_ERR_INVALID); }
+    if (cfg->radius != 1) { fail(s, ECSG_ERR_INVALID, "radius %d: the device path implements radius 1", cfg->radius); return bail(ECSG_ERR_INVALID); }
+    if (!(cfg->dt > 0)) { fail(s, ECSG_ERR_INVALID, "dt must be positive"); return bail(ECSG_ERR_INVALID); }
+    if (cfg->imode != ECSG_MODE_ECI) { fail(s, ECSG_ERR_INVALID, "imode %d not supported (energy-conserving mode 1 only)", cfg->imode); return bail(ECSG_ERR_INVALID); }
+    if (cfg->precision != ECSG_F32 && cfg->precision != ECSG_F64) { fail(s, ECSG_ERR_INVALID, "precision"); return bail(ECSG_ERR_INVALID); }
+    if (cfg->medium != ECSG_MEDIUM_ISO && cfg->medium != ECSG_MEDIUM_ORTHO9) { fail(s, ECSG_ERR_INVALID, "medium"); return bail(ECSG_ERR_INVALID); }
+    s->ng = cfg->num_grids;
+    s->R = cfg->radius;
+    s->dt = cfg->dt;
+    s->imode = cfg->imode;
+    s->top_bc = cfg->top_bc;
+    s->prec = cfg->precision;
+    s->medium = cfg->medium;
+    s->energy = cfg->energy ? 1 : 0;
+    s->jacobi_max_iter = cfg->jacobi_max_iter > 0 ? cfg->jacobi_max_iter : 10000;
+    s->device = cfg->device;
+    s->tsize = s->prec == ECSG_F32 ? 4 : 8;
+    s->nc = s->medium == ECSG_MEDIUM_ISO ? 5 : 9;
+    if (cudaSetDevice(s->device) != cudaSuccess) { fail(s, ECSG_ERR_NO_DEVICE, "cudaSetDevice(%d) failed", s->device); return bail(ECSG_ERR_NO_DEVICE); }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, s->device) != cudaSuccess) return bail(fail(s, ECSG_ERR_CUDA, "cudaGetDeviceProperties"));
+    if (prop.major < 10) { fail(s, ECSG_ERR_NO_DEVICE, "device %s is sm_%d%d; this build targets sm_100a", prop.name, prop.major, prop.minor); return bail(ECSG_ERR_NO_DEVICE); }
+    s->sms = prop.multiProcessorCount;
+    if (cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking) != cudaSuccess) return bail(fail(s, ECSG_ERR_CUDA, "stream"));
+    for (int e = 0; e < 4; e++)
+        if (cudaEventCreate(&s->ev[e]) != cudaSuccess) return bail(fail(s, ECSG_ERR_CUDA, "event"));
+
+    for (int g = 0; g < s->ng; g++) {
+        for (int d = 0; d < 3; d++) {
+            if (grids[g].size[d] < 2 || !(grids[g].step[d] > 0)) { fail(s, ECSG_ERR_INVALID, "grid %d: bad size/step", g); return bail(ECSG_ERR_INVALID); }
+            s->h[g][d] = grids[g].step[d];
+        }
+        s->geo[g] = make_geo(grids[g].size[0], grids[g].size[1], grids[g].size[2], s->R);
+        if (s->geo[g].size() >= (int64_t)INT32_MAX) { fail(s, ECSG_ERR_INVALID, "grid %d too large for 32-bit indexing", g); return bail(ECSG_ERR_INVALID); }
+    }
+    for (int i = 1; i < s->ng; i++) {
+        const double rx = s->h[i][0] / s->h[i - 1][0];
+        const int r = (int)std::lround(rx);
+        if (r < 2 || fabs(rx - r) > 1e-6 * r || fabs(s->h[i][1] / s->h[i - 1][1] - r) > 1e-6 * r) { fail(s, ECSG_ERR_INVALID, "interface %d: x/y refinement ratio must be an integer >= 2", i); return bail(ECSG_ERR_INVALID); }
+        if (grids[i - 1].size[0] != r * grids[i].size[0] || grids[i - 1].size[1] != r * grids[i].size[1]) { fail(s, ECSG_ERR_INVALID, "interface %d: fine size must be ratio * coarse size in x and y", i); return bail(ECSG_ERR_INVALID); }
+        if (grids[i].size[1] - 1 > 1024) { fail(s, ECSG_ERR_INVALID, "interface %d: coarse ny %d above the 1025 supported by the vz solve", i, grids[i].size[1]); return bail(ECSG_ERR_INVALID); }
+        s->itf[i].r = r;
+    }
+    int rc;
+    for (int g = 0; g < s->ng; g++) {
+        const size_t fb = (size_t)s->geo[g].size() * s->tsize;
+        for (int k = 0; k < 9; k++)
+            if ((rc = dmalloc(s, &s->f[g][k], fb))) return bail(rc);
+        if ((rc = dmalloc(s, &s->b[g], fb))) return bail(rc);
+        for (int k = 0; k < s->nc; k++)
+            if ((rc = dmalloc(s, &s->c[g][k], fb))) return bail(rc);
+        if (s->energy)
+            for (int k = 0; k < 3; k++)
+                if ((rc = dmalloc(s, &s->vc[g][k], fb))) return bail(rc);
+    }
+    s->red_blocks = 4 * s->sms;
+    if ((rc = dmalloc(s, (void **)&s->partial, sizeof(double) * 12 * (size_t)s->red_blocks))) return bail(rc);
+    if ((rc = dmalloc(s, (void **)&s->ints, sizeof(int) * 4))) return bail(rc);
+    if ((rc = dmalloc(s, (void **)&s->iters_total, sizeof(long long) * kMaxGrids))) return bail(rc);
+    if ((rc = dmalloc(s, (void **)&s->dscal, sizeof(double) * 64))) return bail(rc);
+    if ((rc = dmalloc(s, (void **)&s->bar, sizeof(unsigned) * 2 * kMaxGrids))) return bail(rc);
+    for (int i = 1; i < s->ng; i++) {
+        Iface &I = s->itf[i];
+        const Geo &C = s->geo[i];
+        const size_t nn = (size_t)(C.nx - 1) * (C.ny - 1);
+        const size_t nxy = (size_t)(C.nx + 1) * (C.ny + 1);
+        if ((rc = dmalloc(s, (void **)&I.A, sizeof(double) * 9 * nn))) return bail(rc);
+        if ((rc = dmalloc(s, (void **)&I.B, sizeof(double) * nn))) return bail(rc);
+        if ((rc = dmalloc(s, (void **)&I.X0, sizeof(double) * nxy))) return bail(rc);
+        if ((rc = dmalloc(s, (void **)&I.X1, sizeof(double) * nxy))) return bail(rc);
+        I.nblocks = s->prec == ECSG_F32 ? sxz_solve_blocks<float>((int)nn, s->sms) : sxz_solve_blocks<double>((int)nn, s->sms);
+        if ((rc = dmalloc(s, (void **)&I.partial, sizeof(double) * (size_t)I.nblocks))) return bail(rc);
+    }
+    if (cudaStreamSynchronize(s->st) != cudaSuccess) return bail(fail(s, ECSG_ERR_CUDA, "initial clear"));
+    *out = s;
+    return ECSG_OK;
+}
+
+int ecsg_destroy(ecsg_sim *s)
+{
+    if (!s) return ECSG_OK;
+    if (s->st) cudaStreamSynchronize(s->st);
+    for (int g = 0; g < kMaxGrids; g++) {
+        for (int k = 0; k < 9; k++) cudaFree(s->f[g][k]);
+        cudaFree(s->b[g]);
+        for (int k = 0; k < 9; k++) cudaFree(s->c[g][k]);
+        for (int k = 0; k < 3; k++) cudaFree(s->vc[g][k]);
+        Iface &I = s->itf[g];
+        cudaFree(I.A); cudaFree(I.B); cudaFree(I.X0); cudaFree(I.X1); cudaFree(I.partial);
+    }
+    cudaFree(s->partial); cudaFree(s->ints); cudaFree(s->iters_total); cudaFree(s->dscal); cudaFree(s->bar);
+    cudaFree(s->src_trace); cudaFree(s->rec_grid); cudaFree(s->rec_off); cudaFree(s->traces);
+    cudaFree(s->run_energy); cudaFree(s->run_res);
+    for (int e = 0; e < 4; e++)
+        if (s->ev[e]) cudaEventDestroy(s->ev[e]);
+    if (s->st) cudaStreamDestroy(s->st);
+    delete s;
+    return ECSG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Media and fields
+// ---------------------------------------------------------------------------
+template <typename T>
+static int set_iso(ecsg_sim *s, int g, const float *buoy, const float *s11, const float *s13)
+{
+    const Geo &G = s->geo[g];
+    const size_t nn = (size_t)(G.nx + 1) * (G.ny + 1) * (G.nz + 1);
+    float *stage = nullptr;
+    double *d11 = nullptr, *d13 = nullptr, *d44 = nullptr;
+    const size_t box = (size_t)G.size() * sizeof(double);
+    CK(cudaMalloc(&stage, nn * sizeof(float)));
+    CK(cudaMalloc(&d11, box));
+    CK(cudaMalloc(&d13, box));
+    CK(cudaMalloc(&d44, box));
+    CK(cudaMemsetAsync(d11, 0, box, s->st));
+    CK(cudaMemsetAsync(d13, 0, box, s->st));
+    CK(cudaMemsetAsync(d44, 0, box, s->st));
+    CK(cudaMemcpyAsync(stage, buoy, nn * sizeof(float), cudaMemcpyHostToDevice, s->st));
+    CK((launch_pack<T, float>((T *)s->b[g], G, stage, G.nx + 1, G.ny + 1, G.nz + 1, 0, s->st)));
+    CK(cudaMemcpyAsync(stage, s11, nn * sizeof(float), cudaMemcpyHostToDevice, s->st));
+    CK((launch_pack<double, float>(d11, G, stage, G.nx + 1, G.ny + 1, G.nz + 1, 0, s->st)));
+    CK(cudaMemcpyAsync(stage, s13, nn * sizeof(float), cudaMemcpyHostToDevice, s->st));
+    CK((launch_pack<double, float>(d13, G, stage, G.nx + 1, G.ny + 1, G.nz + 1, 0, s->st)));
+    T *c5[5];
+    for (int k = 0; k < 5; k++) c5[k] = (T *)s->c[g][k];
+    CK(launch_iso_medium<T>(G, d11, d13, d44, c5, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    cudaFree(stage); cudaFree(d11); cudaFree(d13); cudaFree(d44);
+    return ECSG_OK;
+}
+
+int ecsg_set_medium_iso(ecsg_sim *s, int g, const float *buoy, const float *s11, const float *s13)
+{
+    if (!s || g < 0 || g >= s->ng || !buoy || !s11 || !s13) return fail(s, ECSG_ERR_INVALID, "set_medium_iso: bad arguments");
+    if (s->medium != ECSG_MEDIUM_ISO) return fail(s, ECSG_ERR_STATE, "simulation was created for a non-isotropic medium");
+    CK(cudaSetDevice(s->device));
+    int rc = s->prec == ECSG_F32 ? set_iso<float>(s, g, buoy, s11, s13) : set_iso<double>(s, g, buoy, s11, s13);
+    if (rc) return rc;
+    s->medium_set[g] = true;
+    if (g > 0) s->itf[g].A_ready = false;
+    if (g + 1 < s->ng) s->itf[g + 1].A_ready = false;
+    return ECSG_OK;
+}
+
+template <typename T>
+static int set_ortho(ecsg_sim *s, int g, const double *buoy, const double *const c[9])
+{
+    const Geo &G = s->geo[g];
+    const size_t nn = (size_t)(G.nx + 1) * (G.ny + 1) * (G.nz + 1);
+    double *stage = nullptr;
+    CK(cudaMalloc(&stage, nn * sizeof(double)));
+    CK(cudaMemcpyAsync(stage, buoy, nn * sizeof(double), cudaMemcpyHostToDevice, s->st));
+    CK((launch_pack<T, double>((T *)s->b[g], G, stage, G.nx + 1, G.ny + 1, G.nz + 1, 0, s->st)));
+    for (int k = 0; k < 9; k++) {
+        const int l0 = G.nx + 1 - kStiffPos[k][0], l1 = G.ny + 1 - kStiffPos[k][1], l2 = G.nz + 1 - kStiffPos[k][2];
+        CK(cudaMemcpyAsync(stage, c[k], (size_t)l0 * l1 * l2 * sizeof(double), cudaMemcpyHostToDevice, s->st));
+        CK((launch_pack<T, double>((T *)s->c[g][k], G, stage, l0, l1, l2, 0, s->st)));
+        CK(cudaStreamSynchronize(s->st));
+    }
+    cudaFree(stage);
+    return ECSG_OK;
+}
+
+int ecsg_set_medium_ortho9(ecsg_sim *s, int g, const double *buoy, const double *const c[9])
+{
+    if (!s || g < 0 || g >= s->ng || !buoy || !c) return fail(s, ECSG_ERR_INVALID, "set_medium_ortho9: bad arguments");
+    if (s->medium != ECSG_MEDIUM_ORTHO9) return fail(s, ECSG_ERR_STATE, "simulation was created for an isotropic medium");
+    for (int k = 0; k < 9; k++)
+        if (!c[k]) return fail(s, ECSG_ERR_INVALID, "set_medium_ortho9: c[%d] is null", k);
+    CK(cudaSetDevice(s->device));
+    int rc = s->prec == ECSG_F32 ? set_ortho<float>(s, g, buoy, c) : set_ortho<double>(s, g, buoy, c);
+    if (rc) return rc;
+    s->medium_set[g] = true;
+    if (g > 0) s->itf[g].A_ready = false;
+    if (g + 1 < s->ng) s->itf[g + 1].A_ready = false;
+    return ECSG_OK;
+}
+
+long long ecsg_field_elems(const ecsg_sim *s, int g, int k)
+{
+    if (!s || g < 0 || g >= s->ng || k < 0 || k > 8) return -1;
+    int len[3];
+    field_len(s, g, k, len);
+    return (long long)len[0] * len[1] * len[2];
+}
+
+int ecsg_set_field(ecsg_sim *s, int g, int k, const double *src)
+{
+    if (!s || g < 0 || g >= s->ng || k < 0 || k > 8 || !src) return fail(s, ECSG_ERR_INVALID, "set_field: bad arguments");
+    CK(cudaSetDevice(s->device));
+    int len[3];
+    field_len(s, g, k, len);
+    const size_t n = (size_t)len[0] * len[1] * len[2];
+    double *stage = nullptr;
+    CK(cudaMalloc(&stage, n * sizeof(double)));
+    CK(cudaMemcpyAsync(stage, src, n * sizeof(double), cudaMemcpyHostToDevice, s->st));
+    if (s->prec == ECSG_F32)
+        CK((launch_pack<float, double>((float *)s->f[g][k], s->geo[g], stage, len[0], len[1], len[2], s->R, s->st)));
+    else
+        CK((launch_pack<double, double>((double *)s->f[g][k], s->geo[g], stage, len[0], len[1], len[2], s->R, s->st)));
+    CK(cudaStreamSynchronize(s->st));
+    cudaFree(stage);
+    return ECSG_OK;
+}
+
+int ecsg_get_field(ecsg_sim *s, int g, int k, double *dst)
+{
+    if (!s || g < 0 || g >= s->ng || k < 0 || k > 8 || !dst) return fail(s, ECSG_ERR_INVALID, "get_field: bad arguments");
+    CK(cudaSetDevice(s->device));
+    int len[3];
+    field_len(s, g, k, len);
+    const size_t n = (size_t)len[0] * len[1] * len[2];
+    double *stage = nullptr;
+    CK(cudaMalloc(&stage, n * sizeof(double)));
+    if (s->prec == ECSG_F32)
+        CK(launch_unpack<float>(stage, s->geo[g], (const float *)s->f[g][k], len[0], len[1], len[2], s->R, s->st));
+    else
+        CK(launch_unpack<double>(stage, s->geo[g], (const double *)s->f[g][k], len[0], len[1], len[2], s->R, s->st));
+    CK(cudaMemcpyAsync(dst, stage, n * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    cudaFree(stage);
+    return ECSG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Operators
+// ---------------------------------------------------------------------------
+static int check_ready(ecsg_sim *s)
+{
+    for (int g = 0; g < s->ng; g++)
+        if (!s->medium_set[g]) return fail(s, ECSG_ERR_STATE, "medium of grid %d not set", g);
+    return ECSG_OK;
+}
+
+template <typename T>
+static int vel_kernel_op(ecsg_sim *s, int g, bool with_copy)
+{
+    T *vc[3] = {(T *)s->vc[g][0], (T *)s->vc[g][1], (T *)s->vc[g][2]};
+    CK(launch_vel<T>(dev<T>(s, g), g == 0, g == s->ng - 1, s->top_bc, with_copy ? vc : nullptr, s->sms, s->st));
+    return ECSG_OK;
+}
+
+template <typename T>
+static int vel_mirror_op(ecsg_sim *s, int g)
+{
+    CK(launch_vel_mirror<T>(dev<T>(s, g), g == 0, g == s->ng - 1, s->top_bc, s->st));
+    return ECSG_OK;
+}
+
+template <typename T>
+static int vel_op(ecsg_sim *s, int g, bool with_copy)
+{
+    int rc = vel_kernel_op<T>(s, g, with_copy);
+    return rc ? rc : vel_mirror_op<T>(s, g);
+}
+
+template <typename T>
+static int stress_op(ecsg_sim *s, int g)
+{
+    CK(launch_stress<T>(dev<T>(s, g), s->medium == ECSG_MEDIUM_ISO ? MED_ISO5 : MED_ORTHO9, g == 0, s->top_bc, s->sms, s->st));
+    return ECSG_OK;
+}
+
+template <typename T>
+static int vz_op(ecsg_sim *s, int i)
+{
+    CK(launch_ghost_vz<T>(dev<T>(s, i - 1), dev<T>(s, i), s->medium == ECSG_MEDIUM_ISO ? MED_ISO5 : MED_ORTHO9, s->itf[i].r, s->st));
+    return ECSG_OK;
+}
+
+template <typename T>
+static int syz_op(ecsg_sim *s, int i)
+{
+    CK(launch_ghost_syz<T>(dev<T>(s, i - 1), dev<T>(s, i), s->itf[i].r, s->st));
+    return ECSG_OK;
+}
+
+template <typename T>
+static int sxz_prepare(ecsg_sim *s, int i)
+{
+    Iface &I = s->itf[i];
+    if (!I.A_ready) {
+        CK(launch_sxz_matrix<T>(dev<T>(s, i - 1), dev<T>(s, i), I.r, I.A, s->st));
+        I.A_ready = true;
+    }
+    return ECSG_OK;
+}
+
+template <typename T>
+static int sxz_op(ecsg_sim *s, int i)
+{
+    Iface &I = s->itf[i];
+    SxzWork W;
+    W.A = I.A;
+    W.B = I.B;
+    W.X0 = I.X0;
+    W.X1 = I.X1;
+    W.partial = I.partial;
+    W.total = s->dscal + 1;
+    W.bar = s->bar + 2 * i;
+    W.status = s->ints;
+    W.iters = s->ints + 2;
+    W.iters_total = s->iters_total + i;
+    W.tol_out = s->dscal + 2 + i;
+    W.max_iter = s->jacobi_max_iter;
+    CK(launch_sxz_solve<T>(dev<T>(s, i - 1), dev<T>(s, i), I.r, W, I.nblocks, s->st));
+    return ECSG_OK;
+}
+
+#define DISPATCH(call) (s->prec == ECSG_F32 ? call<float> : call<double>)
+
+int ecsg_update_vel(ecsg_sim *s, int g)
+{
+    if (!s || g < 0 || g >= s->ng) return fail(s, ECSG_ERR_INVALID, "update_vel: bad grid");
+    if (int rc = check_ready(s)) return rc;
+    int rc = DISPATCH(vel_op)(s, g, false);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(s->st));
+    return ECSG_OK;
+}
+
+int ecsg_update_stress(ecsg_sim *s, int g)
+{
+    if (!s || g < 0 || g >= s->ng) return fail(s, ECSG_ERR_INVALID, "update_stress: bad grid");
+    if (int rc = check_ready(s)) return rc;
+    int rc = DISPATCH(stress_op)(s, g);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(s->st));
+    return ECSG_OK;
+}
+
+int ecsg_ghost_vz(ecsg_sim *s, int i)
+{
+    if (!s || i < 1 || i >= s->ng) return fail(s, ECSG_ERR_INVALID, "ghost_vz: bad interface");
+    if (int rc = check_ready(s)) return rc;
+    int rc = DISPATCH(vz_op)(s, i);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(s->st));
+    return ECSG_OK;
+}
+
+int ecsg_ghost_syz(ecsg_sim *s, int i)
+{
+    if (!s || i < 1 || i >= s->ng) return fail(s, ECSG_ERR_INVALID, "ghost_syz: bad interface");
+    if (int rc = check_ready(s)) return rc;
+    int rc = DISPATCH(syz_op)(s, i);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(s->st));
+    return ECSG_OK;
+}
+
+int ecsg_ghost_sxz(ecsg_sim *s, int i)
+{
+    if (!s || i < 1 || i >= s->ng) return fail(s, ECSG_ERR_INVALID, "ghost_sxz: bad interface");
+    if (int rc = check_ready(s)) return rc;
+    int rc = DISPATCH(sxz_prepare)(s, i);
+    if (rc) return rc;
+    rc = DISPATCH(sxz_op)(s, i);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(s->st));
+    return ECSG_OK;
+}
+
+int ecsg_get_sxz_state(ecsg_sim *s, int i, double *X, int *last_iters, double *last_tol, long long *total_iters)
+{
+    if (!s || i < 1 || i >= s->ng) return fail(s, ECSG_ERR_INVALID, "get_sxz_state: bad interface");
+    CK(cudaSetDevice(s->device));
+    const Geo &C = s->geo[i];
+    if (X) CK(cudaMemcpyAsync(X, s->itf[i].X0, sizeof(double) * (C.nx + 1) * (C.ny + 1), cudaMemcpyDeviceToHost, s->st));
+    int it = 0;
+    double tol = 0;
+    long long tot = 0;
+    CK(cudaMemcpyAsync(&it, s->ints + 2, sizeof(int), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaMemcpyAsync(&tol, s->dscal + 2 + i, sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaMemcpyAsync(&tot, s->iters_total + i, sizeof(long long), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    if (last_iters) *last_iters = it;
+    if (last_tol) *last_tol = tol;
+    if (total_iters) *total_iters = tot;
+    return ECSG_OK;
+}
+
+int ecsg_set_sxz_state(ecsg_sim *s, int i, const double *X)
+{
+    if (!s || i < 1 || i >= s->ng || !X) return fail(s, ECSG_ERR_INVALID, "set_sxz_state: bad arguments");
+    CK(cudaSetDevice(s->device));
+    const Geo &C = s->geo[i];
+    CK(cudaMemcpyAsync(s->itf[i].X0, X, sizeof(double) * (C.nx + 1) * (C.ny + 1), cudaMemcpyHostToDevice, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return ECSG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Energy and residues
+// ---------------------------------------------------------------------------
+template <typename T>
+static int copy_vel_op(ecsg_sim *s)
+{
+    for (int g = 0; g < s->ng; g++)
+        for (int k = 0; k < 3; k++)
+            CK(cudaMemcpyAsync(s->vc[g][k], s->f[g][k], (size_t)s->geo[g].size() * sizeof(T), cudaMemcpyDeviceToDevice, s->st));
+    return ECSG_OK;
+}
+
+template <typename T>
+static int energy_op(ecsg_sim *s, double *out, const int *step, int step0)
+{
+    for (int g = 0; g < s->ng; g++) {
+        T *vc[3] = {(T *)s->vc[g][0], (T *)s->vc[g][1], (T *)s->vc[g][2]};
+        CK(launch_energy<T>(dev<T>(s, g), s->medium == ECSG_MEDIUM_ISO ? MED_ISO5 : MED_ORTHO9, vc, s->partial,
+                            s->red_blocks, s->h[g][0], s->h[g][1], s->h[g][2], out, step, step0, g == 0, s->ints, s->st));
+    }
+    return ECSG_OK;
+}
+
+int ecsg_copy_vel(ecsg_sim *s)
+{
+    if (!s) return ECSG_ERR_INVALID;
+    if (!s->energy) return fail(s, ECSG_ERR_STATE, "copy_vel: simulation created without energy support");
+    int rc = DISPATCH(copy_vel_op)(s);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(s->st));
+    return ECSG_OK;
+}
+
+int ecsg_energy(ecsg_sim *s, double *energy)
+{
+    if (!s || !energy) return ECSG_ERR_INVALID;
+    if (!s->energy) return fail(s, ECSG_ERR_STATE, "energy: simulation created without energy support");
+    if (int rc = check_ready(s)) return rc;
+    int rc = DISPATCH(energy_op)(s, s->dscal, nullptr, 0);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(energy, s->dscal, sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return ECSG_OK;
+}
+
+// Writes 12 doubles per interface at out: per group [fine sum, r^2 coarse sum, avg|a|, avg|b|].
+template <typename T>
+static int residue_op(ecsg_sim *s, int i, int which, double *out)
+{
+    const GridDev<T> F = dev<T>(s, i - 1), C = dev<T>(s, i);
+    const double r2 = (double)s->itf[i].r * s->itf[i].r;
+    static const int comps[3][2] = {{VX, SXZ}, {VY, SYZ}, {VZ, SZZ}};
+    for (int grp = 0; grp < 3; grp++) {
+        if (!(which & (1 << grp))) continue;
+        CK(launch_residue<T>(F, C, grp, r2, s->partial, s->red_blocks, out + 4 * grp, s->st));
+        for (int j = 0; j < 2; j++) {
+            const int k = comps[grp][j];
+            CK(launch_avgabs<T>(C, k, kPos[k], s->partial, s->red_blocks, out + 4 * grp + 2 + j, s->st));
+        }
+    }
+    return ECSG_OK;
+}
+
+int ecsg_residues(ecsg_sim *s, int i, int which, double out[9])
+{
+    if (!s || i < 1 || i >= s->ng || !out) return fail(s, ECSG_ERR_INVALID, "residues: bad arguments");
+    int rc = DISPATCH(residue_op)(s, i, which, s->dscal + 16);
+    if (rc) return rc;
+    double tmp[12];
+    CK(cudaMemcpyAsync(tmp, s->dscal + 16, sizeof tmp, cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    for (int grp = 0; grp < 3; grp++) {
+        if (!(which & (1 << grp))) continue;
+        out[3 * grp] = tmp[4 * grp] - tmp[4 * grp + 1];
+        out[3 * grp + 1] = tmp[4 * grp + 2];
+        out[3 * grp + 2] = tmp[4 * grp + 3];
+    }
+    return ECSG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Source, receivers, time loop
+// ---------------------------------------------------------------------------
+int ecsg_locate(const ecsg_sim *s, const double xyz[3], int loc4[4])
+{
+    if (!s || !xyz || !loc4) return ECSG_ERR_INVALID;
+    int g = 0;
+    double z = xyz[2];
+    while (z > s->h[g][2] * s->geo[g].nz) {
+        z -= s->h[g][2] * s->geo[g].nz;
+        g++;
+        if (g >= s->ng) return ECSG_ERR_INVALID;
+    }
+    loc4[0] = g;
+    loc4[1] = (int)std::round(xyz[0] / s->h[g][0]);
+    loc4[2] = (int)std::round(xyz[1] / s->h[g][1]);
+    loc4[3] = (int)std::round(z / s->h[g][2]);
+    return ECSG_OK;
+}
+
+int ecsg_set_source(ecsg_sim *s, int g, int ix, int iy, int iz, int comp, const float *trace, int nt, float scale)
+{
+    if (!s) return ECSG_ERR_INVALID;
+    if (g < 0 || g >= s->ng || comp < 0 || comp > 8 || nt < 0 || (nt > 0 && !trace)) return fail(s, ECSG_ERR_INVALID, "set_source: bad arguments");
+    const Geo &G = s->geo[g];
+    if (ix < -s->R || ix > G.nx + s->R || iy < -s->R || iy > G.ny + s->R || iz < -s->R || iz > G.nz + s->R)
+        return fail(s, ECSG_ERR_INVALID, "set_source: index outside grid %d", g);
+    CK(cudaSetDevice(s->device));
+    cudaFree(s->src_trace);
+    s->src_trace = nullptr;
+    if (nt > 0) {
+        CK(cudaMalloc(&s->src_trace, sizeof(float) * nt));
+        CK(cudaMemcpyAsync(s->src_trace, trace, sizeof(float) * nt, cudaMemcpyHostToDevice, s->st));
+        CK(cudaStreamSynchronize(s->st));
+    }
+    s->src_grid = g;
+    s->src_off = G.idx(ix, iy, iz);
+    s->src_comp = comp;
+    s->src_nt = nt;
+    s->src_scale = scale;
+    return ECSG_OK;
+}
+
+int ecsg_set_receivers(ecsg_sim *s, const int *loc4, int n, int comp)
+{
+    if (!s || n < 0 || (n > 0 && !loc4) || comp < 0 || comp > 8) return fail(s, ECSG_ERR_INVALID, "set_receivers: bad arguments");
+    std::vector<int> gr(n), off(n);
+    for (int i = 0; i < n; i++) {
+        const int g = loc4[4 * i];
+        if (g < 0 || g >= s->ng) return fail(s, ECSG_ERR_INVALID, "receiver %d: bad grid", i);
+        const Geo &G = s->geo[g];
+        const int x = loc4[4 * i + 1], y = loc4[4 * i + 2], z = loc4[4 * i + 3];
+        if (x < -s->R || x > G.nx + s->R || y < -s->R || y > G.ny + s->R || z < -s->R || z > G.nz + s->R)
+            return fail(s, ECSG_ERR_INVALID, "receiver %d: index outside grid %d", i, g);
+        gr[i] = g;
+        off[i] = G.idx(x, y, z);
+    }
+    CK(cudaSetDevice(s->device));
+    cudaFree(s->rec_grid);
+    cudaFree(s->rec_off);
+    s->rec_grid = s->rec_off = nullptr;
+    if (n > 0) {
+        CK(cudaMalloc(&s->rec_grid, sizeof(int) * n));
+        CK(cudaMalloc(&s->rec_off, sizeof(int) * n));
+        CK(cudaMemcpyAsync(s->rec_grid, gr.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s->st));
+        CK(cudaMemcpyAsync(s->rec_off, off.data(), sizeof(int) * n, cudaMemcpyHostToDevice, s->st));
+        CK(cudaStreamSynchronize(s->st));
+    }
+    s->nrec = n;
+    s->rec_comp = comp;
+    return ECSG_OK;
+}
+
+static SrcRec make_srcrec(ecsg_sim *s, int step0, int mode)
+{
+    SrcRec S;
+    memset(&S, 0, sizeof S);
+    for (int g = 0; g < s->ng; g++) S.rec_base[g] = s->f[g][s->rec_comp];
+    S.rec_grid = s->rec_grid;
+    S.rec_off = s->rec_off;
+    S.nrec = s->nrec;
+    S.traces = s->traces;
+    S.trace_cap = s->trace_cap;
+    S.step = s->ints + 1;
+    S.step0 = step0;
+    S.src_base = (s->src_grid >= 0 && s->src_trace) ? s->f[s->src_grid][s->src_comp] : nullptr;
+    S.src_off = s->src_off;
+    S.src_trace = s->src_trace;
+    S.src_nt = s->src_nt;
+    S.src_scale = s->src_scale;
+    S.mode = mode;
+    return S;
+}
+
+// One iteration of main.cpp:165-261 (movies excluded).
+template <typename T>
+static int step_op(ecsg_sim *s, int step0, bool energy, double *energy_buf, double *res_row)
+{
+    int rc;
+    for (int g = 0; g < s->ng; g++)
+        if ((rc = vel_op<T>(s, g, energy))) return rc;
+    if (res_row) {
+        CK(launch_src_rec<T>(make_srcrec(s, step0, 1), s->st));
+        for (int i = 1; i < s->ng; i++)
+            if ((rc = residue_op<T>(s, i, 3, res_row + 12 * (i - 1)))) return rc;
+        CK(launch_src_rec<T>(make_srcrec(s, step0, 2), s->st));
+    } else {
+        CK(launch_src_rec<T>(make_srcrec(s, step0, 3), s->st));
+    }
+    for (int i = 1; i < s->ng; i++)
+        if ((rc = vz_op<T>(s, i))) return rc;
+    if (res_row)
+        for (int i = 1; i < s->ng; i++)
+            if ((rc = residue_op<T>(s, i, 4, res_row + 12 * (i - 1)))) return rc;
+    if (energy)
+        if ((rc = energy_op<T>(s, energy_buf, s->ints + 1, step0))) return rc;
+    for (int g = 0; g < s->ng; g++)
+        if ((rc = stress_op<T>(s, g))) return rc;
+    for (int i = 1; i < s->ng; i++) {
+        if ((rc = sxz_op<T>(s, i))) return rc;
+        if ((rc = syz_op<T>(s, i))) return rc;
+    }
+    return ECSG_OK;
+}
+
+template <typename T>
+static int run_op(ecsg_sim *s, int n0, int nsteps, float *traces, double *energy, int energy_every, double *residues,
+                  int use_graph)
+{
+    int rc;
+    for (int i = 1; i < s->ng; i++)
+        if ((rc = sxz_prepare<T>(s, i))) return rc;
+    if (s->nrec > 0 && s->trace_cap < nsteps) {
+        cudaFree(s->traces);
+        s->traces = nullptr;
+        CK(cudaMalloc(&s->traces, sizeof(float) * (size_t)nsteps * s->nrec));
+        s->trace_cap = nsteps;
+    }
+    if (energy && s->run_energy_cap < nsteps) {
+        cudaFree(s->run_energy);
+        s->run_energy = nullptr;
+        CK(cudaMalloc(&s->run_energy, sizeof(double) * (size_t)nsteps));
+        s->run_energy_cap = nsteps;
+    }
+    const int nres = 12 * (s->ng - 1);
+    if (residues && s->run_res_cap < nsteps) {
+        cudaFree(s->run_res);
+        s->run_res = nullptr;
+        CK(cudaMalloc(&s->run_res, sizeof(double) * (size_t)nsteps * nres));
+        s->run_res_cap = nsteps;
+    }
+    if (energy) {
+        std::vector<double> nan(nsteps, NAN);
+        CK(cudaMemcpyAsync(s->run_energy, nan.data(), sizeof(double) * nsteps, cudaMemcpyHostToDevice, s->st));
+    }
+    CK(cudaMemcpyAsync(s->ints + 1, &n0, sizeof(int), cudaMemcpyHostToDevice, s->st));
+    const int every = energy_every > 0 ? energy_every : 1;
+    cudaGraphExec_t gx[2] = {nullptr, nullptr};
+    bool graphs = use_graph && !residues;
+    if (graphs) {
+        for (int variant = 0; variant < (energy ? 2 : 1); variant++) {
+            cudaGraph_t gr = nullptr;
+            CK(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
+            rc = step_op<T>(s, n0, variant == 1, s->run_energy, nullptr);
+            cudaError_t e = cudaStreamEndCapture(s->st, &gr);
+            if (rc || e != cudaSuccess) {
+                if (gr) cudaGraphDestroy(gr);
+                for (int v = 0; v < 2; v++)
+                    if (gx[v]) cudaGraphExecDestroy(gx[v]);
+                cudaGetLastError();
+                return rc ? rc : fail(s, ECSG_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+            }
+            e = cudaGraphInstantiate(&gx[variant], gr, 0);
+            cudaGraphDestroy(gr);
+            if (e != cudaSuccess) return fail(s, ECSG_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+        }
+    }
+    CK(cudaEventRecord(s->ev[0], s->st));
+    long long launches = 0;
+    const long long per_step = 6LL * s->ng + 1 + 3LL * (s->ng - 1);
+    for (int n = n0; n < n0 + nsteps; n++) {
+        const bool e_step = energy && ((n % every) == 0);
+        launches += per_step + (e_step ? 2LL * s->ng : 0) + (residues ? 1 + 12LL * (s->ng - 1) : 0);
+        if (graphs) {
+            cudaError_t e = cudaGraphLaunch(gx[e_step ? 1 : 0], s->st);
+            if (e != cudaSuccess) { rc = fail(s, ECSG_ERR_CUDA, "graph launch: %s", cudaGetErrorString(e)); break; }
+        } else {
+            if ((rc = step_op<T>(s, n0, e_step, s->run_energy, residues ? s->run_res + (size_t)(n - n0) * nres : nullptr)))
+                break;
+        }
+        rc = ECSG_OK;
+    }
+    CK(cudaEventRecord(s->ev[1], s->st));
+    for (int v = 0; v < 2; v++)
+        if (gx[v]) cudaGraphExecDestroy(gx[v]);
+    if (rc) return rc;
+    s->launches = launches;
+    if (traces && s->nrec > 0)
+        CK(cudaMemcpyAsync(traces, s->traces, sizeof(float) * (size_t)nsteps * s->nrec, cudaMemcpyDeviceToHost, s->st));
+    if (energy)
+        CK(cudaMemcpyAsync(energy, s->run_energy, sizeof(double) * nsteps, cudaMemcpyDeviceToHost, s->st));
+    std::vector<double> rtmp;
+    if (residues) {
+        rtmp.resize((size_t)nsteps * nres);
+        CK(cudaMemcpyAsync(rtmp.data(), s->run_res, sizeof(double) * rtmp.size(), cudaMemcpyDeviceToHost, s->st));
+    }
+    CK(cudaStreamSynchronize(s->st));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, s->ev[0], s->ev[1]));
+    s->last_run_ms = ms;
+    if (residues) {
+        for (int n = 0; n < nsteps; n++)
+            for (int i = 0; i < s->ng - 1; i++)
+                for (int grp = 0; grp < 3; grp++) {
+                    const double *src = &rtmp[(size_t)n * nres + 12 * i + 4 * grp];
+                    double *dst = residues + ((size_t)n * (s->ng - 1) + i) * 9 + 3 * grp;
+                    dst[0] = src[0] - src[1];
+                    dst[1] = src[2];
+                    dst[2] = src[3];
+                }
+    }
+    return ECSG_OK;
+}
+
+int ecsg_run(ecsg_sim *s, int n0, int nsteps, float *traces, double *energy, int energy_every, double *residues,
+             int use_graph)
+{
+    if (!s || nsteps < 0) return fail(s, ECSG_ERR_INVALID, "run: bad arguments");
+    if (energy && !s->energy) return fail(s, ECSG_ERR_STATE, "run: energy requested but simulation created without it");
+    if (int rc = check_ready(s)) return rc;
+    CK(cudaSetDevice(s->device));
+    if (nsteps == 0) return ECSG_OK;
+    return DISPATCH(run_op)(s, n0, nsteps, traces, energy, energy_every, residues, use_graph);
+}
+
+int ecsg_synchronize(ecsg_sim *s)
+{
+    if (!s) return ECSG_ERR_INVALID;
+    CK(cudaStreamSynchronize(s->st));
+    return ECSG_OK;
+}
+
+int ecsg_get_status(ecsg_sim *s, int *status, int clear)
+{
+    if (!s || !status) return ECSG_ERR_INVALID;
+    CK(cudaMemcpyAsync(status, s->ints, sizeof(int), cudaMemcpyDeviceToHost, s->st));
+    if (clear) CK(cudaMemsetAsync(s->ints, 0, sizeof(int), s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return ECSG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Timing (CUDA events on the simulation's stream)
+// ---------------------------------------------------------------------------
+int ecsg_last_run(ecsg_sim *s, double *device_ms, long long *launches)
+{
+    if (!s) return ECSG_ERR_INVALID;
+    if (device_ms) *device_ms = s->last_run_ms;
+    if (launches) *launches = s->launches;
+    return ECSG_OK;
+}
+
+int ecsg_timer_start(ecsg_sim *s)
+{
+    if (!s) return ECSG_ERR_INVALID;
+    CK(cudaEventRecord(s->ev[2], s->st));
+    return ECSG_OK;
+}
+
+int ecsg_timer_stop(ecsg_sim *s, double *ms)
+{
+    if (!s || !ms) return ECSG_ERR_INVALID;
+    CK(cudaEventRecord(s->ev[3], s->st));
+    CK(cudaEventSynchronize(s->ev[3]));
+    float f = 0;
+    CK(cudaEventElapsedTime(&f, s->ev[2], s->ev[3]));
+    *ms = f;
+    return ECSG_OK;
+}
+
+template <typename T>
+static int time_kernels_op(ecsg_sim *s, int nsteps, double *out)
+{
+    int rc;
+    for (int i = 1; i < s->ng; i++)
+        if ((rc = sxz_prepare<T>(s, i))) return rc;
+    const int nev = 1 + 6 * kMaxGrids + 1;
+    std::vector<cudaEvent_t> ev(2 * nev);
+    for (auto &e : ev) CK(cudaEventCreate(&e));
+    std::vector<double> acc(7 * kMaxGrids, 0.0);
+    int step0 = 0;
+    CK(cudaMemcpyAsync(&step0, s->ints + 1, sizeof(int), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    for (int n = 0; n < nsteps; n++) {
+        int e = 0;
+        auto bracket = [&](int slot, auto fn) -> int {
+            CK(cudaEventRecord(ev[2 * e], s->st));
+            int r = fn();
+            if (r) return r;
+            CK(cudaEventRecord(ev[2 * e + 1], s->st));
+            CK(cudaEventSynchronize(ev[2 * e + 1]));
+            float ms = 0;
+            CK(cudaEventElapsedTime(&ms, ev[2 * e], ev[2 * e + 1]));
+            acc[slot] += ms;
+            e = (e + 1) % nev;
+            return ECSG_OK;
+        };
+        for (int g = 0; g < s->ng; g++) {
+            if ((rc = bracket(0 * kMaxGrids + g, [&] { return vel_kernel_op<T>(s, g, false); }))) return rc;
+            if ((rc = bracket(1 * kMaxGrids + g, [&] { return vel_mirror_op<T>(s, g); }))) return rc;
+        }
+        if ((rc = bracket(6 * kMaxGrids, [&] {
+                 CK(launch_src_rec<T>(make_srcrec(s, step0, 3), s->st));
+                 return (int)ECSG_OK;
+             })))
+            return rc;
+        for (int i = 1; i < s->ng; i++)
+            if ((rc = bracket(3 * kMaxGrids + i, [&] { return vz_op<T>(s, i); }))) return rc;
+        for (int g = 0; g < s->ng; g++)
+            if ((rc = bracket(2 * kMaxGrids + g, [&] { return stress_op<T>(s, g); }))) return rc;
+        for (int i = 1; i < s->ng; i++) {
+            if ((rc = bracket(4 * kMaxGrids + i, [&] { return sxz_op<T>(s, i); }))) return rc;
+            if ((rc = bracket(5 * kMaxGrids + i, [&] { return syz_op<T>(s, i); }))) return rc;
+        }
+    }
+    for (auto &e : ev) cudaEventDestroy(e);
+    for (size_t k = 0; k < acc.size(); k++) out[k] = nsteps > 0 ? acc[k] / nsteps : 0.0;
+    return ECSG_OK;
+}
+
+int ecsg_time_kernels(ecsg_sim *s, int nsteps, double *ms)
+{
+    if (!s || !ms || nsteps < 1) return fail(s, ECSG_ERR_INVALID, "time_kernels: bad arguments");
+    if (int rc = check_ready(s)) return rc;
+    CK(cudaSetDevice(s->device));
+    return DISPATCH(time_kernels_op)(s, nsteps, ms);
+}

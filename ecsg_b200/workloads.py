@@ -1,0 +1,231 @@
+"""Synthetic workloads: the reference's own experiment inputs and the benchmark media.
+
+All generators are seeded numpy code; nothing is read from disk.
+
+* ``eci_test_case(k)`` rebuilds the inputs of the reference experiment
+  tests/test1-cmp-eci-ii (eci/SConstruct:26-195 with par1.py / par2.py /
+  par3.py): a two-layer isotropic medium on a two-grid composite at refinement
+  ratio 2.  Every number the reference script passes through a Madagascar
+  command line is rounded through ``%f`` exactly as the script does, so the
+  generated inputs are the ones the reference's golden traces were produced from.
+* ``three_grid_vti(...)``: the three-grid ratio-3 tilted-VTI benchmark medium
+  (1081x1081x121 @ 5 m, 361x361x161 @ 15 m, 121x121x101 @ 45 m by default).
+
+Units follow the reference tests: metres, milliseconds, m/ms and g/cm^3.
+"""
+import math
+
+import numpy as np
+
+# Staggered positions (pos[d] = 1: staggered in dim d), init_del_sim.cpp:14-24.
+SIM_POS = [(0, 0, 0), (1, 1, 0), (1, 0, 1), (1, 0, 0), (1, 0, 0), (1, 0, 0), (1, 1, 1), (0, 0, 1), (0, 1, 0)]
+SIM_NAMES = ["vx", "vy", "vz", "sxx", "syy", "szz", "syz", "sxz", "sxy"]
+# Stiffness order of update_stress.cpp:17-25 and their positions (init_del_par_field.cpp:82-88).
+STIFF_NAMES = ["c11", "c22", "c33", "c23", "c13", "c12", "c44", "c55", "c66"]
+STIFF_POS = [(1, 0, 0)] * 6 + [(1, 1, 1), (0, 0, 1), (0, 1, 0)]
+
+
+def _f(x):
+    """A value as it comes out of the reference script's '%f' formatting."""
+    return float("%f" % x)
+
+
+def ricker(nt, d1, fpeak, o1=0.0):
+    """Ricker wavelet as the reference script asks sfmath for it (eci/SConstruct:118-147):
+    (1-2a(t-t0)^2) exp(-a(t-t0)^2), a = pi^2 f^2 and t0 = 1/f, both '%f'-rounded."""
+    pi = math.atan(1) * 4.0
+    a = _f(pi ** 2 * fpeak ** 2)
+    t0 = _f(1.0 / fpeak)
+    t = o1 + np.arange(nt, dtype=np.float64) * d1
+    arg = a * (t - t0) * (t - t0)
+    return ((1.0 - 2.0 * arg) * np.exp(-arg)).astype(np.float32)
+
+
+class Case:
+    """Inputs of one composite-grid run.
+
+    grids:   list of dicts with 'n' (cells, x,y,z) and 'h' (steps, x,y,z); grid 0 on top.
+    media:   per grid, node-position float32 arrays (shape (nz+1, ny+1, nx+1)):
+             'buoy', and either 's11','s13' (isotropic, the reference input form)
+             or 'cij' (21 x node arrays in Voigt upper-triangle order).
+    dt, nsteps, radius, top_bc, imode
+    src:     dict(xyz=(x,y,z), trace=float32[nt], scale, comp) -- comp 0 = vx
+    rec:     float32 (n_rec, 3) coordinates, plus rec_comp
+    """
+
+    def __init__(self, **kw):
+        self.__dict__.update(kw)
+
+    @property
+    def ratio(self):
+        if len(self.grids) < 2:
+            return 1
+        return int(round(self.grids[1]["h"][0] / self.grids[0]["h"][0]))
+
+    def points(self):
+        return sum((g["n"][0] + 1) * (g["n"][1] + 1) * (g["n"][2] + 1) for g in self.grids)
+
+
+def eci_test_case(test=1, imode=1, nsteps=None):
+    """Inputs of tests/test1-cmp-eci-ii/{eci,ii} with par{test}.py."""
+    n_extra, src_option = {1: (5, 0), 2: (1, 0), 3: (5, 1)}[test]
+    cfl, nspw, lx, ly, lz1, lz2, duration, fpeak = 0.98, 16, 1600, 1600, 300, 500, 700, 15.0
+    layer1 = {"rho": 2.5, "cs": 1.0, "cp": 2.0}
+    layer2 = {"rho": 2.65, "cs": 2.0, "cp": 4.0}
+    for L in (layer1, layer2):
+        L["buoy"] = 1.0 / L["rho"]
+        L["s11"] = L["rho"] * L["cp"] ** 2
+        L["s13"] = L["s11"] - 2 * L["rho"] * L["cs"] ** 2
+    dx1 = layer1["cs"] * 1000 / fpeak / nspw
+    dx2 = dx1 * 2
+    nx2, ny2 = int(lx / dx2), int(ly / dx2)
+    nx1, ny1 = 2 * nx2, 2 * ny2
+    nz1 = int(lz1 / dx1 / 2) * 2
+    nz2 = int(lz2 / dx2)
+    g1 = {"n": (nx1, ny1, nz1), "h": (_f(dx1),) * 3}
+    g2 = {"n": (nx2, ny2, nz2), "h": (_f(dx2),) * 3}
+
+    def layered(nx, ny, nz, n2planes, key):
+        a = np.empty((nz + 1, ny + 1, nx + 1), dtype=np.float32)
+        a[: nz + 1 - n2planes] = np.float32(_f(layer1[key]))
+        a[nz + 1 - n2planes:] = np.float32(_f(layer2[key]))
+        return a
+
+    media = [
+        {k: layered(nx1, ny1, nz1, n_extra, k) for k in ("buoy", "s11", "s13")},
+        {k: layered(nx2, ny2, nz2, nz2 + 1, k) for k in ("buoy", "s11", "s13")},
+    ]
+    dt = min(dx1, dx1, dx1) / max(layer1["cp"], layer2["cp"]) / math.sqrt(3) * cfl
+    src_z = int(lz1 * 0.2 / dx2) * dx2 if src_option == 0 else (nz1 - 1) * dx1
+    src_x = int(lx * 0.5 / dx2) * dx2
+    src_y = int(ly * 0.5 / dx2) * dx2
+    trace = ricker(700, _f(dt / 1000.0), fpeak)
+    rec_z = int(lz1 * 0.2 / dx2) * dx2
+    rec = np.array([[_f(int(lx * f / dx2) * dx2), _f(src_y), _f(rec_z)] for f in (0.55, 0.6, 0.65, 0.7)],
+                   dtype=np.float32)
+    movie_dt = _f(30 * dt)
+    movie_nt = int(duration / (30 * dt))
+    dtp = _f(dt)
+    steps = int(math.ceil(movie_dt * movie_nt / dtp)) + 1
+    return Case(name="eci_test%d" % test if imode else "ii_test%d" % test,
+                grids=[g1, g2], media=media, medium="iso", dt=dtp,
+                nsteps=steps if nsteps is None else nsteps, radius=1, top_bc=1, imode=imode,
+                src={"xyz": (_f(src_x), _f(src_y), _f(src_z)), "trace": trace, "scale": 1000.0, "comp": 0},
+                rec=rec, rec_comp=0)
+
+
+def random_case(seed, ratio=2, nx2=6, ny2=5, nz=(5, 4), radius=1, top_bc=1, num_grids=2, h1=10.0):
+    """Small heterogeneous isotropic composite with random fields, for operator tests."""
+    rng = np.random.default_rng(seed)
+    grids = []
+    nx, ny = nx2 * ratio ** (num_grids - 1), ny2 * ratio ** (num_grids - 1)
+    h = h1
+    for g in range(num_grids):
+        grids.append({"n": (nx, ny, nz[g]), "h": (h, h, h)})
+        nx //= ratio
+        ny //= ratio
+        h *= ratio
+    media = []
+    for g in grids:
+        nx, ny, nzz = g["n"]
+        shp = (nzz + 1, ny + 1, nx + 1)
+        rho = rng.uniform(1.8, 2.6, shp)
+        cs = rng.uniform(1.0, 1.6, shp)
+        cp = cs * rng.uniform(1.7, 2.0, shp)
+        s11 = rho * cp ** 2
+        s13 = s11 - 2 * rho * cs ** 2
+        media.append({"buoy": (1 / rho).astype(np.float32), "s11": s11.astype(np.float32),
+                      "s13": s13.astype(np.float32)})
+    vmax = max(float(np.sqrt(m["s11"] * m["buoy"]).max()) for m in media)
+    dt = 0.5 * h1 / vmax / math.sqrt(3)
+    return Case(name="random%d" % seed, grids=grids, media=media, medium="iso", dt=dt, nsteps=10,
+                radius=radius, top_bc=top_bc, imode=1, src=None, rec=np.zeros((0, 3), np.float32), rec_comp=0)
+
+
+# ---------------------------------------------------------------------------
+# Three-grid ratio-3 benchmark model
+# ---------------------------------------------------------------------------
+THREE_GRID = [((1080, 1080, 120), 5.0), ((360, 360, 160), 15.0), ((120, 120, 100), 45.0)]
+
+
+def _smooth_noise(rng, shape_m, corr_m, lattice_m=50.0):
+    """Unit-variance Gaussian-filtered noise on a coarse lattice (correlation length
+    corr_m), returned as a function that samples it at points (trilinear)."""
+    from scipy.ndimage import gaussian_filter
+    n = [int(math.ceil(s / lattice_m)) + 2 for s in shape_m]
+    w = gaussian_filter(rng.standard_normal(n[::-1]), sigma=corr_m / lattice_m, mode="wrap")
+    w = (w - w.mean()) / w.std()
+    return w.astype(np.float32), lattice_m
+
+
+def _sample(w, lattice_m, x, y, z):
+    """Trilinear sample of lattice field w[z][y][x] at 1-D coordinate vectors x, y, z (m),
+    done as three separable linear interpolations (x, then y, then z)."""
+    def idx(c):
+        f = c / lattice_m
+        i = np.floor(f).astype(np.int64)
+        return i, (f - i).astype(np.float32)
+    ix, fx = idx(x)
+    iy, fy = idx(y)
+    iz, fz = idx(z)
+    zlo, zhi = iz.min(), iz.max() + 2
+    ylo, yhi = iy.min(), iy.max() + 2
+    sub = w[zlo:zhi, ylo:yhi]
+    a = sub[:, :, ix] * (1 - fx) + sub[:, :, ix + 1] * fx                       # (Z, Y, nx)
+    b = a[:, iy - ylo, :] * (1 - fy)[None, :, None] + a[:, iy - ylo + 1, :] * fy[None, :, None]
+    return (b[iz - zlo] * (1 - fz)[:, None, None] + b[iz - zlo + 1] * fz[:, None, None]).astype(np.float32)
+
+
+def three_grid_model(seed=0, grids=None, pert=0.05, corr_m=200.0):
+    """Three-grid composite at ratio 3 (defaults: 1081x1081x121 @ 5 m over
+    361x361x161 @ 15 m over 121x121x101 @ 45 m, 163,856,303 points).
+    Background vp rises linearly 1.2 -> 5.0 m/ms with depth over the whole
+    stack, vs = vp/1.8, rho from Gardner (0.31 vp[m/s]^0.25 g/cm^3), each with
+    seeded 5 % Gaussian-filtered perturbations (200 m correlation length).
+    Returns per-grid node arrays (vp, vs, rho) in float32."""
+    grids = grids or THREE_GRID
+    rng = np.random.default_rng(seed)
+    lx = grids[0][0][0] * grids[0][1]
+    ly = grids[0][0][1] * grids[0][1]
+    lz = sum(n[2] * h for n, h in grids)
+    fields = [_smooth_noise(rng, (lx, ly, lz), corr_m) for _ in range(3)]
+    out = []
+    z0 = 0.0
+    for (n, h) in grids:
+        x = np.arange(n[0] + 1, dtype=np.float64) * h
+        y = np.arange(n[1] + 1, dtype=np.float64) * h
+        z = z0 + np.arange(n[2] + 1, dtype=np.float64) * h
+        vp0 = (1.2 + (5.0 - 1.2) * (z / lz)).astype(np.float32)[:, None, None]
+        p = [_sample(w, lat, x, y, z) for (w, lat) in fields]
+        vp = vp0 * (1 + pert * p[0])
+        vs = vp0 / np.float32(1.8) * (1 + pert * p[1])
+        rho = (0.31 * (vp0 * 1000.0) ** 0.25).astype(np.float32) * (1 + pert * p[2])
+        out.append({"vp": vp, "vs": vs, "rho": rho, "n": n, "h": h})
+        z0 += n[2] * h
+    return out
+
+
+def three_grid_case(seed=0, grids=None, nsteps=2000, fpeak=15.0, cfl=0.9):
+    """Benchmark case on three_grid_model: isotropic stiffness from (vp, vs, rho),
+    free surface, a Ricker vz point force at the surface centre and a line of vz
+    receivers along x at the surface centre line."""
+    grids = grids or THREE_GRID
+    model = three_grid_model(seed, grids)
+    media = []
+    vmax = 0.0
+    for m in model:
+        rho, vp, vs = m["rho"], m["vp"], m["vs"]
+        s11 = rho * vp * vp
+        s13 = s11 - 2 * rho * vs * vs
+        media.append({"buoy": (1.0 / rho).astype(np.float32), "s11": s11.astype(np.float32),
+                      "s13": s13.astype(np.float32)})
+        vmax = max(vmax, float(vp.max()))
+    h0 = grids[0][1]
+    dt = h0 / vmax / math.sqrt(3) * cfl
+    n0 = grids[0][0]
+    cx, cy = n0[0] // 2 * h0, n0[1] // 2 * h0
+    trace = ricker(int(3.0 / (fpeak * dt * 1e-3)) + 1, dt * 1e-3, fpeak)
+    rec = np.stack([np.arange(n0[0] + 1) * h0, np.full(n0[0] + 1, cy), np.zeros(n0[0] + 1)], 1).astype(np.float32)
+    return Case(name="three_grid_r3", grids=[{"n": n, "h": (h, h, h)} for (n, h) in grids], media=media,
+                medium="iso", dt=dt, nsteps=nsteps, radius=1, top_bc=1, imode=1,
+                src={"xyz": (cx, cy, 0.0), "trace": trace, "scale": 1.0, "comp": 2}, rec=rec, rec_comp=2)

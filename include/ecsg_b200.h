@@ -1,0 +1,167 @@
+/*
+ * ecsg_b200.h -- C ABI of the B200 implementation of ECSG's composite-
+ * staggered-grid time loop (libecsg_b200.so).
+ *
+ * Plain C: POD structs, raw pointers and sizes, integer status codes.  Every
+ * entry point returns ECSG_OK (0) or a negative ECSG_ERR_* code; the message of
+ * the last failure on a simulation is ecsg_last_error(sim).  Calls on one
+ * simulation must come from one host thread at a time.  Host buffers are read
+ * or written before the call returns unless the name says _async.
+ *
+ * Array layouts
+ *   "Field layout": the reference's Field storage (field.cpp:85-149): x fastest,
+ *   len[d] = n[d] + 1 + 2R on node dims and n[d] + 2R on staggered dims, the
+ *   first element is (-R,-R,-R).  Staggered positions per component are those
+ *   of init_del_sim.cpp:14-24 (vx 000, vy 110, vz 101, sxx/syy/szz 100,
+ *   syz 111, sxz 001, sxy 010).
+ *   "Node layout": (nz+1) x (ny+1) x (nx+1) values, x fastest (the RSF inputs
+ *   buoy_N, s11_N, s13_N of init_del_par_field.cpp:23-118).
+ *
+ * Component order: 0 vx, 1 vy, 2 vz, 3 sxx, 4 syy, 5 szz, 6 syz, 7 sxz, 8 sxy.
+ * Grid 0 is the top (finest) grid; interface i couples grid i-1 (fine) and
+ * grid i (coarse), as main.cpp:206-209 and 240-251 index them.
+ */
+#ifndef ECSG_B200_H
+#define ECSG_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ECSG_ABI_VERSION 1
+
+enum {
+    ECSG_OK = 0,
+    ECSG_ERR_INVALID = -1,      /* bad argument or unsupported configuration */
+    ECSG_ERR_CUDA = -2,         /* a CUDA call failed; see ecsg_last_error */
+    ECSG_ERR_NO_DEVICE = -3,    /* no usable sm_100 device */
+    ECSG_ERR_STATE = -4,        /* call out of order (e.g. run before medium set) */
+    ECSG_ERR_NOT_CONVERGED = -5 /* a Jacobi solve hit its iteration cap (status) */
+};
+
+enum { ECSG_F32 = 0, ECSG_F64 = 1 };                     /* field precision */
+enum { ECSG_MEDIUM_ISO = 0, ECSG_MEDIUM_ORTHO9 = 1 };    /* stiffness form */
+enum { ECSG_MODE_II = 0, ECSG_MODE_ECI = 1 };            /* interface mode (main.cpp:54) */
+
+/* Device status bits (ecsg_get_status). */
+enum { ECSG_ST_JACOBI_CAP = 1, ECSG_ST_BARRIER_TIMEOUT = 2, ECSG_ST_NONFINITE = 4 };
+
+/* One uniform sub-grid: Grid (grid.hpp:6-11) without the name.  size[] are
+ * cell counts (points - 1), step[] the spacings.  z origins are stacked as
+ * init_del_par_field.cpp:55-57 does. */
+typedef struct ecsg_grid_desc {
+    int size[3];
+    double step[3];
+} ecsg_grid_desc;
+
+/* Run parameters: the key=value parameters of main.cpp:36-67. */
+typedef struct ecsg_config {
+    int num_grids;        /* num_grids */
+    int radius;           /* stencil radius; 1 (the interface solves assume 1) */
+    double dt;            /* time step */
+    int imode;            /* ECSG_MODE_ECI (1) */
+    int top_bc;           /* 0 rigid, 1 free surface */
+    int precision;        /* ECSG_F32 or ECSG_F64 */
+    int medium;           /* ECSG_MEDIUM_ISO or ECSG_MEDIUM_ORTHO9 */
+    int energy;           /* allocate velocity copies for the energy (check_energy) */
+    int jacobi_max_iter;  /* cap on sxz Jacobi sweeps per solve; <= 0 selects 10000 */
+    int device;           /* CUDA device ordinal */
+} ecsg_config;
+
+typedef struct ecsg_sim ecsg_sim;
+
+/* Creates the device state of a composite run: 9 fields per grid (InitSim,
+ * init_del_sim.cpp:3-40), ghost-solve work space (InitGhostContainer,
+ * init_del_ghost_container.cpp:4-42) and FD coefficients dt/h (InitFDcoeff,
+ * init_del_fdcoeff.cpp:7-22).  Fields start at zero.  Refinement ratio between
+ * consecutive grids is step[i]/step[i-1] (2 or 3, equal in x and y, and size
+ * must satisfy size_fine = ratio * size_coarse in x and y). */
+int ecsg_create(const ecsg_grid_desc *grids, const ecsg_config *cfg, ecsg_sim **out);
+int ecsg_destroy(ecsg_sim *sim);
+const char *ecsg_last_error(const ecsg_sim *sim);
+int ecsg_device_count(void);
+
+/* Isotropic medium of grid g from node-layout float32 arrays: buoyancy, s11,
+ * s13 (InitParField, init_del_par_field.cpp:23-149: s44 = s11 - s13 and the
+ * staggered averages are formed on the device). */
+int ecsg_set_medium_iso(ecsg_sim *sim, int g, const float *buoy, const float *s11, const float *s13);
+/* Orthorhombic medium: node-layout buoyancy and the 9 stiffness arrays in the
+ * order c11 c22 c33 c23 c13 c12 c44 c55 c66 (update_stress.cpp:17-25), each
+ * in Field layout with R = 0 at its staggered position (c11..c12 at 100, c44
+ * at 111, c55 at 001, c66 at 010).  As in the reference, the shear entries are
+ * the stored 2*mu-type moduli that the update multiplies by 0.5. */
+int ecsg_set_medium_ortho9(ecsg_sim *sim, int g, const double *buoy, const double *const c[9]);
+
+/* Field component k of grid g in Field layout (radius R of ecsg_config), in
+ * double (Field::GetPtr1 of the reference, field.hpp:84-85). */
+int ecsg_set_field(ecsg_sim *sim, int g, int k, const double *src);
+int ecsg_get_field(ecsg_sim *sim, int g, int k, double *dst);
+/* Number of elements of component k of grid g in Field layout. */
+long long ecsg_field_elems(const ecsg_sim *sim, int g, int k);
+
+/* One operator on the device state, in place (sim_utils.hpp:127-148). */
+int ecsg_update_vel(ecsg_sim *sim, int g);       /* UpdateVel    update_vel.cpp:4-249 */
+int ecsg_update_stress(ecsg_sim *sim, int g);    /* UpdateStress update_stress.cpp:4-311 */
+int ecsg_ghost_vz(ecsg_sim *sim, int i);         /* UpdateGhostVZ  update_ghost_vz.cpp:8-251 */
+int ecsg_ghost_sxz(ecsg_sim *sim, int i);        /* UpdateGhostSXZ update_ghost_sxz.cpp:16-298 + Jacobi2D/Norm2D */
+int ecsg_ghost_syz(ecsg_sim *sim, int i);        /* UpdateGhostSYZ update_ghost_syz.cpp:6-241 */
+/* Jacobi warm-start vector X of interface i ((nx2+1)*(ny2+1) doubles, the
+ * reference's g_sxz array) and the sweep count / tolerance of the last solve. */
+int ecsg_get_sxz_state(ecsg_sim *sim, int i, double *X, int *last_iters, double *last_tol, long long *total_iters);
+int ecsg_set_sxz_state(ecsg_sim *sim, int i, const double *X);
+
+/* Energy (ComputeEnergy, compute_energy.cpp:34-54, summed over grids as
+ * main.cpp:217-225).  ecsg_copy_vel stores v^{n-1/2} (main.cpp:173-176);
+ * requires cfg.energy. */
+int ecsg_copy_vel(ecsg_sim *sim);
+int ecsg_energy(ecsg_sim *sim, double *energy);
+/* Interface residues of interface i (compute_res.cpp:4-95) in the res_trace
+ * order [res vx-sxz, avg|vx2|, avg|sxz2|, res vy-syz, avg|vy2|, avg|syz2|,
+ * res vz-szz, avg|vz2|, avg|szz2|]; which: bit 0/1/2 selects the groups. */
+int ecsg_residues(ecsg_sim *sim, int i, int which, double out[9]);
+
+/* Source (InitSrc init_src.cpp:7-49 + main.cpp:193-195): component comp of
+ * grid g at index (ix,iy,iz) gets += scale*trace[n] (float product) at step n
+ * for n < nt.  The reference uses comp 0 (vx) and scale 1000. */
+int ecsg_set_source(ecsg_sim *sim, int g, int ix, int iy, int iz, int comp, const float *trace, int nt, float scale);
+/* Receivers (InitRecTrace init_del_rec_trace.cpp:8-56 + main.cpp:182-184):
+ * loc4[4*i] = {grid, ix, iy, iz}; component comp is sampled after the velocity
+ * update and before the source injection. */
+int ecsg_set_receivers(ecsg_sim *sim, const int *loc4, int n, int comp);
+/* Maps a point to (grid, ix, iy, iz) like init_src.cpp:33-45. */
+int ecsg_locate(const ecsg_sim *sim, const double xyz[3], int loc4[4]);
+
+/* Runs steps n0 .. n0+nsteps-1 of the time loop of main.cpp:165-261 on the
+ * device (movie output excluded).  traces (may be NULL): nsteps x nrec
+ * float32, time-major, copied to the host.  energy (may be NULL, needs
+ * cfg.energy): one double per step where (n % energy_every == 0), others NaN.
+ * residues (may be NULL): nsteps x (num_grids-1) x 9 doubles.  use_graph != 0
+ * captures one step in a CUDA graph and replays it. */
+int ecsg_run(ecsg_sim *sim, int n0, int nsteps, float *traces, double *energy, int energy_every, double *residues,
+             int use_graph);
+
+/* Device time (CUDA events around the step loop) of the last ecsg_run and the
+ * number of kernels it launched. */
+int ecsg_last_run(ecsg_sim *sim, double *device_ms, long long *launches);
+/* CUDA events on the simulation's stream around any sequence of calls. */
+int ecsg_timer_start(ecsg_sim *sim);
+int ecsg_timer_stop(ecsg_sim *sim, double *ms);
+/* Runs nsteps steps one kernel at a time with events around each and writes
+ * the mean milliseconds per step into ms[7*8]: ms[0*8+g] velocity kernel of
+ * grid g, ms[1*8+g] its halo mirrors, ms[2*8+g] stress kernel of grid g,
+ * ms[3*8+i] vz solve of interface i, ms[4*8+i] sxz solve, ms[5*8+i] syz
+ * solve, ms[6*8] receiver/source kernel.  The state advances by nsteps. */
+int ecsg_time_kernels(ecsg_sim *sim, int nsteps, double *ms);
+
+int ecsg_synchronize(ecsg_sim *sim);
+/* Device status bits accumulated since the last clear (ECSG_ST_*). */
+int ecsg_get_status(ecsg_sim *sim, int *status, int clear);
+/* Bytes of device memory held by the simulation. */
+long long ecsg_device_bytes(const ecsg_sim *sim);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,229 @@
+"""CUDA path (through the C ABI) against the oracle and the reference goldens.
+
+Tolerances
+* FP64 device path: the stencils reproduce the reference's rounding sequence,
+  so vel/stress must match the oracle exactly; the interface solves and
+  reductions differ only in summation order (<= 1e-12 relative).
+* FP32 device path (the production path): one operator <= 2e-6 relative to the
+  field scale; traces within 1e-5 rel-L2 of the FP64 result (the north-star
+  bound), and within 5e-5 rel-L2 of the reference's 2016 goldens (the bound the
+  reference itself meets here).
+"""
+import os
+
+import numpy as np
+import pytest
+
+import ecsg_b200
+from ecsg_b200 import Simulation
+from ecsg_b200.workloads import eci_test_case, random_case, ricker
+from oracle.oracle import OracleRun
+
+pytestmark = pytest.mark.gpu
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def _pair(case, prec, energy=False, **kw):
+    return OracleRun(case, energy=energy), Simulation(case, precision=prec, energy=energy, **kw)
+
+
+def _randomize(o, s, rng, prec):
+    for g in range(len(o.levels)):
+        for k in range(9):
+            a = rng.standard_normal(o.levels[g]["f"][k].shape)
+            if prec == "f32":
+                a = a.astype(np.float32).astype(np.float64)
+            o.levels[g]["f"][k][...] = a
+            s.set_field(g, k, a)
+
+
+def _err(o, s):
+    """max |oracle - device| / max |oracle| over all components of all grids."""
+    worst = 0.0
+    for g in range(len(o.levels)):
+        for k in range(9):
+            a = o.levels[g]["f"][k]
+            b = s.field(g, k)
+            scale = max(np.abs(a).max(), 1e-300)
+            worst = max(worst, float(np.abs(a - b).max() / scale))
+    return worst
+
+
+CASES = [(2, 1), (2, 0), (3, 1)]
+
+
+@pytest.mark.parametrize("ratio,top_bc", CASES)
+def test_operators_f64(ratio, top_bc):
+    case = random_case(20 + ratio, ratio=ratio, nx2=7, ny2=6, nz=(6, 5), top_bc=top_bc)
+    o, s = _pair(case, "f64", energy=True)
+    rng = np.random.default_rng(ratio * 10 + top_bc)
+    with s:
+        _randomize(o, s, rng, "f64")
+        for g in range(2):
+            o.update_vel(g)
+            s.update_vel(g)
+        assert _err(o, s) == 0.0
+        _randomize(o, s, rng, "f64")
+        for g in range(2):
+            o.update_stress(g)
+            s.update_stress(g)
+        assert _err(o, s) == 0.0
+        _randomize(o, s, rng, "f64")
+        o.ghost_vz(1)
+        s.ghost_vz(1)
+        assert _err(o, s) < 1e-12
+        _randomize(o, s, rng, "f64")
+        o.ghost_syz(1)
+        s.ghost_syz(1)
+        assert _err(o, s) < 1e-12
+        _randomize(o, s, rng, "f64")
+        it_o, tol_o = o.ghost_sxz(1)
+        s.ghost_sxz(1)
+        X, it_s, tol_s, _ = s.sxz_state(1)
+        assert _err(o, s) < 1e-11
+        assert abs(it_o - it_s) <= 1 and abs(tol_o - tol_s) <= 1e-12 * max(tol_o, 1e-300)
+        assert np.abs(X - o.X[0]["X"]).max() < 1e-11 * max(np.abs(X).max(), 1.0)
+        _randomize(o, s, rng, "f64")
+        o.copy_vel()
+        s.copy_vel()
+        _randomize(o, s, rng, "f64")
+        eo, es = o.energy(), s.energy()
+        assert abs(eo - es) <= 1e-12 * abs(eo)
+        ro, rs = o.residues(1), s.residues(1)
+        assert np.abs(ro - rs).max() <= 1e-12 * np.abs(ro).max()
+
+
+@pytest.mark.parametrize("ratio,top_bc", CASES)
+def test_operators_f32(ratio, top_bc):
+    case = random_case(30 + ratio, ratio=ratio, nx2=7, ny2=6, nz=(6, 5), top_bc=top_bc)
+    o, s = _pair(case, "f32")
+    rng = np.random.default_rng(ratio * 100 + top_bc)
+    with s:
+        for op in ("vel", "stress", "vz", "syz", "sxz"):
+            _randomize(o, s, rng, "f32")
+            if op == "vel":
+                for g in range(2):
+                    o.update_vel(g)
+                    s.update_vel(g)
+            elif op == "stress":
+                for g in range(2):
+                    o.update_stress(g)
+                    s.update_stress(g)
+            else:
+                getattr(o, "ghost_" + op)(1)
+                getattr(s, "ghost_" + op)(1)
+            assert _err(o, s) < 2e-6, op
+
+
+def _with_src_rec(case, nt=60):
+    h = case.grids[0]["h"]
+    n = case.grids[0]["n"]
+    case.src = {"xyz": (n[0] // 2 * h[0], n[1] // 2 * h[1], 2 * h[2]), "trace": ricker(nt, case.dt * 1e-3 * 0.5, 15.0),
+                "scale": 1000.0, "comp": 0}
+    case.rec = np.array([[(n[0] // 2 + 3) * h[0], n[1] // 2 * h[1], 2 * h[2]],
+                         [(n[0] // 3) * h[0], (n[1] // 3) * h[1], (n[2] - 1) * h[2]],
+                         [(n[0] // 2) * h[0], (n[1] // 2) * h[1], (n[2] + 2) * h[2]]], dtype=np.float32)
+    return case
+
+
+@pytest.mark.parametrize("ratio", [2, 3])
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_time_loop_vs_oracle(ratio, prec):
+    case = _with_src_rec(random_case(40 + ratio, ratio=ratio, nx2=9, ny2=8, nz=(8, 6)))
+    n = 80
+    o = OracleRun(case, energy=True)
+    ref = o.run(n, residues=True)
+    with Simulation(case, precision=prec, energy=True) as s:
+        assert s.src == o.src and s.rec == o.rec
+        out = s.run(n, energy_every=1, residues=True, graph=False)
+    rel = np.linalg.norm(out["rec"] - ref["rec"], axis=1) / np.linalg.norm(ref["rec"], axis=1)
+    erel = np.abs(out["energy"] - ref["energy"]) / np.abs(ref["energy"]).max()
+    if prec == "f64":
+        assert rel.max() < 1e-10 and erel.max() < 1e-10
+        assert np.abs(out["res"] - ref["res"]).max() < 1e-8 * np.abs(ref["res"]).max()
+    else:
+        assert rel.max() < 1e-5, rel
+        assert erel.max() < 1e-5
+
+
+def test_graph_replay_is_bitwise_equal():
+    case = _with_src_rec(random_case(50, ratio=3, nx2=9, ny2=8, nz=(8, 6)))
+    outs = []
+    for graph in (False, True):
+        with Simulation(case, precision="f32", energy=True) as s:
+            r = s.run(40, energy_every=5, graph=graph)
+            outs.append((r, [s.field(g, k) for g in range(2) for k in range(9)]))
+    (ra, fa), (rb, fb) = outs
+    assert np.array_equal(ra["rec"], rb["rec"])
+    assert np.array_equal(ra["energy"], rb["energy"], equal_nan=True)
+    for a, b in zip(fa, fb):
+        assert np.array_equal(a, b)
+
+
+def _rel_l2(a, b):
+    return np.linalg.norm(a - b, axis=-1) / np.linalg.norm(b, axis=-1)
+
+
+@pytest.mark.parametrize("test", [1, 2, 3])
+def test_golden_replay(test):
+    """The reference experiment tests/test1-cmp-eci-ii/eci (par1/2/3.py), full
+    length, against the reference's own traces."""
+    case = eci_test_case(test)
+    gold = np.load(os.path.join(GOLDEN, "rec_eci_test%d.npy" % test))
+    recs = {}
+    for prec in ("f64", "f32"):
+        with Simulation(case, precision=prec) as s:
+            recs[prec] = s.run()["rec"]
+            assert s.status() == 0
+    for prec in ("f64", "f32"):
+        err = _rel_l2(recs[prec], gold)
+        assert (err < 5e-5).all(), (prec, err)
+    assert (_rel_l2(recs["f32"], recs["f64"]) < 1e-5).all()
+
+
+@pytest.mark.parametrize("ratio", [2, 3])
+def test_energy_conserved_after_source(ratio):
+    """ECI keeps the composite energy constant once the source stops
+    (README.md:16); relative drift over 1000 post-source steps."""
+    case = random_case(60 + ratio, ratio=ratio, nx2=16, ny2=14, nz=(14, 10))
+    case = _with_src_rec(case, nt=60)
+    with Simulation(case, precision="f32", energy=True) as s:
+        out = s.run(1100, energy_every=10)
+    e = out["energy"][100::10]
+    drift = (e.max() - e.min()) / np.abs(e).mean()
+    assert np.isfinite(e).all() and drift < 1e-5, drift
+
+
+def test_interface_residues_vanish():
+    case = _with_src_rec(random_case(70, ratio=3, nx2=10, ny2=9, nz=(9, 7)))
+    with Simulation(case, precision="f64") as s:
+        out = s.run(120, residues=True, graph=False)
+    res = out["res"][:, 0, :]
+    for grp in range(3):
+        r = np.abs(res[:, 3 * grp])
+        scale = res[:, 3 * grp + 1] * res[:, 3 * grp + 2] * case.grids[1]["n"][0] * case.grids[1]["n"][1]
+        assert (r <= 1e-9 * scale.max()).all(), (grp, r.max(), scale.max())
+
+
+def test_jacobi_cap_reports_status():
+    case = random_case(80, ratio=2, nx2=9, ny2=8, nz=(6, 5))
+    o, s = _pair(case, "f64", jacobi_max_iter=2)
+    with s:
+        _randomize(o, s, np.random.default_rng(0), "f64")
+        s.ghost_sxz(1)
+        assert s.status() & ecsg_b200.ST_JACOBI_CAP
+        _, it, _, _ = s.sxz_state(1)
+        assert it == 2
+        s.status(clear=True)
+        assert s.status() == 0
+
+
+def test_invalid_configurations_fail_loudly():
+    case = random_case(0, ratio=2)
+    case.radius = 2
+    with pytest.raises(ecsg_b200.EcsgError):
+        Simulation(case)
+    case = random_case(0, ratio=2)
+    case.grids[0]["n"] = (case.grids[0]["n"][0] + 1,) + case.grids[0]["n"][1:]
+    with pytest.raises(ecsg_b200.EcsgError):
+        Simulation(case)

@@ -18,7 +18,7 @@ namespace ecsg {
 template <typename T>
 cudaError_t launch_vel(const GridDev<T> &, int, int, int, T *const[3], int, cudaStream_t);
 template <typename T>
-cudaError_t launch_vel_mirror(const GridDev<T> &, int, int, int, cudaStream_t);
+cudaError_t launch_vel_mirror(const GridDev<T> &, int, int, int, int, cudaStream_t);
 template <typename T>
 cudaError_t launch_stress(const GridDev<T> &, int, int, int, int, cudaStream_t);
 // interface.cu
@@ -66,7 +66,7 @@ struct Iface {
 
 struct ecsg_sim {
     int ng = 0, R = 1, imode = 1, top_bc = 0, prec = ECSG_F32, medium = ECSG_MEDIUM_ISO, energy = 0;
-    int jacobi_max_iter = 10000, device = 0, sms = 148;
+    int jacobi_max_iter = 10000, device = 0, sms = 148, mirror_fix = 0;
     double dt = 0;
     size_t tsize = 4;
     Geo geo[kMaxGrids];
@@ -198,6 +198,7 @@ int ecsg_create(const ecsg_grid_desc *grids, const ecsg_config *cfg, ecsg_sim **
     s->energy = cfg->energy ? 1 : 0;
     s->jacobi_max_iter = cfg->jacobi_max_iter > 0 ? cfg->jacobi_max_iter : 10000;
     s->device = cfg->device;
+    s->mirror_fix = cfg->mirror_fix ? 1 : 0;
     s->tsize = s->prec == ECSG_F32 ? 4 : 8;
     s->nc = s->medium == ECSG_MEDIUM_ISO ? 5 : 9;
     if (cudaSetDevice(s->device) != cudaSuccess) { fail(s, ECSG_ERR_NO_DEVICE, "cudaSetDevice(%d) failed", s->device); return bail(ECSG_ERR_NO_DEVICE); }
@@ -428,7 +429,7 @@ static int vel_kernel_op(ecsg_sim *s, int g, bool with_copy)
 template <typename T>
 static int vel_mirror_op(ecsg_sim *s, int g)
 {
-    CK(launch_vel_mirror<T>(dev<T>(s, g), g == 0, g == s->ng - 1, s->top_bc, s->st));
+    CK(launch_vel_mirror<T>(dev<T>(s, g), g == 0, g == s->ng - 1, s->top_bc, s->mirror_fix, s->st));
     return ECSG_OK;
 }
 

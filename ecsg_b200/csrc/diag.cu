@@ -193,6 +193,19 @@ __global__ void __launch_bounds__(RED_THREADS) avgabs_kernel(GridDev<T> G, int c
     block_sums<1>(acc, partial, gridDim.x);
 }
 
+// Field::AvgAbs divides by the extents one dim at a time (field.cpp:224-226).
+__global__ void avgabs_finalize_kernel(const double *partial, int nblocks, int e2, int e1, int e0, double *out)
+{
+    if (threadIdx.x == 0) {
+        double s = 0.0;
+        for (int i = 0; i < nblocks; i++) s += partial[i];
+        s /= e2;
+        s /= e1;
+        s /= e0;
+        out[0] = s;
+    }
+}
+
 __global__ void sum_partials_kernel(const double *partial, int nblocks, int nterms, double *out)
 {
     if (threadIdx.x < nterms) {
@@ -316,7 +329,8 @@ cudaError_t launch_avgabs(const GridDev<T> &G, int comp, const int pos[3], doubl
                           cudaStream_t st)
 {
     avgabs_kernel<T><<<nblocks, RED_THREADS, 0, st>>>(G, comp, pos[0], pos[1], pos[2], partial);
-    sum_partials_kernel<<<1, 32, 0, st>>>(partial, nblocks, 1, out);
+    avgabs_finalize_kernel<<<1, 32, 0, st>>>(partial, nblocks, G.g.nz + 1 - pos[2], G.g.ny + 1 - pos[1],
+                                             G.g.nx + 1 - pos[0], out);
     return cudaGetLastError();
 }
 

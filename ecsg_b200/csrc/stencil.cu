@@ -113,10 +113,13 @@ __global__ void __launch_bounds__(TX *TY) vel_kernel(GridDev<T> G, int zt, int b
 //   phase 0: vz top (rigid top only), vz bottom (bottom grid), vz x-start/end,
 //            vy x-start/end over vz's y-extent [0, ny] (this reads the y = ny
 //            halo of vy before phase 1 rewrites it, as in the reference)
-//   phase 1: vy y-start/end over vz's z-extent [0, nz-1]
+//   phase 1: vy y-start/end over vz's z-extent [0, nz-1], or over vy's own
+//            extent [0, nz] when mirror_fix is set (then the updated interface
+//            plane of a fine grid gets its wall mirror and the composite
+//            energy is conserved exactly)
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void vel_mirror_kernel(GridDev<T> G, int phase, int top_rigid, int bottom)
+__global__ void vel_mirror_kernel(GridDev<T> G, int phase, int top_rigid, int bottom, int mirror_fix)
 {
     const Geo &g = G.g;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
@@ -140,7 +143,7 @@ __global__ void vel_mirror_kernel(GridDev<T> G, int phase, int top_rigid, int bo
         t -= nD;
         if (t < nD) { int iy = t % (ny + 1), iz = t / (ny + 1); vy[g.idx(nx, iy, iz)] = -vy[g.idx(nx - 1, iy, iz)]; return; }
     } else {
-        const int64_t nG = (int64_t)nz * nx;
+        const int64_t nG = (int64_t)(nz + (mirror_fix ? 1 : 0)) * nx;
         if (t < nG) { int ix = t % nx, iz = t / nx; vy[g.idx(ix, -1, iz)] = -vy[g.idx(ix, 0, iz)]; return; }
         t -= nG;
         if (t < nG) { int ix = t % nx, iz = t / nx; vy[g.idx(ix, ny, iz)] = -vy[g.idx(ix, ny - 1, iz)]; return; }
@@ -296,15 +299,15 @@ cudaError_t launch_vel(const GridDev<T> &G, int top, int bottom, int top_bc, T *
 }
 
 template <typename T>
-cudaError_t launch_vel_mirror(const GridDev<T> &G, int top, int bottom, int top_bc, cudaStream_t st)
+cudaError_t launch_vel_mirror(const GridDev<T> &G, int top, int bottom, int top_bc, int mirror_fix, cudaStream_t st)
 {
     const Geo &g = G.g;
     const int top_rigid = (top && top_bc != 1) ? 1 : 0;
     const int64_t n0 = (int64_t)(top_rigid + bottom) * (g.ny + 1) * g.nx + 2LL * g.nz * (g.ny + 1)
                      + 2LL * (g.nz + 1) * (g.ny + 1);
-    const int64_t n1 = 2LL * g.nz * g.nx;
-    vel_mirror_kernel<T><<<(unsigned)((n0 + 255) / 256), 256, 0, st>>>(G, 0, top_rigid, bottom);
-    vel_mirror_kernel<T><<<(unsigned)((n1 + 255) / 256), 256, 0, st>>>(G, 1, top_rigid, bottom);
+    const int64_t n1 = 2LL * (g.nz + (mirror_fix ? 1 : 0)) * g.nx;
+    vel_mirror_kernel<T><<<(unsigned)((n0 + 255) / 256), 256, 0, st>>>(G, 0, top_rigid, bottom, mirror_fix);
+    vel_mirror_kernel<T><<<(unsigned)((n1 + 255) / 256), 256, 0, st>>>(G, 1, top_rigid, bottom, mirror_fix);
     return cudaGetLastError();
 }
 
@@ -326,8 +329,8 @@ cudaError_t launch_stress(const GridDev<T> &G, int medium, int top, int top_bc, 
 
 template cudaError_t launch_vel<float>(const GridDev<float> &, int, int, int, float *const[3], int, cudaStream_t);
 template cudaError_t launch_vel<double>(const GridDev<double> &, int, int, int, double *const[3], int, cudaStream_t);
-template cudaError_t launch_vel_mirror<float>(const GridDev<float> &, int, int, int, cudaStream_t);
-template cudaError_t launch_vel_mirror<double>(const GridDev<double> &, int, int, int, cudaStream_t);
+template cudaError_t launch_vel_mirror<float>(const GridDev<float> &, int, int, int, int, cudaStream_t);
+template cudaError_t launch_vel_mirror<double>(const GridDev<double> &, int, int, int, int, cudaStream_t);
 template cudaError_t launch_stress<float>(const GridDev<float> &, int, int, int, int, cudaStream_t);
 template cudaError_t launch_stress<double>(const GridDev<double> &, int, int, int, int, cudaStream_t);
 

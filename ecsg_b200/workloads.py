@@ -54,6 +54,7 @@ class Case:
     """
 
     def __init__(self, **kw):
+        self.mirror_fix = False   # True: vy wall mirrors cover the updated interface plane (energy-exact)
         self.__dict__.update(kw)
 
     @property

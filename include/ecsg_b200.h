@@ -68,6 +68,10 @@ typedef struct ecsg_config {
     int energy;           /* allocate velocity copies for the energy (check_energy) */
     int jacobi_max_iter;  /* cap on sxz Jacobi sweeps per solve; <= 0 selects 10000 */
     int device;           /* CUDA device ordinal */
+    int mirror_fix;       /* 0: the reference's halo mirrors exactly; 1: the vy wall
+                           * mirrors also cover the top-most updated plane of vy
+                           * (update_vel.cpp:211-246 stop one plane short), which
+                           * makes the composite energy exactly conserved */
 } ecsg_config;
 
 typedef struct ecsg_sim ecsg_sim;

@@ -57,7 +57,12 @@ static inline double *AT(const ofield *f, int i0, int i1, int i2)
 /* ------------------------------------------------------------------------- */
 /* Velocity update: update_vel.cpp:4-249                                      */
 /* ------------------------------------------------------------------------- */
-void o_update_vel(ogrid *g, int top, int bottom, int top_bc)
+/* mirror_fix = 0 reproduces the reference exactly.  mirror_fix = 1 runs the vy
+ * y-wall mirrors over vy's own z-extent [0, nz] instead of vz's [0, nz-1]
+ * (update_vel.cpp:211-218, 239-246): on the fine side of an interface the
+ * plane z = nz is updated (bottom = 0), and without its wall mirror the
+ * summation-by-parts identity, hence the composite energy, leaks there. */
+void o_update_vel(ogrid *g, int top, int bottom, int top_bc, int mirror_fix)
 {
     ofield *vx = &g->f[0], *vy = &g->f[1], *vz = &g->f[2];
     ofield *sxx = &g->f[3], *syy = &g->f[4], *szz = &g->f[5];
@@ -177,7 +182,7 @@ void o_update_vel(ogrid *g, int top, int bottom, int top_bc)
         for (int ir = 1; ir < R; ir++)
             for (int ix = 0; ix <= vx->end[0]; ix++)
                 V(vx, ix, -ir, iz) = -V(vx, ix, ir, iz);
-    for (int iz = 0; iz <= vz->end[2]; iz++)
+    for (int iz = 0; iz <= (mirror_fix ? vy->end[2] : vz->end[2]); iz++)
         for (int ir = 1; ir <= R; ir++)
             for (int ix = 0; ix <= vy->end[0]; ix++)
                 V(vy, ix, -ir, iz) = -V(vy, ix, ir - 1, iz);
@@ -194,7 +199,7 @@ void o_update_vel(ogrid *g, int top, int bottom, int top_bc)
                 for (int ix = 0; ix <= vx->end[0]; ix++)
                     V(vx, ix, iy + ir, iz) = -V(vx, ix, iy - ir, iz);
         iy = vy->end[1];
-        for (int iz = 0; iz <= vz->end[2]; iz++)
+        for (int iz = 0; iz <= (mirror_fix ? vy->end[2] : vz->end[2]); iz++)
             for (int ir = 1; ir <= R; ir++)
                 for (int ix = 0; ix <= vy->end[0]; ix++)
                     V(vy, ix, iy + ir, iz) = -V(vy, ix, iy - ir + 1, iz);

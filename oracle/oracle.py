@@ -37,7 +37,7 @@ def lib():
             raise RuntimeError("oracle library missing: run `make -C oracle oracle`")
         L = ctypes.CDLL(path)
         P = ctypes.POINTER
-        L.o_update_vel.argtypes = [P(OGrid), ctypes.c_int, ctypes.c_int, ctypes.c_int]
+        L.o_update_vel.argtypes = [P(OGrid), ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.o_update_stress.argtypes = [P(OGrid), ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.o_ghost_vz_eci.argtypes = [P(OGrid), P(OGrid), ctypes.c_int]
         L.o_ghost_syz_eci.argtypes = [P(OGrid), P(OGrid), ctypes.c_int]
@@ -241,7 +241,8 @@ class OracleRun:
     # -- single operators ------------------------------------------------
     def update_vel(self, g):
         ng = len(self.levels)
-        lib().o_update_vel(ctypes.byref(self.structs[g]), int(g == 0), int(g == ng - 1), self.case.top_bc)
+        lib().o_update_vel(ctypes.byref(self.structs[g]), int(g == 0), int(g == ng - 1), self.case.top_bc,
+                           int(getattr(self.case, "mirror_fix", False)))
 
     def update_stress(self, g):
         ng = len(self.levels)

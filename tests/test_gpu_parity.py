@@ -139,7 +139,10 @@ def test_time_loop_vs_oracle(ratio, prec):
     rel = np.linalg.norm(out["rec"] - ref["rec"], axis=1) / np.linalg.norm(ref["rec"], axis=1)
     erel = np.abs(out["energy"] - ref["energy"]) / np.abs(ref["energy"]).max()
     if prec == "f64":
-        assert rel.max() < 1e-10 and erel.max() < 1e-10
+        # traces leave the device as float32 (the reference writes float RSF traces)
+        ref32 = ref["rec"].astype(np.float32).astype(np.float64)
+        rel32 = np.linalg.norm(out["rec"] - ref32, axis=1) / np.linalg.norm(ref32, axis=1)
+        assert rel32.max() < 1e-7 and erel.max() < 1e-10, (rel32, erel.max())
         assert np.abs(out["res"] - ref["res"]).max() < 1e-8 * np.abs(ref["res"]).max()
     else:
         assert rel.max() < 1e-5, rel
@@ -181,17 +184,35 @@ def test_golden_replay(test):
     assert (_rel_l2(recs["f32"], recs["f64"]) < 1e-5).all()
 
 
+@pytest.mark.parametrize("prec,tol", [("f64", 1e-11), ("f32", 1e-5)])
 @pytest.mark.parametrize("ratio", [2, 3])
-def test_energy_conserved_after_source(ratio):
+def test_energy_conserved_after_source(ratio, prec, tol):
     """ECI keeps the composite energy constant once the source stops
-    (README.md:16); relative drift over 1000 post-source steps."""
+    (README.md:16): relative drift over 1000 post-source steps, with the vy wall
+    mirrors extended to the fine interface plane (mirror_fix; the reference's
+    own extent leaks energy there, see test_oracle.py)."""
     case = random_case(60 + ratio, ratio=ratio, nx2=16, ny2=14, nz=(14, 10))
     case = _with_src_rec(case, nt=60)
-    with Simulation(case, precision="f32", energy=True) as s:
+    case.mirror_fix = True
+    with Simulation(case, precision=prec, energy=True) as s:
         out = s.run(1100, energy_every=10)
     e = out["energy"][100::10]
     drift = (e.max() - e.min()) / np.abs(e).mean()
-    assert np.isfinite(e).all() and drift < 1e-5, drift
+    assert np.isfinite(e).all() and drift < tol, drift
+
+
+@pytest.mark.parametrize("ratio", [2, 3])
+def test_mirror_fix_matches_oracle(ratio):
+    case = _with_src_rec(random_case(90 + ratio, ratio=ratio, nx2=9, ny2=8, nz=(8, 6)))
+    case.mirror_fix = True
+    o = OracleRun(case, energy=True)
+    ref = o.run(60)
+    with Simulation(case, precision="f64", energy=True) as s:
+        out = s.run(60, energy_every=1, graph=False)
+        f = [s.field(g, 1) for g in range(2)]
+    assert np.abs(out["energy"] - ref["energy"]).max() < 1e-10 * np.abs(ref["energy"]).max()
+    for g in range(2):
+        assert np.abs(f[g] - o.field(g, 1)).max() < 1e-10 * np.abs(o.field(g, 1)).max()
 
 
 def test_interface_residues_vanish():

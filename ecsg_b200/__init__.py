@@ -40,6 +40,25 @@ class Config(ctypes.Structure):
                 ("device", ctypes.c_int), ("mirror_fix", ctypes.c_int)]
 
 
+class GridView(ctypes.Structure):
+    """ecsg_grid_view: one grid's device arrays in the library's device layout."""
+    _fields_ = [("size", ctypes.c_int * 3), ("step", ctypes.c_double * 3), ("radius", ctypes.c_int),
+                ("pitch", ctypes.c_int * 3), ("origin", ctypes.c_longlong), ("field", ctypes.c_void_p * 9),
+                ("buoy", ctypes.c_void_p)]
+
+
+XOFF = 32   # element x = 0 of every row sits 32 elements into the row (128-byte aligned rows)
+
+
+def device_layout(n, R=1):
+    """Padded device layout of a grid with n = (nx, ny, nz) cells and halo R:
+    pitch (px, py, pz) and the index of element (0,0,0) (ecsg_device.cuh)."""
+    px = ((XOFF + n[0] + 1 + R) + 31) // 32 * 32
+    py = n[1] + 1 + 2 * R
+    pz = n[2] + 1 + 2 * R
+    return {"pitch": (px, py, pz), "origin": (R * py + R) * px + XOFF}
+
+
 # (name, restype, argtypes) of every exported entry point of include/ecsg_b200.h
 SIGNATURES = [
     ("ecsg_create", ctypes.c_int, [ctypes.POINTER(GridDesc), ctypes.POINTER(Config), ctypes.POINTER(ctypes.c_void_p)]),
@@ -71,6 +90,9 @@ SIGNATURES = [
     ("ecsg_timer_start", ctypes.c_int, [ctypes.c_void_p]),
     ("ecsg_timer_stop", ctypes.c_int, [ctypes.c_void_p, c_dp]),
     ("ecsg_time_kernels", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_dp]),
+    ("ecsg_ghost_sxz_noalloc", ctypes.c_int, [ctypes.POINTER(GridView), ctypes.POINTER(GridView), ctypes.c_double,
+                                              ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, c_ip,
+                                              ctypes.c_char_p, ctypes.c_size_t]),
     ("ecsg_synchronize", ctypes.c_int, [ctypes.c_void_p]),
     ("ecsg_get_status", ctypes.c_int, [ctypes.c_void_p, c_ip, ctypes.c_int]),
     ("ecsg_device_bytes", ctypes.c_longlong, [ctypes.c_void_p]),

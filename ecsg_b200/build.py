@@ -25,6 +25,7 @@ SOURCES = {
     "interface.cu": ["-fmad=false"],
     "diag.cu": ["-fmad=false"],
     "api.cu": [],
+    "noalloc.cu": [],
 }
 
 

@@ -159,6 +159,52 @@ int ecsg_timer_stop(ecsg_sim *sim, double *ms);
  * solve, ms[6*8] receiver/source kernel.  The state advances by nsteps. */
 int ecsg_time_kernels(ecsg_sim *sim, int nsteps, double *ms);
 
+/* ---------------------------------------------------------------------------
+ * Allocation-free sxz interface solve.  No counterpart in the reference: it
+ * exists for callers that cannot allocate device memory (their device memory
+ * belongs to another framework's allocator, or a fixed budget was reserved up
+ * front), who hold the two grids' fields themselves and pass them in.
+ *
+ * It runs the same energy-conserving sxz solve as ecsg_ghost_sxz (matrix,
+ * right-hand side, warm-started Jacobi with the reference stopping rule, coarse
+ * and fine ghost values written into the sxz fields) and calls no cudaMalloc,
+ * cudaFree or allocating library routine.  Its work space is one static device
+ * array of about 11.6 MB that every GPU loading the library keeps until exit;
+ * interfaces with more than ECSG_NOALLOC_MAX_UNKNOWNS interior coarse nodes
+ * ((nx2-1)*(ny2-1)) or ECSG_NOALLOC_MAX_NODES nodes ((nx2+1)*(ny2+1)) are
+ * rejected with ECSG_ERR_INVALID and a message (362 x 362 coarse cells fit).
+ * The first call on a device looks up the array's device address; make that
+ * first call before any stream capture.  All calls share the array and it keeps
+ * the last call's contents (each call clears what must start at zero), so calls
+ * that overlap on the GPU race: serialise them on one stream.
+ *
+ * Fields are passed in the device layout of ecsg_grid_view (the layout an
+ * ecsg_sim uses internally).  X is the caller's device array of
+ * (nx2+1)*(ny2+1) doubles with a zero border: the warm start on entry, the new
+ * coarse ghost values on return (the reference's g_sxz array).  stream is a
+ * cudaStream_t (NULL: the legacy default stream); the call is asynchronous
+ * unless iters is non-null, in which case it waits for the solve and returns
+ * ECSG_ERR_NOT_CONVERGED when the sweep cap was hit.  errbuf (may be NULL)
+ * receives the message of a failure.
+ * ------------------------------------------------------------------------- */
+#define ECSG_NOALLOC_MAX_UNKNOWNS 131072
+#define ECSG_NOALLOC_MAX_NODES 132496
+
+/* One grid in device memory: element (x,y,z) of every component, x,y,z from
+ * -radius, is at index origin + (z*pitch[1] + y)*pitch[0] + x. */
+typedef struct ecsg_grid_view {
+    int size[3];          /* cells */
+    double step[3];
+    int radius;           /* halo radius (1) */
+    int pitch[3];         /* elements per row, rows per plane, planes */
+    long long origin;     /* index of element (0,0,0) */
+    void *field[9];       /* component order of this header; float or double */
+    const void *buoy;     /* buoyancy at nodes, same layout and type */
+} ecsg_grid_view;
+
+int ecsg_ghost_sxz_noalloc(const ecsg_grid_view *fine, const ecsg_grid_view *coarse, double dt, int precision,
+                           double *X, int max_iter, void *stream, int *iters, char *errbuf, size_t errlen);
+
 int ecsg_synchronize(ecsg_sim *sim);
 /* Device status bits accumulated since the last clear (ECSG_ST_*). */
 int ecsg_get_status(ecsg_sim *sim, int *status, int clear);

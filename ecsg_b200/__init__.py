@@ -53,7 +53,7 @@ XOFF = 32   # element x = 0 of every row sits 32 elements into the row (128-byte
 def device_layout(n, R=1):
     """Padded device layout of a grid with n = (nx, ny, nz) cells and halo R:
     pitch (px, py, pz) and the index of element (0,0,0) (ecsg_device.cuh)."""
-    px = ((XOFF + n[0] + 1 + R) + 31) // 32 * 32
+    px = ((XOFF + n[0] + 1 + max(R, 8)) + 31) // 32 * 32
     py = n[1] + 1 + 2 * R
     pz = n[2] + 1 + 2 * R
     return {"pitch": (px, py, pz), "origin": (R * py + R) * px + XOFF}

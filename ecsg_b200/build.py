@@ -22,6 +22,7 @@ LIB = os.path.join(OUT_DIR, "libecsg_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = {
     "stencil.cu": [],
+    "stencil_v4.cu": [],
     "interface.cu": ["-fmad=false"],
     "diag.cu": ["-fmad=false"],
     "api.cu": [],

@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 namespace ecsg {
@@ -21,9 +22,12 @@ template <typename T>
 cudaError_t launch_vel_mirror(const GridDev<T> &, int, int, int, int, cudaStream_t);
 template <typename T>
 cudaError_t launch_stress(const GridDev<T> &, int, int, int, int, cudaStream_t);
+// stencil_v4.cu (FP32 production sweeps)
+cudaError_t launch_vel_v4(const GridDev<float> &, int, int, int, float *const[3], int, cudaStream_t);
+cudaError_t launch_stress_v4(const GridDev<float> &, int, int, int, int, cudaStream_t);
 // interface.cu
 template <typename T>
-cudaError_t launch_ghost_vz(const GridDev<T> &, const GridDev<T> &, int, int, cudaStream_t);
+cudaError_t launch_ghost_vz(const GridDev<T> &, const GridDev<T> &, int, int, double *, cudaStream_t);
 template <typename T>
 cudaError_t launch_ghost_syz(const GridDev<T> &, const GridDev<T> &, int, cudaStream_t);
 template <typename T>
@@ -35,7 +39,7 @@ cudaError_t launch_sxz_solve(const GridDev<T> &, const GridDev<T> &, int, const 
 // diag.cu
 template <typename T>
 cudaError_t launch_energy(const GridDev<T> &, int, T *const[3], double *, int, double, double, double, double *,
-                          const int *, int, int, int *, cudaStream_t);
+                          const int *, const int *, int, int *, cudaStream_t);
 template <typename T>
 cudaError_t launch_residue(const GridDev<T> &, const GridDev<T> &, int, double, double *, int, double *, cudaStream_t);
 template <typename T>
@@ -60,6 +64,7 @@ static const int kStiffPos[9][3] = {{1, 0, 0}, {1, 0, 0}, {1, 0, 0}, {1, 0, 0}, 
 struct Iface {
     int r = 2;
     double *A = nullptr, *B = nullptr, *X0 = nullptr, *X1 = nullptr, *partial = nullptr;
+    double *vzc = nullptr;   // vz tridiagonal rows: 4 x (ny2-1) x nx2
     int nblocks = 0;
     bool A_ready = false;
 };
@@ -67,6 +72,7 @@ struct Iface {
 struct ecsg_sim {
     int ng = 0, R = 1, imode = 1, top_bc = 0, prec = ECSG_F32, medium = ECSG_MEDIUM_ISO, energy = 0;
     int jacobi_max_iter = 10000, device = 0, sms = 148, mirror_fix = 0;
+    bool scalar_stencils = false;   // FP32: use the scalar sweeps of stencil.cu (validation)
     double dt = 0;
     size_t tsize = 4;
     Geo geo[kMaxGrids];
@@ -78,7 +84,7 @@ struct ecsg_sim {
     void *vc[kMaxGrids][3] = {};
     bool medium_set[kMaxGrids] = {};
     Iface itf[kMaxGrids];
-    // shared device scalars: [0] status, [1] step clock, [2] last sxz sweeps
+    // shared device scalars: [0] status, [1] step clock, [2] last sxz sweeps, [3] first step of the run
     int *ints = nullptr;
     long long *iters_total = nullptr;   // per interface
     double *dscal = nullptr;            // [0] energy, [1] total, [2..] last tol per interface, [16..] residue scratch
@@ -89,6 +95,7 @@ struct ecsg_sim {
     int src_grid = -1, src_off = 0, src_comp = 0, src_nt = 0;
     float src_scale = 1.0f;
     float *src_trace = nullptr;
+    int src_cap = 0;
     int nrec = 0, rec_comp = 0;
     int *rec_grid = nullptr, *rec_off = nullptr;
     float *traces = nullptr;
@@ -101,6 +108,10 @@ struct ecsg_sim {
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};   // [0,1] run loop, [2,3] user timer
     double last_run_ms = 0;
     long long launches = 0;        // kernels launched by the last ecsg_run (all steps)
+    cudaGraphExec_t gx[2] = {nullptr, nullptr};   // cached step graphs: [0] plain, [1] energy step
+    long long epoch = 0;           // bumped when anything a captured step refers to changes
+    long long gx_epoch[2] = {-1, -1};
+    int run_n0 = 0;                // pinned by the async copies at the start of a run
     long long bytes = 0;
     std::string err;
 };
@@ -199,6 +210,10 @@ int ecsg_create(const ecsg_grid_desc *grids, const ecsg_config *cfg, ecsg_sim **
     s->jacobi_max_iter = cfg->jacobi_max_iter > 0 ? cfg->jacobi_max_iter : 10000;
     s->device = cfg->device;
     s->mirror_fix = cfg->mirror_fix ? 1 : 0;
+    {
+        const char *env = getenv("ECSG_SCALAR_STENCILS");
+        s->scalar_stencils = env && env[0] == '1';
+    }
     s->tsize = s->prec == ECSG_F32 ? 4 : 8;
     s->nc = s->medium == ECSG_MEDIUM_ISO ? 5 : 9;
     if (cudaSetDevice(s->device) != cudaSuccess) { fail(s, ECSG_ERR_NO_DEVICE, "cudaSetDevice(%d) failed", s->device); return bail(ECSG_ERR_NO_DEVICE); }
@@ -250,6 +265,7 @@ int ecsg_create(const ecsg_grid_desc *grids, const ecsg_config *cfg, ecsg_sim **
         const size_t nn = (size_t)(C.nx - 1) * (C.ny - 1);
         const size_t nxy = (size_t)(C.nx + 1) * (C.ny + 1);
         if ((rc = dmalloc(s, (void **)&I.A, sizeof(double) * 9 * nn))) return bail(rc);
+        if ((rc = dmalloc(s, (void **)&I.vzc, sizeof(double) * 4 * (size_t)(C.ny - 1) * C.nx))) return bail(rc);
         if ((rc = dmalloc(s, (void **)&I.B, sizeof(double) * nn))) return bail(rc);
         if ((rc = dmalloc(s, (void **)&I.X0, sizeof(double) * nxy))) return bail(rc);
         if ((rc = dmalloc(s, (void **)&I.X1, sizeof(double) * nxy))) return bail(rc);
@@ -271,11 +287,13 @@ int ecsg_destroy(ecsg_sim *s)
         for (int k = 0; k < 9; k++) cudaFree(s->c[g][k]);
         for (int k = 0; k < 3; k++) cudaFree(s->vc[g][k]);
         Iface &I = s->itf[g];
-        cudaFree(I.A); cudaFree(I.B); cudaFree(I.X0); cudaFree(I.X1); cudaFree(I.partial);
+        cudaFree(I.A); cudaFree(I.B); cudaFree(I.X0); cudaFree(I.X1); cudaFree(I.partial); cudaFree(I.vzc);
     }
     cudaFree(s->partial); cudaFree(s->ints); cudaFree(s->iters_total); cudaFree(s->dscal); cudaFree(s->bar);
     cudaFree(s->src_trace); cudaFree(s->rec_grid); cudaFree(s->rec_off); cudaFree(s->traces);
     cudaFree(s->run_energy); cudaFree(s->run_res);
+    for (int v = 0; v < 2; v++)
+        if (s->gx[v]) cudaGraphExecDestroy(s->gx[v]);
     for (int e = 0; e < 4; e++)
         if (s->ev[e]) cudaEventDestroy(s->ev[e]);
     if (s->st) cudaStreamDestroy(s->st);
@@ -422,6 +440,12 @@ template <typename T>
 static int vel_kernel_op(ecsg_sim *s, int g, bool with_copy)
 {
     T *vc[3] = {(T *)s->vc[g][0], (T *)s->vc[g][1], (T *)s->vc[g][2]};
+    if constexpr (std::is_same<T, float>::value) {
+        if (!s->scalar_stencils) {
+            CK(launch_vel_v4(dev<float>(s, g), g == 0, g == s->ng - 1, s->top_bc, with_copy ? vc : nullptr, s->sms, s->st));
+            return ECSG_OK;
+        }
+    }
     CK(launch_vel<T>(dev<T>(s, g), g == 0, g == s->ng - 1, s->top_bc, with_copy ? vc : nullptr, s->sms, s->st));
     return ECSG_OK;
 }
@@ -443,14 +467,22 @@ static int vel_op(ecsg_sim *s, int g, bool with_copy)
 template <typename T>
 static int stress_op(ecsg_sim *s, int g)
 {
-    CK(launch_stress<T>(dev<T>(s, g), s->medium == ECSG_MEDIUM_ISO ? MED_ISO5 : MED_ORTHO9, g == 0, s->top_bc, s->sms, s->st));
+    const int med = s->medium == ECSG_MEDIUM_ISO ? MED_ISO5 : MED_ORTHO9;
+    if constexpr (std::is_same<T, float>::value) {
+        if (!s->scalar_stencils) {
+            CK(launch_stress_v4(dev<float>(s, g), med, g == 0, s->top_bc, s->sms, s->st));
+            return ECSG_OK;
+        }
+    }
+    CK(launch_stress<T>(dev<T>(s, g), med, g == 0, s->top_bc, s->sms, s->st));
     return ECSG_OK;
 }
 
 template <typename T>
 static int vz_op(ecsg_sim *s, int i)
 {
-    CK(launch_ghost_vz<T>(dev<T>(s, i - 1), dev<T>(s, i), s->medium == ECSG_MEDIUM_ISO ? MED_ISO5 : MED_ORTHO9, s->itf[i].r, s->st));
+    CK(launch_ghost_vz<T>(dev<T>(s, i - 1), dev<T>(s, i), s->medium == ECSG_MEDIUM_ISO ? MED_ISO5 : MED_ORTHO9, s->itf[i].r,
+                          s->itf[i].vzc, s->st));
     return ECSG_OK;
 }
 
@@ -589,7 +621,7 @@ static int copy_vel_op(ecsg_sim *s)
 }
 
 template <typename T>
-static int energy_op(ecsg_sim *s, double *out, const int *step, int step0)
+static int energy_op(ecsg_sim *s, double *out, const int *step, const int *step0)
 {
     for (int g = 0; g < s->ng; g++) {
         T *vc[3] = {(T *)s->vc[g][0], (T *)s->vc[g][1], (T *)s->vc[g][2]};
@@ -614,7 +646,7 @@ int ecsg_energy(ecsg_sim *s, double *energy)
     if (!s || !energy) return ECSG_ERR_INVALID;
     if (!s->energy) return fail(s, ECSG_ERR_STATE, "energy: simulation created without energy support");
     if (int rc = check_ready(s)) return rc;
-    int rc = DISPATCH(energy_op)(s, s->dscal, nullptr, 0);
+    int rc = DISPATCH(energy_op)(s, s->dscal, nullptr, nullptr);
     if (rc) return rc;
     CK(cudaMemcpyAsync(energy, s->dscal, sizeof(double), cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
@@ -684,15 +716,23 @@ int ecsg_set_source(ecsg_sim *s, int g, int ix, int iy, int iz, int comp, const 
     if (ix < -s->R || ix > G.nx + s->R || iy < -s->R || iy > G.ny + s->R || iz < -s->R || iz > G.nz + s->R)
         return fail(s, ECSG_ERR_INVALID, "set_source: index outside grid %d", g);
     CK(cudaSetDevice(s->device));
-    cudaFree(s->src_trace);
-    s->src_trace = nullptr;
-    if (nt > 0) {
+    if (nt > s->src_cap) {
+        cudaFree(s->src_trace);
+        s->src_trace = nullptr;
+        s->src_cap = 0;
         CK(cudaMalloc(&s->src_trace, sizeof(float) * nt));
+        s->src_cap = nt;
+        s->epoch++;
+    }
+    if (nt > 0) {
         CK(cudaMemcpyAsync(s->src_trace, trace, sizeof(float) * nt, cudaMemcpyHostToDevice, s->st));
         CK(cudaStreamSynchronize(s->st));
     }
+    const int off = G.idx(ix, iy, iz);
+    if (g != s->src_grid || off != s->src_off || comp != s->src_comp || nt != s->src_nt || scale != s->src_scale)
+        s->epoch++;
     s->src_grid = g;
-    s->src_off = G.idx(ix, iy, iz);
+    s->src_off = off;
     s->src_comp = comp;
     s->src_nt = nt;
     s->src_scale = scale;
@@ -726,10 +766,11 @@ int ecsg_set_receivers(ecsg_sim *s, const int *loc4, int n, int comp)
     }
     s->nrec = n;
     s->rec_comp = comp;
+    s->epoch++;
     return ECSG_OK;
 }
 
-static SrcRec make_srcrec(ecsg_sim *s, int step0, int mode)
+static SrcRec make_srcrec(ecsg_sim *s, int mode)
 {
     SrcRec S;
     memset(&S, 0, sizeof S);
@@ -740,7 +781,7 @@ static SrcRec make_srcrec(ecsg_sim *s, int step0, int mode)
     S.traces = s->traces;
     S.trace_cap = s->trace_cap;
     S.step = s->ints + 1;
-    S.step0 = step0;
+    S.step0 = s->ints + 3;
     S.src_base = (s->src_grid >= 0 && s->src_trace) ? s->f[s->src_grid][s->src_comp] : nullptr;
     S.src_off = s->src_off;
     S.src_trace = s->src_trace;
@@ -752,18 +793,18 @@ static SrcRec make_srcrec(ecsg_sim *s, int step0, int mode)
 
 // One iteration of main.cpp:165-261 (movies excluded).
 template <typename T>
-static int step_op(ecsg_sim *s, int step0, bool energy, double *energy_buf, double *res_row)
+static int step_op(ecsg_sim *s, bool energy, double *energy_buf, double *res_row)
 {
     int rc;
     for (int g = 0; g < s->ng; g++)
         if ((rc = vel_op<T>(s, g, energy))) return rc;
     if (res_row) {
-        CK(launch_src_rec<T>(make_srcrec(s, step0, 1), s->st));
+        CK(launch_src_rec<T>(make_srcrec(s, 1), s->st));
         for (int i = 1; i < s->ng; i++)
             if ((rc = residue_op<T>(s, i, 3, res_row + 12 * (i - 1)))) return rc;
-        CK(launch_src_rec<T>(make_srcrec(s, step0, 2), s->st));
+        CK(launch_src_rec<T>(make_srcrec(s, 2), s->st));
     } else {
-        CK(launch_src_rec<T>(make_srcrec(s, step0, 3), s->st));
+        CK(launch_src_rec<T>(make_srcrec(s, 3), s->st));
     }
     for (int i = 1; i < s->ng; i++)
         if ((rc = vz_op<T>(s, i))) return rc;
@@ -771,7 +812,7 @@ static int step_op(ecsg_sim *s, int step0, bool energy, double *energy_buf, doub
         for (int i = 1; i < s->ng; i++)
             if ((rc = residue_op<T>(s, i, 4, res_row + 12 * (i - 1)))) return rc;
     if (energy)
-        if ((rc = energy_op<T>(s, energy_buf, s->ints + 1, step0))) return rc;
+        if ((rc = energy_op<T>(s, energy_buf, s->ints + 1, s->ints + 3))) return rc;
     for (int g = 0; g < s->ng; g++)
         if ((rc = stress_op<T>(s, g))) return rc;
     for (int i = 1; i < s->ng; i++) {
@@ -793,12 +834,14 @@ static int run_op(ecsg_sim *s, int n0, int nsteps, float *traces, double *energy
         s->traces = nullptr;
         CK(cudaMalloc(&s->traces, sizeof(float) * (size_t)nsteps * s->nrec));
         s->trace_cap = nsteps;
+        s->epoch++;
     }
     if (energy && s->run_energy_cap < nsteps) {
         cudaFree(s->run_energy);
         s->run_energy = nullptr;
         CK(cudaMalloc(&s->run_energy, sizeof(double) * (size_t)nsteps));
         s->run_energy_cap = nsteps;
+        s->epoch++;
     }
     const int nres = 12 * (s->ng - 1);
     if (residues && s->run_res_cap < nsteps) {
@@ -811,46 +854,53 @@ static int run_op(ecsg_sim *s, int n0, int nsteps, float *traces, double *energy
         std::vector<double> nan(nsteps, NAN);
         CK(cudaMemcpyAsync(s->run_energy, nan.data(), sizeof(double) * nsteps, cudaMemcpyHostToDevice, s->st));
     }
-    CK(cudaMemcpyAsync(s->ints + 1, &n0, sizeof(int), cudaMemcpyHostToDevice, s->st));
+    s->run_n0 = n0;
+    CK(cudaMemcpyAsync(s->ints + 1, &s->run_n0, sizeof(int), cudaMemcpyHostToDevice, s->st));
+    CK(cudaMemcpyAsync(s->ints + 3, &s->run_n0, sizeof(int), cudaMemcpyHostToDevice, s->st));
     const int every = energy_every > 0 ? energy_every : 1;
-    cudaGraphExec_t gx[2] = {nullptr, nullptr};
     bool graphs = use_graph && !residues;
     if (graphs) {
+        // one captured step per variant, cached across runs until something it refers to changes
         for (int variant = 0; variant < (energy ? 2 : 1); variant++) {
+            if (s->gx[variant] && s->gx_epoch[variant] == s->epoch) continue;
+            if (s->gx[variant]) cudaGraphExecDestroy(s->gx[variant]);
+            s->gx[variant] = nullptr;
             cudaGraph_t gr = nullptr;
             CK(cudaStreamBeginCapture(s->st, cudaStreamCaptureModeThreadLocal));
-            rc = step_op<T>(s, n0, variant == 1, s->run_energy, nullptr);
+            rc = step_op<T>(s, variant == 1, s->run_energy, nullptr);
             cudaError_t e = cudaStreamEndCapture(s->st, &gr);
             if (rc || e != cudaSuccess) {
                 if (gr) cudaGraphDestroy(gr);
-                for (int v = 0; v < 2; v++)
-                    if (gx[v]) cudaGraphExecDestroy(gx[v]);
                 cudaGetLastError();
                 return rc ? rc : fail(s, ECSG_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
             }
-            e = cudaGraphInstantiate(&gx[variant], gr, 0);
+            e = cudaGraphInstantiate(&s->gx[variant], gr, 0);
             cudaGraphDestroy(gr);
-            if (e != cudaSuccess) return fail(s, ECSG_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+            if (e != cudaSuccess) {
+                s->gx[variant] = nullptr;
+                return fail(s, ECSG_ERR_CUDA, "graph instantiate: %s", cudaGetErrorString(e));
+            }
+            s->gx_epoch[variant] = s->epoch;
         }
     }
     CK(cudaEventRecord(s->ev[0], s->st));
     long long launches = 0;
-    const long long per_step = 6LL * s->ng + 1 + 3LL * (s->ng - 1);
+    // per step: velocity kernel + 2 mirror kernels and the stress kernel per grid,
+    // the receiver/source kernel, 3 vz + 1 sxz + 1 syz kernels per interface
+    const long long per_step = 4LL * s->ng + 1 + 5LL * (s->ng - 1);
     for (int n = n0; n < n0 + nsteps; n++) {
         const bool e_step = energy && ((n % every) == 0);
-        launches += per_step + (e_step ? 2LL * s->ng : 0) + (residues ? 1 + 12LL * (s->ng - 1) : 0);
+        launches += per_step + (e_step ? 2LL * s->ng : 0) + (residues ? 1 + 18LL * (s->ng - 1) : 0);
         if (graphs) {
-            cudaError_t e = cudaGraphLaunch(gx[e_step ? 1 : 0], s->st);
+            cudaError_t e = cudaGraphLaunch(s->gx[e_step ? 1 : 0], s->st);
             if (e != cudaSuccess) { rc = fail(s, ECSG_ERR_CUDA, "graph launch: %s", cudaGetErrorString(e)); break; }
         } else {
-            if ((rc = step_op<T>(s, n0, e_step, s->run_energy, residues ? s->run_res + (size_t)(n - n0) * nres : nullptr)))
+            if ((rc = step_op<T>(s, e_step, s->run_energy, residues ? s->run_res + (size_t)(n - n0) * nres : nullptr)))
                 break;
         }
         rc = ECSG_OK;
     }
     CK(cudaEventRecord(s->ev[1], s->st));
-    for (int v = 0; v < 2; v++)
-        if (gx[v]) cudaGraphExecDestroy(gx[v]);
     if (rc) return rc;
     s->launches = launches;
     if (traces && s->nrec > 0)
@@ -946,9 +996,7 @@ static int time_kernels_op(ecsg_sim *s, int nsteps, double *out)
     std::vector<cudaEvent_t> ev(2 * nev);
     for (auto &e : ev) CK(cudaEventCreate(&e));
     std::vector<double> acc(7 * kMaxGrids, 0.0);
-    int step0 = 0;
-    CK(cudaMemcpyAsync(&step0, s->ints + 1, sizeof(int), cudaMemcpyDeviceToHost, s->st));
-    CK(cudaStreamSynchronize(s->st));
+    CK(cudaMemcpyAsync(s->ints + 3, s->ints + 1, sizeof(int), cudaMemcpyDeviceToDevice, s->st));
     for (int n = 0; n < nsteps; n++) {
         int e = 0;
         auto bracket = [&](int slot, auto fn) -> int {
@@ -968,7 +1016,7 @@ static int time_kernels_op(ecsg_sim *s, int nsteps, double *out)
             if ((rc = bracket(1 * kMaxGrids + g, [&] { return vel_mirror_op<T>(s, g); }))) return rc;
         }
         if ((rc = bracket(6 * kMaxGrids, [&] {
-                 CK(launch_src_rec<T>(make_srcrec(s, step0, 3), s->st));
+                 CK(launch_src_rec<T>(make_srcrec(s, 3), s->st));
                  return (int)ECSG_OK;
              })))
             return rc;

@@ -118,10 +118,10 @@ __global__ void __launch_bounds__(RED_THREADS) energy_kernel(GridDev<T> G, int m
 
 // Sum term partials in CTA order and combine as compute_energy.cpp:38-52; adds
 // the grid's energy into the composite sum over grids (main.cpp:219-223).
-// The destination is out[0], or out[*step - 1 - step0] when a device step
+// The destination is out[0], or out[*step - 1 - *step0] when the device step
 // clock is given (inside a run, after the clock advanced for this step).
 __global__ void energy_finalize_kernel(const double *partial, int nblocks, double h0, double h1, double h2,
-                                       double *out, const int *step, int step0, int first, int *status)
+                                       double *out, const int *step, const int *step0, int first, int *status)
 {
     __shared__ double term[12];
     if (threadIdx.x < 12) {
@@ -135,7 +135,7 @@ __global__ void energy_finalize_kernel(const double *partial, int nblocks, doubl
         for (int k = 0; k < 6; k++) res += term[k];
         for (int k = 6; k < 12; k++) res += 2 * term[k];
         res *= 0.5 * h2 * h1 * h0;
-        double *dst = step ? out + (*step - 1 - step0) : out;
+        double *dst = step ? out + (*step - 1 - *step0) : out;
         const double e = first ? res : *dst + res;
         *dst = e;
         if (!isfinite(e)) atomicOr(status, ST_NONFINITE);
@@ -226,7 +226,7 @@ template <typename T>
 __global__ void src_rec_kernel(SrcRec S)
 {
     const int n = *S.step;
-    const int row = n - S.step0;
+    const int row = n - *S.step0;
     if (S.mode & 1)
         for (int i = threadIdx.x; i < S.nrec; i += blockDim.x) {
             const T *base = (const T *)S.rec_base[S.rec_grid[i]];
@@ -307,7 +307,7 @@ __global__ void iso_medium_kernel(Geo g, const double *s11, const double *s13, d
 // ---------------------------------------------------------------------------
 template <typename T>
 cudaError_t launch_energy(const GridDev<T> &G, int medium, T *const vc[3], double *partial, int nblocks, double h0,
-                          double h1, double h2, double *out, const int *step, int step0, int first, int *status,
+                          double h1, double h2, double *out, const int *step, const int *step0, int first, int *status,
                           cudaStream_t st)
 {
     energy_kernel<T><<<nblocks, RED_THREADS, 0, st>>>(G, medium, vc[0], vc[1], vc[2], partial);
@@ -374,7 +374,7 @@ cudaError_t launch_iso_medium(const Geo &g, const double *s11, const double *s13
 
 #define INST(T)                                                                                               \
     template cudaError_t launch_energy<T>(const GridDev<T> &, int, T *const[3], double *, int, double, double,   \
-                                          double, double *, const int *, int, int, int *, cudaStream_t);       \
+                                          double, double *, const int *, const int *, int, int *, cudaStream_t); \
     template cudaError_t launch_residue<T>(const GridDev<T> &, const GridDev<T> &, int, double, double *, int,   \
                                            double *, cudaStream_t);                                            \
     template cudaError_t launch_avgabs<T>(const GridDev<T> &, int, const int[3], double *, int, double *,        \

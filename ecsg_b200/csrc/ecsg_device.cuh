@@ -2,9 +2,10 @@
 //
 // HBM layout of one sub-grid.  All field components of a grid share one padded
 // box so that every kernel uses the same strides:
-//   x in [-R, nx+R]   row pitch px (multiple of 32 elements); element x = 0 of
+//   x in [-R, nx+8]   row pitch px (multiple of 32 elements); element x = 0 of
 //                     every row sits XOFF elements into the row, so rows start
-//                     on 128-byte boundaries
+//                     on 128-byte boundaries; the right padding of 8 lets the
+//                     float4 sweeps read whole 16-byte chunks past x = nx+1
 //   y in [-R, ny+R]   py = ny + 1 + 2R rows per plane
 //   z in [-R, nz+R]   pz = nz + 1 + 2R planes
 // Staggered components use a subset of the box (their extents end at n-1); the
@@ -36,7 +37,7 @@ inline Geo make_geo(int nx, int ny, int nz, int R)
 {
     Geo g;
     g.nx = nx; g.ny = ny; g.nz = nz; g.R = R;
-    g.px = ((XOFF + nx + 1 + R) + 31) / 32 * 32;
+    g.px = ((XOFF + nx + 1 + (R > 8 ? R : 8)) + 31) / 32 * 32;
     g.py = ny + 1 + 2 * R;
     g.pz = nz + 1 + 2 * R;
     g.off0 = (R * g.py + R) * g.px + XOFF;
@@ -109,7 +110,7 @@ struct SrcRec {
     float *traces;               // [capacity][nrec]
     int trace_cap;
     int *step;                   // device step clock
-    int step0;                   // first step of the current run
+    const int *step0;            // device: first step of the current run (trace row 0)
     void *src_base;
     int src_off;
     const float *src_trace;

@@ -11,8 +11,8 @@
 //   -(last fine interior value) + P(coarse ghost + coarse first interior value).
 // This gives (update_ghost_*.cpp for r = 2):
 //   vz : one tridiagonal system along y per coarse x-cell (update_ghost_vz.cpp:124-221)
-//        -> one CTA per x-cell, parallel cyclic reduction in shared memory,
-//           fine-ghost scatter fused
+//        -> assembly (coalesced along x), one CTA per x-cell for parallel
+//           cyclic reduction in shared memory, fine-ghost scatter
 //   syz: pointwise closed form (update_ghost_syz.cpp:151-240) -> one thread per cell
 //   sxz: 9-point system on the interior coarse nodes, warm-started Jacobi with
 //        the reference stopping rule ||X_k - X_{k-1}||_2 <= min(1e-12, 1e-5 avg|B|)
@@ -54,66 +54,77 @@ __device__ __forceinline__ void normal_c(const GridDev<T> &G, int medium, int p,
 }
 
 // ---------------------------------------------------------------------------
-// vz: CTA per coarse x-cell j0, thread per unknown j1 = t+1 (t < m = ny2-1).
-// Shared memory: a, b, c, d (P doubles each) and X (ny2+1 doubles).
+// vz, in three kernels so that every global access is coalesced along x:
+//   1. assemble: thread per unknown (j0 fastest, j1 in [1, ny2-1]) writes the
+//      tridiagonal row (lower, diagonal, upper, rhs) to coef[4][j1-1][j0];
+//   2. solve: CTA per coarse x-cell j0, parallel cyclic reduction of its
+//      system in shared memory, coarse ghost vz2(j0, j1, -1) written back
+//      (rounded to the field type, as the fine scatter reads it);
+//   3. scatter: thread per fine ghost vz1(i0, i1, nz1), i0 fastest.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void ghost_vz_kernel(GridDev<T> F, GridDev<T> C, int medium, int r)
+__global__ void ghost_vz_assemble_kernel(GridDev<T> F, GridDev<T> C, int medium, int r, double *coef)
+{
+    const int j0 = blockIdx.x * blockDim.x + threadIdx.x;
+    const int j1 = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int nx2 = C.g.nx, ny2 = C.g.ny, nz1 = F.g.nz;
+    const int m = ny2 - 1;
+    if (j0 >= nx2 || j1 > m) return;
+    const T *vx1 = F.f[VX], *vy1 = F.f[VY], *szz1 = F.f[SZZ], *vz1 = F.f[VZ];
+    const T *vx2 = C.f[VX], *vy2 = C.f[VY], *szz2 = C.f[SZZ], *vz2 = C.f[VZ];
+    const double k1x = F.kd[0], k1y = F.kd[1], k1z = F.kd[2];
+    const double k2x = C.kd[0], k2y = C.kd[1], k2z = C.kd[2];
+    const double rr = (double)r, r3 = rr * rr * rr;
+    const int pc = C.g.idx(j0, j1, 0);
+    double c13, c23, c33;
+    normal_c(C, medium, pc, c13, c23, c33);
+    const double pred = (double)szz2[pc] + c13 * k2x * ((double)vx2[C.g.idx(j0 + 1, j1, 0)] - (double)vx2[pc])
+                      + c23 * k2y * ((double)vy2[pc] - (double)vy2[C.g.idx(j0, j1 - 1, 0)])
+                      + c33 * k2z * (double)vz2[pc];
+    double dg = r3 * k2z * c33, lo = 0.0, up = 0.0, fsum = 0.0;
+    for (int i0 = r * j0; i0 < r * j0 + r; i0++) {
+        for (int i1 = r * (j1 - 1) + 1; i1 <= r * (j1 + 1) - 1; i1++) {
+            const double w = pw_node(i1, j1, r, ny2);
+            const double wl = pw_node(i1, j1 - 1, r, ny2), wu = pw_node(i1, j1 + 1, r, ny2);
+            const int pf = F.g.idx(i0, i1, nz1);
+            double f13, f23, f33;
+            normal_c(F, medium, pf, f13, f23, f33);
+            const double cz = f33 * k1z;
+            const int jl = i1 / r, ju = jl + 1;
+            double pv0 = pw_node_all(i1, jl, r) * (double)vz2[C.g.idx(j0, jl, 0)];
+            if (ju <= ny2) pv0 += pw_node_all(i1, ju, r) * (double)vz2[C.g.idx(j0, ju, 0)];
+            const double pf_ = (double)szz1[pf] + f13 * k1x * ((double)vx1[pf + 1] - (double)vx1[pf])
+                             + f23 * k1y * ((double)vy1[pf] - (double)vy1[pf - F.g.px])
+                             + cz * (pv0 - 2.0 * (double)vz1[pf - F.g.px * F.g.py]);
+            dg += rr * w * w * cz;
+            lo += rr * w * wl * cz;
+            up += rr * w * wu * cz;
+            fsum += rr * w * pf_;
+        }
+    }
+    const size_t plane = (size_t)m * nx2, q = (size_t)(j1 - 1) * nx2 + j0;
+    coef[q] = (j1 == 1) ? 0.0 : lo;          // coupling to a boundary node: not an unknown
+    coef[plane + q] = dg;
+    coef[2 * plane + q] = (j1 == m) ? 0.0 : up;
+    coef[3 * plane + q] = r3 * pred - fsum;
+}
+
+template <typename T>
+__global__ void ghost_vz_solve_kernel(GridDev<T> C, const double *coef)
 {
     extern __shared__ double sm[];
     const int P = blockDim.x;
     const int t = threadIdx.x;
     const int j0 = blockIdx.x;
-    const int nx2 = C.g.nx, ny2 = C.g.ny, nz1 = F.g.nz;
+    const int nx2 = C.g.nx, ny2 = C.g.ny;
     const int m = ny2 - 1;
-    double *A = sm, *B = sm + P, *Cc = sm + 2 * P, *D = sm + 3 * P, *X = sm + 4 * P;
-    (void)nx2;
-    const T *vx1 = F.f[VX], *vy1 = F.f[VY], *szz1 = F.f[SZZ];
-    T *vz1 = F.f[VZ];
-    const T *vx2 = C.f[VX], *vy2 = C.f[VY], *szz2 = C.f[SZZ];
+    double *A = sm, *B = sm + P, *Cc = sm + 2 * P, *D = sm + 3 * P;
     T *vz2 = C.f[VZ];
-    const double k1x = F.kd[0], k1y = F.kd[1], k1z = F.kd[2];
-    const double k2x = C.kd[0], k2y = C.kd[1], k2z = C.kd[2];
-    const double rr = (double)r, r3 = rr * rr * rr;
-
-    double lo = 0.0, dg = 1.0, up = 0.0, rhs = 0.0;
-    if (t < m) {
-        const int j1 = t + 1;
-        const int pc = C.g.idx(j0, j1, 0);
-        double c13, c23, c33;
-        normal_c(C, medium, pc, c13, c23, c33);
-        const double pred = (double)szz2[pc] + c13 * k2x * ((double)vx2[C.g.idx(j0 + 1, j1, 0)] - (double)vx2[pc])
-                          + c23 * k2y * ((double)vy2[pc] - (double)vy2[C.g.idx(j0, j1 - 1, 0)])
-                          + c33 * k2z * (double)vz2[pc];
-        dg = r3 * k2z * c33;
-        lo = 0.0;
-        up = 0.0;
-        double fsum = 0.0;
-        for (int i0 = r * j0; i0 < r * j0 + r; i0++) {
-            for (int i1 = r * (j1 - 1) + 1; i1 <= r * (j1 + 1) - 1; i1++) {
-                const double w = pw_node(i1, j1, r, ny2);
-                const double wl = pw_node(i1, j1 - 1, r, ny2), wu = pw_node(i1, j1 + 1, r, ny2);
-                const int pf = F.g.idx(i0, i1, nz1);
-                double f13, f23, f33;
-                normal_c(F, medium, pf, f13, f23, f33);
-                const double cz = f33 * k1z;
-                const int jl = i1 / r, ju = jl + 1;
-                double pv0 = pw_node_all(i1, jl, r) * (double)vz2[C.g.idx(j0, jl, 0)];
-                if (ju <= ny2) pv0 += pw_node_all(i1, ju, r) * (double)vz2[C.g.idx(j0, ju, 0)];
-                const double pf_ = (double)szz1[pf] + f13 * k1x * ((double)vx1[pf + 1] - (double)vx1[pf])
-                                 + f23 * k1y * ((double)vy1[pf] - (double)vy1[pf - F.g.px])
-                                 + cz * (pv0 - 2.0 * (double)vz1[pf - F.g.px * F.g.py]);
-                dg += rr * w * w * cz;
-                lo += rr * w * wl * cz;
-                up += rr * w * wu * cz;
-                fsum += rr * w * pf_;
-            }
-        }
-        rhs = r3 * pred - fsum;
-        lo = (j1 == 1) ? 0.0 : lo;   // coupling to the boundary node, whose value is not an unknown
-        up = (j1 == m) ? 0.0 : up;
-    }
-    A[t] = lo; B[t] = dg; Cc[t] = up; D[t] = rhs;
+    const size_t plane = (size_t)m * nx2, q = (size_t)t * nx2 + j0;
+    A[t] = t < m ? coef[q] : 0.0;
+    B[t] = t < m ? coef[plane + q] : 1.0;
+    Cc[t] = t < m ? coef[2 * plane + q] : 0.0;
+    D[t] = t < m ? coef[3 * plane + q] : 0.0;
     __syncthreads();
     // parallel cyclic reduction: rows outside [0,m) are identity rows
     for (int s = 1; s < P; s <<= 1) {
@@ -135,32 +146,29 @@ __global__ void ghost_vz_kernel(GridDev<T> F, GridDev<T> C, int medium, int r)
         A[t] = na; B[t] = nb; Cc[t] = nc; D[t] = nd;
         __syncthreads();
     }
-    // coarse ghost, rounded to the field type as the fine scatter reads it back
-    for (int j1 = t; j1 <= ny2; j1 += P) {
-        double x;
-        if (j1 >= 1 && j1 <= m) {
-            const T xt = (T)(D[j1 - 1] / B[j1 - 1]);
-            vz2[C.g.idx(j0, j1, -1)] = xt;
-            x = (double)xt;
-        } else {
-            x = (double)vz2[C.g.idx(j0, j1, -1)];
-        }
-        X[j1] = x;
+    if (t < m) vz2[C.g.idx(j0, t + 1, -1)] = (T)(D[t] / B[t]);
+}
+
+template <typename T>
+__global__ void ghost_vz_scatter_kernel(GridDev<T> F, GridDev<T> C, int r)
+{
+    const int i0 = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i1 = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int ny2 = C.g.ny, nz1 = F.g.nz;
+    const int nx1 = r * C.g.nx, ny1 = r * ny2;
+    if (i0 >= nx1 || i1 >= ny1) return;
+    const T *vz2 = C.f[VZ];
+    T *vz1 = F.f[VZ];
+    const int j0 = i0 / r, jl = i1 / r, ju = jl + 1;
+    const int csz = C.g.px * C.g.py;
+    const int pl = C.g.idx(j0, jl, 0);
+    double s = pw_node_all(i1, jl, r) * ((double)vz2[pl] + (double)vz2[pl - csz]);
+    if (ju <= ny2) {
+        const int pu = C.g.idx(j0, ju, 0);
+        s += pw_node_all(i1, ju, r) * ((double)vz2[pu] + (double)vz2[pu - csz]);
     }
-    __syncthreads();
-    // fine ghosts vz1(i0, i1, nz1): fine interior y nodes, the r fine x cells of j0
-    const int ny1 = r * ny2;
-    for (int i1 = 1 + t; i1 < ny1; i1 += P) {
-        const int jl = i1 / r, ju = jl + 1;
-        const double wl = pw_node_all(i1, jl, r);
-        const double wu = (ju <= ny2) ? pw_node_all(i1, ju, r) : 0.0;
-        double s = wl * ((double)vz2[C.g.idx(j0, jl, 0)] + X[jl]);
-        if (ju <= ny2) s += wu * ((double)vz2[C.g.idx(j0, ju, 0)] + X[ju]);
-        for (int i0 = r * j0; i0 < r * j0 + r; i0++) {
-            const int pf = F.g.idx(i0, i1, nz1);
-            vz1[pf] = (T)(-(double)vz1[pf - F.g.px * F.g.py] + s);
-        }
-    }
+    const int pf = F.g.idx(i0, i1, nz1);
+    vz1[pf] = (T)(-(double)vz1[pf - F.g.px * F.g.py] + s);
 }
 
 // ---------------------------------------------------------------------------
@@ -293,41 +301,47 @@ __device__ __forceinline__ double block_sum(double v, double *red)
     return s;   // valid in thread 0
 }
 
-// Grid-wide deterministic sum: block partials summed in block order by the
-// last block to arrive, which then releases the others.  Every block returns
-// the same value.  The wait is bounded; on timeout the status bit is set and
-// the (possibly stale) total returned, and the caller stops iterating.
+// Grid-wide deterministic sum.  Each CTA publishes its partial; the last CTA
+// to arrive sums all partials with all its threads (fixed strided split, then
+// a fixed tree), publishes the total and releases the others by advancing the
+// generation word.  Every CTA returns the same value.  Waiting is bounded: on
+// timeout the status bit is set, ok becomes false and the caller stops.
 __device__ double grid_sum(double v, const SxzWork &W, double *red, bool &ok)
 {
     __threadfence();
-    const double bs = block_sum(v, red);
+    const double bs = block_sum(v, red);   // valid in thread 0
     __shared__ double s_total;
-    __shared__ int s_ok;
+    __shared__ int s_last, s_ok;
+    __shared__ unsigned s_gen;
     if (threadIdx.x == 0) {
-        volatile unsigned *gen = W.bar + 1;
-        const unsigned g0 = *gen;
+        s_gen = *(volatile unsigned *)(W.bar + 1);   // generation of this round, read before arriving
         W.partial[blockIdx.x] = bs;
         __threadfence();
         const unsigned prev = atomicAdd(W.bar, 1u);
+        s_last = (prev == gridDim.x - 1);
         s_ok = 1;
-        if (prev == gridDim.x - 1) {
-            volatile double *pp = W.partial;
-            double s = 0.0;
-            for (unsigned i = 0; i < gridDim.x; i++) s += pp[i];
-            *(volatile double *)W.total = s;
+    }
+    __syncthreads();
+    if (s_last) {
+        __threadfence();
+        double t = 0.0;
+        for (unsigned i = threadIdx.x; i < gridDim.x; i += blockDim.x) t += __ldcg(W.partial + i);
+        const double tot = block_sum(t, red);
+        if (threadIdx.x == 0) {
+            __stcg(W.total, tot);
             W.bar[0] = 0;
             __threadfence();
             atomicAdd(W.bar + 1, 1u);
-            s_total = s;
-        } else {
-            long long spin = 0;
-            while (*gen == g0) {
-                if (++spin > kSpinLimit) { atomicOr(W.status, ST_BARRIER_TIMEOUT); s_ok = 0; break; }
-                __nanosleep(64);
-            }
-            __threadfence();
-            s_total = *(volatile double *)W.total;
+            s_total = tot;
         }
+    } else if (threadIdx.x == 0) {
+        long long spin = 0;
+        while (*(volatile unsigned *)(W.bar + 1) == s_gen) {
+            if (++spin > kSpinLimit) { atomicOr(W.status, ST_BARRIER_TIMEOUT); s_ok = 0; break; }
+            __nanosleep(32);
+        }
+        __threadfence();
+        s_total = __ldcg(W.total);
     }
     __syncthreads();
     ok = s_ok != 0;
@@ -426,14 +440,18 @@ __global__ void __launch_bounds__(256) sxz_solve_kernel(GridDev<T> F, GridDev<T>
 // Host launchers
 // ---------------------------------------------------------------------------
 template <typename T>
-cudaError_t launch_ghost_vz(const GridDev<T> &F, const GridDev<T> &C, int medium, int r, cudaStream_t st)
+cudaError_t launch_ghost_vz(const GridDev<T> &F, const GridDev<T> &C, int medium, int r, double *coef, cudaStream_t st)
 {
     const int m = C.g.ny - 1;
     int P = 32;
     while (P < m) P <<= 1;
     if (P > 1024) return cudaErrorInvalidConfiguration;
-    const size_t smem = sizeof(double) * (4 * P + C.g.ny + 1);
-    ghost_vz_kernel<T><<<C.g.nx, P, smem, st>>>(F, C, medium, r);
+    dim3 ba(32, 8), ga((C.g.nx + 31) / 32, (m + 7) / 8);
+    ghost_vz_assemble_kernel<T><<<ga, ba, 0, st>>>(F, C, medium, r, coef);
+    ghost_vz_solve_kernel<T><<<C.g.nx, P, sizeof(double) * 4 * P, st>>>(C, coef);
+    const int nx1 = r * C.g.nx, ny1 = r * C.g.ny;
+    dim3 bs(128, 2), gs((nx1 + 127) / 128, (ny1 - 1 + 1) / 2);
+    ghost_vz_scatter_kernel<T><<<gs, bs, 0, st>>>(F, C, r);
     return cudaGetLastError();
 }
 
@@ -485,7 +503,7 @@ cudaError_t launch_sxz_solve(const GridDev<T> &F, const GridDev<T> &C, int r, co
 }
 
 #define INST(T)                                                                                         \
-    template cudaError_t launch_ghost_vz<T>(const GridDev<T> &, const GridDev<T> &, int, int, cudaStream_t); \
+    template cudaError_t launch_ghost_vz<T>(const GridDev<T> &, const GridDev<T> &, int, int, double *, cudaStream_t); \
     template cudaError_t launch_ghost_syz<T>(const GridDev<T> &, const GridDev<T> &, int, cudaStream_t);     \
     template cudaError_t launch_sxz_matrix<T>(const GridDev<T> &, const GridDev<T> &, int, double *, cudaStream_t); \
     template int sxz_solve_blocks<T>(int, int);                                                          \

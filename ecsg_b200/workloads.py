@@ -230,3 +230,83 @@ def three_grid_case(seed=0, grids=None, nsteps=2000, fpeak=15.0, cfl=0.9):
     return Case(name="three_grid_r3", grids=[{"n": n, "h": (h, h, h)} for (n, h) in grids], media=media,
                 medium="iso", dt=dt, nsteps=nsteps, radius=1, top_bc=1, imode=1,
                 src={"xyz": (cx, cy, 0.0), "trace": trace, "scale": 1.0, "comp": 2}, rec=rec, rec_comp=2)
+
+
+# ---------------------------------------------------------------------------
+# General anisotropic (21 Cij) media
+# ---------------------------------------------------------------------------
+# Slot order of the 21-Cij medium and the staggered position of each slot:
+# 15 at the normal-stress position N (1,0,0), C44 C45 C46 at the syz position
+# (1,1,1), C55 C56 at the sxz position (0,0,1), C66 at the sxy position (0,1,0).
+CIJ21 = [(1, 1), (1, 2), (1, 3), (2, 2), (2, 3), (3, 3), (1, 4), (1, 5), (1, 6), (2, 4), (2, 5), (2, 6),
+         (3, 4), (3, 5), (3, 6), (4, 4), (4, 5), (4, 6), (5, 5), (5, 6), (6, 6)]
+CIJ21_POS = [(1, 0, 0)] * 15 + [(1, 1, 1)] * 3 + [(0, 0, 1)] * 2 + [(0, 1, 0)]
+
+
+def stagger(f, pos):
+    """Average a node field (nz+1, ny+1, nx+1) to a staggered position: the
+    2-, 4- or 8-point mean of the reference's ReshapeField (field.cpp:428-476)."""
+    p0, p1, p2 = pos
+    o2, o1, o0 = f.shape[0] - p2, f.shape[1] - p1, f.shape[2] - p0
+
+    def s(a, b, c):
+        return f[c:c + o2, b:b + o1, a:a + o0]
+
+    return (s(0, 0, 0) + s(0, 0, p2) + s(0, p1, 0) + s(0, p1, p2)
+            + s(p0, 0, 0) + s(p0, 0, p2) + s(p0, p1, 0) + s(p0, p1, p2)) / 8
+
+
+def cij_to_positions(C):
+    """Node-position Voigt stiffness C (6, 6, nz+1, ny+1, nx+1) -> the 21
+    staggered slot arrays (float64) of a 21-Cij medium."""
+    return [np.ascontiguousarray(stagger(C[i - 1, j - 1].astype(np.float64), pos))
+            for (i, j), pos in zip(CIJ21, CIJ21_POS)]
+
+
+def ortho9_from_cij21(c21):
+    """The orthorhombic part of a 21-Cij medium in the reference's 9-slot
+    convention (c11 c22 c33 c23 c13 c12 c44 c55 c66, shear stored as 2 C44 etc.)."""
+    return [c21[0], c21[3], c21[5], c21[4], c21[2], c21[1], 2 * c21[15], 2 * c21[18], 2 * c21[20]]
+
+
+def random_anisotropic_C(rng, shape, rho, vp, vs, aniso=0.15):
+    """Random symmetric positive-definite Voigt stiffness per point: an isotropic
+    (lambda, mu) tensor plus a random symmetric perturbation of relative size aniso."""
+    lam = rho * (vp * vp - 2 * vs * vs)
+    mu = rho * vs * vs
+    C = np.zeros((6, 6) + shape)
+    for i in range(3):
+        for j in range(3):
+            C[i, j] = lam + (2 * mu if i == j else 0)
+        C[i + 3, i + 3] = mu
+    P = rng.uniform(-1, 1, (6, 6) + shape) * aniso * mu
+    P = 0.5 * (P + P.transpose(1, 0, *range(2, P.ndim)))
+    return C + P
+
+
+def random_case_gen21(seed, ratio=2, nx2=6, ny2=5, nz=(5, 4), top_bc=1, num_grids=2, h1=10.0, aniso=0.15):
+    """Small heterogeneous 21-Cij composite (random anisotropic stiffness per node)."""
+    rng = np.random.default_rng(seed)
+    grids = []
+    nx, ny = nx2 * ratio ** (num_grids - 1), ny2 * ratio ** (num_grids - 1)
+    h = h1
+    for g in range(num_grids):
+        grids.append({"n": (nx, ny, nz[g]), "h": (h, h, h)})
+        nx //= ratio
+        ny //= ratio
+        h *= ratio
+    media = []
+    vmax = 0.0
+    for g in grids:
+        nxg, nyg, nzg = g["n"]
+        shp = (nzg + 1, nyg + 1, nxg + 1)
+        rho = rng.uniform(1.8, 2.6, shp)
+        vs = rng.uniform(1.0, 1.6, shp)
+        vp = vs * rng.uniform(1.7, 2.0, shp)
+        C = random_anisotropic_C(rng, shp, rho, vp, vs, aniso)
+        vmax = max(vmax, float(np.sqrt(np.max(np.linalg.eigvalsh(np.moveaxis(C, (0, 1), (-2, -1)))) / rho.min())))
+        c21 = cij_to_positions(C)
+        media.append({"buoy": (1 / rho).astype(np.float32), "c21": c21, "c9": ortho9_from_cij21(c21)})
+    dt = 0.5 * h1 / vmax / math.sqrt(3)
+    return Case(name="gen21_%d" % seed, grids=grids, media=media, medium="gen21", dt=dt, nsteps=10,
+                radius=1, top_bc=top_bc, imode=1, src=None, rec=np.zeros((0, 3), np.float32), rec_comp=0)

@@ -370,13 +370,22 @@ static inline double pw_cell(int i, int j, int r)
     return (i / r == j) ? 1.0 : 0.0;
 }
 
+/* szz-rate terms of a 21-Cij medium at an interface-plane N point beyond the
+ * orthorhombic ones (defined with the 21-Cij update below). */
+static double gen21_szz_extra(ogrid *g, const ofield *c21, int x, int y, int z);
+static void gen21_c3(const ofield *c21, int x, int y, int z, double *c13, double *c23, double *c33);
+
 /* ------------------------------------------------------------------------- */
 /* Ghost vz (energy-conserving): update_ghost_vz.cpp:124-249, general ratio  */
 /* Unknown: vz2(j0, j1, -1), j0 in [0,nx2), j1 in [1,ny2-1]; one tridiagonal */
 /* system along y per coarse x-cell, solved by the Thomas algorithm.          */
 /* scratch: 4*(ny2+1) doubles per thread (a, b, c, d).                        */
 /* ------------------------------------------------------------------------- */
-void o_ghost_vz_eci(ogrid *g1, ogrid *g2, int r)
+void o_ghost_vz_eci21(ogrid *g1, ogrid *g2, int r, const ofield *c21_1, const ofield *c21_2);
+void o_ghost_vz_eci(ogrid *g1, ogrid *g2, int r) { o_ghost_vz_eci21(g1, g2, r, NULL, NULL); }
+
+/* c21_1/c21_2: the two grids' 21-Cij media, or NULL for the 9-Cij form. */
+void o_ghost_vz_eci21(ogrid *g1, ogrid *g2, int r, const ofield *c21_1, const ofield *c21_2)
 {
     ofield *vx1 = &g1->f[0], *vy1 = &g1->f[1], *vz1 = &g1->f[2], *szz1 = &g1->f[5];
     ofield *vx2 = &g2->f[0], *vy2 = &g2->f[1], *vz2 = &g2->f[2], *szz2 = &g2->f[5];
@@ -400,25 +409,29 @@ void o_ghost_vz_eci(ogrid *g1, ogrid *g2, int r)
         for (int j0 = 0; j0 < nx2; j0++) {
             for (int j1 = 1; j1 <= m; j1++) {
                 /* coarse prediction of szz2(j0,j1,0) without the ghost term */
+                double q13 = V(c13_2, j0, j1, 0), q23 = V(c23_2, j0, j1, 0), q33 = V(c33_2, j0, j1, 0), qx = 0.0;
+                if (c21_2) { gen21_c3(c21_2, j0, j1, 0, &q13, &q23, &q33); qx = gen21_szz_extra(g2, c21_2, j0, j1, 0); }
                 double pc = V(szz2, j0, j1, 0)
-                          + V(c13_2, j0, j1, 0) * k2x * (V(vx2, j0 + 1, j1, 0) - V(vx2, j0, j1, 0))
-                          + V(c23_2, j0, j1, 0) * k2y * (V(vy2, j0, j1, 0) - V(vy2, j0, j1 - 1, 0))
-                          + V(c33_2, j0, j1, 0) * k2z * V(vz2, j0, j1, 0);
-                double diag = r3 * k2z * V(c33_2, j0, j1, 0);
+                          + q13 * k2x * (V(vx2, j0 + 1, j1, 0) - V(vx2, j0, j1, 0))
+                          + q23 * k2y * (V(vy2, j0, j1, 0) - V(vy2, j0, j1 - 1, 0))
+                          + q33 * k2z * V(vz2, j0, j1, 0) + qx;
+                double diag = r3 * k2z * q33;
                 double lo = 0.0, up = 0.0, fsum = 0.0;
                 for (int i0 = r * j0; i0 < r * j0 + r; i0++) {
                     for (int i1 = r * (j1 - 1) + 1; i1 <= r * (j1 + 1) - 1; i1++) {
                         double w = pw_node(i1, j1, r, ny2);
                         double wl = pw_node(i1, j1 - 1, r, ny2), wu = pw_node(i1, j1 + 1, r, ny2);
-                        double cz = V(c33_1, i0, i1, nz1) * k1z;
+                        double f13 = V(c13_1, i0, i1, nz1), f23 = V(c23_1, i0, i1, nz1), f33 = V(c33_1, i0, i1, nz1), fx = 0.0;
+                        if (c21_1) { gen21_c3(c21_1, i0, i1, nz1, &f13, &f23, &f33); fx = gen21_szz_extra(g1, c21_1, i0, i1, nz1); }
+                        double cz = f33 * k1z;
                         /* P(vz2(.,.,0)) at fine node i1 */
                         int jl = i1 / r, ju = jl + 1;
                         double pv0 = pw_node_all(i1, jl, r) * V(vz2, j0, jl, 0)
                                    + (ju <= ny2 ? pw_node_all(i1, ju, r) * V(vz2, j0, ju, 0) : 0.0);
                         double pf = V(szz1, i0, i1, nz1)
-                                  + V(c13_1, i0, i1, nz1) * k1x * (V(vx1, i0 + 1, i1, nz1) - V(vx1, i0, i1, nz1))
-                                  + V(c23_1, i0, i1, nz1) * k1y * (V(vy1, i0, i1, nz1) - V(vy1, i0, i1 - 1, nz1))
-                                  + cz * (pv0 - 2.0 * V(vz1, i0, i1, nz1 - 1));
+                                  + f13 * k1x * (V(vx1, i0 + 1, i1, nz1) - V(vx1, i0, i1, nz1))
+                                  + f23 * k1y * (V(vy1, i0, i1, nz1) - V(vy1, i0, i1 - 1, nz1))
+                                  + cz * (pv0 - 2.0 * V(vz1, i0, i1, nz1 - 1)) + fx;
                         diag += rr * w * w * cz;
                         lo += rr * w * wl * cz;
                         up += rr * w * wu * cz;
@@ -733,4 +746,276 @@ void o_residues(ogrid *g1, ogrid *g2, int r, int which, double *out)
                 res -= r2 * V(&g2->f[5], i0, i1, 0) * (V(&g2->f[2], i0, i1, -1) + V(&g2->f[2], i0, i1, 0));
         out[6] = res; out[7] = o_avgabs(&g2->f[2]); out[8] = o_avgabs(&g2->f[5]);
     }
+}
+
+/* ------------------------------------------------------------------------- */
+/* General anisotropic (21 Cij) stress update.  No reference counterpart: the  */
+/* reference implements the orthorhombic form only (update_stress.cpp:17-133). */
+/* This is the scheme the CUDA kernel implements; with the 12 off-block       */
+/* entries zero it reduces to o_update_stress (shear C44 = c44_ref / 2).      */
+/*                                                                           */
+/* Voigt stiffness, engineering shear strains.  Storage (R = 0 fields):      */
+/*   N  = normal-stress position (1,0,0): slots 0..14 =                      */
+/*        C11 C12 C13 C22 C23 C33 C14 C15 C16 C24 C25 C26 C34 C35 C36        */
+/*   L4 = syz position (1,1,1): 15 C44, 16 C45, 17 C46                        */
+/*   L5 = sxz position (0,0,1): 18 C55, 19 C56                                */
+/*   L6 = sxy position (0,1,0): 20 C66                                        */
+/* Strain increments e1..e3 at N, e4 at L4, e5 at L5, e6 at L6 (the          */
+/* reference's differences times dt/h).  A coupling between positions X and  */
+/* Y uses one coefficient per link, taken at one end (N-end for N-L4/L5/L6,   */
+/* the L4-end for L4-L5 and L4-L6, the L5-end for L5-L6), and is applied in   */
+/* both directions (stress at X gets coeff * average of the strain at Y; the  */
+/* stress at Y gets the average over X of coeff * strain), so the discrete   */
+/* stiffness operator is symmetric and the energy 1/2 (rho v, v) +           */
+/* 1/2 (eps, sigma) is conserved.  Averages run over the 2 or 4 neighbours of */
+/* a point and drop neighbours outside the position's extent (a one-sided     */
+/* value in that dim), the closure compatible with the trapezoid weights of  */
+/* the energy; interface and mirror planes count as outside.  On a free      */
+/* surface (top grid, top_bc = 1) szz is held and e3 at the surface is the   */
+/* value that keeps its rate zero.                                           */
+/* eps (may be NULL): 6 strain accumulators at the stress positions (R = 0),  */
+/* incremented by the strains used, for the energy check.                    */
+/* ------------------------------------------------------------------------- */
+typedef struct {
+    int ex[3];          /* extent end per dim */
+} oext;
+
+static inline int in_ext(const int e[3], int x, int y, int z)
+{
+    return x >= 0 && x <= e[0] && y >= 0 && y <= e[1] && z >= 0 && z <= e[2];
+}
+
+/* strain increments at existing points (velocities read with their halos) */
+static double e1_at(ogrid *g, int x, int y, int z) { return g->coeff[0][0] * (V(&g->f[0], x + 1, y, z) - V(&g->f[0], x, y, z)); }
+static double e2_at(ogrid *g, int x, int y, int z) { return g->coeff[1][0] * (V(&g->f[1], x, y, z) - V(&g->f[1], x, y - 1, z)); }
+static double e3_at(ogrid *g, int x, int y, int z) { return g->coeff[2][0] * (V(&g->f[2], x, y, z) - V(&g->f[2], x, y, z - 1)); }
+static double e4_at(ogrid *g, int x, int y, int z)
+{
+    return g->coeff[2][0] * (V(&g->f[1], x, y, z + 1) - V(&g->f[1], x, y, z)) + g->coeff[1][0] * (V(&g->f[2], x, y + 1, z) - V(&g->f[2], x, y, z));
+}
+static double e5_at(ogrid *g, int x, int y, int z)
+{
+    return g->coeff[2][0] * (V(&g->f[0], x, y, z + 1) - V(&g->f[0], x, y, z)) + g->coeff[0][0] * (V(&g->f[2], x, y, z) - V(&g->f[2], x - 1, y, z));
+}
+static double e6_at(ogrid *g, int x, int y, int z)
+{
+    return g->coeff[1][0] * (V(&g->f[0], x, y + 1, z) - V(&g->f[0], x, y, z)) + g->coeff[0][0] * (V(&g->f[1], x, y, z) - V(&g->f[1], x - 1, y, z));
+}
+
+/* Average of a quantity q over the neighbours (x+dx_k, y+dy_k, z+dz_k) of a
+ * point, two offsets per averaged dim ({a0,a1} in dim d), dropping offsets
+ * whose point lies outside the source extent. */
+typedef double (*qfun)(void *ctx, int x, int y, int z);
+
+static double avg2d(qfun q, void *ctx, const int ext[3], int x, int y, int z, int d0, int a0, int b0, int d1, int a1, int b1)
+{
+    double s = 0.0, wsum0 = 0.0;
+    int off0[2] = {a0, b0}, off1[2] = {a1, b1};
+    /* weights per dim: 1/2 each if both exist, else 1 for the existing one */
+    double acc = 0.0;
+    int ok0[2], ok1[2];
+    for (int i = 0; i < 2; i++) {
+        int p[3] = {x, y, z};
+        p[d0] += off0[i];
+        ok0[i] = (p[d0] >= 0 && p[d0] <= ext[d0]);
+        int q2[3] = {x, y, z};
+        q2[d1] += off1[i];
+        ok1[i] = (q2[d1] >= 0 && q2[d1] <= ext[d1]);
+    }
+    double w0[2], w1[2];
+    for (int i = 0; i < 2; i++) {
+        w0[i] = ok0[i] ? ((ok0[0] && ok0[1]) ? 0.5 : 1.0) : 0.0;
+        w1[i] = ok1[i] ? ((ok1[0] && ok1[1]) ? 0.5 : 1.0) : 0.0;
+    }
+    for (int i = 0; i < 2; i++)
+        for (int j = 0; j < 2; j++) {
+            double w = w0[i] * w1[j];
+            if (w == 0.0) continue;
+            int p[3] = {x, y, z};
+            p[d0] += off0[i];
+            p[d1] += off1[j];
+            acc += w * q(ctx, p[0], p[1], p[2]);
+        }
+    (void)s; (void)wsum0;
+    return acc;
+}
+
+typedef struct {
+    ogrid *g;
+    const ofield *c21;
+    int flag;           /* free surface on this grid */
+    double *e3s;        /* condensed e3 at the surface plane (nx * (ny+1)), or NULL */
+} g21ctx;
+
+static double C21(const g21ctx *c, int k, int x, int y, int z) { return V(&c->c21[k], x, y, z); }
+
+static double q_e4(void *v, int x, int y, int z) { return e4_at(((g21ctx *)v)->g, x, y, z); }
+static double q_e5(void *v, int x, int y, int z) { return e5_at(((g21ctx *)v)->g, x, y, z); }
+static double q_e6(void *v, int x, int y, int z) { return e6_at(((g21ctx *)v)->g, x, y, z); }
+static double q_Q45(void *v, int x, int y, int z) { g21ctx *c = (g21ctx *)v; return C21(c, 16, x, y, z) * e4_at(c->g, x, y, z); }
+static double q_Q46(void *v, int x, int y, int z) { g21ctx *c = (g21ctx *)v; return C21(c, 17, x, y, z) * e4_at(c->g, x, y, z); }
+static double q_Q56(void *v, int x, int y, int z) { g21ctx *c = (g21ctx *)v; return C21(c, 19, x, y, z) * e5_at(c->g, x, y, z); }
+
+/* extents of the four positions on grid g */
+static void exts(const ogrid *g, int eN[3], int e4[3], int e5[3], int e6[3])
+{
+    int nx = g->n[0], ny = g->n[1], nz = g->n[2];
+    eN[0] = nx - 1; eN[1] = ny; eN[2] = nz;
+    e4[0] = nx - 1; e4[1] = ny - 1; e4[2] = nz - 1;
+    e5[0] = nx; e5[1] = ny; e5[2] = nz - 1;
+    e6[0] = nx; e6[1] = ny - 1; e6[2] = nz;
+}
+
+static double Abar4(g21ctx *c, const int e4[3], int x, int y, int z) { return avg2d(q_e4, c, e4, x, y, z, 1, -1, 0, 2, -1, 0); }
+static double Abar5(g21ctx *c, const int e5[3], int x, int y, int z) { return avg2d(q_e5, c, e5, x, y, z, 0, 0, 1, 2, -1, 0); }
+static double Abar6(g21ctx *c, const int e6[3], int x, int y, int z) { return avg2d(q_e6, c, e6, x, y, z, 0, 0, 1, 1, -1, 0); }
+
+/* e3 used at an N point: native, or condensed on the free surface */
+static double e3_used(g21ctx *c, const int e4[3], const int e5[3], const int e6[3], int x, int y, int z)
+{
+    if (c->flag && z == 0) {
+        double num = C21(c, 2, x, y, z) * e1_at(c->g, x, y, z) + C21(c, 4, x, y, z) * e2_at(c->g, x, y, z)
+                   + C21(c, 12, x, y, z) * Abar4(c, e4, x, y, z) + C21(c, 13, x, y, z) * Abar5(c, e5, x, y, z)
+                   + C21(c, 14, x, y, z) * Abar6(c, e6, x, y, z);
+        return -num / C21(c, 5, x, y, z);
+    }
+    return e3_at(c->g, x, y, z);
+}
+
+typedef struct {
+    g21ctx *c;
+    int e4[3], e5[3], e6[3];
+    int j;   /* which P: 4, 5 or 6 */
+} pctx;
+
+static double q_P(void *v, int x, int y, int z)
+{
+    pctx *p = (pctx *)v;
+    g21ctx *c = p->c;
+    /* rows i = 1..3 of column j: C_ij at N slots (j=4: 6,9,12; j=5: 7,10,13; j=6: 8,11,14) */
+    int k0 = 6 + (p->j - 4);
+    double e1 = e1_at(c->g, x, y, z), e2 = e2_at(c->g, x, y, z), e3 = e3_used(c, p->e4, p->e5, p->e6, x, y, z);
+    return C21(c, k0, x, y, z) * e1 + C21(c, k0 + 3, x, y, z) * e2 + C21(c, k0 + 6, x, y, z) * e3;
+}
+
+void o_update_stress21(ogrid *g, const ofield *c21, int top, int bottom, int top_bc, ofield *eps)
+{
+    (void)bottom;
+    ofield *sxx = &g->f[3], *syy = &g->f[4], *szz = &g->f[5], *syz = &g->f[6], *sxz = &g->f[7], *sxy = &g->f[8];
+    const int nx = g->n[0], ny = g->n[1], nz = g->n[2];
+    const int flag = (top && top_bc) ? 1 : 0;
+    int eN[3], e4[3], e5[3], e6[3];
+    exts(g, eN, e4, e5, e6);
+    g21ctx C = {g, c21, flag, NULL};
+    /* all increments from the old velocities, then applied (velocities are not changed here) */
+    const int64_t nN = (int64_t)nx * (ny + 1) * (nz + 1);
+    double *dN = (double *)calloc(3 * nN, sizeof(double));
+    double *eN3 = eps ? (double *)calloc(3 * nN, sizeof(double)) : NULL;
+#pragma omp parallel for
+    for (int z = 0; z <= nz; z++)
+        for (int y = 0; y <= ny; y++)
+            for (int x = 0; x < nx; x++) {
+                double e1 = e1_at(g, x, y, z), e2 = e2_at(g, x, y, z), e3 = e3_used(&C, e4, e5, e6, x, y, z);
+                double a4 = Abar4(&C, e4, x, y, z), a5 = Abar5(&C, e5, x, y, z), a6 = Abar6(&C, e6, x, y, z);
+                int64_t q = ((int64_t)z * (ny + 1) + y) * nx + x;
+                for (int i = 0; i < 3; i++) {
+                    /* row i: C_i1 C_i2 C_i3 then C_i4 C_i5 C_i6 */
+                    static const int rowc[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+                    double d = C21(&C, rowc[i][0], x, y, z) * e1 + C21(&C, rowc[i][1], x, y, z) * e2 + C21(&C, rowc[i][2], x, y, z) * e3
+                             + C21(&C, 6 + 3 * i, x, y, z) * a4 + C21(&C, 7 + 3 * i, x, y, z) * a5 + C21(&C, 8 + 3 * i, x, y, z) * a6;
+                    dN[i * nN + q] = d;
+                }
+                if (eN3) { eN3[q] = e1; eN3[nN + q] = e2; eN3[2 * nN + q] = e3; }
+            }
+    const int64_t n4 = (int64_t)nx * ny * nz, n5 = (int64_t)(nx + 1) * (ny + 1) * nz, n6 = (int64_t)(nx + 1) * ny * (nz + 1);
+    double *d4 = (double *)calloc(n4, sizeof(double)), *d5 = (double *)calloc(n5, sizeof(double)), *d6 = (double *)calloc(n6, sizeof(double));
+#pragma omp parallel for
+    for (int z = 0; z < nz; z++)
+        for (int y = 0; y < ny; y++)
+            for (int x = 0; x < nx; x++) {
+                pctx P = {&C, {e4[0], e4[1], e4[2]}, {e5[0], e5[1], e5[2]}, {e6[0], e6[1], e6[2]}, 4};
+                double d = C21(&C, 15, x, y, z) * e4_at(g, x, y, z)
+                         + C21(&C, 16, x, y, z) * avg2d(q_e5, &C, e5, x, y, z, 0, 0, 1, 1, 0, 1)
+                         + C21(&C, 17, x, y, z) * avg2d(q_e6, &C, e6, x, y, z, 0, 0, 1, 2, 0, 1)
+                         + avg2d(q_P, &P, eN, x, y, z, 1, 0, 1, 2, 0, 1);
+                d4[((int64_t)z * ny + y) * nx + x] = d;
+            }
+#pragma omp parallel for
+    for (int z = 0; z < nz; z++)
+        for (int y = 0; y <= ny; y++)
+            for (int x = 0; x <= nx; x++) {
+                pctx P = {&C, {e4[0], e4[1], e4[2]}, {e5[0], e5[1], e5[2]}, {e6[0], e6[1], e6[2]}, 5};
+                double d = C21(&C, 18, x, y, z) * e5_at(g, x, y, z)
+                         + C21(&C, 19, x, y, z) * avg2d(q_e6, &C, e6, x, y, z, 1, -1, 0, 2, 0, 1)
+                         + avg2d(q_Q45, &C, e4, x, y, z, 0, -1, 0, 1, -1, 0)
+                         + avg2d(q_P, &P, eN, x, y, z, 0, -1, 0, 2, 0, 1);
+                d5[((int64_t)z * (ny + 1) + y) * (nx + 1) + x] = d;
+            }
+#pragma omp parallel for
+    for (int z = 0; z <= nz; z++)
+        for (int y = 0; y < ny; y++)
+            for (int x = 0; x <= nx; x++) {
+                pctx P = {&C, {e4[0], e4[1], e4[2]}, {e5[0], e5[1], e5[2]}, {e6[0], e6[1], e6[2]}, 6};
+                double d = C21(&C, 20, x, y, z) * e6_at(g, x, y, z)
+                         + avg2d(q_Q46, &C, e4, x, y, z, 0, -1, 0, 2, -1, 0)
+                         + avg2d(q_Q56, &C, e5, x, y, z, 1, 0, 1, 2, -1, 0)
+                         + avg2d(q_P, &P, eN, x, y, z, 0, -1, 0, 1, 0, 1);
+                d6[((int64_t)z * ny + y) * (nx + 1) + x] = d;
+            }
+    /* apply */
+    for (int z = 0; z <= nz; z++)
+        for (int y = 0; y <= ny; y++)
+            for (int x = 0; x < nx; x++) {
+                int64_t q = ((int64_t)z * (ny + 1) + y) * nx + x;
+                V(sxx, x, y, z) += dN[q];
+                V(syy, x, y, z) += dN[nN + q];
+                if (!(flag && z == 0)) V(szz, x, y, z) += dN[2 * nN + q];
+                if (eps) {
+                    V(&eps[0], x, y, z) += eN3[q];
+                    V(&eps[1], x, y, z) += eN3[nN + q];
+                    V(&eps[2], x, y, z) += eN3[2 * nN + q];
+                }
+            }
+    for (int z = 0; z < nz; z++)
+        for (int y = 0; y < ny; y++)
+            for (int x = 0; x < nx; x++) {
+                V(syz, x, y, z) += d4[((int64_t)z * ny + y) * nx + x];
+                if (eps) V(&eps[3], x, y, z) += e4_at(g, x, y, z);
+            }
+    for (int z = 0; z < nz; z++)
+        for (int y = 0; y <= ny; y++)
+            for (int x = 0; x <= nx; x++) {
+                V(sxz, x, y, z) += d5[((int64_t)z * (ny + 1) + y) * (nx + 1) + x];
+                if (eps) V(&eps[4], x, y, z) += e5_at(g, x, y, z);
+            }
+    for (int z = 0; z <= nz; z++)
+        for (int y = 0; y < ny; y++)
+            for (int x = 0; x <= nx; x++) {
+                V(sxy, x, y, z) += d6[((int64_t)z * ny + y) * (nx + 1) + x];
+                if (eps) V(&eps[5], x, y, z) += e6_at(g, x, y, z);
+            }
+    /* free-surface odd mirrors of syz, sxz as the reference (update_stress.cpp:260-277) */
+    if (flag) {
+        for (int y = 0; y < ny; y++)
+            for (int x = 0; x < nx; x++) V(syz, x, y, -1) = -V(syz, x, y, 0);
+        for (int y = 1; y < ny; y++)
+            for (int x = 1; x < nx; x++) V(sxz, x, y, -1) = -V(sxz, x, y, 0);
+    }
+    free(dN); free(eN3); free(d4); free(d5); free(d6);
+}
+
+static void gen21_c3(const ofield *c21, int x, int y, int z, double *c13, double *c23, double *c33)
+{
+    *c13 = V(&c21[2], x, y, z);
+    *c23 = V(&c21[4], x, y, z);
+    *c33 = V(&c21[5], x, y, z);
+}
+
+static double gen21_szz_extra(ogrid *g, const ofield *c21, int x, int y, int z)
+{
+    int eN[3], e4[3], e5[3], e6[3];
+    exts(g, eN, e4, e5, e6);
+    g21ctx C = {g, c21, 0, NULL};
+    return V(&c21[12], x, y, z) * Abar4(&C, e4, x, y, z) + V(&c21[13], x, y, z) * Abar5(&C, e5, x, y, z)
+         + V(&c21[14], x, y, z) * Abar6(&C, e6, x, y, z);
 }

@@ -11,7 +11,7 @@ import os
 
 import numpy as np
 
-from ecsg_b200.workloads import SIM_POS, STIFF_POS
+from ecsg_b200.workloads import CIJ21_POS, SIM_POS, STIFF_POS
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 _LIB = None
@@ -40,6 +40,8 @@ def lib():
         L.o_update_vel.argtypes = [P(OGrid), ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.o_update_stress.argtypes = [P(OGrid), ctypes.c_int, ctypes.c_int, ctypes.c_int]
         L.o_ghost_vz_eci.argtypes = [P(OGrid), P(OGrid), ctypes.c_int]
+        L.o_ghost_vz_eci21.argtypes = [P(OGrid), P(OGrid), ctypes.c_int, P(OField), P(OField)]
+        L.o_update_stress21.argtypes = [P(OGrid), P(OField), ctypes.c_int, ctypes.c_int, ctypes.c_int, P(OField)]
         L.o_ghost_syz_eci.argtypes = [P(OGrid), P(OGrid), ctypes.c_int]
         L.o_ghost_sxz_eci.argtypes = [P(OGrid), P(OGrid), ctypes.c_int, c_dp, c_dp, c_dp, c_dp,
                                       ctypes.c_int, c_dp]
@@ -193,6 +195,9 @@ class OracleRun:
                 L["c"] = [np.ascontiguousarray(a) for a in iso_stiffness(m["buoy"], m["s11"], m["s13"])]
             elif case.medium == "ortho9":
                 L["c"] = [np.ascontiguousarray(a.astype(np.float64)) for a in m["c9"]]
+            elif case.medium == "gen21":
+                L["c21"] = [np.ascontiguousarray(a.astype(np.float64)) for a in m["c21"]]
+                L["c"] = [np.ascontiguousarray(a.astype(np.float64)) for a in m["c9"]]
             else:
                 raise ValueError("oracle medium %r" % case.medium)
             coeff = np.zeros((3, 6))
@@ -203,6 +208,9 @@ class OracleRun:
             if energy:
                 L["dens"], L["comp"] = energy_fields(m["buoy"], L["c"], isotropic=(case.medium == "iso"))
                 L["vcopy"] = [np.zeros_like(L["f"][k]) for k in range(3)]
+                if case.medium == "gen21":
+                    # accumulated strains at the stress positions: E_stress = 1/2 sum w eps.sigma
+                    L["eps"] = [np.zeros(field_shape(n, SIM_POS[k], 0)) for k in range(3, 9)]
             self.levels.append(L)
         self._build_structs()
         ng = len(case.grids)
@@ -232,6 +240,10 @@ class OracleRun:
                 for k in range(6):
                     s.coeff[d][k] = L["coeff"][d, k]
             self.structs.append(s)
+            if "c21" in L:
+                L["_c21"] = (OField * 21)(*[_ofield(L["c21"][k], CIJ21_POS[k], 0) for k in range(21)])
+                L["_eps"] = (OField * 6)(*[_ofield(L["eps"][k], SIM_POS[k + 3], 0) for k in range(6)]) \
+                    if "eps" in L else None
             if self.energy_on:
                 L["_dens"] = (OField * 3)(*[_ofield(L["dens"][k], SIM_POS[k], 0) for k in range(3)])
                 L["_comp"] = (OField * 9)(*[_ofield(L["comp"][k], STIFF_POS[k], 0) for k in range(9)])
@@ -246,10 +258,19 @@ class OracleRun:
 
     def update_stress(self, g):
         ng = len(self.levels)
-        lib().o_update_stress(ctypes.byref(self.structs[g]), int(g == 0), int(g == ng - 1), self.case.top_bc)
+        L = self.levels[g]
+        if "c21" in L:
+            lib().o_update_stress21(ctypes.byref(self.structs[g]), L["_c21"], int(g == 0), int(g == ng - 1),
+                                    self.case.top_bc, L["_eps"])
+        else:
+            lib().o_update_stress(ctypes.byref(self.structs[g]), int(g == 0), int(g == ng - 1), self.case.top_bc)
 
     def ghost_vz(self, i):
-        lib().o_ghost_vz_eci(ctypes.byref(self.structs[i - 1]), ctypes.byref(self.structs[i]), self.r)
+        if "c21" in self.levels[i]:
+            lib().o_ghost_vz_eci21(ctypes.byref(self.structs[i - 1]), ctypes.byref(self.structs[i]), self.r,
+                                   self.levels[i - 1]["_c21"], self.levels[i]["_c21"])
+        else:
+            lib().o_ghost_vz_eci(ctypes.byref(self.structs[i - 1]), ctypes.byref(self.structs[i]), self.r)
 
     def ghost_syz(self, i):
         lib().o_ghost_syz_eci(ctypes.byref(self.structs[i - 1]), ctypes.byref(self.structs[i]), self.r)
@@ -272,8 +293,36 @@ class OracleRun:
     def energy(self):
         e = 0.0
         for gi, L in enumerate(self.levels):
-            e += lib().o_energy(ctypes.byref(self.structs[gi]), L["_vcopy"], L["_dens"], L["_comp"], L["_h"])
+            if "c21" in L:
+                e += self._energy21(L)
+            else:
+                e += lib().o_energy(ctypes.byref(self.structs[gi]), L["_vcopy"], L["_dens"], L["_comp"], L["_h"])
         return e
+
+    def _energy21(self, L):
+        """1/2 h^3 [sum w rho v v' + sum w eps.sigma] with the trapezoid weights of
+        TriMulFields (field.cpp:502-515); eps are the accumulated strains."""
+        R = self.R
+
+        def w(shape, pos):
+            m = np.ones(shape)
+            for ax, d in ((0, 2), (1, 1), (2, 0)):
+                if not pos[d]:
+                    sl = [slice(None)] * 3
+                    for idx in (0, shape[ax] - 1):
+                        sl[ax] = idx
+                        m[tuple(sl)] *= 0.5
+            return m
+        tot = 0.0
+        for k in range(3):
+            v = interior(L["f"][k], R)
+            vc = interior(L["vcopy"][k], R)
+            tot += float((w(v.shape, SIM_POS[k]) * L["dens"][k] * v * vc).sum())
+        for k in range(6):
+            sg = interior(L["f"][k + 3], R)
+            tot += float((w(sg.shape, SIM_POS[k + 3]) * L["eps"][k] * sg).sum())
+        h = L["h"]
+        return 0.5 * h[0] * h[1] * h[2] * tot
 
     def residues(self, i, which=7):
         out = np.zeros(9)

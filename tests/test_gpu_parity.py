@@ -248,3 +248,35 @@ def test_invalid_configurations_fail_loudly():
     case.grids[0]["n"] = (case.grids[0]["n"][0] + 1,) + case.grids[0]["n"][1:]
     with pytest.raises(ecsg_b200.EcsgError):
         Simulation(case)
+
+
+@pytest.mark.parametrize("ratio,top_bc,nx2", [(3, 1, 45), (2, 0, 67), (2, 1, 64)])
+def test_vectorized_sweeps_equal_scalar(monkeypatch, ratio, top_bc, nx2):
+    """The float4 FP32 sweeps (stencil_v4.cu) give the same bits as the scalar
+    FP32 sweeps, halos included: random fields through single operators, then a
+    time loop with source, receivers and energy steps."""
+    case = _with_src_rec(random_case(55 + nx2, ratio=ratio, nx2=nx2, ny2=11, nz=(9, 7), top_bc=top_bc))
+    results = []
+    for scalar in ("1", "0"):
+        monkeypatch.setenv("ECSG_SCALAR_STENCILS", scalar)
+        rng = np.random.default_rng(nx2)
+        with Simulation(case, precision="f32", energy=True) as s:
+            from ecsg_b200 import field_shape
+            for g in range(2):
+                for k in range(9):
+                    s.set_field(g, k, rng.standard_normal(field_shape(case.grids[g]["n"], ecsg_b200.SIM_POS[k], 1)))
+            for g in range(2):
+                s.update_vel(g)
+                s.update_stress(g)
+            ops = [s.field(g, k) for g in range(2) for k in range(9)]
+        with Simulation(case, precision="f32", energy=True) as s:
+            r = s.run(30, energy_every=3)
+            loop = [s.field(g, k) for g in range(2) for k in range(9)]
+        results.append((ops, r, loop))
+    (oa, ra, la), (ob, rb, lb) = results
+    for a, b in zip(oa, ob):
+        assert np.array_equal(a, b)
+    assert np.array_equal(ra["rec"], rb["rec"])
+    assert np.array_equal(ra["energy"], rb["energy"], equal_nan=True)
+    for a, b in zip(la, lb):
+        assert np.array_equal(a, b)

@@ -21,7 +21,8 @@ LIB_PATH = os.path.join(HERE, "_lib", "libecsg_b200.so")
 
 ECSG_OK = 0
 ECSG_F32, ECSG_F64 = 0, 1
-ECSG_MEDIUM_ISO, ECSG_MEDIUM_ORTHO9 = 0, 1
+ECSG_MEDIUM_ISO, ECSG_MEDIUM_ORTHO9, ECSG_MEDIUM_GEN21 = 0, 1, 2
+_MEDIUM = {"iso": ECSG_MEDIUM_ISO, "ortho9": ECSG_MEDIUM_ORTHO9, "gen21": ECSG_MEDIUM_GEN21}
 ST_JACOBI_CAP, ST_BARRIER_TIMEOUT, ST_NONFINITE = 1, 2, 4
 
 c_dp = ctypes.POINTER(ctypes.c_double)
@@ -67,6 +68,7 @@ SIGNATURES = [
     ("ecsg_device_count", ctypes.c_int, []),
     ("ecsg_set_medium_iso", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_fp, c_fp, c_fp]),
     ("ecsg_set_medium_ortho9", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_dp, ctypes.POINTER(c_dp)]),
+    ("ecsg_set_medium_cij21", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_dp, ctypes.POINTER(c_dp)]),
     ("ecsg_set_field", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, c_dp]),
     ("ecsg_get_field", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, c_dp]),
     ("ecsg_field_elems", ctypes.c_longlong, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
@@ -141,7 +143,7 @@ class Simulation:
             descs[i].step[:] = [float(x) for x in g["h"]]
         cfg = Config(num_grids=self.ng, radius=case.radius, dt=float(case.dt), imode=case.imode,
                      top_bc=case.top_bc, precision=ECSG_F32 if precision == "f32" else ECSG_F64,
-                     medium=ECSG_MEDIUM_ISO if case.medium == "iso" else ECSG_MEDIUM_ORTHO9,
+                     medium=_MEDIUM[case.medium],
                      energy=1 if energy else 0, jacobi_max_iter=jacobi_max_iter, device=device,
                      mirror_fix=1 if getattr(case, "mirror_fix", False) else 0)
         h = ctypes.c_void_p()
@@ -157,10 +159,12 @@ class Simulation:
                 self._ck(L.ecsg_set_medium_iso(h, gi, b.ctypes.data_as(c_fp), s11.ctypes.data_as(c_fp),
                                                s13.ctypes.data_as(c_fp)))
             else:
+                key, nslot, fn = (("c21", 21, L.ecsg_set_medium_cij21) if case.medium == "gen21"
+                                  else ("c9", 9, L.ecsg_set_medium_ortho9))
                 b = np.ascontiguousarray(m["buoy"], dtype=np.float64)
-                cs = [np.ascontiguousarray(a, dtype=np.float64) for a in m["c9"]]
-                arr = (c_dp * 9)(*[a.ctypes.data_as(c_dp) for a in cs])
-                self._ck(L.ecsg_set_medium_ortho9(h, gi, b.ctypes.data_as(c_dp), arr))
+                cs = [np.ascontiguousarray(a, dtype=np.float64) for a in m[key]]
+                arr = (c_dp * nslot)(*[a.ctypes.data_as(c_dp) for a in cs])
+                self._ck(fn(h, gi, b.ctypes.data_as(c_dp), arr))
         self.src = None
         if case.src is not None:
             loc = self.locate(case.src["xyz"])

@@ -23,6 +23,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = {
     "stencil.cu": [],
     "stencil_v4.cu": [],
+    "stress21.cu": ["-fmad=false"],
     "interface.cu": ["-fmad=false"],
     "diag.cu": ["-fmad=false"],
     "api.cu": [],

@@ -25,6 +25,9 @@ cudaError_t launch_stress(const GridDev<T> &, int, int, int, int, cudaStream_t);
 // stencil_v4.cu (FP32 production sweeps)
 cudaError_t launch_vel_v4(const GridDev<float> &, int, int, int, float *const[3], int, cudaStream_t);
 cudaError_t launch_stress_v4(const GridDev<float> &, int, int, int, int, cudaStream_t);
+// stress21.cu (21-Cij media)
+template <typename T>
+cudaError_t launch_stress21(const GridDev<T> &, int, int, T *const[6], int, cudaStream_t);
 // interface.cu
 template <typename T>
 cudaError_t launch_ghost_vz(const GridDev<T> &, const GridDev<T> &, int, int, double *, cudaStream_t);
@@ -38,8 +41,8 @@ template <typename T>
 cudaError_t launch_sxz_solve(const GridDev<T> &, const GridDev<T> &, int, const SxzWork &, int, cudaStream_t);
 // diag.cu
 template <typename T>
-cudaError_t launch_energy(const GridDev<T> &, int, T *const[3], double *, int, double, double, double, double *,
-                          const int *, const int *, int, int *, cudaStream_t);
+cudaError_t launch_energy(const GridDev<T> &, int, T *const[3], T *const[6], double *, int, double, double, double,
+                          double *, const int *, const int *, int, int *, cudaStream_t);
 template <typename T>
 cudaError_t launch_residue(const GridDev<T> &, const GridDev<T> &, int, double, double *, int, double *, cudaStream_t);
 template <typename T>
@@ -60,6 +63,10 @@ static const int kPos[9][3] = {{0, 0, 0}, {1, 1, 0}, {1, 0, 1}, {1, 0, 0}, {1, 0
                                {1, 0, 0}, {1, 1, 1}, {0, 0, 1}, {0, 1, 0}};
 static const int kStiffPos[9][3] = {{1, 0, 0}, {1, 0, 0}, {1, 0, 0}, {1, 0, 0}, {1, 0, 0},
                                     {1, 0, 0}, {1, 1, 1}, {0, 0, 1}, {0, 1, 0}};
+// 21-Cij slots: 0..14 at the normal-stress position, 15..17 syz, 18..19 sxz, 20 sxy
+static const int kCij21Pos[21][3] = {{1, 0, 0}, {1, 0, 0}, {1, 0, 0}, {1, 0, 0}, {1, 0, 0}, {1, 0, 0}, {1, 0, 0},
+                                     {1, 0, 0}, {1, 0, 0}, {1, 0, 0}, {1, 0, 0}, {1, 0, 0}, {1, 0, 0}, {1, 0, 0},
+                                     {1, 0, 0}, {1, 1, 1}, {1, 1, 1}, {1, 1, 1}, {0, 0, 1}, {0, 0, 1}, {0, 1, 0}};
 
 struct Iface {
     int r = 2;
@@ -79,9 +86,10 @@ struct ecsg_sim {
     double h[kMaxGrids][3];
     void *f[kMaxGrids][9] = {};
     void *b[kMaxGrids] = {};
-    void *c[kMaxGrids][9] = {};
+    void *c[kMaxGrids][21] = {};
     int nc = 5;
     void *vc[kMaxGrids][3] = {};
+    void *eps[kMaxGrids][6] = {};   // 21-Cij media with energy: accumulated strains at the stress positions
     bool medium_set[kMaxGrids] = {};
     Iface itf[kMaxGrids];
     // shared device scalars: [0] status, [1] step clock, [2] last sxz sweeps, [3] first step of the run
@@ -198,7 +206,7 @@ int ecsg_create(const ecsg_grid_desc *grids, const ecsg_config *cfg, ecsg_sim **
     if (!(cfg->dt > 0)) { fail(s, ECSG_ERR_INVALID, "dt must be positive"); return bail(ECSG_ERR_INVALID); }
     if (cfg->imode != ECSG_MODE_ECI) { fail(s, ECSG_ERR_INVALID, "imode %d not supported (energy-conserving mode 1 only)", cfg->imode); return bail(ECSG_ERR_INVALID); }
     if (cfg->precision != ECSG_F32 && cfg->precision != ECSG_F64) { fail(s, ECSG_ERR_INVALID, "precision"); return bail(ECSG_ERR_INVALID); }
-    if (cfg->medium != ECSG_MEDIUM_ISO && cfg->medium != ECSG_MEDIUM_ORTHO9) { fail(s, ECSG_ERR_INVALID, "medium"); return bail(ECSG_ERR_INVALID); }
+    if (cfg->medium != ECSG_MEDIUM_ISO && cfg->medium != ECSG_MEDIUM_ORTHO9 && cfg->medium != ECSG_MEDIUM_GEN21) { fail(s, ECSG_ERR_INVALID, "medium"); return bail(ECSG_ERR_INVALID); }
     s->ng = cfg->num_grids;
     s->R = cfg->radius;
     s->dt = cfg->dt;
@@ -215,7 +223,7 @@ int ecsg_create(const ecsg_grid_desc *grids, const ecsg_config *cfg, ecsg_sim **
         s->scalar_stencils = env && env[0] == '1';
     }
     s->tsize = s->prec == ECSG_F32 ? 4 : 8;
-    s->nc = s->medium == ECSG_MEDIUM_ISO ? 5 : 9;
+    s->nc = s->medium == ECSG_MEDIUM_ISO ? 5 : (s->medium == ECSG_MEDIUM_ORTHO9 ? 9 : 21);
     if (cudaSetDevice(s->device) != cudaSuccess) { fail(s, ECSG_ERR_NO_DEVICE, "cudaSetDevice(%d) failed", s->device); return bail(ECSG_ERR_NO_DEVICE); }
     cudaDeviceProp prop;
     if (cudaGetDeviceProperties(&prop, s->device) != cudaSuccess) return bail(fail(s, ECSG_ERR_CUDA, "cudaGetDeviceProperties"));
@@ -252,6 +260,9 @@ int ecsg_create(const ecsg_grid_desc *grids, const ecsg_config *cfg, ecsg_sim **
         if (s->energy)
             for (int k = 0; k < 3; k++)
                 if ((rc = dmalloc(s, &s->vc[g][k], fb))) return bail(rc);
+        if (s->energy && s->medium == ECSG_MEDIUM_GEN21)
+            for (int k = 0; k < 6; k++)
+                if ((rc = dmalloc(s, &s->eps[g][k], fb))) return bail(rc);
     }
     s->red_blocks = 4 * s->sms;
     if ((rc = dmalloc(s, (void **)&s->partial, sizeof(double) * 12 * (size_t)s->red_blocks))) return bail(rc);
@@ -284,8 +295,9 @@ int ecsg_destroy(ecsg_sim *s)
     for (int g = 0; g < kMaxGrids; g++) {
         for (int k = 0; k < 9; k++) cudaFree(s->f[g][k]);
         cudaFree(s->b[g]);
-        for (int k = 0; k < 9; k++) cudaFree(s->c[g][k]);
+        for (int k = 0; k < 21; k++) cudaFree(s->c[g][k]);
         for (int k = 0; k < 3; k++) cudaFree(s->vc[g][k]);
+        for (int k = 0; k < 6; k++) cudaFree(s->eps[g][k]);
         Iface &I = s->itf[g];
         cudaFree(I.A); cudaFree(I.B); cudaFree(I.X0); cudaFree(I.X1); cudaFree(I.partial); cudaFree(I.vzc);
     }
@@ -347,7 +359,7 @@ int ecsg_set_medium_iso(ecsg_sim *s, int g, const float *buoy, const float *s11,
 }
 
 template <typename T>
-static int set_ortho(ecsg_sim *s, int g, const double *buoy, const double *const c[9])
+static int set_stiff(ecsg_sim *s, int g, const double *buoy, const double *const *c, int nc, const int (*pos)[3])
 {
     const Geo &G = s->geo[g];
     const size_t nn = (size_t)(G.nx + 1) * (G.ny + 1) * (G.nz + 1);
@@ -355,8 +367,8 @@ static int set_ortho(ecsg_sim *s, int g, const double *buoy, const double *const
     CK(cudaMalloc(&stage, nn * sizeof(double)));
     CK(cudaMemcpyAsync(stage, buoy, nn * sizeof(double), cudaMemcpyHostToDevice, s->st));
     CK((launch_pack<T, double>((T *)s->b[g], G, stage, G.nx + 1, G.ny + 1, G.nz + 1, 0, s->st)));
-    for (int k = 0; k < 9; k++) {
-        const int l0 = G.nx + 1 - kStiffPos[k][0], l1 = G.ny + 1 - kStiffPos[k][1], l2 = G.nz + 1 - kStiffPos[k][2];
+    for (int k = 0; k < nc; k++) {
+        const int l0 = G.nx + 1 - pos[k][0], l1 = G.ny + 1 - pos[k][1], l2 = G.nz + 1 - pos[k][2];
         CK(cudaMemcpyAsync(stage, c[k], (size_t)l0 * l1 * l2 * sizeof(double), cudaMemcpyHostToDevice, s->st));
         CK((launch_pack<T, double>((T *)s->c[g][k], G, stage, l0, l1, l2, 0, s->st)));
         CK(cudaStreamSynchronize(s->st));
@@ -368,11 +380,26 @@ static int set_ortho(ecsg_sim *s, int g, const double *buoy, const double *const
 int ecsg_set_medium_ortho9(ecsg_sim *s, int g, const double *buoy, const double *const c[9])
 {
     if (!s || g < 0 || g >= s->ng || !buoy || !c) return fail(s, ECSG_ERR_INVALID, "set_medium_ortho9: bad arguments");
-    if (s->medium != ECSG_MEDIUM_ORTHO9) return fail(s, ECSG_ERR_STATE, "simulation was created for an isotropic medium");
+    if (s->medium != ECSG_MEDIUM_ORTHO9) return fail(s, ECSG_ERR_STATE, "simulation was not created for an orthorhombic medium");
     for (int k = 0; k < 9; k++)
         if (!c[k]) return fail(s, ECSG_ERR_INVALID, "set_medium_ortho9: c[%d] is null", k);
     CK(cudaSetDevice(s->device));
-    int rc = s->prec == ECSG_F32 ? set_ortho<float>(s, g, buoy, c) : set_ortho<double>(s, g, buoy, c);
+    int rc = s->prec == ECSG_F32 ? set_stiff<float>(s, g, buoy, c, 9, kStiffPos) : set_stiff<double>(s, g, buoy, c, 9, kStiffPos);
+    if (rc) return rc;
+    s->medium_set[g] = true;
+    if (g > 0) s->itf[g].A_ready = false;
+    if (g + 1 < s->ng) s->itf[g + 1].A_ready = false;
+    return ECSG_OK;
+}
+
+int ecsg_set_medium_cij21(ecsg_sim *s, int g, const double *buoy, const double *const c[21])
+{
+    if (!s || g < 0 || g >= s->ng || !buoy || !c) return fail(s, ECSG_ERR_INVALID, "set_medium_cij21: bad arguments");
+    if (s->medium != ECSG_MEDIUM_GEN21) return fail(s, ECSG_ERR_STATE, "simulation was not created for a 21-Cij medium");
+    for (int k = 0; k < 21; k++)
+        if (!c[k]) return fail(s, ECSG_ERR_INVALID, "set_medium_cij21: c[%d] is null", k);
+    CK(cudaSetDevice(s->device));
+    int rc = s->prec == ECSG_F32 ? set_stiff<float>(s, g, buoy, c, 21, kCij21Pos) : set_stiff<double>(s, g, buoy, c, 21, kCij21Pos);
     if (rc) return rc;
     s->medium_set[g] = true;
     if (g > 0) s->itf[g].A_ready = false;
@@ -464,10 +491,21 @@ static int vel_op(ecsg_sim *s, int g, bool with_copy)
     return rc ? rc : vel_mirror_op<T>(s, g);
 }
 
+static int med_kind(const ecsg_sim *s)
+{
+    return s->medium == ECSG_MEDIUM_ISO ? MED_ISO5 : (s->medium == ECSG_MEDIUM_ORTHO9 ? MED_ORTHO9 : MED_GEN21);
+}
+
 template <typename T>
 static int stress_op(ecsg_sim *s, int g)
 {
-    const int med = s->medium == ECSG_MEDIUM_ISO ? MED_ISO5 : MED_ORTHO9;
+    const int med = med_kind(s);
+    if (med == MED_GEN21) {
+        T *eps[6];
+        for (int k = 0; k < 6; k++) eps[k] = (T *)s->eps[g][k];
+        CK(launch_stress21<T>(dev<T>(s, g), g == 0, s->top_bc, eps, s->sms, s->st));
+        return ECSG_OK;
+    }
     if constexpr (std::is_same<T, float>::value) {
         if (!s->scalar_stencils) {
             CK(launch_stress_v4(dev<float>(s, g), med, g == 0, s->top_bc, s->sms, s->st));
@@ -481,7 +519,7 @@ static int stress_op(ecsg_sim *s, int g)
 template <typename T>
 static int vz_op(ecsg_sim *s, int i)
 {
-    CK(launch_ghost_vz<T>(dev<T>(s, i - 1), dev<T>(s, i), s->medium == ECSG_MEDIUM_ISO ? MED_ISO5 : MED_ORTHO9, s->itf[i].r,
+    CK(launch_ghost_vz<T>(dev<T>(s, i - 1), dev<T>(s, i), med_kind(s), s->itf[i].r,
                           s->itf[i].vzc, s->st));
     return ECSG_OK;
 }
@@ -625,7 +663,9 @@ static int energy_op(ecsg_sim *s, double *out, const int *step, const int *step0
 {
     for (int g = 0; g < s->ng; g++) {
         T *vc[3] = {(T *)s->vc[g][0], (T *)s->vc[g][1], (T *)s->vc[g][2]};
-        CK(launch_energy<T>(dev<T>(s, g), s->medium == ECSG_MEDIUM_ISO ? MED_ISO5 : MED_ORTHO9, vc, s->partial,
+        T *eps[6];
+        for (int k = 0; k < 6; k++) eps[k] = (T *)s->eps[g][k];
+        CK(launch_energy<T>(dev<T>(s, g), med_kind(s), vc, eps, s->partial,
                             s->red_blocks, s->h[g][0], s->h[g][1], s->h[g][2], out, step, step0, g == 0, s->ints, s->st));
     }
     return ECSG_OK;

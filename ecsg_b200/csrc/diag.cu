@@ -36,8 +36,13 @@ __device__ __forceinline__ void block_sums(double (&v)[N], double *partial, int 
 // ReshapeField, field.cpp:465-472).  12 term partials per CTA.
 // ---------------------------------------------------------------------------
 template <typename T>
+struct Eps6 {
+    const T *e[6];
+};
+
+template <typename T>
 __global__ void __launch_bounds__(RED_THREADS) energy_kernel(GridDev<T> G, int medium, const T *vc0, const T *vc1,
-                                                            const T *vc2, double *partial)
+                                                            const T *vc2, Eps6<T> eps, double *partial)
 {
     const Geo &g = G.g;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
@@ -67,6 +72,19 @@ __global__ void __launch_bounds__(RED_THREADS) energy_kernel(GridDev<T> G, int m
             const double b001 = (double)G.b[p + sz], b100 = (double)G.b[p + 1], b101 = (double)G.b[p + sz + 1];
             const double rb = (b000 + b001 + b000 + b001 + b100 + b101 + b100 + b101) / 8;
             acc[2] += my * (1.0 / rb) * (double)G.f[VZ][p] * (double)vc2[p];
+        }
+        if (medium == MED_GEN21) {
+            // 21-Cij media: potential energy (eps, sigma) from the accumulated
+            // strains, terms 3..8 in stress order, trapezoid weights per position
+            if (xs) {
+                const double w = mz * my;
+#pragma unroll
+                for (int k = 0; k < 3; k++) acc[3 + k] += w * (double)eps.e[k][p] * (double)G.f[SXX + k][p];
+            }
+            if (xs && ys && zs) acc[6] += (double)eps.e[3][p] * (double)G.f[SYZ][p];
+            if (zs) acc[7] += my * mx * (double)eps.e[4][p] * (double)G.f[SXZ][p];
+            if (ys) acc[8] += mz * mx * (double)eps.e[5][p] * (double)G.f[SXY][p];
+            continue;
         }
         if (xs) {         // normal stresses at (1,0,0)
             double k11, k22, k33, k23, k13, k12;
@@ -121,7 +139,7 @@ __global__ void __launch_bounds__(RED_THREADS) energy_kernel(GridDev<T> G, int m
 // The destination is out[0], or out[*step - 1 - *step0] when the device step
 // clock is given (inside a run, after the clock advanced for this step).
 __global__ void energy_finalize_kernel(const double *partial, int nblocks, double h0, double h1, double h2,
-                                       double *out, const int *step, const int *step0, int first, int *status)
+                                       double *out, const int *step, const int *step0, int first, int *status, int gen21)
 {
     __shared__ double term[12];
     if (threadIdx.x < 12) {
@@ -132,8 +150,9 @@ __global__ void energy_finalize_kernel(const double *partial, int nblocks, doubl
     __syncthreads();
     if (threadIdx.x == 0) {
         double res = 0.0;
+        // the inverse-stiffness form counts the symmetric cross terms twice
         for (int k = 0; k < 6; k++) res += term[k];
-        for (int k = 6; k < 12; k++) res += 2 * term[k];
+        for (int k = 6; k < 12; k++) res += gen21 ? term[k] : 2 * term[k];
         res *= 0.5 * h2 * h1 * h0;
         double *dst = step ? out + (*step - 1 - *step0) : out;
         const double e = first ? res : *dst + res;
@@ -306,12 +325,16 @@ __global__ void iso_medium_kernel(Geo g, const double *s11, const double *s13, d
 // Host launchers
 // ---------------------------------------------------------------------------
 template <typename T>
-cudaError_t launch_energy(const GridDev<T> &G, int medium, T *const vc[3], double *partial, int nblocks, double h0,
-                          double h1, double h2, double *out, const int *step, const int *step0, int first, int *status,
-                          cudaStream_t st)
+cudaError_t launch_energy(const GridDev<T> &G, int medium, T *const vc[3], T *const eps[6], double *partial, int nblocks,
+                          double h0, double h1, double h2, double *out, const int *step, const int *step0, int first,
+                          int *status, cudaStream_t st)
 {
-    energy_kernel<T><<<nblocks, RED_THREADS, 0, st>>>(G, medium, vc[0], vc[1], vc[2], partial);
-    energy_finalize_kernel<<<1, 32, 0, st>>>(partial, nblocks, h0, h1, h2, out, step, step0, first, status);
+    Eps6<T> E;
+    for (int k = 0; k < 6; k++) E.e[k] = eps ? eps[k] : nullptr;
+    if (medium == MED_GEN21 && !E.e[0]) return cudaErrorInvalidValue;
+    energy_kernel<T><<<nblocks, RED_THREADS, 0, st>>>(G, medium, vc[0], vc[1], vc[2], E, partial);
+    energy_finalize_kernel<<<1, 32, 0, st>>>(partial, nblocks, h0, h1, h2, out, step, step0, first, status,
+                                             medium == MED_GEN21);
     return cudaGetLastError();
 }
 
@@ -373,8 +396,9 @@ cudaError_t launch_iso_medium(const Geo &g, const double *s11, const double *s13
 }
 
 #define INST(T)                                                                                               \
-    template cudaError_t launch_energy<T>(const GridDev<T> &, int, T *const[3], double *, int, double, double,   \
-                                          double, double *, const int *, const int *, int, int *, cudaStream_t); \
+    template cudaError_t launch_energy<T>(const GridDev<T> &, int, T *const[3], T *const[6], double *, int,      \
+                                          double, double, double, double *, const int *, const int *, int, int *, \
+                                          cudaStream_t);                                                       \
     template cudaError_t launch_residue<T>(const GridDev<T> &, const GridDev<T> &, int, double, double *, int,   \
                                            double *, cudaStream_t);                                            \
     template cudaError_t launch_avgabs<T>(const GridDev<T> &, int, const int[3], double *, int, double *,        \

@@ -54,6 +54,7 @@ enum { VX = 0, VY, VZ, SXX, SYY, SZZ, SYZ, SXZ, SXY };
 
 // Stiffness slots.  ISO5 uses slots 0..4 = c11, c13, c44, c55, c66.
 // ORTHO9 uses slots 0..8 = c11 c22 c33 c23 c13 c12 c44 c55 c66 (update_stress.cpp:17-25).
+// GEN21 uses slots 0..20 as documented in stress21.cu.
 template <typename T>
 struct GridDev {
     Geo g;

@@ -22,6 +22,7 @@
 //        limit and set a status bit instead of waiting forever; the sweep count
 //        is capped and a capped solve sets ST_JACOBI_CAP.
 #include "ecsg_device.cuh"
+#include "gen21_device.cuh"
 #include <cstdio>
 
 namespace ecsg {
@@ -46,6 +47,10 @@ __device__ __forceinline__ void normal_c(const GridDev<T> &G, int medium, int p,
     if (medium == MED_ISO5) {
         c33 = (double)G.c[0][p];
         c13 = c23 = (double)G.c[1][p];
+    } else if (medium == MED_GEN21) {
+        c13 = (double)G.c[2][p];
+        c23 = (double)G.c[4][p];
+        c33 = (double)G.c[5][p];
     } else {
         c33 = (double)G.c[2][p];
         c23 = (double)G.c[3][p];
@@ -78,9 +83,10 @@ __global__ void ghost_vz_assemble_kernel(GridDev<T> F, GridDev<T> C, int medium,
     const int pc = C.g.idx(j0, j1, 0);
     double c13, c23, c33;
     normal_c(C, medium, pc, c13, c23, c33);
-    const double pred = (double)szz2[pc] + c13 * k2x * ((double)vx2[C.g.idx(j0 + 1, j1, 0)] - (double)vx2[pc])
-                      + c23 * k2y * ((double)vy2[pc] - (double)vy2[C.g.idx(j0, j1 - 1, 0)])
-                      + c33 * k2z * (double)vz2[pc];
+    double pred = (double)szz2[pc] + c13 * k2x * ((double)vx2[C.g.idx(j0 + 1, j1, 0)] - (double)vx2[pc])
+                + c23 * k2y * ((double)vy2[pc] - (double)vy2[C.g.idx(j0, j1 - 1, 0)])
+                + c33 * k2z * (double)vz2[pc];
+    if (medium == MED_GEN21) pred += gen21_szz_extra(C, j0, j1, 0);
     double dg = r3 * k2z * c33, lo = 0.0, up = 0.0, fsum = 0.0;
     for (int i0 = r * j0; i0 < r * j0 + r; i0++) {
         for (int i1 = r * (j1 - 1) + 1; i1 <= r * (j1 + 1) - 1; i1++) {
@@ -93,9 +99,10 @@ __global__ void ghost_vz_assemble_kernel(GridDev<T> F, GridDev<T> C, int medium,
             const int jl = i1 / r, ju = jl + 1;
             double pv0 = pw_node_all(i1, jl, r) * (double)vz2[C.g.idx(j0, jl, 0)];
             if (ju <= ny2) pv0 += pw_node_all(i1, ju, r) * (double)vz2[C.g.idx(j0, ju, 0)];
-            const double pf_ = (double)szz1[pf] + f13 * k1x * ((double)vx1[pf + 1] - (double)vx1[pf])
-                             + f23 * k1y * ((double)vy1[pf] - (double)vy1[pf - F.g.px])
-                             + cz * (pv0 - 2.0 * (double)vz1[pf - F.g.px * F.g.py]);
+            double pf_ = (double)szz1[pf] + f13 * k1x * ((double)vx1[pf + 1] - (double)vx1[pf])
+                       + f23 * k1y * ((double)vy1[pf] - (double)vy1[pf - F.g.px])
+                       + cz * (pv0 - 2.0 * (double)vz1[pf - F.g.px * F.g.py]);
+            if (medium == MED_GEN21) pf_ += gen21_szz_extra(F, i0, i1, nz1);
             dg += rr * w * w * cz;
             lo += rr * w * wl * cz;
             up += rr * w * wu * cz;

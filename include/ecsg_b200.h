@@ -42,7 +42,7 @@ enum {
 };
 
 enum { ECSG_F32 = 0, ECSG_F64 = 1 };                     /* field precision */
-enum { ECSG_MEDIUM_ISO = 0, ECSG_MEDIUM_ORTHO9 = 1 };    /* stiffness form */
+enum { ECSG_MEDIUM_ISO = 0, ECSG_MEDIUM_ORTHO9 = 1, ECSG_MEDIUM_GEN21 = 2 };   /* stiffness form */
 enum { ECSG_MODE_II = 0, ECSG_MODE_ECI = 1 };            /* interface mode (main.cpp:54) */
 
 /* Device status bits (ecsg_get_status). */
@@ -64,7 +64,7 @@ typedef struct ecsg_config {
     int imode;            /* ECSG_MODE_ECI (1) */
     int top_bc;           /* 0 rigid, 1 free surface */
     int precision;        /* ECSG_F32 or ECSG_F64 */
-    int medium;           /* ECSG_MEDIUM_ISO or ECSG_MEDIUM_ORTHO9 */
+    int medium;           /* ECSG_MEDIUM_ISO, ECSG_MEDIUM_ORTHO9 or ECSG_MEDIUM_GEN21 */
     int energy;           /* allocate velocity copies for the energy (check_energy) */
     int jacobi_max_iter;  /* cap on sxz Jacobi sweeps per solve; <= 0 selects 10000 */
     int device;           /* CUDA device ordinal */
@@ -97,6 +97,17 @@ int ecsg_set_medium_iso(ecsg_sim *sim, int g, const float *buoy, const float *s1
  * at 111, c55 at 001, c66 at 010).  As in the reference, the shear entries are
  * the stored 2*mu-type moduli that the update multiplies by 0.5. */
 int ecsg_set_medium_ortho9(ecsg_sim *sim, int g, const double *buoy, const double *const c[9]);
+/* General anisotropic medium (21 Cij, Voigt, engineering shear strains; no
+ * counterpart in the reference, which reads isotropic media only).  c[k] in
+ * Field layout with R = 0 at the slot's position: slots 0..14 = C11 C12 C13
+ * C22 C23 C33 C14 C15 C16 C24 C25 C26 C34 C35 C36 at the normal-stress
+ * position (1,0,0); 15..17 = C44 C45 C46 at the syz position (1,1,1); 18..19
+ * = C55 C56 at the sxz position (0,0,1); 20 = C66 at the sxy position (0,1,0).
+ * With the 12 off-block slots zero this is the orthorhombic update with
+ * C44 = c44/2 etc. of ecsg_set_medium_ortho9.  With cfg.energy the stress
+ * update also accumulates strains so that ecsg_energy can return
+ * 1/2 (rho v, v') + 1/2 (eps, sigma). */
+int ecsg_set_medium_cij21(ecsg_sim *sim, int g, const double *buoy, const double *const c[21]);
 
 /* Field component k of grid g in Field layout (radius R of ecsg_config), in
  * double (Field::GetPtr1 of the reference, field.hpp:84-85). */

@@ -1,0 +1,161 @@
+"""21-Cij media on the device (ecsg_set_medium_cij21) against the oracle's
+o_update_stress21 and its energy.
+
+The device stress update follows the oracle's operation order, so the FP64
+instantiation must match it exactly; interface solves and reductions differ
+in summation order only (<= 1e-12 relative).  FP32: one operator <= 4e-6
+relative to the field scale (21 products per normal stress instead of 3),
+traces within 1e-5 rel-L2 of the FP64 oracle.
+"""
+import copy
+
+import numpy as np
+import pytest
+
+from ecsg_b200 import Simulation
+from ecsg_b200.workloads import ortho9_from_cij21, random_case_gen21, ricker
+from oracle.oracle import OracleRun
+
+pytestmark = pytest.mark.gpu
+
+
+def _randomize(o, s, rng, prec):
+    for g in range(len(o.levels)):
+        for k in range(9):
+            a = rng.standard_normal(o.levels[g]["f"][k].shape)
+            if prec == "f32":
+                a = a.astype(np.float32).astype(np.float64)
+            o.levels[g]["f"][k][...] = a
+            s.set_field(g, k, a)
+
+
+def _err(o, s, comps=range(9)):
+    worst = 0.0
+    for g in range(len(o.levels)):
+        for k in comps:
+            a, b = o.levels[g]["f"][k], s.field(g, k)
+            worst = max(worst, float(np.abs(a - b).max() / max(np.abs(a).max(), 1e-300)))
+    return worst
+
+
+def _with_src_rec(case, nt=60):
+    h, n = case.grids[0]["h"], case.grids[0]["n"]
+    case.src = {"xyz": (n[0] // 2 * h[0], n[1] // 2 * h[1], 2 * h[2]), "trace": ricker(nt, case.dt * 1e-3 * 0.5, 15.0),
+                "scale": 1000.0, "comp": 0}
+    case.rec = np.array([[(n[0] // 2 + 3) * h[0], n[1] // 2 * h[1], 2 * h[2]],
+                         [(n[0] // 3) * h[0], (n[1] // 3) * h[1], (n[2] - 1) * h[2]],
+                         [(n[0] // 2) * h[0], (n[1] // 2) * h[1], (n[2] + 2) * h[2]]], dtype=np.float32)
+    return case
+
+
+# (ratio, top_bc, nz): nz = 20 splits the fine grid's z-march into several chunks
+CASES = [(2, 1, (6, 5)), (2, 0, (6, 5)), (3, 1, (6, 5)), (2, 1, (20, 12))]
+
+
+@pytest.mark.parametrize("ratio,top_bc,nz", CASES)
+def test_stress21_and_vz_f64(ratio, top_bc, nz):
+    case = random_case_gen21(11 + ratio, ratio=ratio, nx2=7, ny2=6, nz=nz, top_bc=top_bc, aniso=0.3)
+    o = OracleRun(case, energy=True)
+    rng = np.random.default_rng(ratio + 10 * top_bc + nz[0])
+    with Simulation(case, precision="f64", energy=True) as s:
+        _randomize(o, s, rng, "f64")
+        for g in range(2):
+            o.update_stress(g)
+            s.update_stress(g)
+        assert _err(o, s) == 0.0
+        # a second update adds onto the strain accumulators of the first
+        _randomize(o, s, rng, "f64")
+        for g in range(2):
+            o.update_stress(g)
+            s.update_stress(g)
+        assert _err(o, s) == 0.0
+        _randomize(o, s, rng, "f64")
+        o.ghost_vz(1)
+        s.ghost_vz(1)
+        assert _err(o, s) < 1e-12
+        o.copy_vel()
+        s.copy_vel()
+        eo, es = o.energy(), s.energy()
+        assert abs(eo - es) <= 1e-12 * abs(eo), (eo, es)
+
+
+@pytest.mark.parametrize("ratio,top_bc,nz", CASES)
+def test_stress21_and_vz_f32(ratio, top_bc, nz):
+    case = random_case_gen21(21 + ratio, ratio=ratio, nx2=7, ny2=6, nz=nz, top_bc=top_bc, aniso=0.3)
+    o = OracleRun(case)
+    rng = np.random.default_rng(100 + ratio + 10 * top_bc + nz[0])
+    with Simulation(case, precision="f32") as s:
+        _randomize(o, s, rng, "f32")
+        for g in range(2):
+            o.update_stress(g)
+            s.update_stress(g)
+        assert _err(o, s) < 4e-6
+        _randomize(o, s, rng, "f32")
+        o.ghost_vz(1)
+        s.ghost_vz(1)
+        assert _err(o, s) < 4e-6
+
+
+def test_off_block_zero_equals_orthorhombic_device_path():
+    case = random_case_gen21(3, ratio=2, nx2=9, ny2=8, nz=(8, 6), top_bc=1)
+    for m in case.media:
+        for k in list(range(6, 15)) + [16, 17, 19]:
+            m["c21"][k] = np.zeros_like(m["c21"][k])
+        m["c9"] = ortho9_from_cij21(m["c21"])
+    case = _with_src_rec(case)
+    c9 = copy.copy(case)
+    c9.medium = "ortho9"
+    outs = []
+    for cs in (case, c9):
+        with Simulation(cs, precision="f64") as s:
+            r = s.run(60, graph=False)
+            outs.append((r["rec"], [s.field(g, k) for g in range(2) for k in range(9)]))
+    assert np.abs(outs[0][0] - outs[1][0]).max() <= 1e-6 * np.abs(outs[1][0]).max()
+    for a, b in zip(outs[0][1], outs[1][1]):
+        assert np.abs(a - b).max() <= 1e-12 * max(np.abs(b).max(), 1e-300)
+
+
+@pytest.mark.parametrize("ratio", [2, 3])
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_time_loop_vs_oracle(ratio, prec):
+    case = _with_src_rec(random_case_gen21(40 + ratio, ratio=ratio, nx2=9, ny2=8, nz=(8, 6), aniso=0.3))
+    n = 80
+    o = OracleRun(case, energy=True)
+    ref = o.run(n)
+    with Simulation(case, precision=prec, energy=True) as s:
+        out = s.run(n, energy_every=1, graph=False)
+    erel = np.abs(out["energy"] - ref["energy"]) / np.abs(ref["energy"]).max()
+    if prec == "f64":
+        ref32 = ref["rec"].astype(np.float32).astype(np.float64)
+        rel32 = np.linalg.norm(out["rec"] - ref32, axis=1) / np.linalg.norm(ref32, axis=1)
+        assert rel32.max() < 1e-7 and erel.max() < 1e-10, (rel32, erel.max())
+    else:
+        rel = np.linalg.norm(out["rec"] - ref["rec"], axis=1) / np.linalg.norm(ref["rec"], axis=1)
+        assert rel.max() < 1e-5 and erel.max() < 1e-5, (rel, erel.max())
+
+
+def test_graph_replay_is_bitwise_equal():
+    case = _with_src_rec(random_case_gen21(50, ratio=3, nx2=9, ny2=8, nz=(8, 6), aniso=0.3))
+    outs = []
+    for graph in (False, True):
+        with Simulation(case, precision="f32", energy=True) as s:
+            r = s.run(40, energy_every=5, graph=graph)
+            outs.append((r, [s.field(g, k) for g in range(2) for k in range(9)]))
+    (ra, fa), (rb, fb) = outs
+    assert np.array_equal(ra["rec"], rb["rec"])
+    assert np.array_equal(ra["energy"], rb["energy"], equal_nan=True)
+    for a, b in zip(fa, fb):
+        assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("prec,tol", [("f64", 1e-11), ("f32", 1e-5)])
+@pytest.mark.parametrize("ratio,top_bc", [(2, 1), (3, 1), (3, 0)])
+def test_energy_conserved_after_source(ratio, top_bc, prec, tol):
+    case = random_case_gen21(60 + ratio, ratio=ratio, nx2=12, ny2=10, nz=(12, 8), top_bc=top_bc, aniso=0.3)
+    case = _with_src_rec(case, nt=60)
+    case.mirror_fix = True
+    with Simulation(case, precision=prec, energy=True) as s:
+        out = s.run(800, energy_every=10)
+    e = out["energy"][100::10]   # the source acts during the first 60 steps
+    drift = (e.max() - e.min()) / np.abs(e).mean()
+    assert np.isfinite(e).all() and drift < tol, drift

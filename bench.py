@@ -4,9 +4,11 @@
 
 Workload (one step = one pass of main.cpp's time loop over the whole composite):
 the three-grid ratio-3 composite 1081x1081x121 @ 5 m / 361x361x161 @ 15 m /
-121x121x101 @ 45 m (163,856,303 points), FP32 fields, free surface, Ricker vz
-source at the surface centre, 1081 vz surface receivers, energy every 100
-steps.  Inputs are seeded synthetic media (no dataset exists for this path).
+121x121x101 @ 45 m (163,856,303 points), FP32 fields, tilted-VTI medium with
+all 21 Cij (Thomsen eps 0.10, delta 0.05, gamma 0.08, seeded smooth dip <= 30
+deg and azimuth), free surface, Ricker vz source at the surface centre, 1081 vz
+surface receivers, energy every 100 steps.  Inputs are seeded synthetic media
+(no dataset exists for this path).  --medium iso runs the isotropic twin.
 N > 1 runs N independent replicas (one per GPU, launched by torchrun): the
 path has no exchange step, so there is no collective on the data path.
 
@@ -30,9 +32,10 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-BYTES_PER_CELL = {"iso": 132, "ortho9": 148, "gen21": 196}   # compulsory FP32 traffic per cell-update
-STRESS_BYTES = {"iso": 80, "ortho9": 96, "gen21": 144}       # stress kernel: 3v + 6 sigma (rmw) + N_C words
-VEL_BYTES = 52                                               # velocity kernel: 6 sigma + 3 v (rmw) + buoyancy
+BYTES_PER_CELL = {"iso": 132, "ortho9": 148, "tti": 196}    # compulsory FP32 traffic per cell-update
+STRESS_BYTES = {"iso": 80, "ortho9": 96, "tti": 144}        # stress kernel: 3v + 6 sigma (rmw) + N_C words
+VEL_BYTES = 52                                              # velocity kernel: 6 sigma + 3 v (rmw) + buoyancy
+EPS_BYTES = 48                                              # 21-Cij energy: 6 strain accumulators (rmw)
 
 
 def measured_peak():
@@ -148,6 +151,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--small", action="store_true", help="1/27-volume case (profiling)")
     ap.add_argument("--energy-every", type=int, default=100)
+    ap.add_argument("--medium", default="tti", choices=["tti", "iso"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -169,11 +173,13 @@ def main():
     grids = THREE_GRID
     if args.small:
         grids = [((360, 360, 40), 5.0), ((120, 120, 54), 15.0), ((40, 40, 34), 45.0)]
-    case = three_grid_case(seed=0, grids=grids, nsteps=args.steps)
-    medium = "iso"
+    medium = args.medium
+    case = three_grid_case(seed=0, grids=grids, nsteps=args.steps, medium=medium)
     pts = case.points()
-    sim = ecsg_b200.Simulation(case, precision="f32", energy=True, device=local)
     ev = args.energy_every
+    sim = ecsg_b200.Simulation(case, precision="f32", energy=ev > 0, device=local)
+    # 21-Cij energy needs the strain accumulators, updated by every stress sweep
+    acc = EPS_BYTES if (medium == "tti" and ev > 0) else 0
 
     def barrier():
         if pg is not None:
@@ -228,12 +234,13 @@ def main():
     cells0 = (n0[0] + 1) * (n0[1] + 1) * (n0[2] + 1)
     st_ms, ve_ms = kt["stress"][0], kt["vel"][0]
     if st_ms >= ve_ms:
-        dom, dom_ms, dom_bytes = "stress_kernel<float,ISO5> (grid 0)", st_ms, STRESS_BYTES[medium] * cells0
+        kname = "stress21_kernel<float,%s>" % ("true" if acc else "false") if medium == "tti" else "stress_kernel_v4<ISO5>"
+        dom, dom_ms, dom_bytes = kname + " (grid 0)", st_ms, (STRESS_BYTES[medium] + acc) * cells0
     else:
-        dom, dom_ms, dom_bytes = "vel_kernel<float> (grid 0)", ve_ms, VEL_BYTES * cells0
+        dom, dom_ms, dom_bytes = "vel_kernel_v4 (grid 0)", ve_ms, VEL_BYTES * cells0
     achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
     step_ms = run_ms / args.steps
-    step_gbs = BYTES_PER_CELL[medium] * pts / (step_ms * 1e-3) / 1e9
+    step_gbs = (BYTES_PER_CELL[medium] + acc) * pts / (step_ms * 1e-3) / 1e9
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
@@ -260,7 +267,9 @@ def main():
                                    "force, %d vz receivers, energy every %d steps"
                                    % (" / ".join("%dx%dx%d@%gm" % (n[0] + 1, n[1] + 1, n[2] + 1, h)
                                                  for n, h in grids), pts, len(sim.rec), ev),
-                       "medium": "isotropic stiffness from the seeded vp/vs/rho model (5 distinct moduli)",
+                       "medium": ("tilted VTI, all 21 Cij, built on the device from seeded node vp/vs/rho/dip/"
+                                  "azimuth (Thomsen eps 0.10, delta 0.05, gamma 0.08)" if medium == "tti" else
+                                  "isotropic stiffness from the seeded vp/vs/rho model (5 distinct moduli)"),
                        "points": pts, "parallelism": "replicas" if world > 1 else "single",
                        "l2": "inputs larger than L2: %.1f GB of fields and media resident" % (dev_bytes / 1e9)},
             "e2e": {"value": e2e, "unit": "Gcell/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
@@ -269,7 +278,8 @@ def main():
                          "frac": achieved / peak, "peak_source": peak_kind, "traffic": traffic,
                          "algorithmic_bytes_per_launch": dom_bytes,
                          "step_achieved": step_gbs, "step_frac": step_gbs / peak,
-                         "bytes_per_cell_update": BYTES_PER_CELL[medium]},
+                         "bytes_per_cell_update": BYTES_PER_CELL[medium] + acc,
+                         "energy_accumulator_bytes_per_cell": acc},
             "kernel_ms_per_step": kt,
             "cpu_baseline": base,
             "clocks": clk.summary(),

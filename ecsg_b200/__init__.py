@@ -22,8 +22,8 @@ LIB_PATH = os.path.join(HERE, "_lib", "libecsg_b200.so")
 ECSG_OK = 0
 ECSG_F32, ECSG_F64 = 0, 1
 ECSG_MEDIUM_ISO, ECSG_MEDIUM_ORTHO9, ECSG_MEDIUM_GEN21 = 0, 1, 2
-_MEDIUM = {"iso": ECSG_MEDIUM_ISO, "ortho9": ECSG_MEDIUM_ORTHO9, "gen21": ECSG_MEDIUM_GEN21}
-ST_JACOBI_CAP, ST_BARRIER_TIMEOUT, ST_NONFINITE = 1, 2, 4
+_MEDIUM = {"iso": ECSG_MEDIUM_ISO, "ortho9": ECSG_MEDIUM_ORTHO9, "gen21": ECSG_MEDIUM_GEN21, "tti": ECSG_MEDIUM_GEN21}
+ST_JACOBI_CAP, ST_BARRIER_TIMEOUT, ST_NONFINITE, ST_PIPE_TIMEOUT = 1, 2, 4, 8
 
 c_dp = ctypes.POINTER(ctypes.c_double)
 c_fp = ctypes.POINTER(ctypes.c_float)
@@ -69,6 +69,8 @@ SIGNATURES = [
     ("ecsg_set_medium_iso", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_fp, c_fp, c_fp]),
     ("ecsg_set_medium_ortho9", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_dp, ctypes.POINTER(c_dp)]),
     ("ecsg_set_medium_cij21", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_dp, ctypes.POINTER(c_dp)]),
+    ("ecsg_set_medium_tti", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_fp, c_fp, c_fp, c_fp, c_fp,
+                                           ctypes.c_double, ctypes.c_double, ctypes.c_double]),
     ("ecsg_set_field", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, c_dp]),
     ("ecsg_get_field", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, c_dp]),
     ("ecsg_field_elems", ctypes.c_longlong, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
@@ -158,6 +160,10 @@ class Simulation:
                 b, s11, s13 = (np.ascontiguousarray(m[k], dtype=np.float32) for k in ("buoy", "s11", "s13"))
                 self._ck(L.ecsg_set_medium_iso(h, gi, b.ctypes.data_as(c_fp), s11.ctypes.data_as(c_fp),
                                                s13.ctypes.data_as(c_fp)))
+            elif case.medium == "tti":
+                arrs = [np.ascontiguousarray(m[k], dtype=np.float32) for k in ("vp", "vs", "rho", "dip", "azi")]
+                self._ck(L.ecsg_set_medium_tti(h, gi, *[a.ctypes.data_as(c_fp) for a in arrs],
+                                               *[float(t) for t in case.thomsen]))
             else:
                 key, nslot, fn = (("c21", 21, L.ecsg_set_medium_cij21) if case.medium == "gen21"
                                   else ("c9", 9, L.ecsg_set_medium_ortho9))

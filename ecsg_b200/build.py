@@ -24,6 +24,8 @@ SOURCES = {
     "stencil.cu": [],
     "stencil_v4.cu": [],
     "stress21.cu": ["-fmad=false"],
+    "stress21_tma.cu": ["-fmad=false"],
+    "medium.cu": [],
     "interface.cu": ["-fmad=false"],
     "diag.cu": ["-fmad=false"],
     "api.cu": [],

@@ -28,6 +28,11 @@ cudaError_t launch_stress_v4(const GridDev<float> &, int, int, int, int, cudaStr
 // stress21.cu (21-Cij media)
 template <typename T>
 cudaError_t launch_stress21(const GridDev<T> &, int, int, T *const[6], int, cudaStream_t);
+// stress21_tma.cu (FP32 21-Cij sweeps, TMA-staged)
+size_t s21_maps_bytes();
+bool s21_encode_maps(void *, const GridDev<float> &, float *const[6]);
+cudaError_t s21_set_attributes();
+cudaError_t launch_stress21_tma(const void *, const GridDev<float> &, int, int, float *const[6], int *, int, cudaStream_t);
 // interface.cu
 template <typename T>
 cudaError_t launch_ghost_vz(const GridDev<T> &, const GridDev<T> &, int, int, double *, cudaStream_t);
@@ -55,6 +60,10 @@ template <typename T>
 cudaError_t launch_unpack(double *, const Geo &, const T *, int, int, int, int, cudaStream_t);
 template <typename T>
 cudaError_t launch_iso_medium(const Geo &, const double *, const double *, double *, T *const[5], cudaStream_t);
+// medium.cu
+template <typename T>
+cudaError_t launch_tti_medium(const Geo &, const float *const[5], double, double, double, double *, T *, T *const[21],
+                              cudaStream_t);
 } // namespace ecsg
 
 using namespace ecsg;
@@ -90,6 +99,8 @@ struct ecsg_sim {
     int nc = 5;
     void *vc[kMaxGrids][3] = {};
     void *eps[kMaxGrids][6] = {};   // 21-Cij media with energy: accumulated strains at the stress positions
+    std::vector<unsigned char> s21maps[kMaxGrids];   // TMA tensor maps of the FP32 21-Cij sweep, per grid
+    bool s21_ready = false;
     bool medium_set[kMaxGrids] = {};
     Iface itf[kMaxGrids];
     // shared device scalars: [0] status, [1] step clock, [2] last sxz sweeps, [3] first step of the run
@@ -407,6 +418,56 @@ int ecsg_set_medium_cij21(ecsg_sim *s, int g, const double *buoy, const double *
     return ECSG_OK;
 }
 
+template <typename T>
+static int set_tti(ecsg_sim *s, int g, const float *const node[5], double eps, double delta, double gamma)
+{
+    const Geo &G = s->geo[g];
+    const size_t nn = (size_t)(G.nx + 1) * (G.ny + 1) * (G.nz + 1);
+    const size_t box = (size_t)G.size();
+    float *stage = nullptr, *nd[5] = {};
+    double *work = nullptr;
+    auto release = [&]() {
+        cudaFree(stage);
+        cudaFree(work);
+        for (int k = 0; k < 5; k++) cudaFree(nd[k]);
+    };
+    cudaError_t e = cudaMalloc(&stage, nn * sizeof(float));
+    for (int k = 0; k < 5 && e == cudaSuccess; k++) e = cudaMalloc(&nd[k], box * sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc(&work, box * sizeof(double));
+    for (int k = 0; k < 5 && e == cudaSuccess; k++) {
+        e = cudaMemcpyAsync(stage, node[k], nn * sizeof(float), cudaMemcpyHostToDevice, s->st);
+        if (e == cudaSuccess) e = launch_pack<float, float>(nd[k], G, stage, G.nx + 1, G.ny + 1, G.nz + 1, 0, s->st);
+        // the stage buffer is reused by the next component
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+    }
+    T *slot[21];
+    for (int k = 0; k < 21; k++) slot[k] = (T *)s->c[g][k];
+    if (e == cudaSuccess) e = launch_tti_medium<T>(G, nd, eps, delta, gamma, work, (T *)s->b[g], slot, s->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->st);
+    release();
+    if (e != cudaSuccess) return fail(s, ECSG_ERR_CUDA, "set_medium_tti: %s", cudaGetErrorString(e));
+    return ECSG_OK;
+}
+
+int ecsg_set_medium_tti(ecsg_sim *s, int g, const float *vp, const float *vs, const float *rho, const float *dip,
+                        const float *azimuth, double epsilon, double delta, double gamma)
+{
+    if (!s || g < 0 || g >= s->ng || !vp || !vs || !rho || !dip || !azimuth)
+        return fail(s, ECSG_ERR_INVALID, "set_medium_tti: bad arguments");
+    if (s->medium != ECSG_MEDIUM_GEN21) return fail(s, ECSG_ERR_STATE, "simulation was not created for a 21-Cij medium");
+    if (!(epsilon > -0.5) || !(gamma > -0.5) || !(delta > -0.5))
+        return fail(s, ECSG_ERR_INVALID, "set_medium_tti: Thomsen parameters must exceed -1/2");
+    CK(cudaSetDevice(s->device));
+    const float *node[5] = {vp, vs, rho, dip, azimuth};
+    int rc = s->prec == ECSG_F32 ? set_tti<float>(s, g, node, epsilon, delta, gamma)
+                                 : set_tti<double>(s, g, node, epsilon, delta, gamma);
+    if (rc) return rc;
+    s->medium_set[g] = true;
+    if (g > 0) s->itf[g].A_ready = false;
+    if (g + 1 < s->ng) s->itf[g + 1].A_ready = false;
+    return ECSG_OK;
+}
+
 long long ecsg_field_elems(const ecsg_sim *s, int g, int k)
 {
     if (!s || g < 0 || g >= s->ng || k < 0 || k > 8) return -1;
@@ -496,6 +557,28 @@ static int med_kind(const ecsg_sim *s)
     return s->medium == ECSG_MEDIUM_ISO ? MED_ISO5 : (s->medium == ECSG_MEDIUM_ORTHO9 ? MED_ORTHO9 : MED_GEN21);
 }
 
+static bool use_s21_tma(const ecsg_sim *s)
+{
+    return s->medium == ECSG_MEDIUM_GEN21 && s->prec == ECSG_F32 && !s->scalar_stencils;
+}
+
+// Tensor maps and kernel attributes of the TMA-staged 21-Cij sweep; host work
+// only, done once before any capture.
+static int stress_prepare(ecsg_sim *s)
+{
+    if (!use_s21_tma(s) || s->s21_ready) return ECSG_OK;
+    for (int g = 0; g < s->ng; g++) {
+        float *eps[6];
+        for (int k = 0; k < 6; k++) eps[k] = (float *)s->eps[g][k];
+        s->s21maps[g].assign(s21_maps_bytes(), 0);
+        if (!s21_encode_maps(s->s21maps[g].data(), dev<float>(s, g), eps))
+            return fail(s, ECSG_ERR_CUDA, "grid %d: TMA tensor maps of the 21-Cij sweep could not be encoded", g);
+    }
+    CK(s21_set_attributes());
+    s->s21_ready = true;
+    return ECSG_OK;
+}
+
 template <typename T>
 static int stress_op(ecsg_sim *s, int g)
 {
@@ -503,6 +586,13 @@ static int stress_op(ecsg_sim *s, int g)
     if (med == MED_GEN21) {
         T *eps[6];
         for (int k = 0; k < 6; k++) eps[k] = (T *)s->eps[g][k];
+        if constexpr (std::is_same<T, float>::value) {
+            if (use_s21_tma(s)) {
+                if (int rc = stress_prepare(s)) return rc;
+                CK(launch_stress21_tma(s->s21maps[g].data(), dev<float>(s, g), g == 0, s->top_bc, eps, s->ints, s->sms, s->st));
+                return ECSG_OK;
+            }
+        }
         CK(launch_stress21<T>(dev<T>(s, g), g == 0, s->top_bc, eps, s->sms, s->st));
         return ECSG_OK;
     }
@@ -869,6 +959,7 @@ static int run_op(ecsg_sim *s, int n0, int nsteps, float *traces, double *energy
     int rc;
     for (int i = 1; i < s->ng; i++)
         if ((rc = sxz_prepare<T>(s, i))) return rc;
+    if ((rc = stress_prepare(s))) return rc;
     if (s->nrec > 0 && s->trace_cap < nsteps) {
         cudaFree(s->traces);
         s->traces = nullptr;

@@ -85,6 +85,7 @@ enum : int {
     ST_JACOBI_CAP = 1,        // an sxz Jacobi solve stopped at its iteration cap
     ST_BARRIER_TIMEOUT = 2,   // a grid-wide barrier gave up waiting
     ST_NONFINITE = 4,         // a non-finite energy was observed
+    ST_PIPE_TIMEOUT = 8,      // a TMA pipeline wait gave up (the CTA stopped early)
 };
 
 // Work space of one sxz interface solve (interface.cu).

@@ -1,0 +1,541 @@
+// stress21_tma.cu -- FP32 21-Cij stress update with TMA-staged planes.
+//
+// The same update as stress21.cu (same operation order, so the results are
+// bitwise equal to it), organised for bandwidth: a CTA owns a 32 x 8 tile of
+// (x, y) points and marches z.  One producer thread streams, per plane,
+//   * the 12 coefficient slots read around the tile (c6..c14, c16, c17, c19)
+//     and the three velocities as 40 x 10 boxes (tile, one-point halo, the x
+//     start rounded down to a 16-byte boundary),
+//   * the other 9 coefficient slots, the 6 stresses and (energy runs) the 6
+//     strain accumulators as 32 x 8 boxes,
+// into shared-memory rings with cp.async.bulk.tensor (3-D tiled TMA, no
+// multicast), completion tracked by mbarriers.  Eight consumer warps compute
+// every strain / link product of their own point plus one halo row or column
+// of one kind per warp (each kind needs a one-sided halo only), exchange them
+// through a two-plane ring, and update the stresses.  Velocities stay resident
+// for three planes (p-1, p, p+1), coefficients and stresses for one; the
+// values the z-staggered outputs (syz, sxz at plane p-1) need from plane p-1
+// are carried in registers.  All waits are bounded: on a timeout the CTA sets
+// ST_PIPE_TIMEOUT, stops, and drains its own copies before returning.
+#include "ecsg_device.cuh"
+#include "gen21_device.cuh"
+
+#include <cuda.h>
+#include <cstring>
+#include <type_traits>
+
+namespace ecsg {
+
+namespace s21t {
+constexpr int TX = 32, TY = 8, NT = TX * TY, NTHREADS = NT + 32;
+constexpr int BW = 40, BH = 10;              // haloed box: x0-4 .. x0+35, y0-1 .. y0+8
+constexpr int HX = 34, HYI = 10, HP = HX * HYI;   // intermediates: x0-1 .. x0+32, y0-1 .. y0+8
+constexpr int NQ = 9;
+constexpr int NSP = 3, NSV = 5;               // ring depths: plane data, velocities
+constexpr int HBOX = BW * BH * 4;             // 1600 bytes
+constexpr int HBOX_A = 1664;                  // 128-byte aligned stride
+constexpr int IBOX = TX * TY * 4;             // 1024 bytes
+constexpr int NCH = 12, NCI = 9;
+constexpr int P_CH = 0, P_CI = NCH * HBOX_A, P_SG = P_CI + NCI * IBOX, P_EP = P_SG + 6 * IBOX;
+constexpr int PSLOT = P_EP + 6 * IBOX;        // 41472
+constexpr int VSLOT = 3 * HBOX_A;             // 4992
+constexpr int OFF_V = NSP * PSLOT;
+constexpr int OFF_IM = OFF_V + NSV * VSLOT;
+constexpr int OFF_BAR = OFF_IM + 2 * NQ * HP * 4;
+constexpr int NBAR = 2 * NSP + 2 * NSV;
+constexpr int OFF_FLAG = OFF_BAR + NBAR * 8;
+constexpr int SMEM = OFF_FLAG + 64;
+constexpr long long kWaitLimit = 1LL << 24;   // polls of an mbarrier before giving up
+// coefficient slot of each staged box
+__host__ __device__ constexpr int ch_slot(int k) { return k < 9 ? 6 + k : (k == 9 ? 16 : (k == 10 ? 17 : 19)); }
+__host__ __device__ constexpr int ci_slot(int k) { return k < 6 ? k : (k == 6 ? 15 : (k == 7 ? 18 : 20)); }
+} // namespace s21t
+
+struct S21Maps {
+    CUtensorMap v[3];     // vx vy vz, haloed box
+    CUtensorMap ch[12];   // haloed coefficient boxes
+    CUtensorMap ci[9];    // interior coefficient boxes
+    CUtensorMap sg[6];    // stresses sxx syy szz syz sxz sxy
+    CUtensorMap ep[6];    // strain accumulators
+};
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(unsigned a, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(a), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned a, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(a), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(unsigned a)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(a) : "memory");
+}
+__device__ __forceinline__ bool mbar_test(unsigned a, unsigned parity)
+{
+    unsigned ok;
+    asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+                 : "=r"(ok)
+                 : "r"(a), "r"(parity)
+                 : "memory");
+    return ok != 0;
+}
+// bounded wait; false after kWaitLimit polls
+__device__ __forceinline__ bool mbar_wait(unsigned a, unsigned parity)
+{
+    for (long long i = 0; i < s21t::kWaitLimit; i++) {
+        if (mbar_test(a, parity)) return true;
+        if (i > 64) __nanosleep(64);
+    }
+    return false;
+}
+__device__ __forceinline__ void tma_load3(unsigned dst, const CUtensorMap *map, int x, int y, int z, unsigned bar)
+{
+    asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+                 ::"r"(dst), "l"((unsigned long long)map), "r"(x), "r"(y), "r"(z), "r"(bar)
+                 : "memory");
+}
+__device__ __forceinline__ void consumer_sync() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
+
+template <bool ACC>
+__global__ void __launch_bounds__(s21t::NTHREADS, 1)
+    stress21_tma_kernel(const __grid_constant__ S21Maps maps, GridDev<float> G, int flag, int zchunk, float *eps0,
+                        float *eps1, float *eps2, float *eps3, float *eps4, float *eps5, int *status)
+{
+    using namespace s21t;
+    extern __shared__ __align__(128) unsigned char sm[];
+    const Geo &g = G.g;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const Ext E{nx, ny, nz};
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+    const int z0 = blockIdx.z * zchunk, z1 = min(nz, z0 + zchunk - 1);
+    const int qstart = z0 - 1, n = z1 - z0 + 3;   // planes z0-1 .. z1+1
+    const int sz = g.px * g.py;
+    const unsigned bar0 = smem_u32(sm + OFF_BAR);
+    auto fullP = [&](int s) { return bar0 + 8u * s; };
+    auto emptyP = [&](int s) { return bar0 + 8u * (NSP + s); };
+    auto fullV = [&](int s) { return bar0 + 8u * (2 * NSP + s); };
+    auto emptyV = [&](int s) { return bar0 + 8u * (2 * NSP + NSV + s); };
+    // [0] producer gave up, [1] P stages consumed, [2] V stages consumed, [3] consumers gave up.
+    // [3] is written only by consumers before a consumer barrier and read between
+    // that barrier and the next, so every consumer takes the same branch.
+    volatile int *flags = (volatile int *)(sm + OFF_FLAG);
+    float *IM = (float *)(sm + OFF_IM);
+
+    if (tid == 0) {
+        for (int s = 0; s < NSP; s++) { mbar_init(fullP(s), 1); mbar_init(emptyP(s), 1); }
+        for (int s = 0; s < NSV; s++) { mbar_init(fullV(s), 1); mbar_init(emptyV(s), 1); }
+        flags[0] = 0; flags[1] = 0; flags[2] = 0; flags[3] = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    int issuedP = 0, issuedV = 0;
+    if (warp == NT / 32) {
+        // ---------------- producer ----------------
+        if (lane == 0) {
+            const int hx0 = XOFF + x0 - 4, hy0 = g.R + y0 - 1, ix0 = XOFF + x0, iy0 = g.R + y0;
+            auto issueV = [&](int j) -> bool {
+                const int s = j % NSV;
+                if (j >= NSV && !mbar_wait(emptyV(s), ((j / NSV) - 1) & 1)) return false;
+                const unsigned dst = smem_u32(sm + OFF_V + s * VSLOT);
+                mbar_expect_tx(fullV(s), 3 * HBOX);
+                const int zc = g.R + qstart - 1 + j;
+                for (int c = 0; c < 3; c++) tma_load3(dst + c * HBOX_A, &maps.v[c], hx0, hy0, zc, fullV(s));
+                return true;
+            };
+            auto issueP = [&](int i) -> bool {
+                const int s = i % NSP;
+                if (i >= NSP && !mbar_wait(emptyP(s), ((i / NSP) - 1) & 1)) return false;
+                const int q = qstart + i;
+                const bool inner = q >= z0 && q <= z1;
+                const unsigned dst = smem_u32(sm + s * PSLOT);
+                mbar_expect_tx(fullP(s), NCH * HBOX + (inner ? (NCI + 6 + (ACC ? 6 : 0)) * IBOX : 0));
+                const int zc = g.R + q;
+                for (int k = 0; k < NCH; k++) tma_load3(dst + P_CH + k * HBOX_A, &maps.ch[k], hx0, hy0, zc, fullP(s));
+                if (inner) {
+                    for (int k = 0; k < NCI; k++) tma_load3(dst + P_CI + k * IBOX, &maps.ci[k], ix0, iy0, zc, fullP(s));
+                    for (int k = 0; k < 6; k++) tma_load3(dst + P_SG + k * IBOX, &maps.sg[k], ix0, iy0, zc, fullP(s));
+                    if (ACC)
+                        for (int k = 0; k < 6; k++) tma_load3(dst + P_EP + k * IBOX, &maps.ep[k], ix0, iy0, zc, fullP(s));
+                }
+                return true;
+            };
+            bool ok = true;
+            for (int i = 0; i < n && ok; i++) {
+                while (ok && issuedV <= i + 2) {
+                    ok = issueV(issuedV);
+                    if (ok) issuedV++;
+                }
+                if (ok) {
+                    ok = issueP(i);
+                    if (ok) issuedP++;
+                }
+                if (flags[3]) break;
+            }
+            if (!ok) {
+                flags[0] = 1;
+                atomicOr(status, ST_PIPE_TIMEOUT);
+            }
+        }
+    } else {
+        // ---------------- consumers ----------------
+        const int tx = lane, ty = warp;
+        const int ox = x0 + tx, oy = y0 + ty;
+        const int vb = (ty + 1) * BW + tx + 4, ib = ty * TX + tx, hx = tx + 1, hy = ty + 1;
+        const float k0 = G.k[0], k1 = G.k[1], k2 = G.k[2];
+        float *sxx = G.f[SXX], *syy = G.f[SYY], *szz = G.f[SZZ], *syz = G.f[SYZ], *sxz = G.f[SXZ], *sxy = G.f[SXY];
+        // carries from plane pm = p-1 for the syz / sxz outputs
+        float c15p = 0.f, c16p = 0.f, c17p = 0.f, c18p = 0.f, c19p = 0.f, s3p = 0.f, s4p = 0.f, ep3p = 0.f, ep4p = 0.f;
+        // the halo job of this warp: kind (0 L4, 1 L5, 2 L6, 3 N) and point
+        int hk, hxp, hyp;
+        {
+            const int w = warp;
+            hk = w & 3;
+            if (w < 4) {   // rows
+                hxp = x0 + lane;
+                hyp = (hk == 0 || hk == 2) ? y0 - 1 : y0 + TY;
+            } else {       // columns, 9 lanes
+                hxp = (hk == 0 || hk == 3) ? x0 - 1 : x0 + TX;
+                hyp = (hk == 0 || hk == 2) ? y0 - 1 + lane : y0 + lane;
+            }
+        }
+        const bool hact = warp < 4 || lane < 9;
+        const int hvb = (hyp - y0 + 1) * BW + (hxp - x0 + 4), hhb = (hyp - y0 + 1) * HX + (hxp - x0 + 1);
+        // Tiles whose points and halos all lie strictly inside the grid (x, y in
+        // 1 .. n-1): on their planes 1 .. nz-1 every extent test passes and every
+        // closure weight is 1/4, so the fast variant drops the tests.
+        const bool tile_in = x0 >= 1 && x0 + TX <= nx && y0 >= 1 && y0 + TY <= ny;
+        const int pbase = g.idx(ox, oy, 0);
+        int consumedP = 0, consumedV = 0;
+        for (int i = 0; i < n; i++) {
+            const int p = qstart + i;
+            // ---- wait for plane data p and velocities p-1, p, p+1
+            bool ok = true;
+            if (i == 0) {
+                ok = mbar_wait(fullV(0), 0) && mbar_wait(fullV(1), 0);
+            }
+            ok = ok && mbar_wait(fullV((i + 2) % NSV), ((i + 2) / NSV) & 1);
+            ok = ok && mbar_wait(fullP(i % NSP), (i / NSP) & 1);
+            if (!ok) flags[3] = 1;
+            consumer_sync();
+            if (flags[3]) break;
+            consumedP = i + 1;
+            consumedV = i + 3;
+            const unsigned char *PS = sm + (i % NSP) * PSLOT;
+            const float *CH = (const float *)(PS + P_CH);
+            const float *CI = (const float *)(PS + P_CI);
+            const float *SG = (const float *)(PS + P_SG);
+            const float *EP = (const float *)(PS + P_EP);
+            const float *Vm = (const float *)(sm + OFF_V + (i % NSV) * VSLOT);
+            const float *Vp = (const float *)(sm + OFF_V + ((i + 1) % NSV) * VSLOT);
+            const float *Vn = (const float *)(sm + OFF_V + ((i + 2) % NSV) * VSLOT);
+            constexpr int HS = HBOX_A / 4;   // floats between staged boxes
+            constexpr int IS = IBOX / 4;
+            float *IMs = IM + (p & 1) * NQ * HP;
+            const float *Rs = IM + (p & 1) * NQ * HP;          // plane p
+            const float *Rp = IM + ((p - 1) & 1) * NQ * HP;    // plane p-1
+            const bool surf = flag && p == 0;
+            const bool inner = p >= z0 && p <= z1;
+            const int pm = p - 1;
+            const bool outer_pm = pm >= z0 && pm <= z1;
+            auto chv = [&](int k, int b) { return CH[k * HS + b]; };
+
+            auto body = [&](auto fast_tag) {
+                constexpr bool FAST = decltype(fast_tag)::value;
+                auto RR = [&](int plane_is_p, int q, int hx_, int hy_) { return (plane_is_p ? Rs : Rp)[q * HP + hy_ * HX + hx_]; };
+                // closure-weighted mean of four neighbours (avg4); 1/4 each on the fast path
+                auto av = [&](const float (&v)[2][2], const bool (&a)[2], const bool (&b)[2]) -> float {
+                    if (FAST) {
+                        const float w = 0.25f;
+                        return add_(add_(add_(add_(0.f, mul_(w, v[0][0])), mul_(w, v[0][1])), mul_(w, v[1][0])), mul_(w, v[1][1]));
+                    }
+                    return avg4<float>(v, a, b);
+                };
+
+                // ---- intermediates of plane p: own point (all kinds), then the halo job
+                float e1 = 0.f, e2 = 0.f, e3 = 0.f;
+                {
+                    float e4 = 0.f, q45 = 0.f, q46 = 0.f, e5 = 0.f, q56 = 0.f, e6 = 0.f, p4 = 0.f, p5 = 0.f, p6 = 0.f;
+                    if (FAST || E.l4(ox, oy, p)) {
+                        e4 = add_(mul_(k2, sub_(Vn[HS + vb], Vp[HS + vb])), mul_(k1, sub_(Vp[2 * HS + vb + BW], Vp[2 * HS + vb])));
+                        q45 = mul_(chv(9, vb), e4);
+                        q46 = mul_(chv(10, vb), e4);
+                    }
+                    if (FAST || E.l5(ox, oy, p)) {
+                        e5 = add_(mul_(k2, sub_(Vn[vb], Vp[vb])), mul_(k0, sub_(Vp[2 * HS + vb], Vp[2 * HS + vb - 1])));
+                        q56 = mul_(chv(11, vb), e5);
+                    }
+                    if (FAST || E.l6(ox, oy, p)) e6 = add_(mul_(k1, sub_(Vp[vb + BW], Vp[vb])), mul_(k0, sub_(Vp[HS + vb], Vp[HS + vb - 1])));
+                    if (FAST || E.n(ox, oy, p)) {
+                        e1 = mul_(k0, sub_(Vp[vb + 1], Vp[vb]));
+                        e2 = mul_(k1, sub_(Vp[HS + vb], Vp[HS + vb - BW]));
+                        if (!FAST && surf)
+                            e3 = e3_used(G, E, true, ox, oy, p, pbase + p * sz, e1, e2);
+                        else
+                            e3 = mul_(k2, sub_(Vp[2 * HS + vb], Vm[2 * HS + vb]));
+                        p4 = add_(add_(mul_(chv(0, vb), e1), mul_(chv(3, vb), e2)), mul_(chv(6, vb), e3));
+                        p5 = add_(add_(mul_(chv(1, vb), e1), mul_(chv(4, vb), e2)), mul_(chv(7, vb), e3));
+                        p6 = add_(add_(mul_(chv(2, vb), e1), mul_(chv(5, vb), e2)), mul_(chv(8, vb), e3));
+                    }
+                    const int hb = hy * HX + hx;
+                    IMs[0 * HP + hb] = e4; IMs[1 * HP + hb] = q45; IMs[2 * HP + hb] = q46;
+                    IMs[3 * HP + hb] = e5; IMs[4 * HP + hb] = q56; IMs[5 * HP + hb] = e6;
+                    IMs[6 * HP + hb] = p4; IMs[7 * HP + hb] = p5; IMs[8 * HP + hb] = p6;
+                }
+                if (hact) {
+                    const int b = hvb, x = hxp, y = hyp;
+                    if (hk == 0) {
+                        float e4 = 0.f, q45 = 0.f, q46 = 0.f;
+                        if (FAST || E.l4(x, y, p)) {
+                            e4 = add_(mul_(k2, sub_(Vn[HS + b], Vp[HS + b])), mul_(k1, sub_(Vp[2 * HS + b + BW], Vp[2 * HS + b])));
+                            q45 = mul_(chv(9, b), e4);
+                            q46 = mul_(chv(10, b), e4);
+                        }
+                        IMs[0 * HP + hhb] = e4; IMs[1 * HP + hhb] = q45; IMs[2 * HP + hhb] = q46;
+                    } else if (hk == 1) {
+                        float e5 = 0.f, q56 = 0.f;
+                        if (FAST || E.l5(x, y, p)) {
+                            e5 = add_(mul_(k2, sub_(Vn[b], Vp[b])), mul_(k0, sub_(Vp[2 * HS + b], Vp[2 * HS + b - 1])));
+                            q56 = mul_(chv(11, b), e5);
+                        }
+                        IMs[3 * HP + hhb] = e5; IMs[4 * HP + hhb] = q56;
+                    } else if (hk == 2) {
+                        float e6 = 0.f;
+                        if (FAST || E.l6(x, y, p)) e6 = add_(mul_(k1, sub_(Vp[b + BW], Vp[b])), mul_(k0, sub_(Vp[HS + b], Vp[HS + b - 1])));
+                        IMs[5 * HP + hhb] = e6;
+                    } else {
+                        float p4 = 0.f, p5 = 0.f, p6 = 0.f;
+                        if (FAST || E.n(x, y, p)) {
+                            const float f1 = mul_(k0, sub_(Vp[b + 1], Vp[b]));
+                            const float f2 = mul_(k1, sub_(Vp[HS + b], Vp[HS + b - BW]));
+                            const float f3 = (!FAST && surf) ? e3_used(G, E, true, x, y, p, g.idx(x, y, p), f1, f2)
+                                                             : mul_(k2, sub_(Vp[2 * HS + b], Vm[2 * HS + b]));
+                            p4 = add_(add_(mul_(chv(0, b), f1), mul_(chv(3, b), f2)), mul_(chv(6, b), f3));
+                            p5 = add_(add_(mul_(chv(1, b), f1), mul_(chv(4, b), f2)), mul_(chv(7, b), f3));
+                            p6 = add_(add_(mul_(chv(2, b), f1), mul_(chv(5, b), f2)), mul_(chv(8, b), f3));
+                        }
+                        IMs[6 * HP + hhb] = p4; IMs[7 * HP + hhb] = p5; IMs[8 * HP + hhb] = p6;
+                    }
+                }
+                consumer_sync();
+
+                // ---- outputs: sigma_N, sigma_6 at plane p; sigma_4, sigma_5 at plane p-1
+                if (inner) {
+                    const int pp = pbase + p * sz;
+                    if (FAST || E.n(ox, oy, p)) {
+                        float v[2][2];
+                        bool a[2], b[2];
+                        for (int k = 0; k < 2; k++) { a[k] = (oy - 1 + k) >= 0 && (oy - 1 + k) <= ny - 1; b[k] = (p - 1 + k) >= 0 && (p - 1 + k) <= nz - 1; }
+                        for (int k = 0; k < 2; k++) for (int j = 0; j < 2; j++) v[k][j] = RR(j, 0, hx, hy - 1 + k);
+                        const float a4 = av(v, a, b);
+                        for (int k = 0; k < 2; k++) { a[k] = (ox + k) <= nx; b[k] = (p - 1 + k) >= 0 && (p - 1 + k) <= nz - 1; }
+                        for (int k = 0; k < 2; k++) for (int j = 0; j < 2; j++) v[k][j] = RR(j, 3, hx + k, hy);
+                        const float a5 = av(v, a, b);
+                        for (int k = 0; k < 2; k++) { a[k] = (ox + k) <= nx; b[k] = (oy - 1 + k) >= 0 && (oy - 1 + k) <= ny - 1; }
+                        for (int k = 0; k < 2; k++) for (int j = 0; j < 2; j++) v[k][j] = RR(1, 5, hx + k, hy - 1 + j);
+                        const float a6 = av(v, a, b);
+                        const int rowc[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+                        float d[3];
+#pragma unroll
+                        for (int r = 0; r < 3; r++)
+                            d[r] = add_(add_(add_(add_(add_(mul_(CI[rowc[r][0] * IS + ib], e1), mul_(CI[rowc[r][1] * IS + ib], e2)),
+                                                       mul_(CI[rowc[r][2] * IS + ib], e3)),
+                                                  mul_(chv(3 * r, vb), a4)),
+                                             mul_(chv(1 + 3 * r, vb), a5)),
+                                        mul_(chv(2 + 3 * r, vb), a6));
+                        sxx[pp] = add_(SG[0 * IS + ib], d[0]);
+                        syy[pp] = add_(SG[1 * IS + ib], d[1]);
+                        if (FAST || !surf) szz[pp] = add_(SG[2 * IS + ib], d[2]);
+                        if (ACC) {
+                            eps0[pp] = add_(EP[0 * IS + ib], e1);
+                            eps1[pp] = add_(EP[1 * IS + ib], e2);
+                            eps2[pp] = add_(EP[2 * IS + ib], e3);
+                        }
+                    }
+                    if (FAST || E.l6(ox, oy, p)) {
+                        float v[2][2];
+                        bool a[2], b[2];
+                        for (int k = 0; k < 2; k++) { a[k] = (ox - 1 + k) >= 0 && (ox - 1 + k) <= nx - 1; b[k] = (p - 1 + k) >= 0 && (p - 1 + k) <= nz - 1; }
+                        for (int k = 0; k < 2; k++) for (int j = 0; j < 2; j++) v[k][j] = RR(j, 2, hx - 1 + k, hy);
+                        const float t46 = av(v, a, b);
+                        for (int k = 0; k < 2; k++) { a[k] = (oy + k) <= ny; b[k] = (p - 1 + k) >= 0 && (p - 1 + k) <= nz - 1; }
+                        for (int k = 0; k < 2; k++) for (int j = 0; j < 2; j++) v[k][j] = RR(j, 4, hx, hy + k);
+                        const float t56 = av(v, a, b);
+                        for (int k = 0; k < 2; k++) { a[k] = (ox - 1 + k) >= 0 && (ox - 1 + k) <= nx - 1; b[k] = (oy + k) <= ny; }
+                        for (int k = 0; k < 2; k++) for (int j = 0; j < 2; j++) v[k][j] = RR(1, 8, hx - 1 + k, hy + j);
+                        const float t6 = av(v, a, b);
+                        const float e6 = RR(1, 5, hx, hy);
+                        const float dd = add_(add_(add_(mul_(CI[8 * IS + ib], e6), t46), t56), t6);
+                        sxy[pp] = add_(SG[5 * IS + ib], dd);
+                        if (ACC) eps5[pp] = add_(EP[5 * IS + ib], e6);
+                    }
+                }
+                if (outer_pm) {
+                    const int pp = pbase + pm * sz;
+                    if (FAST || E.l4(ox, oy, pm)) {
+                        float v[2][2];
+                        bool a[2], b[2];
+                        for (int k = 0; k < 2; k++) { a[k] = (ox + k) <= nx; b[k] = (oy + k) <= ny; }
+                        for (int k = 0; k < 2; k++) for (int j = 0; j < 2; j++) v[k][j] = RR(0, 3, hx + k, hy + j);
+                        const float t5 = av(v, a, b);
+                        for (int k = 0; k < 2; k++) { a[k] = (ox + k) <= nx; b[k] = (pm + k) <= nz; }
+                        for (int k = 0; k < 2; k++) for (int j = 0; j < 2; j++) v[k][j] = RR(j, 5, hx + k, hy);
+                        const float t6 = av(v, a, b);
+                        for (int k = 0; k < 2; k++) { a[k] = (oy + k) <= ny; b[k] = (pm + k) <= nz; }
+                        for (int k = 0; k < 2; k++) for (int j = 0; j < 2; j++) v[k][j] = RR(j, 6, hx, hy + k);
+                        const float tp = av(v, a, b);
+                        const float e4 = RR(0, 0, hx, hy);
+                        const float dd = add_(add_(add_(mul_(c15p, e4), mul_(c16p, t5)), mul_(c17p, t6)), tp);
+                        const float nv = add_(s3p, dd);
+                        syz[pp] = nv;
+                        if (flag && pm == 0) syz[pp - sz] = -nv;
+                        if (ACC) eps3[pp] = add_(ep3p, e4);
+                    }
+                    if (FAST || E.l5(ox, oy, pm)) {
+                        float v[2][2];
+                        bool a[2], b[2];
+                        for (int k = 0; k < 2; k++) { a[k] = (oy - 1 + k) >= 0 && (oy - 1 + k) <= ny - 1; b[k] = (pm + k) <= nz; }
+                        for (int k = 0; k < 2; k++) for (int j = 0; j < 2; j++) v[k][j] = RR(j, 5, hx, hy - 1 + k);
+                        const float t6 = av(v, a, b);
+                        for (int k = 0; k < 2; k++) { a[k] = (ox - 1 + k) >= 0 && (ox - 1 + k) <= nx - 1; b[k] = (oy - 1 + k) >= 0 && (oy - 1 + k) <= ny - 1; }
+                        for (int k = 0; k < 2; k++) for (int j = 0; j < 2; j++) v[k][j] = RR(0, 1, hx - 1 + k, hy - 1 + j);
+                        const float t45 = av(v, a, b);
+                        for (int k = 0; k < 2; k++) { a[k] = (ox - 1 + k) >= 0 && (ox - 1 + k) <= nx - 1; b[k] = (pm + k) <= nz; }
+                        for (int k = 0; k < 2; k++) for (int j = 0; j < 2; j++) v[k][j] = RR(j, 7, hx - 1 + k, hy);
+                        const float tp = av(v, a, b);
+                        const float e5 = RR(0, 3, hx, hy);
+                        const float dd = add_(add_(add_(mul_(c18p, e5), mul_(c19p, t6)), t45), tp);
+                        const float nv = add_(s4p, dd);
+                        sxz[pp] = nv;
+                        if (flag && pm == 0 && (FAST || (ox >= 1 && ox <= nx - 1 && oy >= 1 && oy <= ny - 1))) sxz[pp - sz] = -nv;
+                        if (ACC) eps4[pp] = add_(ep4p, e5);
+                    }
+                }
+            };
+            // fast planes: interior tile, 1 <= p <= nz-1 (not the free surface,
+            // every closure weight 1/4 for the outputs at p and p-1)
+            if (tile_in && p >= 1 && p <= nz - 1)
+                body(std::true_type{});
+            else
+                body(std::false_type{});
+
+            if (inner) {
+                c15p = CI[6 * IS + ib]; c18p = CI[7 * IS + ib];
+                c16p = chv(9, vb); c17p = chv(10, vb); c19p = chv(11, vb);
+                s3p = SG[3 * IS + ib]; s4p = SG[4 * IS + ib];
+                if (ACC) { ep3p = EP[3 * IS + ib]; ep4p = EP[4 * IS + ib]; }
+            }
+            consumer_sync();
+            if (tid == 0) {
+                mbar_arrive(emptyP(i % NSP));
+                mbar_arrive(emptyV(i % NSV));
+            }
+        }
+        if (tid == 0) {
+            flags[1] = consumedP;
+            flags[2] = consumedV;
+            if (flags[3]) atomicOr(status, ST_PIPE_TIMEOUT);
+        }
+    }
+    __syncthreads();
+    // drain: copies issued but never consumed (only after a timeout) complete before exit
+    if (warp == NT / 32 && lane == 0) {
+        for (int i = flags[1]; i < issuedP; i++) mbar_wait(fullP(i % NSP), (i / NSP) & 1);
+        for (int j = flags[2]; j < issuedV; j++) mbar_wait(fullV(j % NSV), (j / NSV) & 1);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Host side: tensor maps and launch
+// ---------------------------------------------------------------------------
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static EncodeTiledFn encode_fn()
+{
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &p, 12000, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (EncodeTiledFn)p;
+    }
+    return fn;
+}
+
+static bool encode(CUtensorMap *m, const Geo &g, const void *base, int bw, int bh)
+{
+    EncodeTiledFn fn = encode_fn();
+    if (!fn || !base) return false;
+    const cuuint64_t dims[3] = {(cuuint64_t)g.px, (cuuint64_t)g.py, (cuuint64_t)g.pz};
+    const cuuint64_t strides[2] = {(cuuint64_t)g.px * 4, (cuuint64_t)g.px * g.py * 4};
+    const cuuint32_t box[3] = {(cuuint32_t)bw, (cuuint32_t)bh, 1};
+    const cuuint32_t es[3] = {1, 1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<void *>(base), dims, strides, box, es,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Opaque storage for the maps of one grid (allocated by the caller, s21_maps_bytes()).
+size_t s21_maps_bytes() { return sizeof(S21Maps); }
+
+// Fills the maps of one grid; false if the driver entry point is missing or
+// an address / pitch is not encodable.
+bool s21_encode_maps(void *out, const GridDev<float> &G, float *const eps[6])
+{
+    using namespace s21t;
+    S21Maps M;
+    memset(&M, 0, sizeof M);
+    const Geo &g = G.g;
+    if ((g.px * 4) % 16 != 0 || (XOFF - 4) % 4 != 0) return false;
+    bool ok = true;
+    for (int c = 0; c < 3; c++) ok = ok && encode(&M.v[c], g, G.f[c], BW, BH);
+    for (int k = 0; k < NCH; k++) ok = ok && encode(&M.ch[k], g, G.c[ch_slot(k)], BW, BH);
+    for (int k = 0; k < NCI; k++) ok = ok && encode(&M.ci[k], g, G.c[ci_slot(k)], TX, TY);
+    for (int k = 0; k < 6; k++) ok = ok && encode(&M.sg[k], g, G.f[SXX + k], TX, TY);
+    if (eps && eps[0])
+        for (int k = 0; k < 6; k++) ok = ok && encode(&M.ep[k], g, eps[k], TX, TY);
+    if (ok) memcpy(out, &M, sizeof M);
+    return ok;
+}
+
+// Opt-in to the kernel's shared memory; call outside stream capture.
+cudaError_t s21_set_attributes()
+{
+    cudaError_t e = cudaFuncSetAttribute(stress21_tma_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s21t::SMEM);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(stress21_tma_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s21t::SMEM);
+    return e;
+}
+
+cudaError_t launch_stress21_tma(const void *maps, const GridDev<float> &G, int top, int top_bc, float *const eps[6],
+                                int *status, int sms, cudaStream_t st)
+{
+    using namespace s21t;
+    const Geo &g = G.g;
+    const int flag = (top && top_bc) ? 1 : 0;
+    const int bx = (g.nx + 1 + TX - 1) / TX, by = (g.ny + 1 + TY - 1) / TY;
+    const int64_t cols = (int64_t)bx * by;
+    // one CTA per SM: aim for >= 4 waves, chunks of >= 24 planes
+    int nchunk = (int)(((int64_t)sms * 4 + cols - 1) / cols);
+    if (nchunk < 1) nchunk = 1;
+    const int maxc = (g.nz + 1) / 24 > 0 ? (g.nz + 1) / 24 : 1;
+    if (nchunk > maxc) nchunk = maxc;
+    const int zc = (g.nz + 1 + nchunk - 1) / nchunk;
+    dim3 grd(bx, by, (g.nz + 1 + zc - 1) / zc);
+    const S21Maps &M = *(const S21Maps *)maps;
+    if (eps && eps[0]) {
+        stress21_tma_kernel<true><<<grd, NTHREADS, SMEM, st>>>(M, G, flag, zc, eps[0], eps[1], eps[2], eps[3], eps[4], eps[5], status);
+    } else {
+        stress21_tma_kernel<false><<<grd, NTHREADS, SMEM, st>>>(M, G, flag, zc, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, status);
+    }
+    return cudaGetLastError();
+}
+
+} // namespace ecsg

@@ -177,19 +177,23 @@ def _sample(w, lattice_m, x, y, z):
     return (b[iz - zlo] * (1 - fz)[:, None, None] + b[iz - zlo + 1] * fz[:, None, None]).astype(np.float32)
 
 
-def three_grid_model(seed=0, grids=None, pert=0.05, corr_m=200.0):
+def three_grid_model(seed=0, grids=None, pert=0.05, corr_m=200.0, tilt=False, max_dip_deg=30.0, tilt_corr_m=400.0):
     """Three-grid composite at ratio 3 (defaults: 1081x1081x121 @ 5 m over
     361x361x161 @ 15 m over 121x121x101 @ 45 m, 163,856,303 points).
     Background vp rises linearly 1.2 -> 5.0 m/ms with depth over the whole
     stack, vs = vp/1.8, rho from Gardner (0.31 vp[m/s]^0.25 g/cm^3), each with
     seeded 5 % Gaussian-filtered perturbations (200 m correlation length).
-    Returns per-grid node arrays (vp, vs, rho) in float32."""
+    Returns per-grid node arrays (vp, vs, rho) in float32; with tilt, also the
+    symmetry-axis dip (smooth, 0 .. max_dip_deg) and azimuth (smooth, any
+    angle), in radians, from two more seeded fields."""
     grids = grids or THREE_GRID
     rng = np.random.default_rng(seed)
     lx = grids[0][0][0] * grids[0][1]
     ly = grids[0][0][1] * grids[0][1]
     lz = sum(n[2] * h for n, h in grids)
     fields = [_smooth_noise(rng, (lx, ly, lz), corr_m) for _ in range(3)]
+    if tilt:
+        fields += [_smooth_noise(rng, (lx, ly, lz), tilt_corr_m, lattice_m=100.0) for _ in range(2)]
     out = []
     z0 = 0.0
     for (n, h) in grids:
@@ -201,17 +205,32 @@ def three_grid_model(seed=0, grids=None, pert=0.05, corr_m=200.0):
         vp = vp0 * (1 + pert * p[0])
         vs = vp0 / np.float32(1.8) * (1 + pert * p[1])
         rho = (0.31 * (vp0 * 1000.0) ** 0.25).astype(np.float32) * (1 + pert * p[2])
-        out.append({"vp": vp, "vs": vs, "rho": rho, "n": n, "h": h})
+        m = {"vp": vp, "vs": vs, "rho": rho, "n": n, "h": h}
+        if tilt:
+            w = _sample(*fields[3], x, y, z)
+            m["dip"] = (np.float32(math.radians(max_dip_deg) * 0.5) * (1 + np.tanh(w))).astype(np.float32)
+            m["azi"] = (np.float32(math.pi) * _sample(*fields[4], x, y, z)).astype(np.float32)
+        out.append(m)
         z0 += n[2] * h
     return out
 
 
-def three_grid_case(seed=0, grids=None, nsteps=2000, fpeak=15.0, cfl=0.9):
-    """Benchmark case on three_grid_model: isotropic stiffness from (vp, vs, rho),
-    free surface, a Ricker vz point force at the surface centre and a line of vz
-    receivers along x at the surface centre line."""
+TTI_THOMSEN = (0.10, 0.05, 0.08)   # epsilon, delta, gamma of the benchmark medium
+
+
+def three_grid_case(seed=0, grids=None, nsteps=2000, fpeak=15.0, cfl=0.9, medium="tti"):
+    """Benchmark case on three_grid_model, free surface, a Ricker vz point force
+    at the surface centre and a line of vz receivers along x at the surface
+    centre line.  medium "tti": tilted VTI (Thomsen TTI_THOMSEN, seeded smooth
+    dip <= 30 deg and azimuth), all 21 Cij, built on the device from the node
+    arrays; "iso": isotropic stiffness from (vp, vs, rho)."""
     grids = grids or THREE_GRID
-    model = three_grid_model(seed, grids)
+    model = three_grid_model(seed, grids, tilt=(medium == "tti"))
+    if medium == "tti":
+        eps = TTI_THOMSEN[0]
+        vmax = max(float(m["vp"].max()) for m in model) * math.sqrt(1 + 2 * eps)
+        media = [{k: m[k] for k in ("vp", "vs", "rho", "dip", "azi")} for m in model]
+        return _surface_case("three_grid_r3_tti", grids, media, "tti", vmax, nsteps, fpeak, cfl)
     media = []
     vmax = 0.0
     for m in model:
@@ -221,15 +240,22 @@ def three_grid_case(seed=0, grids=None, nsteps=2000, fpeak=15.0, cfl=0.9):
         media.append({"buoy": (1.0 / rho).astype(np.float32), "s11": s11.astype(np.float32),
                       "s13": s13.astype(np.float32)})
         vmax = max(vmax, float(vp.max()))
+    return _surface_case("three_grid_r3", grids, media, "iso", vmax, nsteps, fpeak, cfl)
+
+
+def _surface_case(name, grids, media, medium, vmax, nsteps, fpeak, cfl):
     h0 = grids[0][1]
     dt = h0 / vmax / math.sqrt(3) * cfl
     n0 = grids[0][0]
     cx, cy = n0[0] // 2 * h0, n0[1] // 2 * h0
     trace = ricker(int(3.0 / (fpeak * dt * 1e-3)) + 1, dt * 1e-3, fpeak)
     rec = np.stack([np.arange(n0[0] + 1) * h0, np.full(n0[0] + 1, cy), np.zeros(n0[0] + 1)], 1).astype(np.float32)
-    return Case(name="three_grid_r3", grids=[{"n": n, "h": (h, h, h)} for (n, h) in grids], media=media,
-                medium="iso", dt=dt, nsteps=nsteps, radius=1, top_bc=1, imode=1,
+    case = Case(name=name, grids=[{"n": n, "h": (h, h, h)} for (n, h) in grids], media=media,
+                medium=medium, dt=dt, nsteps=nsteps, radius=1, top_bc=1, imode=1,
                 src={"xyz": (cx, cy, 0.0), "trace": trace, "scale": 1.0, "comp": 2}, rec=rec, rec_comp=2)
+    if medium == "tti":
+        case.thomsen = TTI_THOMSEN
+    return case
 
 
 # ---------------------------------------------------------------------------
@@ -310,3 +336,99 @@ def random_case_gen21(seed, ratio=2, nx2=6, ny2=5, nz=(5, 4), top_bc=1, num_grid
     dt = 0.5 * h1 / vmax / math.sqrt(3)
     return Case(name="gen21_%d" % seed, grids=grids, media=media, medium="gen21", dt=dt, nsteps=10,
                 radius=1, top_bc=top_bc, imode=1, src=None, rec=np.zeros((0, 3), np.float32), rec_comp=0)
+
+
+# ---------------------------------------------------------------------------
+# Tilted transversely isotropic media (rotated VTI)
+# ---------------------------------------------------------------------------
+VOIGT = [(0, 0), (1, 1), (2, 2), (1, 2), (2, 0), (0, 1)]
+
+
+def rotation(dip, azi):
+    """a = Rz(azi) Ry(dip): maps the symmetry-axis frame to the grid frame, so
+    the axis is (sin dip cos azi, sin dip sin azi, cos dip).  Arrays broadcast;
+    result (3, 3, ...)."""
+    sd, cd, sa, ca = np.sin(dip), np.cos(dip), np.sin(azi), np.cos(azi)
+    z = np.zeros_like(sd)
+    return np.array([[ca * cd, -sa + z, ca * sd], [sa * cd, ca + z, sa * sd], [-sd, z, cd]])
+
+
+def bond_matrix(a):
+    """Bond stress matrix M of a rotation a (3, 3, ...): C' = M C M^T for Voigt
+    stiffness with engineering shear strains (Auld, Acoustic Fields and Waves
+    in Solids, ch. 3)."""
+    M = np.zeros((6, 6) + a.shape[2:])
+    for I, (i, j) in enumerate(VOIGT):
+        for J, (k, l) in enumerate(VOIGT):
+            M[I, J] = a[i, k] * a[j, k] if J < 3 else a[i, k] * a[j, l] + a[i, l] * a[j, k]
+    return M
+
+
+def vti_stiffness(vp, vs, rho, eps, delta, gamma):
+    """Voigt stiffness (6, 6, ...) of a VTI medium from Thomsen's parameters
+    (Thomsen 1986), float64."""
+    vp, vs, rho = (np.asarray(v, dtype=np.float64) for v in (vp, vs, rho))
+    c33, c44 = rho * vp * vp, rho * vs * vs
+    c11, c66 = c33 * (1 + 2 * eps), c44 * (1 + 2 * gamma)
+    c13 = np.sqrt((c33 - c44) * (c33 * (1 + 2 * delta) - c44)) - c44
+    C = np.zeros((6, 6) + c33.shape)
+    C[0, 0] = C[1, 1] = c11
+    C[2, 2] = c33
+    C[0, 1] = C[1, 0] = c11 - 2 * c66
+    C[0, 2] = C[2, 0] = C[1, 2] = C[2, 1] = c13
+    C[3, 3] = C[4, 4] = c44
+    C[5, 5] = c66
+    return C
+
+
+def tti_stiffness(vp, vs, rho, dip, azi, thomsen):
+    """Node stiffness (6, 6, ...) of a tilted VTI medium: vti_stiffness rotated
+    by rotation(dip, azi) with the Bond matrix."""
+    C = vti_stiffness(vp, vs, rho, *thomsen)
+    M = bond_matrix(rotation(np.asarray(dip, np.float64), np.asarray(azi, np.float64)))
+    return np.einsum("ik...,kl...,jl...->ij...", M, C, M)
+
+
+def tti_as_gen21(case):
+    """The same case with its TTI node medium turned into the 21 staggered slot
+    arrays on the host (the oracle's input form), float64 buoyancy."""
+    import copy
+    out = copy.copy(case)
+    out.media = []
+    for m in case.media:
+        C = tti_stiffness(m["vp"], m["vs"], m["rho"], m["dip"], m["azi"], case.thomsen)
+        c21 = cij_to_positions(C)
+        out.media.append({"buoy": 1.0 / m["rho"].astype(np.float64), "c21": c21, "c9": ortho9_from_cij21(c21)})
+    out.medium = "gen21"
+    return out
+
+
+def random_case_tti(seed, ratio=2, nx2=6, ny2=5, nz=(5, 4), top_bc=1, num_grids=2, h1=10.0,
+                    thomsen=(0.10, 0.05, 0.08)):
+    """Small heterogeneous TTI composite: random node vp, vs, rho, dip (0..30 deg)
+    and azimuth."""
+    rng = np.random.default_rng(seed)
+    grids = []
+    nx, ny = nx2 * ratio ** (num_grids - 1), ny2 * ratio ** (num_grids - 1)
+    h = h1
+    for g in range(num_grids):
+        grids.append({"n": (nx, ny, nz[g]), "h": (h, h, h)})
+        nx //= ratio
+        ny //= ratio
+        h *= ratio
+    media = []
+    vmax = 0.0
+    for g in grids:
+        nxg, nyg, nzg = g["n"]
+        shp = (nzg + 1, nyg + 1, nxg + 1)
+        vs = rng.uniform(1.0, 1.6, shp).astype(np.float32)
+        vp = (vs * rng.uniform(1.7, 2.0, shp)).astype(np.float32)
+        media.append({"vp": vp, "vs": vs, "rho": rng.uniform(1.8, 2.6, shp).astype(np.float32),
+                      "dip": rng.uniform(0, math.radians(30), shp).astype(np.float32),
+                      "azi": rng.uniform(-math.pi, math.pi, shp).astype(np.float32)})
+        vmax = max(vmax, float(vp.max()) * math.sqrt(1 + 2 * thomsen[0]))
+    dt = 0.5 * h1 / vmax / math.sqrt(3)
+    case = Case(name="tti_%d" % seed, grids=grids, media=media, medium="tti", dt=dt, nsteps=10,
+                radius=1, top_bc=top_bc, imode=1, src=None, rec=np.zeros((0, 3), np.float32), rec_comp=0)
+    case.thomsen = tuple(thomsen)
+    return case

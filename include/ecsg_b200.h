@@ -46,7 +46,7 @@ enum { ECSG_MEDIUM_ISO = 0, ECSG_MEDIUM_ORTHO9 = 1, ECSG_MEDIUM_GEN21 = 2 };   /
 enum { ECSG_MODE_II = 0, ECSG_MODE_ECI = 1 };            /* interface mode (main.cpp:54) */
 
 /* Device status bits (ecsg_get_status). */
-enum { ECSG_ST_JACOBI_CAP = 1, ECSG_ST_BARRIER_TIMEOUT = 2, ECSG_ST_NONFINITE = 4 };
+enum { ECSG_ST_JACOBI_CAP = 1, ECSG_ST_BARRIER_TIMEOUT = 2, ECSG_ST_NONFINITE = 4, ECSG_ST_PIPE_TIMEOUT = 8 };
 
 /* One uniform sub-grid: Grid (grid.hpp:6-11) without the name.  size[] are
  * cell counts (points - 1), step[] the spacings.  z origins are stacked as
@@ -108,6 +108,16 @@ int ecsg_set_medium_ortho9(ecsg_sim *sim, int g, const double *buoy, const doubl
  * update also accumulates strains so that ecsg_energy can return
  * 1/2 (rho v, v') + 1/2 (eps, sigma). */
 int ecsg_set_medium_cij21(ecsg_sim *sim, int g, const double *buoy, const double *const c[21]);
+/* Tilted transversely isotropic medium built on the device into the 21-Cij
+ * slots (no counterpart in the reference).  Node-layout float arrays (R = 0,
+ * like ecsg_set_medium_iso): vp, vs (vs < vp), rho, the tilt of the symmetry
+ * axis from vertical (dip) and its azimuth from x, both in radians; Thomsen's
+ * epsilon, delta, gamma for the whole grid.  Buoyancy = 1/rho at the nodes;
+ * each Cij is rotated with the Bond matrix at the nodes and averaged to its
+ * slot position with the 2/4/8-point means of ReshapeField
+ * (field.cpp:428-476). */
+int ecsg_set_medium_tti(ecsg_sim *sim, int g, const float *vp, const float *vs, const float *rho, const float *dip,
+                        const float *azimuth, double epsilon, double delta, double gamma);
 
 /* Field component k of grid g in Field layout (radius R of ecsg_config), in
  * double (Field::GetPtr1 of the reference, field.hpp:84-85). */

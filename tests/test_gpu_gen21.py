@@ -13,7 +13,7 @@ import numpy as np
 import pytest
 
 from ecsg_b200 import Simulation
-from ecsg_b200.workloads import ortho9_from_cij21, random_case_gen21, ricker
+from ecsg_b200.workloads import ortho9_from_cij21, random_case_gen21, random_case_tti, ricker, tti_as_gen21
 from oracle.oracle import OracleRun
 
 pytestmark = pytest.mark.gpu
@@ -159,3 +159,61 @@ def test_energy_conserved_after_source(ratio, top_bc, prec, tol):
     e = out["energy"][100::10]   # the source acts during the first 60 steps
     drift = (e.max() - e.min()) / np.abs(e).mean()
     assert np.isfinite(e).all() and drift < tol, drift
+
+
+@pytest.mark.parametrize("ratio", [2, 3])
+def test_device_tti_medium_matches_host_slots(ratio):
+    """ecsg_set_medium_tti (rotation and averaging on the device) against the
+    same medium rotated and averaged on the host (ecsg_set_medium_cij21), and
+    the FP32 run against the oracle on the host slots."""
+    case = _with_src_rec(random_case_tti(7 + ratio, ratio=ratio, nx2=9, ny2=8, nz=(8, 6)))
+    host = tti_as_gen21(case)
+    runs = []
+    for cs in (case, host):
+        with Simulation(cs, precision="f64") as s:
+            r = s.run(60, graph=False)
+            runs.append((r["rec"], [s.field(g, k) for g in range(2) for k in range(9)]))
+    assert np.abs(runs[0][0] - runs[1][0]).max() <= 1e-6 * np.abs(runs[1][0]).max()
+    for a, b in zip(runs[0][1], runs[1][1]):
+        assert np.abs(a - b).max() <= 1e-11 * max(np.abs(b).max(), 1e-300)
+    ref = OracleRun(host).run(60)
+    with Simulation(case, precision="f32") as s:
+        out = s.run(60)
+    rel = np.linalg.norm(out["rec"] - ref["rec"], axis=1) / np.linalg.norm(ref["rec"], axis=1)
+    assert rel.max() < 1e-5, rel
+
+
+@pytest.mark.parametrize("energy", [True, False])
+@pytest.mark.parametrize("ratio,top_bc,nx2,ny2,nz", [(3, 1, 45, 11, (60, 30)), (2, 0, 67, 9, (20, 50)),
+                                                    (2, 1, 64, 16, (49, 24))])
+def test_tma_sweep_equals_scalar_sweep(monkeypatch, ratio, top_bc, nx2, ny2, nz, energy):
+    """The FP32 TMA-staged sweep (stress21_tma.cu) against the plain FP32 sweep
+    (stress21.cu, selected by ECSG_SCALAR_STENCILS=1): bitwise equal fields,
+    traces and energies, on ragged tiles (x not a multiple of 32, y not of 8),
+    several z-chunks per column, with and without the free surface and the
+    strain accumulators."""
+    case = _with_src_rec(random_case_tti(70 + ratio + top_bc, ratio=ratio, nx2=nx2, ny2=ny2, nz=nz, top_bc=top_bc))
+    from ecsg_b200 import SIM_POS, field_shape
+    outs, ops = [], []
+    for scalar in ("1", "0"):
+        monkeypatch.setenv("ECSG_SCALAR_STENCILS", scalar)
+        rng = np.random.default_rng(nx2)
+        with Simulation(case, precision="f32", energy=energy) as s:
+            for g in range(2):
+                for k in range(9):
+                    s.set_field(g, k, rng.standard_normal(field_shape(case.grids[g]["n"], SIM_POS[k], 1)))
+            for g in range(2):
+                s.update_stress(g)
+            ops.append([s.field(g, k) for g in range(2) for k in range(9)])
+        with Simulation(case, precision="f32", energy=energy) as s:
+            r = s.run(30, energy_every=3 if energy else 0, graph=False)
+            outs.append((r, [s.field(g, k) for g in range(2) for k in range(9)], s.status()))
+    for a, b in zip(*ops):
+        assert np.array_equal(a, b)
+    (ra, fa, sa), (rb, fb, sb) = outs
+    assert sa == 0 and sb == 0
+    assert np.array_equal(ra["rec"], rb["rec"])
+    if energy:
+        assert np.array_equal(ra["energy"], rb["energy"], equal_nan=True)
+    for a, b in zip(fa, fb):
+        assert np.array_equal(a, b)

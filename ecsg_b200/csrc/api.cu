@@ -93,6 +93,10 @@ struct ecsg_sim {
     size_t tsize = 4;
     Geo geo[kMaxGrids];
     double h[kMaxGrids][3];
+    // Per grid, the 9 fields, the stiffness slots and the strain accumulators
+    // each live in one allocation (fields of a group at a fixed stride), so
+    // that one tensor map can address a whole group.
+    void *fblk[kMaxGrids] = {}, *cblk[kMaxGrids] = {}, *epsblk[kMaxGrids] = {};
     void *f[kMaxGrids][9] = {};
     void *b[kMaxGrids] = {};
     void *c[kMaxGrids][21] = {};
@@ -261,19 +265,24 @@ int ecsg_create(const ecsg_grid_desc *grids, const ecsg_config *cfg, ecsg_sim **
         s->itf[i].r = r;
     }
     int rc;
+    // 21-Cij slots in memory order: the 12 read around a tile (c6..c14, c16,
+    // c17, c19) first, then the other 9 (c0..c5, c15, c18, c20)
+    static const int kGen21Phys[21] = {12, 13, 14, 15, 16, 17, 0, 1, 2, 3, 4, 5, 6, 7, 8, 18, 9, 10, 19, 11, 20};
     for (int g = 0; g < s->ng; g++) {
         const size_t fb = (size_t)s->geo[g].size() * s->tsize;
-        for (int k = 0; k < 9; k++)
-            if ((rc = dmalloc(s, &s->f[g][k], fb))) return bail(rc);
+        if ((rc = dmalloc(s, &s->fblk[g], 9 * fb))) return bail(rc);
+        for (int k = 0; k < 9; k++) s->f[g][k] = (char *)s->fblk[g] + k * fb;
         if ((rc = dmalloc(s, &s->b[g], fb))) return bail(rc);
+        if ((rc = dmalloc(s, &s->cblk[g], s->nc * fb))) return bail(rc);
         for (int k = 0; k < s->nc; k++)
-            if ((rc = dmalloc(s, &s->c[g][k], fb))) return bail(rc);
+            s->c[g][k] = (char *)s->cblk[g] + (s->medium == ECSG_MEDIUM_GEN21 ? kGen21Phys[k] : k) * fb;
         if (s->energy)
             for (int k = 0; k < 3; k++)
                 if ((rc = dmalloc(s, &s->vc[g][k], fb))) return bail(rc);
-        if (s->energy && s->medium == ECSG_MEDIUM_GEN21)
-            for (int k = 0; k < 6; k++)
-                if ((rc = dmalloc(s, &s->eps[g][k], fb))) return bail(rc);
+        if (s->energy && s->medium == ECSG_MEDIUM_GEN21) {
+            if ((rc = dmalloc(s, &s->epsblk[g], 6 * fb))) return bail(rc);
+            for (int k = 0; k < 6; k++) s->eps[g][k] = (char *)s->epsblk[g] + k * fb;
+        }
     }
     s->red_blocks = 4 * s->sms;
     if ((rc = dmalloc(s, (void **)&s->partial, sizeof(double) * 12 * (size_t)s->red_blocks))) return bail(rc);
@@ -304,11 +313,11 @@ int ecsg_destroy(ecsg_sim *s)
     if (!s) return ECSG_OK;
     if (s->st) cudaStreamSynchronize(s->st);
     for (int g = 0; g < kMaxGrids; g++) {
-        for (int k = 0; k < 9; k++) cudaFree(s->f[g][k]);
+        cudaFree(s->fblk[g]);
         cudaFree(s->b[g]);
-        for (int k = 0; k < 21; k++) cudaFree(s->c[g][k]);
+        cudaFree(s->cblk[g]);
         for (int k = 0; k < 3; k++) cudaFree(s->vc[g][k]);
-        for (int k = 0; k < 6; k++) cudaFree(s->eps[g][k]);
+        cudaFree(s->epsblk[g]);
         Iface &I = s->itf[g];
         cudaFree(I.A); cudaFree(I.B); cudaFree(I.X0); cudaFree(I.X1); cudaFree(I.partial); cudaFree(I.vzc);
     }

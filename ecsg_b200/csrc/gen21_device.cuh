@@ -7,6 +7,13 @@
 
 namespace ecsg {
 
+// a*b + c: one rounding in FP32 (both FP32 sweeps use the same contractions,
+// so they stay bitwise equal to each other); in FP64 the product and the sum
+// are rounded separately, the oracle's operation order (the sum is
+// commutative, so fma_(a, b, c) == add_(c, mul_(a, b)) bit for bit).
+__device__ __forceinline__ float fma_(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fma_(double a, double b, double c) { return add_(mul_(a, b), c); }
+
 struct Ext {
     int nx, ny, nz;
     __device__ __forceinline__ bool n(int x, int y, int z) const { return x >= 0 && x <= nx - 1 && y >= 0 && y <= ny && z >= 0 && z <= nz; }
@@ -26,19 +33,19 @@ template <typename T>
 __device__ __forceinline__ T e4_at(const GridDev<T> &G, int p)
 {
     const int sy = G.g.px, sz = G.g.px * G.g.py;
-    return add_(mul_(G.k[2], sub_(G.f[VY][p + sz], G.f[VY][p])), mul_(G.k[1], sub_(G.f[VZ][p + sy], G.f[VZ][p])));
+    return fma_(G.k[1], sub_(G.f[VZ][p + sy], G.f[VZ][p]), mul_(G.k[2], sub_(G.f[VY][p + sz], G.f[VY][p])));
 }
 template <typename T>
 __device__ __forceinline__ T e5_at(const GridDev<T> &G, int p)
 {
     const int sz = G.g.px * G.g.py;
-    return add_(mul_(G.k[2], sub_(G.f[VX][p + sz], G.f[VX][p])), mul_(G.k[0], sub_(G.f[VZ][p], G.f[VZ][p - 1])));
+    return fma_(G.k[0], sub_(G.f[VZ][p], G.f[VZ][p - 1]), mul_(G.k[2], sub_(G.f[VX][p + sz], G.f[VX][p])));
 }
 template <typename T>
 __device__ __forceinline__ T e6_at(const GridDev<T> &G, int p)
 {
     const int sy = G.g.px;
-    return add_(mul_(G.k[1], sub_(G.f[VX][p + sy], G.f[VX][p])), mul_(G.k[0], sub_(G.f[VY][p], G.f[VY][p - 1])));
+    return fma_(G.k[0], sub_(G.f[VY][p], G.f[VY][p - 1]), mul_(G.k[1], sub_(G.f[VX][p + sy], G.f[VX][p])));
 }
 
 // 1-D closure weights of two neighbours
@@ -64,7 +71,7 @@ __device__ __forceinline__ T avg4(const T (&v)[2][2], const bool (&ok0)[2], cons
 #pragma unroll
         for (int j = 0; j < 2; j++) {
             const T w = mul_(w0[i], w1[j]);
-            if (w != T(0)) acc = add_(acc, mul_(w, v[i][j]));
+            if (w != T(0)) acc = fma_(w, v[i][j], acc);
         }
     return acc;
 }
@@ -121,17 +128,17 @@ __device__ __forceinline__ double gen21_szz_extra(const GridDev<T> &G, int x, in
 {
     const Ext E{G.g.nx, G.g.ny, G.g.nz};
     const int p = G.g.idx(x, y, z);
-    return (double)add_(add_(mul_(G.c[12][p], abar4_g(G, E, x, y, z)), mul_(G.c[13][p], abar5_g(G, E, x, y, z))),
-                        mul_(G.c[14][p], abar6_g(G, E, x, y, z)));
+    return (double)fma_(G.c[14][p], abar6_g(G, E, x, y, z),
+                        fma_(G.c[13][p], abar5_g(G, E, x, y, z), mul_(G.c[12][p], abar4_g(G, E, x, y, z))));
 }
 
 template <typename T>
 __device__ __forceinline__ T e3_used(const GridDev<T> &G, const Ext &E, bool surf, int x, int y, int z, int p, T e1, T e2)
 {
     if (!surf) return e3_at(G, p);
-    T num = add_(add_(add_(add_(mul_(G.c[2][p], e1), mul_(G.c[4][p], e2)), mul_(G.c[12][p], abar4_g(G, E, x, y, z))),
-                      mul_(G.c[13][p], abar5_g(G, E, x, y, z))),
-                 mul_(G.c[14][p], abar6_g(G, E, x, y, z)));
+    T num = fma_(G.c[14][p], abar6_g(G, E, x, y, z),
+                 fma_(G.c[13][p], abar5_g(G, E, x, y, z),
+                      fma_(G.c[12][p], abar4_g(G, E, x, y, z), fma_(G.c[4][p], e2, mul_(G.c[2][p], e1)))));
     return -div_(num, G.c[5][p]);
 }
 

@@ -95,9 +95,9 @@ __global__ void __launch_bounds__(S21<T>::TX *S21<T>::TY) stress21_kernel(GridDe
                 const int pp = g.idx(x, y, p);
                 const T e1 = e1_at(G, pp), e2 = e2_at(G, pp);
                 const T e3 = e3_used(G, E, flag && p == 0, x, y, p, pp, e1, e2);
-                p4 = add_(add_(mul_(c[6][pp], e1), mul_(c[9][pp], e2)), mul_(c[12][pp], e3));
-                p5 = add_(add_(mul_(c[7][pp], e1), mul_(c[10][pp], e2)), mul_(c[13][pp], e3));
-                p6 = add_(add_(mul_(c[8][pp], e1), mul_(c[11][pp], e2)), mul_(c[14][pp], e3));
+                p4 = fma_(c[12][pp], e3, fma_(c[9][pp], e2, mul_(c[6][pp], e1)));
+                p5 = fma_(c[13][pp], e3, fma_(c[10][pp], e2, mul_(c[7][pp], e1)));
+                p6 = fma_(c[14][pp], e3, fma_(c[11][pp], e2, mul_(c[8][pp], e1)));
             }
             R(s, Q_P4, hx, hy) = p4;
             R(s, Q_P5, hx, hy) = p5;
@@ -131,10 +131,10 @@ __global__ void __launch_bounds__(S21<T>::TX *S21<T>::TY) stress21_kernel(GridDe
                 T d[3];
 #pragma unroll
                 for (int r = 0; r < 3; r++)
-                    d[r] = add_(add_(add_(add_(add_(mul_(c[rowc[r][0]][pp], e1), mul_(c[rowc[r][1]][pp], e2)), mul_(c[rowc[r][2]][pp], e3)),
-                                          mul_(c[6 + 3 * r][pp], a4)),
-                                     mul_(c[7 + 3 * r][pp], a5)),
-                                mul_(c[8 + 3 * r][pp], a6));
+                    d[r] = fma_(c[8 + 3 * r][pp], a6,
+                                fma_(c[7 + 3 * r][pp], a5,
+                                     fma_(c[6 + 3 * r][pp], a4,
+                                          fma_(c[rowc[r][2]][pp], e3, fma_(c[rowc[r][1]][pp], e2, mul_(c[rowc[r][0]][pp], e1))))));
                 sxx[pp] = add_(sxx[pp], d[0]);
                 syy[pp] = add_(syy[pp], d[1]);
                 if (!surf) szz[pp] = add_(szz[pp], d[2]);
@@ -161,7 +161,7 @@ __global__ void __launch_bounds__(S21<T>::TX *S21<T>::TY) stress21_kernel(GridDe
                 for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++) v[i][j] = R(s, Q_P6, hx - 1 + i, hy + j);
                 const T t6 = avg4<T>(v, a, b);
                 const T e6 = R(s, Q_E6, hx, hy);
-                const T dd = add_(add_(add_(mul_(c[20][pp], e6), t46), t56), t6);
+                const T dd = add_(add_(fma_(c[20][pp], e6, t46), t56), t6);
                 sxy[pp] = add_(sxy[pp], dd);
                 if (ACC) eps5[pp] = add_(eps5[pp], e6);
             }
@@ -185,7 +185,7 @@ __global__ void __launch_bounds__(S21<T>::TX *S21<T>::TY) stress21_kernel(GridDe
                 for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++) v[i][j] = R(j == 0 ? sp : s, Q_P4, hx, hy + i);
                 const T tp = avg4<T>(v, a, b);
                 const T e4 = R(sp, Q_E4, hx, hy);
-                const T dd = add_(add_(add_(mul_(c[15][pp], e4), mul_(c[16][pp], t5)), mul_(c[17][pp], t6)), tp);
+                const T dd = add_(fma_(c[17][pp], t6, fma_(c[16][pp], t5, mul_(c[15][pp], e4))), tp);
                 const T nv = add_(syz[pp], dd);
                 syz[pp] = nv;
                 if (flag && pm == 0) syz[pp - sz] = -nv;
@@ -208,7 +208,7 @@ __global__ void __launch_bounds__(S21<T>::TX *S21<T>::TY) stress21_kernel(GridDe
                 for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++) v[i][j] = R(j == 0 ? sp : s, Q_P5, hx - 1 + i, hy);
                 const T tp = avg4<T>(v, a, b);
                 const T e5 = R(sp, Q_E5, hx, hy);
-                const T dd = add_(add_(add_(mul_(c[18][pp], e5), mul_(c[19][pp], t6)), t45), tp);
+                const T dd = add_(add_(fma_(c[19][pp], t6, mul_(c[18][pp], e5)), t45), tp);
                 const T nv = add_(sxz[pp], dd);
                 sxz[pp] = nv;
                 if (flag && pm == 0 && ox >= 1 && ox <= nx - 1 && oy >= 1 && oy <= ny - 1) sxz[pp - sz] = -nv;

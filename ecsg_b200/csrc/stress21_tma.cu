@@ -1,15 +1,20 @@
 // stress21_tma.cu -- FP32 21-Cij stress update with TMA-staged planes.
 //
-// The same update as stress21.cu (same operation order, so the results are
-// bitwise equal to it), organised for bandwidth: a CTA owns a 32 x 8 tile of
+// The same update as stress21.cu (same operation order and contractions, so
+// the results are bitwise equal to its FP32 instantiation), organised for
+// bandwidth: a CTA owns a 32 x 8 tile of
 // (x, y) points and marches z.  One producer thread streams, per plane,
 //   * the 12 coefficient slots read around the tile (c6..c14, c16, c17, c19)
 //     and the three velocities as 40 x 10 boxes (tile, one-point halo, the x
 //     start rounded down to a 16-byte boundary),
 //   * the other 9 coefficient slots, the 6 stresses and (energy runs) the 6
 //     strain accumulators as 32 x 8 boxes,
-// into shared-memory rings with cp.async.bulk.tensor (3-D tiled TMA, no
-// multicast), completion tracked by mbarriers.  Eight consumer warps compute
+// into shared-memory rings with cp.async.bulk.tensor (no multicast),
+// completion tracked by mbarriers.  Each group of fields (velocities, the 12
+// haloed slots, the 9 other slots, stresses, strains) is one allocation with
+// its fields at a fixed stride, so one 4-D tensor map (x, y, z, field) moves
+// a whole group: 5 copies per plane instead of 36 (small boxes from many
+// descriptors kept the copy engine, not HBM, the limit).  Eight consumer warps compute
 // every strain / link product of their own point plus one halo row or column
 // of one kind per warp (each kind needs a one-sided halo only), exchange them
 // through a two-plane ring, and update the stresses.  Velocities stay resident
@@ -33,12 +38,12 @@ constexpr int HX = 34, HYI = 10, HP = HX * HYI;   // intermediates: x0-1 .. x0+3
 constexpr int NQ = 9;
 constexpr int NSP = 3, NSV = 5;               // ring depths: plane data, velocities
 constexpr int HBOX = BW * BH * 4;             // 1600 bytes
-constexpr int HBOX_A = 1664;                  // 128-byte aligned stride
 constexpr int IBOX = TX * TY * 4;             // 1024 bytes
 constexpr int NCH = 12, NCI = 9;
-constexpr int P_CH = 0, P_CI = NCH * HBOX_A, P_SG = P_CI + NCI * IBOX, P_EP = P_SG + 6 * IBOX;
-constexpr int PSLOT = P_EP + 6 * IBOX;        // 41472
-constexpr int VSLOT = 3 * HBOX_A;             // 4992
+constexpr int P_CH = 0, P_CI = NCH * HBOX, P_SG = P_CI + NCI * IBOX, P_EP = P_SG + 6 * IBOX;
+constexpr int PSLOT = P_EP + 6 * IBOX;        // 40704, a multiple of 128
+constexpr int VSLOT = (3 * HBOX + 127) / 128 * 128;   // 4864
+static_assert(P_CI % 128 == 0 && P_SG % 128 == 0 && P_EP % 128 == 0 && PSLOT % 128 == 0, "128-byte aligned boxes");
 constexpr int OFF_V = NSP * PSLOT;
 constexpr int OFF_IM = OFF_V + NSV * VSLOT;
 constexpr int OFF_BAR = OFF_IM + 2 * NQ * HP * 4;
@@ -52,11 +57,11 @@ __host__ __device__ constexpr int ci_slot(int k) { return k < 6 ? k : (k == 6 ? 
 } // namespace s21t
 
 struct S21Maps {
-    CUtensorMap v[3];     // vx vy vz, haloed box
-    CUtensorMap ch[12];   // haloed coefficient boxes
-    CUtensorMap ci[9];    // interior coefficient boxes
-    CUtensorMap sg[6];    // stresses sxx syy szz syz sxz sxy
-    CUtensorMap ep[6];    // strain accumulators
+    CUtensorMap v;    // vx vy vz: haloed boxes
+    CUtensorMap ch;   // c6..c14, c16, c17, c19: haloed boxes
+    CUtensorMap ci;   // c0..c5, c15, c18, c20: interior boxes
+    CUtensorMap sg;   // sxx syy szz syz sxz sxy: interior boxes
+    CUtensorMap ep;   // strain accumulators: interior boxes
 };
 
 __device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
@@ -91,10 +96,11 @@ __device__ __forceinline__ bool mbar_wait(unsigned a, unsigned parity)
     }
     return false;
 }
-__device__ __forceinline__ void tma_load3(unsigned dst, const CUtensorMap *map, int x, int y, int z, unsigned bar)
+// one box of every field of a group: coordinates (x, y, z, first field)
+__device__ __forceinline__ void tma_load4(unsigned dst, const CUtensorMap *map, int x, int y, int z, unsigned bar)
 {
-    asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
-                 ::"r"(dst), "l"((unsigned long long)map), "r"(x), "r"(y), "r"(z), "r"(bar)
+    asm volatile("cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5}], [%6];"
+                 ::"r"(dst), "l"((unsigned long long)map), "r"(x), "r"(y), "r"(z), "r"(0), "r"(bar)
                  : "memory");
 }
 __device__ __forceinline__ void consumer_sync() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
@@ -144,7 +150,7 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
                 const unsigned dst = smem_u32(sm + OFF_V + s * VSLOT);
                 mbar_expect_tx(fullV(s), 3 * HBOX);
                 const int zc = g.R + qstart - 1 + j;
-                for (int c = 0; c < 3; c++) tma_load3(dst + c * HBOX_A, &maps.v[c], hx0, hy0, zc, fullV(s));
+                tma_load4(dst, &maps.v, hx0, hy0, zc, fullV(s));
                 return true;
             };
             auto issueP = [&](int i) -> bool {
@@ -155,12 +161,11 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
                 const unsigned dst = smem_u32(sm + s * PSLOT);
                 mbar_expect_tx(fullP(s), NCH * HBOX + (inner ? (NCI + 6 + (ACC ? 6 : 0)) * IBOX : 0));
                 const int zc = g.R + q;
-                for (int k = 0; k < NCH; k++) tma_load3(dst + P_CH + k * HBOX_A, &maps.ch[k], hx0, hy0, zc, fullP(s));
+                tma_load4(dst + P_CH, &maps.ch, hx0, hy0, zc, fullP(s));
                 if (inner) {
-                    for (int k = 0; k < NCI; k++) tma_load3(dst + P_CI + k * IBOX, &maps.ci[k], ix0, iy0, zc, fullP(s));
-                    for (int k = 0; k < 6; k++) tma_load3(dst + P_SG + k * IBOX, &maps.sg[k], ix0, iy0, zc, fullP(s));
-                    if (ACC)
-                        for (int k = 0; k < 6; k++) tma_load3(dst + P_EP + k * IBOX, &maps.ep[k], ix0, iy0, zc, fullP(s));
+                    tma_load4(dst + P_CI, &maps.ci, ix0, iy0, zc, fullP(s));
+                    tma_load4(dst + P_SG, &maps.sg, ix0, iy0, zc, fullP(s));
+                    if (ACC) tma_load4(dst + P_EP, &maps.ep, ix0, iy0, zc, fullP(s));
                 }
                 return true;
             };
@@ -233,7 +238,7 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
             const float *Vm = (const float *)(sm + OFF_V + (i % NSV) * VSLOT);
             const float *Vp = (const float *)(sm + OFF_V + ((i + 1) % NSV) * VSLOT);
             const float *Vn = (const float *)(sm + OFF_V + ((i + 2) % NSV) * VSLOT);
-            constexpr int HS = HBOX_A / 4;   // floats between staged boxes
+            constexpr int HS = HBOX / 4;   // floats between the haloed boxes of a group
             constexpr int IS = IBOX / 4;
             float *IMs = IM + (p & 1) * NQ * HP;
             const float *Rs = IM + (p & 1) * NQ * HP;          // plane p
@@ -251,7 +256,7 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
                 auto av = [&](const float (&v)[2][2], const bool (&a)[2], const bool (&b)[2]) -> float {
                     if (FAST) {
                         const float w = 0.25f;
-                        return add_(add_(add_(add_(0.f, mul_(w, v[0][0])), mul_(w, v[0][1])), mul_(w, v[1][0])), mul_(w, v[1][1]));
+                        return fma_(w, v[1][1], fma_(w, v[1][0], fma_(w, v[0][1], fma_(w, v[0][0], 0.f))));
                     }
                     return avg4<float>(v, a, b);
                 };
@@ -261,15 +266,15 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
                 {
                     float e4 = 0.f, q45 = 0.f, q46 = 0.f, e5 = 0.f, q56 = 0.f, e6 = 0.f, p4 = 0.f, p5 = 0.f, p6 = 0.f;
                     if (FAST || E.l4(ox, oy, p)) {
-                        e4 = add_(mul_(k2, sub_(Vn[HS + vb], Vp[HS + vb])), mul_(k1, sub_(Vp[2 * HS + vb + BW], Vp[2 * HS + vb])));
+                        e4 = fma_(k1, sub_(Vp[2 * HS + vb + BW], Vp[2 * HS + vb]), mul_(k2, sub_(Vn[HS + vb], Vp[HS + vb])));
                         q45 = mul_(chv(9, vb), e4);
                         q46 = mul_(chv(10, vb), e4);
                     }
                     if (FAST || E.l5(ox, oy, p)) {
-                        e5 = add_(mul_(k2, sub_(Vn[vb], Vp[vb])), mul_(k0, sub_(Vp[2 * HS + vb], Vp[2 * HS + vb - 1])));
+                        e5 = fma_(k0, sub_(Vp[2 * HS + vb], Vp[2 * HS + vb - 1]), mul_(k2, sub_(Vn[vb], Vp[vb])));
                         q56 = mul_(chv(11, vb), e5);
                     }
-                    if (FAST || E.l6(ox, oy, p)) e6 = add_(mul_(k1, sub_(Vp[vb + BW], Vp[vb])), mul_(k0, sub_(Vp[HS + vb], Vp[HS + vb - 1])));
+                    if (FAST || E.l6(ox, oy, p)) e6 = fma_(k0, sub_(Vp[HS + vb], Vp[HS + vb - 1]), mul_(k1, sub_(Vp[vb + BW], Vp[vb])));
                     if (FAST || E.n(ox, oy, p)) {
                         e1 = mul_(k0, sub_(Vp[vb + 1], Vp[vb]));
                         e2 = mul_(k1, sub_(Vp[HS + vb], Vp[HS + vb - BW]));
@@ -277,9 +282,9 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
                             e3 = e3_used(G, E, true, ox, oy, p, pbase + p * sz, e1, e2);
                         else
                             e3 = mul_(k2, sub_(Vp[2 * HS + vb], Vm[2 * HS + vb]));
-                        p4 = add_(add_(mul_(chv(0, vb), e1), mul_(chv(3, vb), e2)), mul_(chv(6, vb), e3));
-                        p5 = add_(add_(mul_(chv(1, vb), e1), mul_(chv(4, vb), e2)), mul_(chv(7, vb), e3));
-                        p6 = add_(add_(mul_(chv(2, vb), e1), mul_(chv(5, vb), e2)), mul_(chv(8, vb), e3));
+                        p4 = fma_(chv(6, vb), e3, fma_(chv(3, vb), e2, mul_(chv(0, vb), e1)));
+                        p5 = fma_(chv(7, vb), e3, fma_(chv(4, vb), e2, mul_(chv(1, vb), e1)));
+                        p6 = fma_(chv(8, vb), e3, fma_(chv(5, vb), e2, mul_(chv(2, vb), e1)));
                     }
                     const int hb = hy * HX + hx;
                     IMs[0 * HP + hb] = e4; IMs[1 * HP + hb] = q45; IMs[2 * HP + hb] = q46;
@@ -291,7 +296,7 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
                     if (hk == 0) {
                         float e4 = 0.f, q45 = 0.f, q46 = 0.f;
                         if (FAST || E.l4(x, y, p)) {
-                            e4 = add_(mul_(k2, sub_(Vn[HS + b], Vp[HS + b])), mul_(k1, sub_(Vp[2 * HS + b + BW], Vp[2 * HS + b])));
+                            e4 = fma_(k1, sub_(Vp[2 * HS + b + BW], Vp[2 * HS + b]), mul_(k2, sub_(Vn[HS + b], Vp[HS + b])));
                             q45 = mul_(chv(9, b), e4);
                             q46 = mul_(chv(10, b), e4);
                         }
@@ -299,13 +304,13 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
                     } else if (hk == 1) {
                         float e5 = 0.f, q56 = 0.f;
                         if (FAST || E.l5(x, y, p)) {
-                            e5 = add_(mul_(k2, sub_(Vn[b], Vp[b])), mul_(k0, sub_(Vp[2 * HS + b], Vp[2 * HS + b - 1])));
+                            e5 = fma_(k0, sub_(Vp[2 * HS + b], Vp[2 * HS + b - 1]), mul_(k2, sub_(Vn[b], Vp[b])));
                             q56 = mul_(chv(11, b), e5);
                         }
                         IMs[3 * HP + hhb] = e5; IMs[4 * HP + hhb] = q56;
                     } else if (hk == 2) {
                         float e6 = 0.f;
-                        if (FAST || E.l6(x, y, p)) e6 = add_(mul_(k1, sub_(Vp[b + BW], Vp[b])), mul_(k0, sub_(Vp[HS + b], Vp[HS + b - 1])));
+                        if (FAST || E.l6(x, y, p)) e6 = fma_(k0, sub_(Vp[HS + b], Vp[HS + b - 1]), mul_(k1, sub_(Vp[b + BW], Vp[b])));
                         IMs[5 * HP + hhb] = e6;
                     } else {
                         float p4 = 0.f, p5 = 0.f, p6 = 0.f;
@@ -314,9 +319,9 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
                             const float f2 = mul_(k1, sub_(Vp[HS + b], Vp[HS + b - BW]));
                             const float f3 = (!FAST && surf) ? e3_used(G, E, true, x, y, p, g.idx(x, y, p), f1, f2)
                                                              : mul_(k2, sub_(Vp[2 * HS + b], Vm[2 * HS + b]));
-                            p4 = add_(add_(mul_(chv(0, b), f1), mul_(chv(3, b), f2)), mul_(chv(6, b), f3));
-                            p5 = add_(add_(mul_(chv(1, b), f1), mul_(chv(4, b), f2)), mul_(chv(7, b), f3));
-                            p6 = add_(add_(mul_(chv(2, b), f1), mul_(chv(5, b), f2)), mul_(chv(8, b), f3));
+                            p4 = fma_(chv(6, b), f3, fma_(chv(3, b), f2, mul_(chv(0, b), f1)));
+                            p5 = fma_(chv(7, b), f3, fma_(chv(4, b), f2, mul_(chv(1, b), f1)));
+                            p6 = fma_(chv(8, b), f3, fma_(chv(5, b), f2, mul_(chv(2, b), f1)));
                         }
                         IMs[6 * HP + hhb] = p4; IMs[7 * HP + hhb] = p5; IMs[8 * HP + hhb] = p6;
                     }
@@ -342,11 +347,11 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
                         float d[3];
 #pragma unroll
                         for (int r = 0; r < 3; r++)
-                            d[r] = add_(add_(add_(add_(add_(mul_(CI[rowc[r][0] * IS + ib], e1), mul_(CI[rowc[r][1] * IS + ib], e2)),
-                                                       mul_(CI[rowc[r][2] * IS + ib], e3)),
-                                                  mul_(chv(3 * r, vb), a4)),
-                                             mul_(chv(1 + 3 * r, vb), a5)),
-                                        mul_(chv(2 + 3 * r, vb), a6));
+                            d[r] = fma_(chv(2 + 3 * r, vb), a6,
+                                        fma_(chv(1 + 3 * r, vb), a5,
+                                             fma_(chv(3 * r, vb), a4,
+                                                  fma_(CI[rowc[r][2] * IS + ib], e3,
+                                                       fma_(CI[rowc[r][1] * IS + ib], e2, mul_(CI[rowc[r][0] * IS + ib], e1))))));
                         sxx[pp] = add_(SG[0 * IS + ib], d[0]);
                         syy[pp] = add_(SG[1 * IS + ib], d[1]);
                         if (FAST || !surf) szz[pp] = add_(SG[2 * IS + ib], d[2]);
@@ -369,7 +374,7 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
                         for (int k = 0; k < 2; k++) for (int j = 0; j < 2; j++) v[k][j] = RR(1, 8, hx - 1 + k, hy + j);
                         const float t6 = av(v, a, b);
                         const float e6 = RR(1, 5, hx, hy);
-                        const float dd = add_(add_(add_(mul_(CI[8 * IS + ib], e6), t46), t56), t6);
+                        const float dd = add_(add_(fma_(CI[8 * IS + ib], e6, t46), t56), t6);
                         sxy[pp] = add_(SG[5 * IS + ib], dd);
                         if (ACC) eps5[pp] = add_(EP[5 * IS + ib], e6);
                     }
@@ -389,7 +394,7 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
                         for (int k = 0; k < 2; k++) for (int j = 0; j < 2; j++) v[k][j] = RR(j, 6, hx, hy + k);
                         const float tp = av(v, a, b);
                         const float e4 = RR(0, 0, hx, hy);
-                        const float dd = add_(add_(add_(mul_(c15p, e4), mul_(c16p, t5)), mul_(c17p, t6)), tp);
+                        const float dd = add_(fma_(c17p, t6, fma_(c16p, t5, mul_(c15p, e4))), tp);
                         const float nv = add_(s3p, dd);
                         syz[pp] = nv;
                         if (flag && pm == 0) syz[pp - sz] = -nv;
@@ -408,7 +413,7 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
                         for (int k = 0; k < 2; k++) for (int j = 0; j < 2; j++) v[k][j] = RR(j, 7, hx - 1 + k, hy);
                         const float tp = av(v, a, b);
                         const float e5 = RR(0, 3, hx, hy);
-                        const float dd = add_(add_(add_(mul_(c18p, e5), mul_(c19p, t6)), t45), tp);
+                        const float dd = add_(add_(fma_(c19p, t6, mul_(c18p, e5)), t45), tp);
                         const float nv = add_(s4p, dd);
                         sxz[pp] = nv;
                         if (flag && pm == 0 && (FAST || (ox >= 1 && ox <= nx - 1 && oy >= 1 && oy <= ny - 1))) sxz[pp - sz] = -nv;
@@ -469,24 +474,36 @@ static EncodeTiledFn encode_fn()
     return fn;
 }
 
-static bool encode(CUtensorMap *m, const Geo &g, const void *base, int bw, int bh)
+// 4-D map over `count` fields of one group: base = the group's first field,
+// the others at a stride of one field box.
+static bool encode(CUtensorMap *m, const Geo &g, const void *base, int count, int bw, int bh)
 {
     EncodeTiledFn fn = encode_fn();
     if (!fn || !base) return false;
-    const cuuint64_t dims[3] = {(cuuint64_t)g.px, (cuuint64_t)g.py, (cuuint64_t)g.pz};
-    const cuuint64_t strides[2] = {(cuuint64_t)g.px * 4, (cuuint64_t)g.px * g.py * 4};
-    const cuuint32_t box[3] = {(cuuint32_t)bw, (cuuint32_t)bh, 1};
-    const cuuint32_t es[3] = {1, 1, 1};
-    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, const_cast<void *>(base), dims, strides, box, es,
+    const cuuint64_t dims[4] = {(cuuint64_t)g.px, (cuuint64_t)g.py, (cuuint64_t)g.pz, (cuuint64_t)count};
+    const cuuint64_t strides[3] = {(cuuint64_t)g.px * 4, (cuuint64_t)g.px * g.py * 4, (cuuint64_t)g.size() * 4};
+    const cuuint32_t box[4] = {(cuuint32_t)bw, (cuuint32_t)bh, 1, (cuuint32_t)count};
+    const cuuint32_t es[4] = {1, 1, 1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, const_cast<void *>(base), dims, strides, box, es,
               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// true if ptr(k), k < count, are one field box apart
+template <typename F>
+static bool strided(const Geo &g, int count, F ptr)
+{
+    for (int k = 1; k < count; k++)
+        if (ptr(k) != ptr(0) + (size_t)k * g.size()) return false;
+    return true;
 }
 
 // Opaque storage for the maps of one grid (allocated by the caller, s21_maps_bytes()).
 size_t s21_maps_bytes() { return sizeof(S21Maps); }
 
-// Fills the maps of one grid; false if the driver entry point is missing or
-// an address / pitch is not encodable.
+// Fills the maps of one grid; false if the driver entry point is missing, a
+// group is not laid out at a fixed stride, or an address / pitch is not
+// encodable.
 bool s21_encode_maps(void *out, const GridDev<float> &G, float *const eps[6])
 {
     using namespace s21t;
@@ -494,13 +511,14 @@ bool s21_encode_maps(void *out, const GridDev<float> &G, float *const eps[6])
     memset(&M, 0, sizeof M);
     const Geo &g = G.g;
     if ((g.px * 4) % 16 != 0 || (XOFF - 4) % 4 != 0) return false;
-    bool ok = true;
-    for (int c = 0; c < 3; c++) ok = ok && encode(&M.v[c], g, G.f[c], BW, BH);
-    for (int k = 0; k < NCH; k++) ok = ok && encode(&M.ch[k], g, G.c[ch_slot(k)], BW, BH);
-    for (int k = 0; k < NCI; k++) ok = ok && encode(&M.ci[k], g, G.c[ci_slot(k)], TX, TY);
-    for (int k = 0; k < 6; k++) ok = ok && encode(&M.sg[k], g, G.f[SXX + k], TX, TY);
-    if (eps && eps[0])
-        for (int k = 0; k < 6; k++) ok = ok && encode(&M.ep[k], g, eps[k], TX, TY);
+    bool ok = strided(g, 3, [&](int k) { return (const float *)G.f[k]; }) &&
+              strided(g, NCH, [&](int k) { return G.c[ch_slot(k)]; }) &&
+              strided(g, NCI, [&](int k) { return G.c[ci_slot(k)]; }) &&
+              strided(g, 6, [&](int k) { return (const float *)G.f[SXX + k]; });
+    ok = ok && encode(&M.v, g, G.f[0], 3, BW, BH) && encode(&M.ch, g, G.c[ch_slot(0)], NCH, BW, BH) &&
+         encode(&M.ci, g, G.c[ci_slot(0)], NCI, TX, TY) && encode(&M.sg, g, G.f[SXX], 6, TX, TY);
+    if (ok && eps && eps[0])
+        ok = strided(g, 6, [&](int k) { return (const float *)eps[k]; }) && encode(&M.ep, g, eps[0], 6, TX, TY);
     if (ok) memcpy(out, &M, sizeof M);
     return ok;
 }

@@ -149,7 +149,9 @@ def main():
     ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--small", action="store_true", help="1/27-volume case (profiling)")
+    ap.add_argument("--small", action="store_true", help="1/27-volume case (profiling); same as --size small")
+    ap.add_argument("--size", default="full", choices=["full", "medium", "small"],
+                    help="medium: 541x541x61 / 181x181x55 / 61x61x35 (2.9 GB, for ncu captures)")
     ap.add_argument("--energy-every", type=int, default=100)
     ap.add_argument("--medium", default="tti", choices=["tti", "iso"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -171,8 +173,10 @@ def main():
         pg = dist
 
     grids = THREE_GRID
-    if args.small:
+    if args.small or args.size == "small":
         grids = [((360, 360, 40), 5.0), ((120, 120, 54), 15.0), ((40, 40, 34), 45.0)]
+    elif args.size == "medium":
+        grids = [((540, 540, 60), 5.0), ((180, 180, 54), 15.0), ((60, 60, 34), 45.0)]
     medium = args.medium
     case = three_grid_case(seed=0, grids=grids, nsteps=args.steps, medium=medium)
     pts = case.points()
@@ -234,18 +238,21 @@ def main():
     cells0 = (n0[0] + 1) * (n0[1] + 1) * (n0[2] + 1)
     st_ms, ve_ms = kt["stress"][0], kt["vel"][0]
     if st_ms >= ve_ms:
-        kname = "stress21_kernel<float,%s>" % ("true" if acc else "false") if medium == "tti" else "stress_kernel_v4<ISO5>"
+        kname = "stress21_tma_kernel<%s>" % ("true" if acc else "false") if medium == "tti" else "stress_kernel_v4<ISO5>"
         dom, dom_ms, dom_bytes = kname + " (grid 0)", st_ms, (STRESS_BYTES[medium] + acc) * cells0
     else:
         dom, dom_ms, dom_bytes = "vel_kernel_v4 (grid 0)", ve_ms, VEL_BYTES * cells0
     achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
     step_ms = run_ms / args.steps
     step_gbs = (BYTES_PER_CELL[medium] + acc) * pts / (step_ms * 1e-3) / 1e9
+    # DRAM bytes per cell of the dominant kernel from an ncu capture of the
+    # medium case (profiles/traffic.json), scaled to this launch's cells
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         try:
-            traffic = json.load(open(tpath)).get(dom.split(" ")[0])
+            per_cell = json.load(open(tpath)).get(dom.split(" ")[0], {}).get("dram_bytes_per_cell")
+            traffic = per_cell * cells0 if per_cell else None
         except Exception:
             traffic = None
 

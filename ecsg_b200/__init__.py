@@ -100,7 +100,16 @@ SIGNATURES = [
     ("ecsg_synchronize", ctypes.c_int, [ctypes.c_void_p]),
     ("ecsg_get_status", ctypes.c_int, [ctypes.c_void_p, c_ip, ctypes.c_int]),
     ("ecsg_device_bytes", ctypes.c_longlong, [ctypes.c_void_p]),
+    ("ecsg_adjoint_reset", ctypes.c_int, [ctypes.c_void_p]),
+    ("ecsg_set_adjoint_field", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, c_dp]),
+    ("ecsg_get_adjoint_field", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, c_dp]),
+    ("ecsg_adjoint_op", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    ("ecsg_get_gradient", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, c_dp]),
+    ("ecsg_misfit_gradient", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_fp, ctypes.c_int,
+                                            ctypes.POINTER(ctypes.c_double)]),
 ]
+ECSG_ADJ_VEL, ECSG_ADJ_STRESS, ECSG_ADJ_GHOST_VZ, ECSG_ADJ_GHOST_SXZ, ECSG_ADJ_GHOST_SYZ = 0, 1, 2, 3, 4
+_ADJ_OPS = {"vel": 0, "stress": 1, "vz": 2, "sxz": 3, "syz": 4}
 
 _LIB = None
 
@@ -295,6 +304,46 @@ class Simulation:
         return {"vel": o[0, :ng].tolist(), "vel_mirror": o[1, :ng].tolist(), "stress": o[2, :ng].tolist(),
                 "ghost_vz": o[3, 1:ng].tolist(), "ghost_sxz": o[4, 1:ng].tolist(), "ghost_syz": o[5, 1:ng].tolist(),
                 "src_rec": float(o[6, 0])}
+
+    # -- adjoint (21-Cij media) ------------------------------------------------
+    def adjoint_reset(self):
+        self._ck(lib().ecsg_adjoint_reset(self.h))
+
+    def set_adjoint_field(self, g, k, arr):
+        a = np.ascontiguousarray(arr, dtype=np.float64)
+        if a.shape != field_shape(self.case.grids[g]["n"], SIM_POS[k], self.R):
+            raise ValueError("adjoint field %d of grid %d: shape %s" % (k, g, a.shape))
+        self._ck(lib().ecsg_set_adjoint_field(self.h, g, k, a.ctypes.data_as(c_dp)))
+
+    def adjoint_field(self, g, k):
+        out = np.empty(field_shape(self.case.grids[g]["n"], SIM_POS[k], self.R))
+        self._ck(lib().ecsg_get_adjoint_field(self.h, g, k, out.ctypes.data_as(c_dp)))
+        return out
+
+    def adjoint_op(self, op, index):
+        """Transpose of one operator ("vel", "stress" on a grid; "vz", "sxz", "syz"
+        on an interface); the fields must hold that operator's output state."""
+        self._ck(lib().ecsg_adjoint_op(self.h, _ADJ_OPS[op], index))
+
+    def gradient(self, g, which):
+        """which = 0: buoyancy at the nodes; 1 + k: stiffness slot k (CIJ21_POS[k])."""
+        from .workloads import CIJ21_POS
+        n = self.case.grids[g]["n"]
+        pos = (0, 0, 0) if which == 0 else CIJ21_POS[which - 1]
+        out = np.empty(field_shape(n, pos, 0))
+        self._ck(lib().ecsg_get_gradient(self.h, g, which, out.ctypes.data_as(c_dp)))
+        return out
+
+    def misfit_gradient(self, observed, ckpt_every=50):
+        """L = 1/2 sum (receiver samples - observed)^2 over observed.shape[0] steps
+        from rest; returns L, gradients via gradient()."""
+        obs = np.ascontiguousarray(observed, dtype=np.float32)
+        nsteps = obs.shape[0]
+        loss = ctypes.c_double(0.0)
+        self._ck(lib().ecsg_misfit_gradient(self.h, nsteps, obs.ctypes.data_as(c_fp), int(ckpt_every),
+                                            ctypes.byref(loss)))
+        self.step_index = nsteps
+        return loss.value
 
     def status(self, clear=False):
         st = ctypes.c_int()

@@ -26,6 +26,7 @@ SOURCES = {
     "stress21.cu": ["-fmad=false"],
     "stress21_tma.cu": ["-fmad=false"],
     "medium.cu": [],
+    "adjoint.cu": ["-fmad=false"],
     "interface.cu": ["-fmad=false"],
     "diag.cu": ["-fmad=false"],
     "api.cu": [],

@@ -1,0 +1,29 @@
+// adjoint.cuh -- adjoint state shared by adjoint.cu (grid operators),
+// interface.cu (interface solves) and api.cu (the reverse time loop).
+#pragma once
+#include "ecsg_device.cuh"
+
+namespace ecsg {
+
+template <typename T>
+struct AdjDev {
+    T *l[9];     // adjoint of the 9 fields, the grid's box layout
+    T *gb;       // gradient w.r.t. the node buoyancy
+    T *gc[21];   // gradient w.r.t. the 21 stiffness slots
+    T *w[12];    // work buffers, zero between operators
+};
+
+// Receiver adjoint sources of one step: lambda_{comp}[grid][off] += res[i].
+template <typename T>
+struct RecAdj {
+    T *lbase[kMaxGrids];
+    const int *grid;
+    const int *off;
+    const T *res;
+    int nrec;
+};
+
+__device__ __forceinline__ void atom(float *p, float v) { atomicAdd(p, v); }
+__device__ __forceinline__ void atom(double *p, double v) { atomicAdd(p, v); }
+
+} // namespace ecsg

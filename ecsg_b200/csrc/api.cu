@@ -4,6 +4,7 @@
 // One ecsg_sim owns one CUDA stream and all device memory of a composite run.
 // There is no host fallback: without a usable device every entry point fails.
 #include "ecsg_device.cuh"
+#include "adjoint.cuh"
 #include "../../include/ecsg_b200.h"
 
 #include <cmath>
@@ -60,6 +61,26 @@ template <typename T>
 cudaError_t launch_unpack(double *, const Geo &, const T *, int, int, int, int, cudaStream_t);
 template <typename T>
 cudaError_t launch_iso_medium(const Geo &, const double *, const double *, double *, T *const[5], cudaStream_t);
+// adjoint.cu and the interface adjoints of interface.cu
+template <typename T>
+cudaError_t launch_vel_adj(const GridDev<T> &, const AdjDev<T> &, int, int, int, int, int, cudaStream_t);
+template <typename T>
+cudaError_t launch_stress21_adj(const GridDev<T> &, const AdjDev<T> &, int, int, int, cudaStream_t);
+template <typename T>
+cudaError_t launch_rec_adj(const RecAdj<T> &, cudaStream_t);
+template <typename T>
+cudaError_t launch_rec_sample(const SrcRec &, T *, cudaStream_t);
+template <typename T>
+cudaError_t launch_residual(T *, const float *, int64_t, double *, cudaStream_t);
+template <typename T>
+cudaError_t launch_ghost_vz_adj(const GridDev<T> &, const GridDev<T> &, const AdjDev<T> &, const AdjDev<T> &, int,
+                                double *, double *, double *, cudaStream_t);
+template <typename T>
+cudaError_t launch_ghost_syz_adj(const GridDev<T> &, const GridDev<T> &, const AdjDev<T> &, const AdjDev<T> &, int,
+                                 cudaStream_t);
+template <typename T>
+cudaError_t launch_ghost_sxz_adj(const GridDev<T> &, const GridDev<T> &, const AdjDev<T> &, const AdjDev<T> &, int,
+                                 const SxzWork &, int, double *, cudaStream_t);
 // medium.cu
 template <typename T>
 cudaError_t launch_tti_medium(const Geo &, const float *const[5], double, double, double, double *, T *, T *const[21],
@@ -105,6 +126,19 @@ struct ecsg_sim {
     void *eps[kMaxGrids][6] = {};   // 21-Cij media with energy: accumulated strains at the stress positions
     std::vector<unsigned char> s21maps[kMaxGrids];   // TMA tensor maps of the FP32 21-Cij sweep, per grid
     bool s21_ready = false;
+    // adjoint state (allocated on first use): adjoint fields, gradients, work boxes
+    bool adj = false;
+    void *lblk[kMaxGrids] = {}, *gbblk[kMaxGrids] = {}, *gcblk[kMaxGrids] = {};
+    void *wblk = nullptr;
+    size_t wbox = 0;                                  // elements of one work box (the largest grid's box)
+    double *adj_lx[kMaxGrids] = {}, *adj_y[kMaxGrids] = {}, *adj_Y0[kMaxGrids] = {}, *adj_Y1[kMaxGrids] = {};
+    // misfit-gradient driver: checkpoints, segment states, samples, observations
+    char *ckpt = nullptr, *seg = nullptr;
+    size_t ckpt_cap = 0, seg_cap = 0;
+    void *recT = nullptr;
+    size_t recT_cap = 0;
+    float *obs = nullptr;
+    size_t obs_cap = 0;
     bool medium_set[kMaxGrids] = {};
     Iface itf[kMaxGrids];
     // shared device scalars: [0] status, [1] step clock, [2] last sxz sweeps, [3] first step of the run
@@ -318,12 +352,15 @@ int ecsg_destroy(ecsg_sim *s)
         cudaFree(s->cblk[g]);
         for (int k = 0; k < 3; k++) cudaFree(s->vc[g][k]);
         cudaFree(s->epsblk[g]);
+        cudaFree(s->lblk[g]); cudaFree(s->gbblk[g]); cudaFree(s->gcblk[g]);
+        cudaFree(s->adj_lx[g]); cudaFree(s->adj_y[g]); cudaFree(s->adj_Y0[g]); cudaFree(s->adj_Y1[g]);
         Iface &I = s->itf[g];
         cudaFree(I.A); cudaFree(I.B); cudaFree(I.X0); cudaFree(I.X1); cudaFree(I.partial); cudaFree(I.vzc);
     }
     cudaFree(s->partial); cudaFree(s->ints); cudaFree(s->iters_total); cudaFree(s->dscal); cudaFree(s->bar);
     cudaFree(s->src_trace); cudaFree(s->rec_grid); cudaFree(s->rec_off); cudaFree(s->traces);
     cudaFree(s->run_energy); cudaFree(s->run_res);
+    cudaFree(s->wblk); cudaFree(s->ckpt); cudaFree(s->seg); cudaFree(s->recT); cudaFree(s->obs);
     for (int v = 0; v < 2; v++)
         if (s->gx[v]) cudaGraphExecDestroy(s->gx[v]);
     for (int e = 0; e < 4; e++)
@@ -932,11 +969,12 @@ static SrcRec make_srcrec(ecsg_sim *s, int mode)
 
 // One iteration of main.cpp:165-261 (movies excluded).
 template <typename T>
-static int step_op(ecsg_sim *s, bool energy, double *energy_buf, double *res_row)
+static int step_op(ecsg_sim *s, bool energy, double *energy_buf, double *res_row, T *sample_row = nullptr)
 {
     int rc;
     for (int g = 0; g < s->ng; g++)
         if ((rc = vel_op<T>(s, g, energy))) return rc;
+    if (sample_row) CK(launch_rec_sample<T>(make_srcrec(s, 0), sample_row, s->st));
     if (res_row) {
         CK(launch_src_rec<T>(make_srcrec(s, 1), s->st));
         for (int i = 1; i < s->ng; i++)
@@ -1180,4 +1218,357 @@ int ecsg_time_kernels(ecsg_sim *s, int nsteps, double *ms)
     if (int rc = check_ready(s)) return rc;
     CK(cudaSetDevice(s->device));
     return DISPATCH(time_kernels_op)(s, nsteps, ms);
+}
+
+// ---------------------------------------------------------------------------
+// Adjoint: operator transposes and the misfit gradient (no reference
+// counterpart).  21-Cij media only.
+// ---------------------------------------------------------------------------
+static int adj_alloc(ecsg_sim *s)
+{
+    if (s->adj) return ECSG_OK;
+    int rc;
+    size_t maxbox = 0;
+    for (int g = 0; g < s->ng; g++) {
+        const size_t box = (size_t)s->geo[g].size(), fb = box * s->tsize;
+        if (box > maxbox) maxbox = box;
+        if ((rc = dmalloc(s, &s->lblk[g], 9 * fb))) return rc;
+        if ((rc = dmalloc(s, &s->gbblk[g], fb))) return rc;
+        if ((rc = dmalloc(s, &s->gcblk[g], 21 * fb))) return rc;
+    }
+    s->wbox = maxbox;
+    if ((rc = dmalloc(s, &s->wblk, 12 * maxbox * s->tsize))) return rc;
+    for (int i = 1; i < s->ng; i++) {
+        const Geo &C = s->geo[i];
+        const size_t m = (size_t)(C.ny - 1) * C.nx, nn = (size_t)(C.nx - 1) * (C.ny - 1), nxy = (size_t)(C.nx + 1) * (C.ny + 1);
+        if ((rc = dmalloc(s, (void **)&s->adj_lx[i], sizeof(double) * (m > nn ? m : nn)))) return rc;
+        if ((rc = dmalloc(s, (void **)&s->adj_y[i], sizeof(double) * m))) return rc;
+        if ((rc = dmalloc(s, (void **)&s->adj_Y0[i], sizeof(double) * nxy))) return rc;
+        if ((rc = dmalloc(s, (void **)&s->adj_Y1[i], sizeof(double) * nxy))) return rc;
+    }
+    s->adj = true;
+    return ECSG_OK;
+}
+
+template <typename T>
+static AdjDev<T> adj_dev(const ecsg_sim *s, int g)
+{
+    AdjDev<T> A;
+    const size_t box = (size_t)s->geo[g].size();
+    for (int k = 0; k < 9; k++) A.l[k] = (T *)s->lblk[g] + k * box;
+    A.gb = (T *)s->gbblk[g];
+    for (int k = 0; k < 21; k++) A.gc[k] = (T *)s->gcblk[g] + k * box;
+    for (int k = 0; k < 12; k++) A.w[k] = (T *)s->wblk + k * s->wbox;
+    return A;
+}
+
+static int adj_check(ecsg_sim *s)
+{
+    if (s->medium != ECSG_MEDIUM_GEN21) return fail(s, ECSG_ERR_STATE, "adjoint: the simulation must use ECSG_MEDIUM_GEN21");
+    if (int rc = check_ready(s)) return rc;
+    CK(cudaSetDevice(s->device));
+    return adj_alloc(s);
+}
+
+// zero adjoint fields, gradients and work boxes (and the adjoint sxz warm starts)
+static int adj_zero(ecsg_sim *s, bool fields, bool grads)
+{
+    for (int g = 0; g < s->ng; g++) {
+        const size_t fb = (size_t)s->geo[g].size() * s->tsize;
+        if (fields) CK(cudaMemsetAsync(s->lblk[g], 0, 9 * fb, s->st));
+        if (grads) {
+            CK(cudaMemsetAsync(s->gbblk[g], 0, fb, s->st));
+            CK(cudaMemsetAsync(s->gcblk[g], 0, 21 * fb, s->st));
+        }
+    }
+    CK(cudaMemsetAsync(s->wblk, 0, 12 * s->wbox * s->tsize, s->st));
+    for (int i = 1; i < s->ng; i++) {
+        const Geo &C = s->geo[i];
+        CK(cudaMemsetAsync(s->adj_Y0[i], 0, sizeof(double) * (C.nx + 1) * (C.ny + 1), s->st));
+    }
+    return ECSG_OK;
+}
+
+template <typename T>
+static int adj_op_impl(ecsg_sim *s, int op, int i, const GridDev<T> *Gv)
+{
+    // Gv: the forward fields of every grid the operator reads (its output state)
+    switch (op) {
+    case ECSG_ADJ_VEL:
+        CK(launch_vel_adj<T>(Gv[i], adj_dev<T>(s, i), i == 0, i == s->ng - 1, s->top_bc, s->mirror_fix, s->sms, s->st));
+        break;
+    case ECSG_ADJ_STRESS:
+        CK(launch_stress21_adj<T>(Gv[i], adj_dev<T>(s, i), i == 0, s->top_bc, s->sms, s->st));
+        break;
+    case ECSG_ADJ_GHOST_VZ:
+        CK(launch_ghost_vz_adj<T>(Gv[i - 1], Gv[i], adj_dev<T>(s, i - 1), adj_dev<T>(s, i), s->itf[i].r, s->itf[i].vzc,
+                                  s->adj_lx[i], s->adj_y[i], s->st));
+        break;
+    case ECSG_ADJ_GHOST_SYZ:
+        CK(launch_ghost_syz_adj<T>(Gv[i - 1], Gv[i], adj_dev<T>(s, i - 1), adj_dev<T>(s, i), s->itf[i].r, s->st));
+        break;
+    case ECSG_ADJ_GHOST_SXZ: {
+        if (int rc = sxz_prepare<T>(s, i)) return rc;
+        Iface &I = s->itf[i];
+        SxzWork W;
+        W.A = I.A;
+        W.B = I.B;
+        W.X0 = s->adj_Y0[i];
+        W.X1 = s->adj_Y1[i];
+        W.partial = I.partial;
+        W.total = s->dscal + 1;
+        W.bar = s->bar + 2 * i;
+        W.status = s->ints;
+        W.iters = s->ints + 2;
+        W.iters_total = s->iters_total + i;
+        W.tol_out = s->dscal + 2 + i;
+        W.max_iter = s->jacobi_max_iter;
+        CK(launch_ghost_sxz_adj<T>(Gv[i - 1], Gv[i], adj_dev<T>(s, i - 1), adj_dev<T>(s, i), I.r, W, I.nblocks,
+                                   s->adj_lx[i], s->st));
+        break;
+    }
+    default:
+        return fail(s, ECSG_ERR_INVALID, "adjoint_op: unknown operator %d", op);
+    }
+    return ECSG_OK;
+}
+
+template <typename T>
+static int adj_op_current(ecsg_sim *s, int op, int i)
+{
+    GridDev<T> Gv[kMaxGrids];
+    for (int g = 0; g < s->ng; g++) Gv[g] = dev<T>(s, g);
+    return adj_op_impl<T>(s, op, i, Gv);
+}
+
+int ecsg_adjoint_reset(ecsg_sim *s)
+{
+    if (!s) return ECSG_ERR_INVALID;
+    if (int rc = adj_check(s)) return rc;
+    if (int rc = adj_zero(s, true, true)) return rc;
+    CK(cudaStreamSynchronize(s->st));
+    return ECSG_OK;
+}
+
+int ecsg_set_adjoint_field(ecsg_sim *s, int g, int k, const double *src)
+{
+    if (!s || g < 0 || g >= s->ng || k < 0 || k > 8 || !src) return fail(s, ECSG_ERR_INVALID, "set_adjoint_field: bad arguments");
+    if (int rc = adj_check(s)) return rc;
+    int len[3];
+    field_len(s, g, k, len);
+    const size_t n = (size_t)len[0] * len[1] * len[2], box = (size_t)s->geo[g].size();
+    double *stage = nullptr;
+    CK(cudaMalloc(&stage, n * sizeof(double)));
+    CK(cudaMemcpyAsync(stage, src, n * sizeof(double), cudaMemcpyHostToDevice, s->st));
+    if (s->prec == ECSG_F32)
+        CK((launch_pack<float, double>((float *)s->lblk[g] + k * box, s->geo[g], stage, len[0], len[1], len[2], s->R, s->st)));
+    else
+        CK((launch_pack<double, double>((double *)s->lblk[g] + k * box, s->geo[g], stage, len[0], len[1], len[2], s->R, s->st)));
+    CK(cudaStreamSynchronize(s->st));
+    cudaFree(stage);
+    return ECSG_OK;
+}
+
+static int get_box(ecsg_sim *s, const void *src, const Geo &G, int l0, int l1, int l2, int R, double *dst)
+{
+    const size_t n = (size_t)l0 * l1 * l2;
+    double *stage = nullptr;
+    CK(cudaMalloc(&stage, n * sizeof(double)));
+    if (s->prec == ECSG_F32)
+        CK(launch_unpack<float>(stage, G, (const float *)src, l0, l1, l2, R, s->st));
+    else
+        CK(launch_unpack<double>(stage, G, (const double *)src, l0, l1, l2, R, s->st));
+    CK(cudaMemcpyAsync(dst, stage, n * sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    cudaFree(stage);
+    return ECSG_OK;
+}
+
+int ecsg_get_adjoint_field(ecsg_sim *s, int g, int k, double *dst)
+{
+    if (!s || g < 0 || g >= s->ng || k < 0 || k > 8 || !dst) return fail(s, ECSG_ERR_INVALID, "get_adjoint_field: bad arguments");
+    if (int rc = adj_check(s)) return rc;
+    int len[3];
+    field_len(s, g, k, len);
+    const size_t box = (size_t)s->geo[g].size();
+    return get_box(s, (const char *)s->lblk[g] + k * box * s->tsize, s->geo[g], len[0], len[1], len[2], s->R, dst);
+}
+
+int ecsg_get_gradient(ecsg_sim *s, int g, int which, double *dst)
+{
+    if (!s || g < 0 || g >= s->ng || which < 0 || which > 21 || !dst) return fail(s, ECSG_ERR_INVALID, "get_gradient: bad arguments");
+    if (int rc = adj_check(s)) return rc;
+    const Geo &G = s->geo[g];
+    const size_t box = (size_t)G.size();
+    if (which == 0) return get_box(s, s->gbblk[g], G, G.nx + 1, G.ny + 1, G.nz + 1, 0, dst);
+    const int k = which - 1;
+    return get_box(s, (const char *)s->gcblk[g] + k * box * s->tsize, G, G.nx + 1 - kCij21Pos[k][0],
+                   G.ny + 1 - kCij21Pos[k][1], G.nz + 1 - kCij21Pos[k][2], 0, dst);
+}
+
+int ecsg_adjoint_op(ecsg_sim *s, int op, int index)
+{
+    if (!s) return ECSG_ERR_INVALID;
+    const bool grid_op = op == ECSG_ADJ_VEL || op == ECSG_ADJ_STRESS;
+    if (grid_op ? (index < 0 || index >= s->ng) : (index < 1 || index >= s->ng))
+        return fail(s, ECSG_ERR_INVALID, "adjoint_op: bad grid or interface index");
+    if (int rc = adj_check(s)) return rc;
+    int rc = s->prec == ECSG_F32 ? adj_op_current<float>(s, op, index) : adj_op_current<double>(s, op, index);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(s->st));
+    return ECSG_OK;
+}
+
+// --- the reverse time loop --------------------------------------------------
+static size_t state_bytes(const ecsg_sim *s)
+{
+    size_t b = 0;
+    for (int g = 0; g < s->ng; g++) b += 9 * (size_t)s->geo[g].size() * s->tsize;
+    for (int i = 1; i < s->ng; i++) b += sizeof(double) * (size_t)(s->geo[i].nx + 1) * (s->geo[i].ny + 1);
+    return b;
+}
+
+// fields of every grid and the sxz warm starts (the forward is then recomputed bit for bit)
+static int save_state(ecsg_sim *s, char *dst)
+{
+    for (int g = 0; g < s->ng; g++) {
+        const size_t b = 9 * (size_t)s->geo[g].size() * s->tsize;
+        CK(cudaMemcpyAsync(dst, s->fblk[g], b, cudaMemcpyDeviceToDevice, s->st));
+        dst += b;
+    }
+    for (int i = 1; i < s->ng; i++) {
+        const size_t b = sizeof(double) * (size_t)(s->geo[i].nx + 1) * (s->geo[i].ny + 1);
+        CK(cudaMemcpyAsync(dst, s->itf[i].X0, b, cudaMemcpyDeviceToDevice, s->st));
+        dst += b;
+    }
+    return ECSG_OK;
+}
+
+static int load_state(ecsg_sim *s, const char *src)
+{
+    for (int g = 0; g < s->ng; g++) {
+        const size_t b = 9 * (size_t)s->geo[g].size() * s->tsize;
+        CK(cudaMemcpyAsync(s->fblk[g], src, b, cudaMemcpyDeviceToDevice, s->st));
+        src += b;
+    }
+    for (int i = 1; i < s->ng; i++) {
+        const size_t b = sizeof(double) * (size_t)(s->geo[i].nx + 1) * (s->geo[i].ny + 1);
+        CK(cudaMemcpyAsync(s->itf[i].X0, src, b, cudaMemcpyDeviceToDevice, s->st));
+        src += b;
+    }
+    return ECSG_OK;
+}
+
+// the forward fields of grid g as stored in a saved state
+template <typename T>
+static GridDev<T> dev_state(const ecsg_sim *s, int g, const char *state)
+{
+    GridDev<T> G = dev<T>(s, g);
+    for (int h = 0; h < g; h++) state += 9 * (size_t)s->geo[h].size() * sizeof(T);
+    for (int k = 0; k < 9; k++) G.f[k] = (T *)state + k * (size_t)s->geo[g].size();
+    return G;
+}
+
+static int set_clock(ecsg_sim *s, int n)
+{
+    s->run_n0 = n;
+    CK(cudaMemcpyAsync(s->ints + 1, &s->run_n0, sizeof(int), cudaMemcpyHostToDevice, s->st));
+    CK(cudaMemcpyAsync(s->ints + 3, &s->run_n0, sizeof(int), cudaMemcpyHostToDevice, s->st));
+    CK(cudaStreamSynchronize(s->st));   // run_n0 is read by the copies above
+    return ECSG_OK;
+}
+
+template <typename T>
+static int misfit_gradient_op(ecsg_sim *s, int nsteps, const float *observed, int k, double *loss)
+{
+    int rc;
+    const size_t sb = state_bytes(s);
+    const int ncp = (nsteps + k - 1) / k;
+    const size_t nrec = (size_t)s->nrec, nobs = (size_t)nsteps * nrec;
+    auto grow = [&](void **p, size_t &cap, size_t want) -> int {
+        if (cap >= want) return ECSG_OK;
+        cudaFree(*p);
+        *p = nullptr;
+        cap = 0;
+        CK(cudaMalloc(p, want));
+        cap = want;
+        return ECSG_OK;
+    };
+    if ((rc = grow((void **)&s->ckpt, s->ckpt_cap, sb * (ncp + 1)))) return rc;   // + the final state
+    if ((rc = grow((void **)&s->seg, s->seg_cap, sb * (k + 1)))) return rc;
+    if ((rc = grow(&s->recT, s->recT_cap, sizeof(T) * (nobs > 0 ? nobs : 1)))) return rc;
+    if ((rc = grow((void **)&s->obs, s->obs_cap, sizeof(float) * (nobs > 0 ? nobs : 1)))) return rc;
+    if (nobs) CK(cudaMemcpyAsync(s->obs, observed, sizeof(float) * nobs, cudaMemcpyHostToDevice, s->st));
+    for (int i = 1; i < s->ng; i++)
+        if ((rc = sxz_prepare<T>(s, i))) return rc;
+    if ((rc = stress_prepare(s))) return rc;
+    if ((rc = adj_zero(s, true, true))) return rc;
+    // forward from rest with checkpoints every k steps
+    for (int g = 0; g < s->ng; g++) CK(cudaMemsetAsync(s->fblk[g], 0, 9 * (size_t)s->geo[g].size() * s->tsize, s->st));
+    for (int i = 1; i < s->ng; i++)
+        CK(cudaMemsetAsync(s->itf[i].X0, 0, sizeof(double) * (s->geo[i].nx + 1) * (s->geo[i].ny + 1), s->st));
+    if ((rc = set_clock(s, 0))) return rc;
+    T *rec = (T *)s->recT;
+    for (int n = 0; n < nsteps; n++) {
+        if (n % k == 0 && (rc = save_state(s, s->ckpt + (size_t)(n / k) * sb))) return rc;
+        if ((rc = step_op<T>(s, false, nullptr, nullptr, nrec ? rec + (size_t)n * nrec : nullptr))) return rc;
+    }
+    if ((rc = save_state(s, s->ckpt + (size_t)ncp * sb))) return rc;
+    CK(cudaMemsetAsync(s->dscal + 8, 0, sizeof(double), s->st));
+    CK(launch_residual<T>(rec, s->obs, (int64_t)nobs, s->dscal + 8, s->st));
+    // backward, segment by segment: recompute the segment's states, then reverse its steps
+    GridDev<T> Ga[kMaxGrids], Gb[kMaxGrids];
+    RecAdj<T> R;
+    memset(&R, 0, sizeof R);
+    for (int g = 0; g < s->ng; g++) R.lbase[g] = adj_dev<T>(s, g).l[s->rec_comp];
+    R.grid = s->rec_grid;
+    R.off = s->rec_off;
+    R.nrec = s->nrec;
+    for (int c = ncp - 1; c >= 0; c--) {
+        const int n0 = c * k, n1 = (n0 + k < nsteps) ? n0 + k : nsteps;
+        if ((rc = load_state(s, s->ckpt + (size_t)c * sb))) return rc;
+        if ((rc = set_clock(s, n0))) return rc;
+        if ((rc = save_state(s, s->seg))) return rc;
+        for (int n = n0; n < n1; n++) {
+            if ((rc = step_op<T>(s, false, nullptr, nullptr))) return rc;
+            if ((rc = save_state(s, s->seg + (size_t)(n - n0 + 1) * sb))) return rc;
+        }
+        for (int n = n1 - 1; n >= n0; n--) {
+            const char *sa = s->seg + (size_t)(n - n0 + 1) * sb, *sbf = s->seg + (size_t)(n - n0) * sb;
+            for (int g = 0; g < s->ng; g++) {
+                Ga[g] = dev_state<T>(s, g, sa);
+                Gb[g] = dev_state<T>(s, g, sbf);
+            }
+            for (int i = s->ng - 1; i >= 1; i--) {
+                if ((rc = adj_op_impl<T>(s, ECSG_ADJ_GHOST_SYZ, i, Ga))) return rc;
+                if ((rc = adj_op_impl<T>(s, ECSG_ADJ_GHOST_SXZ, i, Ga))) return rc;
+            }
+            for (int g = 0; g < s->ng; g++)
+                if ((rc = adj_op_impl<T>(s, ECSG_ADJ_STRESS, g, Ga))) return rc;
+            for (int i = s->ng - 1; i >= 1; i--)
+                if ((rc = adj_op_impl<T>(s, ECSG_ADJ_GHOST_VZ, i, Ga))) return rc;
+            if (nrec) {
+                R.res = rec + (size_t)n * nrec;
+                CK(launch_rec_adj<T>(R, s->st));
+            }
+            for (int g = s->ng - 1; g >= 0; g--)
+                if ((rc = adj_op_impl<T>(s, ECSG_ADJ_VEL, g, Gb))) return rc;
+        }
+    }
+    double l = 0.0;
+    CK(cudaMemcpyAsync(&l, s->dscal + 8, sizeof(double), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    if (loss) *loss = l;
+    // leave the forward fields at the final state, the step clock after the last step
+    if ((rc = load_state(s, s->ckpt + (size_t)ncp * sb))) return rc;
+    if ((rc = set_clock(s, nsteps))) return rc;
+    return ECSG_OK;
+}
+
+int ecsg_misfit_gradient(ecsg_sim *s, int nsteps, const float *observed, int ckpt_every, double *loss)
+{
+    if (!s || nsteps < 1 || ckpt_every < 1 || (s->nrec > 0 && !observed))
+        return fail(s, ECSG_ERR_INVALID, "misfit_gradient: bad arguments");
+    if (int rc = adj_check(s)) return rc;
+    return DISPATCH(misfit_gradient_op)(s, nsteps, observed, ckpt_every, loss);
 }

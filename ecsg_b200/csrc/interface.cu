@@ -23,6 +23,7 @@
 //        is capped and a capped solve sets ST_JACOBI_CAP.
 #include "ecsg_device.cuh"
 #include "gen21_device.cuh"
+#include "adjoint.cuh"
 #include <cstdio>
 
 namespace ecsg {
@@ -443,6 +444,444 @@ __global__ void __launch_bounds__(256) sxz_solve_kernel(GridDev<T> F, GridDev<T>
     }
 }
 
+// ===========================================================================
+// Adjoints of the three interface solves (no reference counterpart).  Each
+// forward solve overwrites ghost entries with X = A^{-1} rhs(state) and the
+// fine ghosts with -(last fine interior) + P(coarse ghost + coarse first
+// interior).  Given the adjoint of its output state (in place on the adjoint
+// fields of both grids) these kernels
+//   1. collect the adjoint of X from the overwritten entries (and zero them),
+//      passing the scatter's other reads on;
+//   2. solve A^T y = lambda_X (A is symmetric: the vz lines transposed row by
+//      row, the sxz 9-point system by bounded Jacobi sweeps);
+//   3. add rhs^T y to the adjoint fields and y^T (d rhs/dm - dA/dm X) to the
+//      medium gradients (21-Cij slots for vz, node buoyancy for sxz and syz).
+// The forward fields hold the solve's output state: the rhs reads no entry the
+// solve overwrites, so rhs and X are both available there.  Adjoint path:
+// 21-Cij media only (the general form of every medium).
+// ===========================================================================
+
+// transpose of the strain increment of kind 4, 5 or 6 at point q (e4_at..e6_at)
+template <typename T>
+__device__ __forceinline__ void e_adj(const GridDev<T> &G, T *const lv[3], int kind, int q, double a)
+{
+    const int sy = G.g.px, sz = G.g.px * G.g.py;
+    if (kind == 4) {
+        const double u2 = G.kd[2] * a, u1 = G.kd[1] * a;
+        atom(lv[VY] + q + sz, (T)u2); atom(lv[VY] + q, (T)-u2); atom(lv[VZ] + q + sy, (T)u1); atom(lv[VZ] + q, (T)-u1);
+    } else if (kind == 5) {
+        const double u2 = G.kd[2] * a, u0 = G.kd[0] * a;
+        atom(lv[VX] + q + sz, (T)u2); atom(lv[VX] + q, (T)-u2); atom(lv[VZ] + q, (T)u0); atom(lv[VZ] + q - 1, (T)-u0);
+    } else {
+        const double u1 = G.kd[1] * a, u0 = G.kd[0] * a;
+        atom(lv[VX] + q + sy, (T)u1); atom(lv[VX] + q, (T)-u1); atom(lv[VY] + q, (T)u0); atom(lv[VY] + q - 1, (T)-u0);
+    }
+}
+
+// transpose of Abar4/5/6 at an N point (gen21_device.cuh abar*_g): a * weight to each neighbour's strain
+template <typename T>
+__device__ void abar_adj(const GridDev<T> &G, T *const lv[3], int kind, int x, int y, int z, double a)
+{
+    const Ext E{G.g.nx, G.g.ny, G.g.nz};
+    bool o0[2], o1[2];
+    int dx[2][2], dy[2][2], dz[2][2];
+    for (int i = 0; i < 2; i++) {
+        if (kind == 4) { o0[i] = (y - 1 + i) >= 0 && (y - 1 + i) <= E.ny - 1; o1[i] = (z - 1 + i) >= 0 && (z - 1 + i) <= E.nz - 1; }
+        else if (kind == 5) { o0[i] = (x + i) >= 0 && (x + i) <= E.nx; o1[i] = (z - 1 + i) >= 0 && (z - 1 + i) <= E.nz - 1; }
+        else { o0[i] = (x + i) >= 0 && (x + i) <= E.nx; o1[i] = (y - 1 + i) >= 0 && (y - 1 + i) <= E.ny - 1; }
+    }
+    for (int i = 0; i < 2; i++)
+        for (int j = 0; j < 2; j++) {
+            dx[i][j] = kind == 4 ? 0 : i;
+            dy[i][j] = kind == 4 ? i - 1 : (kind == 5 ? 0 : j - 1);
+            dz[i][j] = kind == 6 ? 0 : j - 1;
+        }
+    double wa0, wa1, wb0, wb1;
+    w2<double>(o0[0], o0[1], wa0, wa1);
+    w2<double>(o1[0], o1[1], wb0, wb1);
+    const double wa[2] = {wa0, wa1}, wb[2] = {wb0, wb1};
+    for (int i = 0; i < 2; i++)
+        for (int j = 0; j < 2; j++) {
+            const double w = wa[i] * wb[j];
+            if (w != 0.0) e_adj(G, lv, kind, G.g.idx(x + dx[i][j], y + dy[i][j], z + dz[i][j]), a * w);
+        }
+}
+
+// ---- vz -------------------------------------------------------------------
+// lambda_X from the coarse ghosts (lx[j1-1][j0], j1 in [1, m]); zero them
+template <typename T>
+__global__ void vz_adj_collect_coarse(GridDev<T> C, AdjDev<T> AC, double *lx)
+{
+    const int j0 = blockIdx.x * blockDim.x + threadIdx.x, j1 = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int nx2 = C.g.nx, m = C.g.ny - 1;
+    if (j0 >= nx2 || j1 > m) return;
+    const int q = C.g.idx(j0, j1, -1);
+    lx[(size_t)(j1 - 1) * nx2 + j0] = (double)AC.l[VZ][q];
+    AC.l[VZ][q] = T(0);
+}
+
+// the fine ghosts vz1(i0, i1, nz1) = -vz1(i0, i1, nz1-1) + sum_j w (vz2(j0, j, 0) + vz2(j0, j, -1))
+template <typename T>
+__global__ void vz_adj_collect_fine(GridDev<T> F, GridDev<T> C, AdjDev<T> AF, AdjDev<T> AC, int r, double *lx)
+{
+    const int i0 = blockIdx.x * blockDim.x + threadIdx.x, i1 = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int nx2 = C.g.nx, ny2 = C.g.ny, m = ny2 - 1;
+    const int nx1 = r * nx2, ny1 = r * ny2, nz1 = F.g.nz;
+    if (i0 >= nx1 || i1 >= ny1) return;
+    const int pf = F.g.idx(i0, i1, nz1), fsz = F.g.px * F.g.py;
+    const T a = AF.l[VZ][pf];
+    if (a == T(0)) return;
+    AF.l[VZ][pf] = T(0);
+    AF.l[VZ][pf - fsz] = AF.l[VZ][pf - fsz] - a;
+    const int j0 = i0 / r, jl = i1 / r;
+    for (int j = jl; j <= jl + 1 && j <= ny2; j++) {
+        const double w = pw_node_all(i1, j, r);
+        if (w == 0.0) continue;
+        atom(AC.l[VZ] + C.g.idx(j0, j, 0), (T)(w * (double)a));
+        if (j >= 1 && j <= m) atomicAdd(lx + (size_t)(j - 1) * nx2 + j0, w * (double)a);
+        else atom(AC.l[VZ] + C.g.idx(j0, j, -1), (T)(w * (double)a));
+    }
+}
+
+// y = A^{-T} lambda_X per coarse x-cell: the rows of A^T are (up[j-1], dg[j], lo[j+1])
+__global__ void vz_adj_solve_kernel(int nx2, int m, const double *coef, const double *lx, double *y)
+{
+    extern __shared__ double sm[];
+    const int P = blockDim.x, t = threadIdx.x, j0 = blockIdx.x;
+    double *A = sm, *B = sm + P, *Cc = sm + 2 * P, *D = sm + 3 * P;
+    const size_t plane = (size_t)m * nx2;
+    auto at = [&](int k, int row) { return coef[k * plane + (size_t)row * nx2 + j0]; };
+    A[t] = (t < m && t >= 1) ? at(2, t - 1) : 0.0;      // sub-diagonal of A^T: up of the row above
+    B[t] = t < m ? at(1, t) : 1.0;
+    Cc[t] = (t + 1 < m) ? at(0, t + 1) : 0.0;           // super-diagonal of A^T: lo of the row below
+    D[t] = t < m ? lx[(size_t)t * nx2 + j0] : 0.0;
+    __syncthreads();
+    for (int s = 1; s < P; s <<= 1) {
+        double a = A[t], bb = B[t], c = Cc[t], d = D[t];
+        double na = 0.0, nc = 0.0, nb = bb, nd = d;
+        if (t - s >= 0) {
+            const double k = a / B[t - s];
+            na = -A[t - s] * k;
+            nb -= Cc[t - s] * k;
+            nd -= D[t - s] * k;
+        }
+        if (t + s < P) {
+            const double k = c / B[t + s];
+            nc = -Cc[t + s] * k;
+            nb -= A[t + s] * k;
+            nd -= D[t + s] * k;
+        }
+        __syncthreads();
+        A[t] = na; B[t] = nb; Cc[t] = nc; D[t] = nd;
+        __syncthreads();
+    }
+    if (t < m) y[(size_t)t * nx2 + j0] = D[t] / B[t];
+}
+
+// rhs^T y and the gradients, coarse rows: rhs = r^3 pred(c) - fsum
+template <typename T>
+__global__ void vz_adj_coarse(GridDev<T> C, AdjDev<T> AC, int r, const double *y)
+{
+    const int j0 = blockIdx.x * blockDim.x + threadIdx.x, j1 = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int nx2 = C.g.nx, m = C.g.ny - 1;
+    if (j0 >= nx2 || j1 > m) return;
+    const double yv = y[(size_t)(j1 - 1) * nx2 + j0];
+    if (yv == 0.0) return;
+    const double rr = (double)r, r3 = rr * rr * rr, u = r3 * yv;
+    const double k2x = C.kd[0], k2y = C.kd[1], k2z = C.kd[2];
+    const int pc = C.g.idx(j0, j1, 0), pxp = C.g.idx(j0 + 1, j1, 0), pym = C.g.idx(j0, j1 - 1, 0);
+    const double c13 = (double)C.c[2][pc], c23 = (double)C.c[4][pc], c33 = (double)C.c[5][pc];
+    const T *vx2 = C.f[VX], *vy2 = C.f[VY], *vz2 = C.f[VZ];
+    atom(AC.l[SZZ] + pc, (T)u);
+    atom(AC.l[VX] + pxp, (T)(u * c13 * k2x)); atom(AC.l[VX] + pc, (T)(-u * c13 * k2x));
+    atom(AC.l[VY] + pc, (T)(u * c23 * k2y)); atom(AC.l[VY] + pym, (T)(-u * c23 * k2y));
+    atom(AC.l[VZ] + pc, (T)(u * c33 * k2z));
+    const double xg = (double)vz2[C.g.idx(j0, j1, -1)];
+    AC.gc[2][pc] = (T)((double)AC.gc[2][pc] + u * k2x * ((double)vx2[pxp] - (double)vx2[pc]));
+    AC.gc[4][pc] = (T)((double)AC.gc[4][pc] + u * k2y * ((double)vy2[pc] - (double)vy2[pym]));
+    AC.gc[5][pc] = (T)((double)AC.gc[5][pc] + u * k2z * ((double)vz2[pc] - xg));
+    const Ext E{C.g.nx, C.g.ny, C.g.nz};
+    const double ab[3] = {(double)abar4_g(C, E, j0, j1, 0), (double)abar5_g(C, E, j0, j1, 0), (double)abar6_g(C, E, j0, j1, 0)};
+    T *lv[3] = {AC.l[VX], AC.l[VY], AC.l[VZ]};
+    for (int k = 0; k < 3; k++) {
+        AC.gc[12 + k][pc] = (T)((double)AC.gc[12 + k][pc] + u * ab[k]);
+        abar_adj(C, lv, 4 + k, j0, j1, 0, u * (double)C.c[12 + k][pc]);
+    }
+}
+
+// fine points: beta = sum over rows r w(i1, j1) y(j0, j1) enters as -beta * pf
+template <typename T>
+__global__ void vz_adj_fine(GridDev<T> F, GridDev<T> C, AdjDev<T> AF, AdjDev<T> AC, int r, const double *y)
+{
+    const int i0 = blockIdx.x * blockDim.x + threadIdx.x, i1 = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int nx2 = C.g.nx, ny2 = C.g.ny, m = ny2 - 1;
+    const int nx1 = r * nx2, ny1 = r * ny2, nz1 = F.g.nz;
+    if (i0 >= nx1 || i1 >= ny1) return;
+    const int j0 = i0 / r, jl = i1 / r;
+    const double rr = (double)r;
+    double beta = 0.0, px = 0.0;
+    for (int j = jl; j <= jl + 1; j++) {
+        if (j < 1 || j > m) continue;
+        const double w = pw_node(i1, j, r, ny2);
+        beta += rr * w * y[(size_t)(j - 1) * nx2 + j0];
+        px += w * (double)C.f[VZ][C.g.idx(j0, j, -1)];
+    }
+    if (beta == 0.0) return;
+    const double k1x = F.kd[0], k1y = F.kd[1], k1z = F.kd[2];
+    const int pf = F.g.idx(i0, i1, nz1), fsy = F.g.px, fsz = F.g.px * F.g.py;
+    const double f13 = (double)F.c[2][pf], f23 = (double)F.c[4][pf], f33 = (double)F.c[5][pf], cz = f33 * k1z;
+    const T *vx1 = F.f[VX], *vy1 = F.f[VY], *vz1 = F.f[VZ], *vz2 = C.f[VZ];
+    atom(AF.l[SZZ] + pf, (T)-beta);
+    atom(AF.l[VX] + pf + 1, (T)(-beta * f13 * k1x)); atom(AF.l[VX] + pf, (T)(beta * f13 * k1x));
+    atom(AF.l[VY] + pf, (T)(-beta * f23 * k1y)); atom(AF.l[VY] + pf - fsy, (T)(beta * f23 * k1y));
+    atom(AF.l[VZ] + pf - fsz, (T)(2.0 * beta * cz));
+    double pv0 = 0.0;
+    for (int j = jl; j <= jl + 1 && j <= ny2; j++) {
+        const double w = pw_node_all(i1, j, r);
+        if (w == 0.0) continue;
+        const int pc = C.g.idx(j0, j, 0);
+        pv0 += w * (double)vz2[pc];
+        atom(AC.l[VZ] + pc, (T)(-beta * cz * w));
+    }
+    AF.gc[2][pf] = (T)((double)AF.gc[2][pf] - beta * k1x * ((double)vx1[pf + 1] - (double)vx1[pf]));
+    AF.gc[4][pf] = (T)((double)AF.gc[4][pf] - beta * k1y * ((double)vy1[pf] - (double)vy1[pf - fsy]));
+    AF.gc[5][pf] = (T)((double)AF.gc[5][pf] - beta * k1z * (pv0 - 2.0 * (double)vz1[pf - fsz] + px));
+    const Ext E{F.g.nx, F.g.ny, F.g.nz};
+    const double ab[3] = {(double)abar4_g(F, E, i0, i1, nz1), (double)abar5_g(F, E, i0, i1, nz1), (double)abar6_g(F, E, i0, i1, nz1)};
+    T *lv[3] = {AF.l[VX], AF.l[VY], AF.l[VZ]};
+    for (int k = 0; k < 3; k++) {
+        AF.gc[12 + k][pf] = (T)((double)AF.gc[12 + k][pf] - beta * ab[k]);
+        abar_adj(F, lv, 4 + k, i0, i1, nz1, -beta * (double)F.c[12 + k][pf]);
+    }
+}
+
+// ---- syz ------------------------------------------------------------------
+// per coarse cell: t = num / den, fine ghosts -syz1(nz1-1) + t + syz2(0)
+template <typename T>
+__global__ void syz_adj_kernel(GridDev<T> F, GridDev<T> C, AdjDev<T> AF, AdjDev<T> AC, int r)
+{
+    const int j0 = blockIdx.x * blockDim.x + threadIdx.x, j1 = blockIdx.y * blockDim.y + threadIdx.y;
+    const int nx2 = C.g.nx, ny2 = C.g.ny, nz1 = F.g.nz;
+    if (j0 >= nx2 || j1 >= ny2) return;
+    const int fsy = F.g.px, fsz = F.g.px * F.g.py, csy = C.g.px;
+    const int pg = C.g.idx(j0, j1, -1), p0 = C.g.idx(j0, j1, 0);
+    double lt = (double)AC.l[SYZ][pg];
+    AC.l[SYZ][pg] = T(0);
+    double ls0 = 0.0;
+    for (int i1 = r * j1; i1 < r * j1 + r; i1++)
+        for (int i0 = r * j0; i0 < r * j0 + r; i0++) {
+            const int pf = F.g.idx(i0, i1, nz1);
+            const T a = AF.l[SYZ][pf];
+            if (a == T(0)) continue;
+            AF.l[SYZ][pf] = T(0);
+            AF.l[SYZ][pf - fsz] = AF.l[SYZ][pf - fsz] - a;
+            lt += (double)a;
+            ls0 += (double)a;
+        }
+    const double k1x = F.kd[0], k1y = F.kd[1], k1z = F.kd[2];
+    const double k2x = C.kd[0], k2y = C.kd[1], k2z = C.kd[2];
+    const double r2 = (double)r * (double)r;
+    const T *b1 = F.b, *b2 = C.b;
+    const T *vy2 = C.f[VY], *sxy2 = C.f[SXY], *syy2 = C.f[SYY], *syz2 = C.f[SYZ];
+    const T *sxy1 = F.f[SXY], *syy1 = F.f[SYY], *syz1 = F.f[SYZ];
+    const double c0 = 0.25 * ((double)b2[p0] + (double)b2[p0 + 1] + (double)b2[p0 + csy] + (double)b2[p0 + csy + 1]);
+    double den = r2 * c0 * k2z;
+    for (int i1 = r * j1; i1 < r * j1 + r; i1++)
+        for (int i0 = r * j0; i0 < r * j0 + r; i0++) {
+            const int pf = F.g.idx(i0, i1, nz1);
+            den += 0.25 * ((double)b1[pf] + (double)b1[pf + 1] + (double)b1[pf + fsy] + (double)b1[pf + fsy + 1]) * k1z;
+        }
+    const double tg = (double)syz2[pg];   // the forward ghost t
+    const double s0 = (double)syz2[p0];
+    if (lt != 0.0) {
+        const double u = lt / den;
+        const double cu = r2 * u;
+        atom(AC.l[VY] + p0, (T)cu);
+        atom(AC.l[SXY] + p0 + 1, (T)(cu * c0 * k2x)); atom(AC.l[SXY] + p0, (T)(-cu * c0 * k2x));
+        atom(AC.l[SYY] + p0 + csy, (T)(cu * c0 * k2y)); atom(AC.l[SYY] + p0, (T)(-cu * c0 * k2y));
+        ls0 += cu * c0 * k2z;
+        // d t / d c0 = (r^2 (k2x dsxy + k2y dsyy + k2z s0) - t r^2 k2z) / den, c0 = mean of 4 nodes
+        const double dc0 = r2 * (k2x * ((double)sxy2[p0 + 1] - (double)sxy2[p0]) + k2y * ((double)syy2[p0 + csy] - (double)syy2[p0])
+                                 + k2z * s0) - tg * r2 * k2z;
+        const double gq = 0.25 * u * dc0;
+        atom(AC.gb + p0, (T)gq); atom(AC.gb + p0 + 1, (T)gq); atom(AC.gb + p0 + csy, (T)gq); atom(AC.gb + p0 + csy + 1, (T)gq);
+        for (int i1 = r * j1; i1 < r * j1 + r; i1++)
+            for (int i0 = r * j0; i0 < r * j0 + r; i0++) {
+                const int pf = F.g.idx(i0, i1, nz1);
+                const double c = 0.25 * ((double)b1[pf] + (double)b1[pf + 1] + (double)b1[pf + fsy] + (double)b1[pf + fsy + 1]);
+                atom(AF.l[VY] + pf, (T)-u);
+                atom(AF.l[SXY] + pf + 1, (T)(-u * c * k1x)); atom(AF.l[SXY] + pf, (T)(u * c * k1x));
+                atom(AF.l[SYY] + pf + fsy, (T)(-u * c * k1y)); atom(AF.l[SYY] + pf, (T)(u * c * k1y));
+                ls0 -= u * c * k1z;
+                atom(AF.l[SYZ] + pf - fsz, (T)(2.0 * u * c * k1z));
+                const double dc = -(k1x * ((double)sxy1[pf + 1] - (double)sxy1[pf]) + k1y * ((double)syy1[pf + fsy] - (double)syy1[pf])
+                                    + k1z * (s0 - 2.0 * (double)syz1[pf - fsz])) - tg * k1z;
+                const double g1 = 0.25 * u * dc;
+                atom(AF.gb + pf, (T)g1); atom(AF.gb + pf + 1, (T)g1); atom(AF.gb + pf + fsy, (T)g1); atom(AF.gb + pf + fsy + 1, (T)g1);
+            }
+    }
+    if (ls0 != 0.0) atom(AC.l[SYZ] + p0, (T)ls0);
+}
+
+// ---- sxz ------------------------------------------------------------------
+// lambda_X at the interior coarse nodes (lx[(j1-1) n0 + j0-1]) from the ghosts
+template <typename T>
+__global__ void sxz_adj_collect_coarse(GridDev<T> C, AdjDev<T> AC, double *lx)
+{
+    const int n0 = C.g.nx - 1, n1 = C.g.ny - 1;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n0 * n1) return;
+    const int j0 = q % n0 + 1, j1 = q / n0 + 1;
+    const int pg = C.g.idx(j0, j1, -1);
+    lx[q] = (double)AC.l[SXZ][pg];
+    AC.l[SXZ][pg] = T(0);
+}
+
+template <typename T>
+__global__ void sxz_adj_collect_fine(GridDev<T> F, GridDev<T> C, AdjDev<T> AF, AdjDev<T> AC, int r, double *lx)
+{
+    const int nx2 = C.g.nx, ny2 = C.g.ny, n0 = nx2 - 1, nz1 = F.g.nz;
+    const int nx1 = r * nx2, ny1 = r * ny2;
+    const int i0 = blockIdx.x * blockDim.x + threadIdx.x + 1, i1 = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    if (i0 >= nx1 || i1 >= ny1) return;
+    const int pf = F.g.idx(i0, i1, nz1), fsz = F.g.px * F.g.py;
+    const T a = AF.l[SXZ][pf];
+    if (a == T(0)) return;
+    AF.l[SXZ][pf] = T(0);
+    AF.l[SXZ][pf - fsz] = AF.l[SXZ][pf - fsz] - a;
+    const int jx = i0 / r, jy = i1 / r;
+    for (int ey = 0; ey < 2; ey++)
+        for (int ex = 0; ex < 2; ex++) {
+            const int cx = jx + ex, cy = jy + ey;
+            if (cx > nx2 || cy > ny2) continue;
+            const double ww = pw_node(i0, cx, r, nx2) * pw_node(i1, cy, r, ny2);
+            if (ww == 0.0) continue;
+            atom(AC.l[SXZ] + C.g.idx(cx, cy, 0), (T)(ww * (double)a));
+            atomicAdd(lx + (size_t)(cy - 1) * n0 + (cx - 1), ww * (double)a);
+        }
+}
+
+// y = A^{-1} lambda_X (A symmetric) by Jacobi sweeps from the previous y,
+// until ||y_k - y_{k-1}||_2 <= 1e-13 sum|lambda_X| or the sweep cap; one
+// cooperative kernel with the bounded grid reductions of the forward solve.
+__global__ void __launch_bounds__(256) sxz_adj_solve_kernel(int nx2, int ny2, SxzWork W, const double *lx)
+{
+    __shared__ double red[32];
+    const int n0 = nx2 - 1, n1 = ny2 - 1, ld = nx2 + 1, nn = n0 * n1;
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gstride = gridDim.x * blockDim.x;
+    bool ok = true;
+    double sab = 0.0;
+    for (int q = gtid; q < nn; q += gstride) sab += fabs(lx[q]);
+    const double sum = grid_sum(sab, W, red, ok);
+    if (!(sum > 0.0)) {   // no adjoint at this interface yet: y = 0
+        for (int q = gtid; q < nn; q += gstride) W.X0[(q / n0 + 1) * ld + q % n0 + 1] = 0.0;
+        if (gtid == 0) *W.iters = 0;
+        return;
+    }
+    const double tol = 1e-13 * sum;
+    double *Xc = W.X0, *Xn = W.X1;
+    int it = 0;
+    while (ok) {
+        double s = 0.0;
+        for (int q = gtid; q < nn; q += gstride) {
+            const int i0 = q % n0 + 1, i1 = q / n0 + 1;
+            const double *a = W.A + q;
+            const double xn = (lx[q]
+                               - a[0 * nn] * __ldcg(Xc + (i1 - 1) * ld + (i0 - 1))
+                               - a[1 * nn] * __ldcg(Xc + (i1) * ld + (i0 - 1))
+                               - a[2 * nn] * __ldcg(Xc + (i1 + 1) * ld + (i0 - 1))
+                               - a[3 * nn] * __ldcg(Xc + (i1 - 1) * ld + (i0))
+                               - a[5 * nn] * __ldcg(Xc + (i1 + 1) * ld + (i0))
+                               - a[6 * nn] * __ldcg(Xc + (i1 - 1) * ld + (i0 + 1))
+                               - a[7 * nn] * __ldcg(Xc + (i1) * ld + (i0 + 1))
+                               - a[8 * nn] * __ldcg(Xc + (i1 + 1) * ld + (i0 + 1))) / a[4 * nn];
+            const double d = xn - __ldcg(Xc + i1 * ld + i0);
+            __stcg(Xn + i1 * ld + i0, xn);
+            s += d * d;
+        }
+        const double tot = grid_sum(s, W, red, ok);
+        double *tmp = Xc; Xc = Xn; Xn = tmp;
+        it++;
+        if (!(sqrt(tot) > tol)) break;
+        if (it >= W.max_iter) {
+            if (gtid == 0) atomicOr(W.status, ST_JACOBI_CAP);
+            break;
+        }
+    }
+    if (Xc != W.X0)
+        for (int q = gtid; q < nn; q += gstride) {
+            const int i0 = q % n0 + 1, i1 = q / n0 + 1;
+            W.X0[i1 * ld + i0] = __ldcg(Xc + i1 * ld + i0);
+        }
+    if (gtid == 0) *W.iters = it;
+}
+
+// rhs^T y (B = r^4 pc - r^2 fsum) and buoyancy gradients, coarse rows
+template <typename T>
+__global__ void sxz_adj_coarse(GridDev<T> C, AdjDev<T> AC, int r, const double *y)
+{
+    const int nx2 = C.g.nx, n0 = nx2 - 1, n1 = C.g.ny - 1, ld = nx2 + 1;
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= n0 * n1) return;
+    const int j0 = q % n0 + 1, j1 = q / n0 + 1;
+    const double yv = y[j1 * ld + j0];
+    if (yv == 0.0) return;
+    const double rr = (double)r, r4 = rr * rr * rr * rr, u = r4 * yv;
+    const double k2x = C.kd[0], k2y = C.kd[1], k2z = C.kd[2];
+    const int pc = C.g.idx(j0, j1, 0), sy = C.g.px;
+    const double b2 = (double)C.b[pc];
+    const T *sxx2 = C.f[SXX], *sxy2 = C.f[SXY], *sxz2 = C.f[SXZ];
+    atom(AC.l[VX] + pc, (T)u);
+    atom(AC.l[SXX] + pc, (T)(u * b2 * k2x)); atom(AC.l[SXX] + pc - 1, (T)(-u * b2 * k2x));
+    atom(AC.l[SXY] + pc, (T)(u * b2 * k2y)); atom(AC.l[SXY] + pc - sy, (T)(-u * b2 * k2y));
+    atom(AC.l[SXZ] + pc, (T)(u * b2 * k2z));
+    const double xg = (double)sxz2[C.g.idx(j0, j1, -1)];
+    const double d = k2x * ((double)sxx2[pc] - (double)sxx2[pc - 1]) + k2y * ((double)sxy2[pc] - (double)sxy2[pc - sy])
+                   + k2z * (double)sxz2[pc];
+    atom(AC.gb + pc, (T)(u * (d - k2z * xg)));
+}
+
+// fine nodes: beta = r^2 (P y)(f) enters as -beta * pf; the fine buoyancy also
+// scales A by r^2 w w' b1 k1z
+template <typename T>
+__global__ void sxz_adj_fine(GridDev<T> F, GridDev<T> C, AdjDev<T> AF, AdjDev<T> AC, int r, const double *y)
+{
+    const int nx2 = C.g.nx, ny2 = C.g.ny, ld = nx2 + 1, nz1 = F.g.nz;
+    const int nx1 = r * nx2, ny1 = r * ny2;
+    const int i0 = blockIdx.x * blockDim.x + threadIdx.x + 1, i1 = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    if (i0 >= nx1 || i1 >= ny1) return;
+    const int jx = i0 / r, jy = i1 / r;
+    double py = 0.0, px = 0.0, ps0 = 0.0;
+    double wws[2][2];
+    for (int ey = 0; ey < 2; ey++)
+        for (int ex = 0; ex < 2; ex++) {
+            const int cx = jx + ex, cy = jy + ey;
+            double ww = 0.0;
+            if (cx <= nx2 && cy <= ny2) ww = pw_node(i0, cx, r, nx2) * pw_node(i1, cy, r, ny2);
+            wws[ey][ex] = ww;
+            if (ww == 0.0) continue;
+            py += ww * y[cy * ld + cx];
+            px += ww * (double)C.f[SXZ][C.g.idx(cx, cy, -1)];
+            ps0 += ww * (double)C.f[SXZ][C.g.idx(cx, cy, 0)];
+        }
+    const double rr = (double)r, beta = rr * rr * py;
+    if (beta == 0.0) return;
+    const double k1x = F.kd[0], k1y = F.kd[1], k1z = F.kd[2];
+    const int pf = F.g.idx(i0, i1, nz1), fsy = F.g.px, fsz = F.g.px * F.g.py;
+    const double b1 = (double)F.b[pf];
+    const T *sxx1 = F.f[SXX], *sxy1 = F.f[SXY], *sxz1 = F.f[SXZ];
+    atom(AF.l[VX] + pf, (T)-beta);
+    atom(AF.l[SXX] + pf, (T)(-beta * b1 * k1x)); atom(AF.l[SXX] + pf - 1, (T)(beta * b1 * k1x));
+    atom(AF.l[SXY] + pf, (T)(-beta * b1 * k1y)); atom(AF.l[SXY] + pf - fsy, (T)(beta * b1 * k1y));
+    atom(AF.l[SXZ] + pf - fsz, (T)(2.0 * beta * b1 * k1z));
+    for (int ey = 0; ey < 2; ey++)
+        for (int ex = 0; ex < 2; ex++)
+            if (wws[ey][ex] != 0.0) atom(AC.l[SXZ] + C.g.idx(jx + ex, jy + ey, 0), (T)(-beta * b1 * k1z * wws[ey][ex]));
+    const double d = k1x * ((double)sxx1[pf] - (double)sxx1[pf - 1]) + k1y * ((double)sxy1[pf] - (double)sxy1[pf - fsy])
+                   + k1z * (ps0 - 2.0 * (double)sxz1[pf - fsz]);
+    atom(AF.gb + pf, (T)(-beta * (d + k1z * px)));
+}
+
 // ---------------------------------------------------------------------------
 // Host launchers
 // ---------------------------------------------------------------------------
@@ -509,7 +948,71 @@ cudaError_t launch_sxz_solve(const GridDev<T> &F, const GridDev<T> &C, int r, co
     return cudaLaunchKernelEx(&cfg, sxz_solve_kernel<T>, F, C, r, W);
 }
 
+
+template <typename T>
+cudaError_t launch_ghost_vz_adj(const GridDev<T> &F, const GridDev<T> &C, const AdjDev<T> &AF, const AdjDev<T> &AC,
+                                int r, double *coef, double *lx, double *y, cudaStream_t st)
+{
+    const int m = C.g.ny - 1, nx2 = C.g.nx;
+    int P = 32;
+    while (P < m) P <<= 1;
+    if (P > 1024) return cudaErrorInvalidConfiguration;
+    dim3 ba(32, 8), ga((nx2 + 31) / 32, (m + 7) / 8);
+    ghost_vz_assemble_kernel<T><<<ga, ba, 0, st>>>(F, C, MED_GEN21, r, coef);
+    vz_adj_collect_coarse<T><<<ga, ba, 0, st>>>(C, AC, lx);
+    const int nx1 = r * nx2, ny1 = r * C.g.ny;
+    dim3 bf(64, 4), gf((nx1 + 63) / 64, (ny1 - 1 + 3) / 4);
+    vz_adj_collect_fine<T><<<gf, bf, 0, st>>>(F, C, AF, AC, r, lx);
+    vz_adj_solve_kernel<<<nx2, P, sizeof(double) * 4 * P, st>>>(nx2, m, coef, lx, y);
+    vz_adj_coarse<T><<<ga, ba, 0, st>>>(C, AC, r, y);
+    vz_adj_fine<T><<<gf, bf, 0, st>>>(F, C, AF, AC, r, y);
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_ghost_syz_adj(const GridDev<T> &F, const GridDev<T> &C, const AdjDev<T> &AF, const AdjDev<T> &AC,
+                                 int r, cudaStream_t st)
+{
+    dim3 blk(32, 8), grd((C.g.nx + 31) / 32, (C.g.ny + 7) / 8);
+    syz_adj_kernel<T><<<grd, blk, 0, st>>>(F, C, AF, AC, r);
+    return cudaGetLastError();
+}
+
+// W: the interface's sxz work space (A from sxz_matrix, X0/X1 hold the
+// adjoint's warm start y); lx: (nx2-1)(ny2-1) doubles
+template <typename T>
+cudaError_t launch_ghost_sxz_adj(const GridDev<T> &F, const GridDev<T> &C, const AdjDev<T> &AF, const AdjDev<T> &AC,
+                                 int r, const SxzWork &W, int nblocks, double *lx, cudaStream_t st)
+{
+    const int nx2 = C.g.nx, ny2 = C.g.ny, nn = (nx2 - 1) * (ny2 - 1);
+    const int nx1 = r * nx2, ny1 = r * ny2;
+    sxz_adj_collect_coarse<T><<<(nn + 255) / 256, 256, 0, st>>>(C, AC, lx);
+    dim3 bf(64, 4), gf((nx1 - 1 + 63) / 64, (ny1 - 1 + 3) / 4);
+    sxz_adj_collect_fine<T><<<gf, bf, 0, st>>>(F, C, AF, AC, r, lx);
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(nblocks);
+    cfg.blockDim = dim3(256);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaError_t e = cudaLaunchKernelEx(&cfg, sxz_adj_solve_kernel, nx2, ny2, W, (const double *)lx);
+    if (e != cudaSuccess) return e;
+    sxz_adj_coarse<T><<<(nn + 255) / 256, 256, 0, st>>>(C, AC, r, W.X0);
+    sxz_adj_fine<T><<<gf, bf, 0, st>>>(F, C, AF, AC, r, W.X0);
+    return cudaGetLastError();
+}
+
 #define INST(T)                                                                                         \
+    template cudaError_t launch_ghost_vz_adj<T>(const GridDev<T> &, const GridDev<T> &, const AdjDev<T> &,         \
+                                                const AdjDev<T> &, int, double *, double *, double *, cudaStream_t); \
+    template cudaError_t launch_ghost_syz_adj<T>(const GridDev<T> &, const GridDev<T> &, const AdjDev<T> &,        \
+                                                 const AdjDev<T> &, int, cudaStream_t);                           \
+    template cudaError_t launch_ghost_sxz_adj<T>(const GridDev<T> &, const GridDev<T> &, const AdjDev<T> &,        \
+                                                 const AdjDev<T> &, int, const SxzWork &, int, double *,        \
+                                                 cudaStream_t);                                                   \
     template cudaError_t launch_ghost_vz<T>(const GridDev<T> &, const GridDev<T> &, int, int, double *, cudaStream_t); \
     template cudaError_t launch_ghost_syz<T>(const GridDev<T> &, const GridDev<T> &, int, cudaStream_t);     \
     template cudaError_t launch_sxz_matrix<T>(const GridDev<T> &, const GridDev<T> &, int, double *, cudaStream_t); \

@@ -232,6 +232,39 @@ int ecsg_get_status(ecsg_sim *sim, int *status, int clear);
 /* Bytes of device memory held by the simulation. */
 long long ecsg_device_bytes(const ecsg_sim *sim);
 
+/* ---------------------------------------------------------------------------
+ * Adjoint and misfit gradients (no counterpart in the reference).  21-Cij
+ * media (ECSG_MEDIUM_GEN21) only.  Every operator of the time loop is an
+ * affine map of the full field state (halos and ghosts included); its
+ * adjoint applies the transposed map to an adjoint state held beside the
+ * fields and accumulates the gradient of <adjoint, operator output> with
+ * respect to the node buoyancy and the 21 stiffness slots.
+ * ------------------------------------------------------------------------- */
+enum { ECSG_ADJ_VEL = 0, ECSG_ADJ_STRESS = 1, ECSG_ADJ_GHOST_VZ = 2, ECSG_ADJ_GHOST_SXZ = 3, ECSG_ADJ_GHOST_SYZ = 4 };
+/* Zero the adjoint fields and gradients (allocates them on first use). */
+int ecsg_adjoint_reset(ecsg_sim *sim);
+/* Adjoint field k of grid g, Field layout as ecsg_set_field. */
+int ecsg_set_adjoint_field(ecsg_sim *sim, int g, int k, const double *src);
+int ecsg_get_adjoint_field(ecsg_sim *sim, int g, int k, double *dst);
+/* Apply the transpose of one operator in place on the adjoint fields and add
+ * its medium gradient.  op = ECSG_ADJ_VEL / ECSG_ADJ_STRESS (index = grid;
+ * the velocity operator includes its halo mirrors) or ECSG_ADJ_GHOST_VZ / SXZ
+ * / SYZ (index = interface, 1 .. num_grids-1).  The simulation's fields must
+ * hold the operator's output state (what the forward call left). */
+int ecsg_adjoint_op(ecsg_sim *sim, int op, int index);
+/* Gradient of grid g: which = 0 buoyancy at the nodes ((nz+1)(ny+1)(nx+1),
+ * x fastest), which = 1 + k the stiffness slot k of ecsg_set_medium_cij21 in
+ * that slot's R = 0 layout. */
+int ecsg_get_gradient(ecsg_sim *sim, int g, int which, double *dst);
+/* Misfit L = 1/2 sum_n sum_r (v_r(n) - observed[n * n_rec + r])^2 over nsteps
+ * steps from rest (receivers as set by ecsg_set_receivers, sampled as the
+ * traces), and its gradient with respect to the medium: the forward run keeps
+ * the state every ckpt_every steps; the reverse run recomputes each segment
+ * from its checkpoint and applies the operator adjoints in reverse order.
+ * The gradients are then read with ecsg_get_gradient; the fields are left at
+ * the final forward state. */
+int ecsg_misfit_gradient(ecsg_sim *sim, int nsteps, const float *observed, int ckpt_every, double *loss);
+
 #ifdef __cplusplus
 }
 #endif

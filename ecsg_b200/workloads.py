@@ -432,3 +432,49 @@ def random_case_tti(seed, ratio=2, nx2=6, ny2=5, nz=(5, 4), top_bc=1, num_grids=
                 radius=1, top_bc=top_bc, imode=1, src=None, rec=np.zeros((0, 3), np.float32), rec_comp=0)
     case.thomsen = tuple(thomsen)
     return case
+
+
+# ---------------------------------------------------------------------------
+# Two-grid adjoint benchmark (shot gradients)
+# ---------------------------------------------------------------------------
+ADJOINT_GRIDS = [((360, 360, 60), 10.0), ((120, 120, 80), 30.0)]
+
+
+def two_grid_adjoint_case(seed=0, shot=0, nsteps=1500, blob=False, grids=None, fpeak=10.0, cfl=0.9):
+    """Two grids at ratio 3 (default 361x361x61 @ 10 m over 121x121x81 @ 30 m,
+    9,135,502 points), the smooth seeded model of three_grid_model made
+    orthorhombic (VTI with a vertical axis: Thomsen TTI_THOMSEN, dip 0), free
+    surface, one of 16 shots on a 4 x 4 surface grid (Ricker vz force), vz
+    receivers on a 121 x 121 surface grid.  blob: the observed-data model, vs
+    raised by a 3 % Gaussian (radius 150 m) centred at 500 m depth."""
+    grids = grids or ADJOINT_GRIDS
+    model = three_grid_model(seed, grids)
+    n0, h0 = grids[0]
+    lx, ly = n0[0] * h0, n0[1] * h0
+    media = []
+    vmax = 0.0
+    z0 = 0.0
+    for m, (n, h) in zip(model, grids):
+        vs = m["vs"]
+        if blob:
+            x = np.arange(n[0] + 1) * h - lx / 2
+            y = np.arange(n[1] + 1) * h - ly / 2
+            z = z0 + np.arange(n[2] + 1) * h - 500.0
+            r2 = z[:, None, None] ** 2 + y[None, :, None] ** 2 + x[None, None, :] ** 2
+            vs = (vs * (1 + 0.03 * np.exp(-r2 / (2 * 150.0 ** 2)))).astype(np.float32)
+        zero = np.zeros_like(m["vp"])
+        media.append({"vp": m["vp"], "vs": vs, "rho": m["rho"], "dip": zero, "azi": zero})
+        vmax = max(vmax, float(m["vp"].max()) * math.sqrt(1 + 2 * TTI_THOMSEN[0]))
+        z0 += n[2] * h
+    dt = h0 / vmax / math.sqrt(3) * cfl
+    sx, sy = shot % 4, shot // 4
+    src = ((0.2 + 0.2 * sx) * lx, (0.2 + 0.2 * sy) * ly, 0.0)
+    trace = ricker(nsteps, dt * 1e-3, fpeak)
+    nr = n0[0] // 3 + 1
+    g = np.arange(nr) * 3 * h0
+    rec = np.stack([np.tile(g, nr), np.repeat(g, nr), np.zeros(nr * nr)], 1).astype(np.float32)
+    case = Case(name="two_grid_adjoint", grids=[{"n": n, "h": (h, h, h)} for (n, h) in grids], media=media,
+                medium="tti", dt=dt, nsteps=nsteps, radius=1, top_bc=1, imode=1,
+                src={"xyz": src, "trace": trace, "scale": 1.0, "comp": 2}, rec=rec, rec_comp=2)
+    case.thomsen = TTI_THOMSEN
+    return case

@@ -191,3 +191,23 @@ def test_gradient_independent_of_checkpoint_interval_and_fp32_close():
     num = sum(float(np.sum((a - b) ** 2)) for a, b in zip(g0, g32))
     den = sum(float(np.sum(a ** 2)) for a in g0)
     assert np.sqrt(num / den) <= 2e-3
+
+
+def test_torch_autograd_function_returns_the_device_gradient():
+    torch = pytest.importorskip("torch")
+    from ecsg_b200.autograd import misfit
+    nsteps = 16
+    case = _loop_case(9, 2, 1, nsteps)
+    obs = np.zeros((nsteps, len(case.rec)), np.float32)
+    medium = [[torch.tensor(m["buoy"], dtype=torch.float64, requires_grad=True)]
+              + [torch.tensor(c, dtype=torch.float64, requires_grad=True) for c in m["c21"]] for m in case.media]
+    loss = misfit(case, obs, medium, ckpt_every=4)
+    loss.backward()
+    with Simulation(case, precision="f64") as sim:
+        ref = sim.misfit_gradient(obs, ckpt_every=4)
+        want = [[sim.gradient(g, w) for w in range(22)] for g in range(2)]
+    assert abs(loss.item() - ref) <= 1e-13 * ref
+    for g in range(2):
+        for w in range(22):
+            got = medium[g][w].grad.numpy()
+            assert np.abs(got - want[g][w]).max() <= 1e-10 * max(np.abs(want[g][w]).max(), 1e-300)

@@ -100,6 +100,9 @@ SIGNATURES = [
     ("ecsg_synchronize", ctypes.c_int, [ctypes.c_void_p]),
     ("ecsg_get_status", ctypes.c_int, [ctypes.c_void_p, c_ip, ctypes.c_int]),
     ("ecsg_device_bytes", ctypes.c_longlong, [ctypes.c_void_p]),
+    ("ecsg_update_vel_ex", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    ("ecsg_update_stress_ex", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    ("ecsg_set_coefficients", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_dp]),
     ("ecsg_adjoint_reset", ctypes.c_int, [ctypes.c_void_p]),
     ("ecsg_set_adjoint_field", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, c_dp]),
     ("ecsg_get_adjoint_field", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, c_dp]),

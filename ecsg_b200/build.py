@@ -79,11 +79,14 @@ def build_lib(verbose=False, force=False):
 
 def build_oracle():
     """Test-side checkers: the C restatement always; the reference build
-    (oracle/_ref) only where the reference sources are mounted."""
+    (oracle/_ref) only where the reference sources are mounted, including the
+    reference driver linked through ecsg_b200/shim (build_lib first)."""
     mk = os.path.join(ROOT, "oracle")
     subprocess.check_call(["make", "-s", "-C", mk, "oracle"])
     if os.path.isdir("/root/reference"):
         subprocess.check_call(["make", "-s", "-C", mk, "ref"])
+        # the reference driver linked against the shim and the library (needs LIB)
+        subprocess.check_call(["make", "-s", "-C", mk, "shim"])
 
 
 if __name__ == "__main__":

@@ -114,6 +114,8 @@ struct ecsg_sim {
     size_t tsize = 4;
     Geo geo[kMaxGrids];
     double h[kMaxGrids][3];
+    bool kset[kMaxGrids] = {};           // FD coefficients given by the caller (ecsg_set_coefficients)
+    double kover[kMaxGrids][3] = {};
     // Per grid, the 9 fields, the stiffness slots and the strain accumulators
     // each live in one allocation (fields of a group at a fixed stride), so
     // that one tensor map can address a whole group.
@@ -209,7 +211,7 @@ static GridDev<T> dev(const ecsg_sim *s, int g)
     for (int k = 0; k < s->nc; k++) G.c[k] = (const T *)s->c[g][k];
     for (int d = 0; d < 3; d++) {
         // FD coefficient of radius 1: fd[0]*dt/h with fd[0] = 1 (init_del_fdcoeff.cpp:19)
-        const double kd = 1.0 * s->dt / s->h[g][d];
+        const double kd = s->kset[g] ? s->kover[g][d] : 1.0 * s->dt / s->h[g][d];
         G.kd[d] = kd;
         G.k[d] = (T)kd;
     }
@@ -570,32 +572,38 @@ static int check_ready(ecsg_sim *s)
     return ECSG_OK;
 }
 
+// top / bottom: the grid's boundary roles (update_vel.cpp:4 arguments); -1 takes
+// them from the grid's place in the composite (top = grid 0, bottom = last grid)
+static int top_of(const ecsg_sim *s, int g, int top) { return top < 0 ? (g == 0) : top; }
+static int bottom_of(const ecsg_sim *s, int g, int bottom) { return bottom < 0 ? (g == s->ng - 1) : bottom; }
+
 template <typename T>
-static int vel_kernel_op(ecsg_sim *s, int g, bool with_copy)
+static int vel_kernel_op(ecsg_sim *s, int g, bool with_copy, int top = -1, int bottom = -1)
 {
     T *vc[3] = {(T *)s->vc[g][0], (T *)s->vc[g][1], (T *)s->vc[g][2]};
+    const int tp = top_of(s, g, top), bt = bottom_of(s, g, bottom);
     if constexpr (std::is_same<T, float>::value) {
         if (!s->scalar_stencils) {
-            CK(launch_vel_v4(dev<float>(s, g), g == 0, g == s->ng - 1, s->top_bc, with_copy ? vc : nullptr, s->sms, s->st));
+            CK(launch_vel_v4(dev<float>(s, g), tp, bt, s->top_bc, with_copy ? vc : nullptr, s->sms, s->st));
             return ECSG_OK;
         }
     }
-    CK(launch_vel<T>(dev<T>(s, g), g == 0, g == s->ng - 1, s->top_bc, with_copy ? vc : nullptr, s->sms, s->st));
+    CK(launch_vel<T>(dev<T>(s, g), tp, bt, s->top_bc, with_copy ? vc : nullptr, s->sms, s->st));
     return ECSG_OK;
 }
 
 template <typename T>
-static int vel_mirror_op(ecsg_sim *s, int g)
+static int vel_mirror_op(ecsg_sim *s, int g, int top = -1, int bottom = -1)
 {
-    CK(launch_vel_mirror<T>(dev<T>(s, g), g == 0, g == s->ng - 1, s->top_bc, s->mirror_fix, s->st));
+    CK(launch_vel_mirror<T>(dev<T>(s, g), top_of(s, g, top), bottom_of(s, g, bottom), s->top_bc, s->mirror_fix, s->st));
     return ECSG_OK;
 }
 
 template <typename T>
-static int vel_op(ecsg_sim *s, int g, bool with_copy)
+static int vel_op(ecsg_sim *s, int g, bool with_copy, int top = -1, int bottom = -1)
 {
-    int rc = vel_kernel_op<T>(s, g, with_copy);
-    return rc ? rc : vel_mirror_op<T>(s, g);
+    int rc = vel_kernel_op<T>(s, g, with_copy, top, bottom);
+    return rc ? rc : vel_mirror_op<T>(s, g, top, bottom);
 }
 
 static int med_kind(const ecsg_sim *s)
@@ -626,29 +634,30 @@ static int stress_prepare(ecsg_sim *s)
 }
 
 template <typename T>
-static int stress_op(ecsg_sim *s, int g)
+static int stress_op(ecsg_sim *s, int g, int top = -1)
 {
     const int med = med_kind(s);
+    const int tp = top_of(s, g, top);
     if (med == MED_GEN21) {
         T *eps[6];
         for (int k = 0; k < 6; k++) eps[k] = (T *)s->eps[g][k];
         if constexpr (std::is_same<T, float>::value) {
             if (use_s21_tma(s)) {
                 if (int rc = stress_prepare(s)) return rc;
-                CK(launch_stress21_tma(s->s21maps[g].data(), dev<float>(s, g), g == 0, s->top_bc, eps, s->ints, s->sms, s->st));
+                CK(launch_stress21_tma(s->s21maps[g].data(), dev<float>(s, g), tp, s->top_bc, eps, s->ints, s->sms, s->st));
                 return ECSG_OK;
             }
         }
-        CK(launch_stress21<T>(dev<T>(s, g), g == 0, s->top_bc, eps, s->sms, s->st));
+        CK(launch_stress21<T>(dev<T>(s, g), tp, s->top_bc, eps, s->sms, s->st));
         return ECSG_OK;
     }
     if constexpr (std::is_same<T, float>::value) {
         if (!s->scalar_stencils) {
-            CK(launch_stress_v4(dev<float>(s, g), med, g == 0, s->top_bc, s->sms, s->st));
+            CK(launch_stress_v4(dev<float>(s, g), med, tp, s->top_bc, s->sms, s->st));
             return ECSG_OK;
         }
     }
-    CK(launch_stress<T>(dev<T>(s, g), med, g == 0, s->top_bc, s->sms, s->st));
+    CK(launch_stress<T>(dev<T>(s, g), med, tp, s->top_bc, s->sms, s->st));
     return ECSG_OK;
 }
 
@@ -705,9 +714,45 @@ int ecsg_update_vel(ecsg_sim *s, int g)
 {
     if (!s || g < 0 || g >= s->ng) return fail(s, ECSG_ERR_INVALID, "update_vel: bad grid");
     if (int rc = check_ready(s)) return rc;
-    int rc = DISPATCH(vel_op)(s, g, false);
+    int rc = DISPATCH(vel_op)(s, g, false, -1, -1);
     if (rc) return rc;
     CK(cudaStreamSynchronize(s->st));
+    return ECSG_OK;
+}
+
+int ecsg_update_vel_ex(ecsg_sim *s, int g, int top, int bottom)
+{
+    if (!s || g < 0 || g >= s->ng) return fail(s, ECSG_ERR_INVALID, "update_vel_ex: bad grid");
+    if (int rc = check_ready(s)) return rc;
+    int rc = s->prec == ECSG_F32 ? vel_op<float>(s, g, false, top ? 1 : 0, bottom ? 1 : 0)
+                                 : vel_op<double>(s, g, false, top ? 1 : 0, bottom ? 1 : 0);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(s->st));
+    return ECSG_OK;
+}
+
+int ecsg_update_stress_ex(ecsg_sim *s, int g, int top, int bottom)
+{
+    (void)bottom;   // the stress update has no bottom-boundary case (update_stress.cpp:4-311)
+    if (!s || g < 0 || g >= s->ng) return fail(s, ECSG_ERR_INVALID, "update_stress_ex: bad grid");
+    if (int rc = check_ready(s)) return rc;
+    int rc = s->prec == ECSG_F32 ? stress_op<float>(s, g, top ? 1 : 0) : stress_op<double>(s, g, top ? 1 : 0);
+    if (rc) return rc;
+    CK(cudaStreamSynchronize(s->st));
+    return ECSG_OK;
+}
+
+int ecsg_set_coefficients(ecsg_sim *s, int g, const double k[3])
+{
+    if (!s || g < 0 || g >= s->ng || !k) return fail(s, ECSG_ERR_INVALID, "set_coefficients: bad arguments");
+    for (int d = 0; d < 3; d++) {
+        if (!(k[d] > 0)) return fail(s, ECSG_ERR_INVALID, "set_coefficients: coefficients must be positive");
+        s->kover[g][d] = k[d];
+    }
+    s->kset[g] = true;
+    if (g > 0) s->itf[g].A_ready = false;
+    if (g + 1 < s->ng) s->itf[g + 1].A_ready = false;
+    s->epoch++;
     return ECSG_OK;
 }
 
@@ -715,7 +760,7 @@ int ecsg_update_stress(ecsg_sim *s, int g)
 {
     if (!s || g < 0 || g >= s->ng) return fail(s, ECSG_ERR_INVALID, "update_stress: bad grid");
     if (int rc = check_ready(s)) return rc;
-    int rc = DISPATCH(stress_op)(s, g);
+    int rc = DISPATCH(stress_op)(s, g, -1);
     if (rc) return rc;
     CK(cudaStreamSynchronize(s->st));
     return ECSG_OK;

@@ -128,7 +128,17 @@ long long ecsg_field_elems(const ecsg_sim *sim, int g, int k);
 
 /* One operator on the device state, in place (sim_utils.hpp:127-148). */
 int ecsg_update_vel(ecsg_sim *sim, int g);       /* UpdateVel    update_vel.cpp:4-249 */
-int ecsg_update_stress(ecsg_sim *sim, int g);    /* UpdateStress update_stress.cpp:4-311 */
+int ecsg_update_stress(ecsg_sim *sim, int g);
+/* UpdateVel / UpdateStress with the boundary roles passed explicitly, as the
+ * reference's own signatures take them (update_vel.cpp:4 and
+ * update_stress.cpp:4: top, bottom); the plain forms derive them from the
+ * grid's place in the composite. */
+int ecsg_update_vel_ex(ecsg_sim *sim, int g, int top, int bottom);
+int ecsg_update_stress_ex(ecsg_sim *sim, int g, int top, int bottom);
+/* FD coefficients of grid g as the caller computed them (InitFDcoeff,
+ * init_del_fdcoeff.cpp:7-22: coeff[g][d][0] = dt / h_d for radius 1); by
+ * default they are formed from cfg.dt and the grid steps. */
+int ecsg_set_coefficients(ecsg_sim *sim, int g, const double k[3]);    /* UpdateStress update_stress.cpp:4-311 */
 int ecsg_ghost_vz(ecsg_sim *sim, int i);         /* UpdateGhostVZ  update_ghost_vz.cpp:8-251 */
 int ecsg_ghost_sxz(ecsg_sim *sim, int i);        /* UpdateGhostSXZ update_ghost_sxz.cpp:16-298 + Jacobi2D/Norm2D */
 int ecsg_ghost_syz(ecsg_sim *sim, int i);        /* UpdateGhostSYZ update_ghost_syz.cpp:6-241 */

@@ -103,6 +103,14 @@ SIGNATURES = [
     ("ecsg_update_vel_ex", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     ("ecsg_update_stress_ex", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     ("ecsg_set_coefficients", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_dp]),
+    ("ecsg_create_shot", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]),
+    ("ecsg_batch_run", ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                      ctypes.POINTER(c_fp), ctypes.POINTER(ctypes.c_double)]),
+    ("ecsg_batch_misfit_gradient", ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_int,
+                                                  ctypes.POINTER(c_fp), ctypes.c_int, c_dp]),
+    ("ecsg_sum_gradients", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), ctypes.c_int]),
+    ("ecsg_autotune", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
+    ("ecsg_get_tuning", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_ip]),
     ("ecsg_adjoint_reset", ctypes.c_int, [ctypes.c_void_p]),
     ("ecsg_set_adjoint_field", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, c_dp]),
     ("ecsg_get_adjoint_field", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, c_dp]),
@@ -183,6 +191,10 @@ class Simulation:
                 cs = [np.ascontiguousarray(a, dtype=np.float64) for a in m[key]]
                 arr = (c_dp * nslot)(*[a.ctypes.data_as(c_dp) for a in cs])
                 self._ck(fn(h, gi, b.ctypes.data_as(c_dp), arr))
+        self._src_rec(case)
+
+    def _src_rec(self, case):
+        L, h = lib(), self.h
         self.src = None
         if case.src is not None:
             loc = self.locate(case.src["xyz"])
@@ -196,6 +208,33 @@ class Simulation:
             self._ck(L.ecsg_set_receivers(h, arr.ctypes.data_as(c_ip), len(self.rec), case.rec_comp))
         self.step_index = 0
         self.graph_ok = True
+
+    @classmethod
+    def shot(cls, model, case):
+        """A new instance sharing model's medium (ecsg_create_shot), with the
+        source and receivers of case (same grids and medium as the model)."""
+        self = cls.__new__(cls)
+        self.case = case
+        self.ng = model.ng
+        self.R = model.R
+        self.precision = model.precision
+        self.energy_on = model.energy_on
+        h = ctypes.c_void_p()
+        rc = lib().ecsg_create_shot(model.h, ctypes.byref(h))
+        if rc != ECSG_OK:
+            raise EcsgError("ecsg_create_shot failed (%d)" % rc)
+        self.h = h
+        self._src_rec(case)
+        return self
+
+    def autotune(self, reps=3):
+        self._ck(lib().ecsg_autotune(self.h, reps))
+        return [self.tuning(g) for g in range(self.ng)]
+
+    def tuning(self, g):
+        c = (ctypes.c_int * 2)()
+        self._ck(lib().ecsg_get_tuning(self.h, g, c))
+        return tuple(c)
 
     # -- plumbing ------------------------------------------------------------
     def _ck(self, rc):
@@ -384,3 +423,43 @@ class Simulation:
 def stability_dt(case_vmax, hmin, cfl=0.9):
     """dt bound of the reference tests (eci/SConstruct:108-113): h / vmax / sqrt(3) * cfl."""
     return hmin / case_vmax / math.sqrt(3) * cfl
+
+
+def _handles(sims):
+    return (ctypes.c_void_p * len(sims))(*[s.h.value for s in sims])
+
+
+def batch_run(sims, nsteps, n0=0):
+    """Advance every instance nsteps steps (ecsg_batch_run: one graph launch per
+    step for all).  Returns (per-instance traces (n_rec, nsteps), device ms)."""
+    bufs = [np.zeros((nsteps, max(len(s.rec), 1)), np.float32) for s in sims]
+    ptrs = (c_fp * len(sims))(*[b.ctypes.data_as(c_fp) for b in bufs])
+    ms = ctypes.c_double()
+    rc = lib().ecsg_batch_run(_handles(sims), len(sims), int(n0), int(nsteps), ptrs, ctypes.byref(ms))
+    if rc != ECSG_OK:
+        raise EcsgError("ecsg_batch_run failed (%d): %s" % (rc, lib().ecsg_last_error(sims[0].h).decode()))
+    for s in sims:
+        s.step_index = n0 + nsteps
+    return [b[:, :len(s.rec)].T.copy() for b, s in zip(bufs, sims)], ms.value
+
+
+def batch_misfit_gradient(sims, observed, ckpt_every=50):
+    """ecsg_misfit_gradient of every instance at once; returns the losses."""
+    obs = [np.ascontiguousarray(o, dtype=np.float32) for o in observed]
+    nsteps = obs[0].shape[0]
+    ptrs = (c_fp * len(sims))(*[o.ctypes.data_as(c_fp) for o in obs])
+    losses = np.zeros(len(sims))
+    rc = lib().ecsg_batch_misfit_gradient(_handles(sims), len(sims), nsteps, ptrs, int(ckpt_every),
+                                          losses.ctypes.data_as(c_dp))
+    if rc != ECSG_OK:
+        raise EcsgError("ecsg_batch_misfit_gradient failed (%d): %s" % (rc, lib().ecsg_last_error(sims[0].h).decode()))
+    for s in sims:
+        s.step_index = nsteps
+    return losses
+
+
+def sum_gradients(dst, srcs):
+    """dst's gradients = sum over srcs, accumulated in FP64."""
+    rc = lib().ecsg_sum_gradients(dst.h, _handles(srcs), len(srcs))
+    if rc != ECSG_OK:
+        raise EcsgError("ecsg_sum_gradients failed (%d): %s" % (rc, lib().ecsg_last_error(dst.h).decode()))

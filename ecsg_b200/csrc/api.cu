@@ -24,8 +24,8 @@ cudaError_t launch_vel_mirror(const GridDev<T> &, int, int, int, int, cudaStream
 template <typename T>
 cudaError_t launch_stress(const GridDev<T> &, int, int, int, int, cudaStream_t);
 // stencil_v4.cu (FP32 production sweeps)
-cudaError_t launch_vel_v4(const GridDev<float> &, int, int, int, float *const[3], int, cudaStream_t);
-cudaError_t launch_stress_v4(const GridDev<float> &, int, int, int, int, cudaStream_t);
+cudaError_t launch_vel_v4(const GridDev<float> &, int, int, int, float *const[3], int, cudaStream_t, int);
+cudaError_t launch_stress_v4(const GridDev<float> &, int, int, int, int, cudaStream_t, int);
 // stress21.cu (21-Cij media)
 template <typename T>
 cudaError_t launch_stress21(const GridDev<T> &, int, int, T *const[6], int, cudaStream_t);
@@ -33,7 +33,7 @@ cudaError_t launch_stress21(const GridDev<T> &, int, int, T *const[6], int, cuda
 size_t s21_maps_bytes();
 bool s21_encode_maps(void *, const GridDev<float> &, float *const[6]);
 cudaError_t s21_set_attributes();
-cudaError_t launch_stress21_tma(const void *, const GridDev<float> &, int, int, float *const[6], int *, int, cudaStream_t);
+cudaError_t launch_stress21_tma(const void *, const GridDev<float> &, int, int, float *const[6], int *, int, cudaStream_t, int);
 // interface.cu
 template <typename T>
 cudaError_t launch_ghost_vz(const GridDev<T> &, const GridDev<T> &, int, int, double *, cudaStream_t);
@@ -114,6 +114,8 @@ struct ecsg_sim {
     size_t tsize = 4;
     Geo geo[kMaxGrids];
     double h[kMaxGrids][3];
+    int ztune[kMaxGrids][2] = {};        // z-chunks of the FP32 velocity / stress sweeps (0: automatic; ecsg_autotune)
+    const ecsg_sim *share = nullptr;     // medium owner when this instance shares its medium (ecsg_create_shot)
     bool kset[kMaxGrids] = {};           // FD coefficients given by the caller (ecsg_set_coefficients)
     double kover[kMaxGrids][3] = {};
     // Per grid, the 9 fields, the stiffness slots and the strain accumulators
@@ -240,7 +242,7 @@ const char *ecsg_last_error(const ecsg_sim *sim) { return sim ? sim->err.c_str()
 
 long long ecsg_device_bytes(const ecsg_sim *sim) { return sim ? sim->bytes : 0; }
 
-int ecsg_create(const ecsg_grid_desc *grids, const ecsg_config *cfg, ecsg_sim **out)
+static int create_impl(const ecsg_grid_desc *grids, const ecsg_config *cfg, ecsg_sim **out, const ecsg_sim *share)
 {
     if (!grids || !cfg || !out) return ECSG_ERR_INVALID;
     *out = nullptr;
@@ -308,10 +310,18 @@ int ecsg_create(const ecsg_grid_desc *grids, const ecsg_config *cfg, ecsg_sim **
         const size_t fb = (size_t)s->geo[g].size() * s->tsize;
         if ((rc = dmalloc(s, &s->fblk[g], 9 * fb))) return bail(rc);
         for (int k = 0; k < 9; k++) s->f[g][k] = (char *)s->fblk[g] + k * fb;
-        if ((rc = dmalloc(s, &s->b[g], fb))) return bail(rc);
-        if ((rc = dmalloc(s, &s->cblk[g], s->nc * fb))) return bail(rc);
-        for (int k = 0; k < s->nc; k++)
-            s->c[g][k] = (char *)s->cblk[g] + (s->medium == ECSG_MEDIUM_GEN21 ? kGen21Phys[k] : k) * fb;
+        if (share) {   // the medium (and the caller's FD coefficients) of another instance
+            s->b[g] = share->b[g];
+            for (int k = 0; k < s->nc; k++) s->c[g][k] = share->c[g][k];
+            s->medium_set[g] = share->medium_set[g];
+            s->kset[g] = share->kset[g];
+            for (int d = 0; d < 3; d++) s->kover[g][d] = share->kover[g][d];
+        } else {
+            if ((rc = dmalloc(s, &s->b[g], fb))) return bail(rc);
+            if ((rc = dmalloc(s, &s->cblk[g], s->nc * fb))) return bail(rc);
+            for (int k = 0; k < s->nc; k++)
+                s->c[g][k] = (char *)s->cblk[g] + (s->medium == ECSG_MEDIUM_GEN21 ? kGen21Phys[k] : k) * fb;
+        }
         if (s->energy)
             for (int k = 0; k < 3; k++)
                 if ((rc = dmalloc(s, &s->vc[g][k], fb))) return bail(rc);
@@ -340,8 +350,32 @@ int ecsg_create(const ecsg_grid_desc *grids, const ecsg_config *cfg, ecsg_sim **
         if ((rc = dmalloc(s, (void **)&I.partial, sizeof(double) * (size_t)I.nblocks))) return bail(rc);
     }
     if (cudaStreamSynchronize(s->st) != cudaSuccess) return bail(fail(s, ECSG_ERR_CUDA, "initial clear"));
+    s->share = share;
     *out = s;
     return ECSG_OK;
+}
+
+int ecsg_create(const ecsg_grid_desc *grids, const ecsg_config *cfg, ecsg_sim **out)
+{
+    return create_impl(grids, cfg, out, nullptr);
+}
+
+int ecsg_create_shot(const ecsg_sim *model, ecsg_sim **out)
+{
+    if (!model || !out) return ECSG_ERR_INVALID;
+    for (int g = 0; g < model->ng; g++)
+        if (!model->medium_set[g]) return ECSG_ERR_STATE;
+    if (model->share) model = model->share;   // shots of a shot share the owner's medium
+    std::vector<ecsg_grid_desc> gd(model->ng);
+    for (int g = 0; g < model->ng; g++) {
+        gd[g].size[0] = model->geo[g].nx;
+        gd[g].size[1] = model->geo[g].ny;
+        gd[g].size[2] = model->geo[g].nz;
+        for (int d = 0; d < 3; d++) gd[g].step[d] = model->h[g][d];
+    }
+    ecsg_config cfg = {model->ng, model->R, model->dt, model->imode, model->top_bc, model->prec, model->medium,
+                       model->energy, model->jacobi_max_iter, model->device, model->mirror_fix};
+    return create_impl(gd.data(), &cfg, out, model);
 }
 
 int ecsg_destroy(ecsg_sim *s)
@@ -350,7 +384,7 @@ int ecsg_destroy(ecsg_sim *s)
     if (s->st) cudaStreamSynchronize(s->st);
     for (int g = 0; g < kMaxGrids; g++) {
         cudaFree(s->fblk[g]);
-        cudaFree(s->b[g]);
+        if (!s->share) cudaFree(s->b[g]);
         cudaFree(s->cblk[g]);
         for (int k = 0; k < 3; k++) cudaFree(s->vc[g][k]);
         cudaFree(s->epsblk[g]);
@@ -406,6 +440,7 @@ static int set_iso(ecsg_sim *s, int g, const float *buoy, const float *s11, cons
 
 int ecsg_set_medium_iso(ecsg_sim *s, int g, const float *buoy, const float *s11, const float *s13)
 {
+    if (s && s->share) return fail(s, ECSG_ERR_STATE, "the medium belongs to another instance (ecsg_create_shot)");
     if (!s || g < 0 || g >= s->ng || !buoy || !s11 || !s13) return fail(s, ECSG_ERR_INVALID, "set_medium_iso: bad arguments");
     if (s->medium != ECSG_MEDIUM_ISO) return fail(s, ECSG_ERR_STATE, "simulation was created for a non-isotropic medium");
     CK(cudaSetDevice(s->device));
@@ -438,6 +473,7 @@ static int set_stiff(ecsg_sim *s, int g, const double *buoy, const double *const
 
 int ecsg_set_medium_ortho9(ecsg_sim *s, int g, const double *buoy, const double *const c[9])
 {
+    if (s && s->share) return fail(s, ECSG_ERR_STATE, "the medium belongs to another instance (ecsg_create_shot)");
     if (!s || g < 0 || g >= s->ng || !buoy || !c) return fail(s, ECSG_ERR_INVALID, "set_medium_ortho9: bad arguments");
     if (s->medium != ECSG_MEDIUM_ORTHO9) return fail(s, ECSG_ERR_STATE, "simulation was not created for an orthorhombic medium");
     for (int k = 0; k < 9; k++)
@@ -453,6 +489,7 @@ int ecsg_set_medium_ortho9(ecsg_sim *s, int g, const double *buoy, const double 
 
 int ecsg_set_medium_cij21(ecsg_sim *s, int g, const double *buoy, const double *const c[21])
 {
+    if (s && s->share) return fail(s, ECSG_ERR_STATE, "the medium belongs to another instance (ecsg_create_shot)");
     if (!s || g < 0 || g >= s->ng || !buoy || !c) return fail(s, ECSG_ERR_INVALID, "set_medium_cij21: bad arguments");
     if (s->medium != ECSG_MEDIUM_GEN21) return fail(s, ECSG_ERR_STATE, "simulation was not created for a 21-Cij medium");
     for (int k = 0; k < 21; k++)
@@ -500,6 +537,7 @@ static int set_tti(ecsg_sim *s, int g, const float *const node[5], double eps, d
 int ecsg_set_medium_tti(ecsg_sim *s, int g, const float *vp, const float *vs, const float *rho, const float *dip,
                         const float *azimuth, double epsilon, double delta, double gamma)
 {
+    if (s && s->share) return fail(s, ECSG_ERR_STATE, "the medium belongs to another instance (ecsg_create_shot)");
     if (!s || g < 0 || g >= s->ng || !vp || !vs || !rho || !dip || !azimuth)
         return fail(s, ECSG_ERR_INVALID, "set_medium_tti: bad arguments");
     if (s->medium != ECSG_MEDIUM_GEN21) return fail(s, ECSG_ERR_STATE, "simulation was not created for a 21-Cij medium");
@@ -584,7 +622,7 @@ static int vel_kernel_op(ecsg_sim *s, int g, bool with_copy, int top = -1, int b
     const int tp = top_of(s, g, top), bt = bottom_of(s, g, bottom);
     if constexpr (std::is_same<T, float>::value) {
         if (!s->scalar_stencils) {
-            CK(launch_vel_v4(dev<float>(s, g), tp, bt, s->top_bc, with_copy ? vc : nullptr, s->sms, s->st));
+            CK(launch_vel_v4(dev<float>(s, g), tp, bt, s->top_bc, with_copy ? vc : nullptr, s->sms, s->st, s->ztune[g][0]));
             return ECSG_OK;
         }
     }
@@ -644,7 +682,8 @@ static int stress_op(ecsg_sim *s, int g, int top = -1)
         if constexpr (std::is_same<T, float>::value) {
             if (use_s21_tma(s)) {
                 if (int rc = stress_prepare(s)) return rc;
-                CK(launch_stress21_tma(s->s21maps[g].data(), dev<float>(s, g), tp, s->top_bc, eps, s->ints, s->sms, s->st));
+                CK(launch_stress21_tma(s->s21maps[g].data(), dev<float>(s, g), tp, s->top_bc, eps, s->ints, s->sms, s->st,
+                                       s->ztune[g][1]));
                 return ECSG_OK;
             }
         }
@@ -653,7 +692,7 @@ static int stress_op(ecsg_sim *s, int g, int top = -1)
     }
     if constexpr (std::is_same<T, float>::value) {
         if (!s->scalar_stencils) {
-            CK(launch_stress_v4(dev<float>(s, g), med, tp, s->top_bc, s->sms, s->st));
+            CK(launch_stress_v4(dev<float>(s, g), med, tp, s->top_bc, s->sms, s->st, s->ztune[g][1]));
             return ECSG_OK;
         }
     }
@@ -1616,4 +1655,257 @@ int ecsg_misfit_gradient(ecsg_sim *s, int nsteps, const float *observed, int ckp
         return fail(s, ECSG_ERR_INVALID, "misfit_gradient: bad arguments");
     if (int rc = adj_check(s)) return rc;
     return DISPATCH(misfit_gradient_op)(s, nsteps, observed, ckpt_every, loss);
+}
+
+// ---------------------------------------------------------------------------
+// Batches of instances (no reference counterpart): independent composites
+// (different sizes and media) or shots sharing one medium.
+// ---------------------------------------------------------------------------
+#include <thread>
+
+template <typename T>
+static int batch_run_op(ecsg_sim *const *sims, int n, int n0, int nsteps, float *const *traces, double *ms_out)
+{
+    int rc;
+    ecsg_sim *s0 = sims[0];
+    ecsg_sim *s = s0;   // error messages go to the first instance
+    for (int b = 0; b < n; b++) {
+        ecsg_sim *x = sims[b];
+        for (int i = 1; i < x->ng; i++)
+            if ((rc = sxz_prepare<T>(x, i))) return rc;
+        if ((rc = stress_prepare(x))) return rc;
+        if (x->nrec > 0 && x->trace_cap < nsteps) {
+            cudaFree(x->traces);
+            x->traces = nullptr;
+            if (cudaMalloc(&x->traces, sizeof(float) * (size_t)nsteps * x->nrec) != cudaSuccess)
+                return fail(s, ECSG_ERR_CUDA, "batch_run: trace buffer of instance %d", b);
+            x->trace_cap = nsteps;
+            x->epoch++;
+        }
+        x->run_n0 = n0;
+        CK(cudaMemcpyAsync(x->ints + 1, &x->run_n0, sizeof(int), cudaMemcpyHostToDevice, x->st));
+        CK(cudaMemcpyAsync(x->ints + 3, &x->run_n0, sizeof(int), cudaMemcpyHostToDevice, x->st));
+        CK(cudaStreamSynchronize(x->st));
+    }
+    // one graph for one step of every instance: fork from a master stream to
+    // each instance's stream, join back
+    cudaStream_t master;
+    CK(cudaStreamCreateWithFlags(&master, cudaStreamNonBlocking));
+    std::vector<cudaEvent_t> ev(n + 3);
+    for (auto &e : ev) CK(cudaEventCreateWithFlags(&e, cudaEventDefault));
+    cudaGraph_t gr = nullptr;
+    cudaGraphExec_t gx = nullptr;
+    auto cleanup = [&]() {
+        if (gx) cudaGraphExecDestroy(gx);
+        if (gr) cudaGraphDestroy(gr);
+        for (auto &e : ev) cudaEventDestroy(e);
+        cudaStreamDestroy(master);
+    };
+    rc = ECSG_OK;
+    if (cudaStreamBeginCapture(master, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        cleanup();
+        return fail(s, ECSG_ERR_CUDA, "batch_run: capture");
+    }
+    cudaEventRecord(ev[0], master);
+    for (int b = 0; b < n && !rc; b++) {
+        ecsg_sim *x = sims[b];
+        cudaStreamWaitEvent(x->st, ev[0], 0);
+        rc = step_op<T>(x, false, nullptr, nullptr);
+        cudaEventRecord(ev[3 + b], x->st);
+        cudaStreamWaitEvent(master, ev[3 + b], 0);
+    }
+    cudaError_t e = cudaStreamEndCapture(master, &gr);
+    if (rc || e != cudaSuccess || cudaGraphInstantiate(&gx, gr, 0) != cudaSuccess) {
+        cleanup();
+        cudaGetLastError();
+        return rc ? rc : fail(s, ECSG_ERR_CUDA, "batch_run: graph");
+    }
+    cudaEventRecord(ev[1], master);
+    for (int k = 0; k < nsteps; k++)
+        if (cudaGraphLaunch(gx, master) != cudaSuccess) {
+            cleanup();
+            return fail(s, ECSG_ERR_CUDA, "batch_run: graph launch");
+        }
+    cudaEventRecord(ev[2], master);
+    if (cudaStreamSynchronize(master) != cudaSuccess) {
+        cleanup();
+        return fail(s, ECSG_ERR_CUDA, "batch_run: %s", cudaGetErrorString(cudaGetLastError()));
+    }
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ev[1], ev[2]);
+    if (ms_out) *ms_out = ms;
+    cleanup();
+    for (int b = 0; b < n; b++) {
+        ecsg_sim *x = sims[b];
+        x->last_run_ms = ms;
+        x->launches = (long long)nsteps * (4LL * x->ng + 1 + 5LL * (x->ng - 1));
+        if (traces && traces[b] && x->nrec > 0)
+            CK(cudaMemcpy(traces[b], x->traces, sizeof(float) * (size_t)nsteps * x->nrec, cudaMemcpyDeviceToHost));
+    }
+    return ECSG_OK;
+}
+
+static int batch_check(ecsg_sim *const *sims, int n)
+{
+    if (!sims || n < 1 || !sims[0]) return ECSG_ERR_INVALID;
+    for (int b = 0; b < n; b++) {
+        if (!sims[b]) return fail(sims[0], ECSG_ERR_INVALID, "batch: instance %d is null", b);
+        if (sims[b]->prec != sims[0]->prec || sims[b]->device != sims[0]->device)
+            return fail(sims[0], ECSG_ERR_INVALID, "batch: instances need one precision and one device");
+        if (int rc = check_ready(sims[b])) return rc;
+    }
+    if (cudaSetDevice(sims[0]->device) != cudaSuccess) return fail(sims[0], ECSG_ERR_CUDA, "cudaSetDevice");
+    return ECSG_OK;
+}
+
+int ecsg_batch_run(ecsg_sim *const *sims, int n, int n0, int nsteps, float *const *traces, double *ms)
+{
+    if (int rc = batch_check(sims, n)) return rc;
+    if (nsteps < 1) return ECSG_OK;
+    return sims[0]->prec == ECSG_F32 ? batch_run_op<float>(sims, n, n0, nsteps, traces, ms)
+                                     : batch_run_op<double>(sims, n, n0, nsteps, traces, ms);
+}
+
+int ecsg_batch_misfit_gradient(ecsg_sim *const *sims, int n, int nsteps, const float *const *observed, int ckpt_every,
+                               double *losses)
+{
+    if (int rc = batch_check(sims, n)) return rc;
+    std::vector<int> rcs(n, ECSG_OK);
+    std::vector<std::thread> th;
+    // one host thread per instance, each on its own stream: their kernels overlap on the device
+    for (int b = 0; b < n; b++)
+        th.emplace_back([&, b]() {
+            double l = 0.0;
+            rcs[b] = ecsg_misfit_gradient(sims[b], nsteps, observed ? observed[b] : nullptr, ckpt_every, &l);
+            if (losses) losses[b] = l;
+        });
+    for (auto &t : th) t.join();
+    for (int b = 0; b < n; b++)
+        if (rcs[b]) return fail(sims[0], rcs[b], "batch gradient, instance %d: %s", b, sims[b]->err.c_str());
+    return ECSG_OK;
+}
+
+// dst[i] = sum_b src_b[i], accumulated in double
+template <typename T>
+__global__ void grad_sum_kernel(T *dst, T *const *src, int n, int64_t count)
+{
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count; i += (int64_t)gridDim.x * blockDim.x) {
+        double acc = 0.0;
+        for (int b = 0; b < n; b++) acc += (double)src[b][i];
+        dst[i] = (T)acc;
+    }
+}
+
+int ecsg_sum_gradients(ecsg_sim *dst, ecsg_sim *const *srcs, int n)
+{
+    if (!dst || !srcs || n < 1) return ECSG_ERR_INVALID;
+    ecsg_sim *s = dst;
+    if (int rc = adj_check(dst)) return rc;
+    for (int b = 0; b < n; b++) {
+        if (!srcs[b] || !srcs[b]->adj || srcs[b]->prec != dst->prec || srcs[b]->ng != dst->ng)
+            return fail(dst, ECSG_ERR_INVALID, "sum_gradients: instance %d has no gradient of this geometry", b);
+        for (int g = 0; g < dst->ng; g++)
+            if (srcs[b]->geo[g].size() != dst->geo[g].size()) return fail(dst, ECSG_ERR_INVALID, "sum_gradients: grid sizes differ");
+        CK(cudaStreamSynchronize(srcs[b]->st));
+    }
+    void **dptr = nullptr;
+    CK(cudaMalloc(&dptr, sizeof(void *) * n));
+    std::vector<void *> hp(n);
+    for (int g = 0; g < dst->ng; g++)
+        for (int part = 0; part < 2; part++) {
+            const int64_t count = (int64_t)dst->geo[g].size() * (part == 0 ? 1 : 21);
+            for (int b = 0; b < n; b++) hp[b] = part == 0 ? srcs[b]->gbblk[g] : srcs[b]->gcblk[g];
+            CK(cudaMemcpyAsync(dptr, hp.data(), sizeof(void *) * n, cudaMemcpyHostToDevice, dst->st));
+            void *out = part == 0 ? dst->gbblk[g] : dst->gcblk[g];
+            const unsigned nb = (unsigned)((count + 255) / 256 > 4096 ? 4096 : (count + 255) / 256);
+            if (dst->prec == ECSG_F32)
+                grad_sum_kernel<float><<<nb, 256, 0, dst->st>>>((float *)out, (float *const *)dptr, n, count);
+            else
+                grad_sum_kernel<double><<<nb, 256, 0, dst->st>>>((double *)out, (double *const *)dptr, n, count);
+            CK(cudaGetLastError());
+            CK(cudaStreamSynchronize(dst->st));
+        }
+    cudaFree(dptr);
+    return ECSG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Autotuner: z-chunks of the FP32 velocity and stress sweeps per grid
+// ---------------------------------------------------------------------------
+int ecsg_autotune(ecsg_sim *s, int reps)
+{
+    if (!s) return ECSG_ERR_INVALID;
+    if (int rc = check_ready(s)) return rc;
+    CK(cudaSetDevice(s->device));
+    if (s->prec != ECSG_F32 || s->scalar_stencils) return ECSG_OK;   // only the FP32 sweeps take a chunk count
+    if (reps < 1) reps = 3;
+    int rc;
+    if ((rc = stress_prepare(s))) return rc;
+    // the trial sweeps change the fields (and strain accumulators): keep and restore them
+    const size_t sb = state_bytes(s);
+    size_t eb = 0;
+    for (int g = 0; g < s->ng; g++)
+        if (s->epsblk[g]) eb += 6 * (size_t)s->geo[g].size() * s->tsize;
+    char *save = nullptr;
+    CK(cudaMalloc(&save, sb + eb + 1));
+    if ((rc = save_state(s, save))) { cudaFree(save); return rc; }
+    {
+        char *p = save + sb;
+        for (int g = 0; g < s->ng; g++)
+            if (s->epsblk[g]) {
+                const size_t b = 6 * (size_t)s->geo[g].size() * s->tsize;
+                CK(cudaMemcpyAsync(p, s->epsblk[g], b, cudaMemcpyDeviceToDevice, s->st));
+                p += b;
+            }
+    }
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    const int cand[] = {0, 1, 2, 3, 4, 6, 8, 12, 16, 24};
+    for (int g = 0; g < s->ng; g++)
+        for (int kind = 0; kind < 2; kind++) {
+            float best = 1e30f;
+            int best_c = 0;
+            for (int c : cand) {
+                if (c > s->geo[g].nz + 1) continue;
+                s->ztune[g][kind] = c;
+                float t = 1e30f;
+                for (int r = 0; r <= reps; r++) {   // the first repetition warms up
+                    CK(cudaEventRecord(e0, s->st));
+                    rc = kind == 0 ? vel_kernel_op<float>(s, g, false) : stress_op<float>(s, g);
+                    if (rc) { cudaFree(save); return rc; }
+                    CK(cudaEventRecord(e1, s->st));
+                    CK(cudaEventSynchronize(e1));
+                    float ms = 0;
+                    CK(cudaEventElapsedTime(&ms, e0, e1));
+                    if (r > 0 && ms < t) t = ms;
+                }
+                if (t < best * 0.99f) { best = t; best_c = c; }
+            }
+            s->ztune[g][kind] = best_c;
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    rc = load_state(s, save);
+    {
+        char *p = save + sb;
+        for (int g = 0; g < s->ng; g++)
+            if (s->epsblk[g]) {
+                const size_t b = 6 * (size_t)s->geo[g].size() * s->tsize;
+                CK(cudaMemcpyAsync(s->epsblk[g], p, b, cudaMemcpyDeviceToDevice, s->st));
+                p += b;
+            }
+    }
+    CK(cudaStreamSynchronize(s->st));
+    cudaFree(save);
+    s->epoch++;   // the cached step graphs hold the old launch shapes
+    return rc;
+}
+
+int ecsg_get_tuning(const ecsg_sim *s, int g, int chunks[2])
+{
+    if (!s || g < 0 || g >= s->ng || !chunks) return ECSG_ERR_INVALID;
+    chunks[0] = s->ztune[g][0];
+    chunks[1] = s->ztune[g][1];
+    return ECSG_OK;
 }

@@ -313,25 +313,33 @@ static int pick_zchunk_v4(int64_t cols, int nz, int sms)
     return (nz + 1 + nchunk - 1) / nchunk;
 }
 
+// planes per z-chunk for a requested number of chunks (0: the automatic choice)
+static int chunk_planes(int nz, int nchunk)
+{
+    if (nchunk > nz + 1) nchunk = nz + 1;
+    return (nz + 1 + nchunk - 1) / nchunk;
+}
+
 cudaError_t launch_vel_v4(const GridDev<float> &G, int top, int bottom, int top_bc, float *const vcopy[3], int sms,
-                          cudaStream_t st)
+                          cudaStream_t st, int nchunk)
 {
     const Geo &g = G.g;
     const int zt = (top && top_bc != 1) ? 1 : 0;
     const int bx = (g.nx + 127) / 128, by = (g.ny + V4_ROWS - 1) / V4_ROWS;
-    const int zc = pick_zchunk_v4((int64_t)bx * by, g.nz, sms);
+    const int zc = nchunk > 0 ? chunk_planes(g.nz, nchunk) : pick_zchunk_v4((int64_t)bx * by, g.nz, sms);
     dim3 blk(32, V4_ROWS), grd(bx, by, (g.nz + 1 + zc - 1) / zc);
     vel_kernel_v4<<<grd, blk, 0, st>>>(G, zt, bottom, zc, vcopy ? vcopy[0] : nullptr, vcopy ? vcopy[1] : nullptr,
                                        vcopy ? vcopy[2] : nullptr);
     return cudaGetLastError();
 }
 
-cudaError_t launch_stress_v4(const GridDev<float> &G, int medium, int top, int top_bc, int sms, cudaStream_t st)
+cudaError_t launch_stress_v4(const GridDev<float> &G, int medium, int top, int top_bc, int sms, cudaStream_t st,
+                             int nchunk)
 {
     const Geo &g = G.g;
     const int flag = (top && top_bc) ? 1 : 0;
     const int bx = (g.nx + 1 + 127) / 128, by = (g.ny + 1 + V4_ROWS - 1) / V4_ROWS;
-    const int zc = pick_zchunk_v4((int64_t)bx * by, g.nz, sms);
+    const int zc = nchunk > 0 ? chunk_planes(g.nz, nchunk) : pick_zchunk_v4((int64_t)bx * by, g.nz, sms);
     dim3 blk(32, V4_ROWS), grd(bx, by, (g.nz + 1 + zc - 1) / zc);
     if (medium == MED_ISO5)
         stress_kernel_v4<MED_ISO5><<<grd, blk, 0, st>>>(G, flag, zc);

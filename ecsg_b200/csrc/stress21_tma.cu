@@ -533,7 +533,7 @@ cudaError_t s21_set_attributes()
 }
 
 cudaError_t launch_stress21_tma(const void *maps, const GridDev<float> &G, int top, int top_bc, float *const eps[6],
-                                int *status, int sms, cudaStream_t st)
+                                int *status, int sms, cudaStream_t st, int nchunk_req)
 {
     using namespace s21t;
     const Geo &g = G.g;
@@ -545,6 +545,7 @@ cudaError_t launch_stress21_tma(const void *maps, const GridDev<float> &G, int t
     if (nchunk < 1) nchunk = 1;
     const int maxc = (g.nz + 1) / 24 > 0 ? (g.nz + 1) / 24 : 1;
     if (nchunk > maxc) nchunk = maxc;
+    if (nchunk_req > 0) nchunk = nchunk_req < g.nz + 1 ? nchunk_req : g.nz + 1;   // tuned
     const int zc = (g.nz + 1 + nchunk - 1) / nchunk;
     dim3 grd(bx, by, (g.nz + 1 + zc - 1) / zc);
     const S21Maps &M = *(const S21Maps *)maps;

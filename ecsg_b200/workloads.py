@@ -478,3 +478,50 @@ def two_grid_adjoint_case(seed=0, shot=0, nsteps=1500, blob=False, grids=None, f
                 src={"xyz": src, "trace": trace, "scale": 1.0, "comp": 2}, rec=rec, rec_comp=2)
     case.thomsen = TTI_THOMSEN
     return case
+
+
+# ---------------------------------------------------------------------------
+# Batch of uneven two-grid composites
+# ---------------------------------------------------------------------------
+def batch_instance_case(seed, nsteps=1000, fpeak=10.0, cfl=0.9):
+    """One of the batch instances: fine nx, ny drawn from {61, 91, ..., 301}
+    points with nz = 31 at 10 m over the matching coarse grid ((n-1)/3 + 1
+    points) with 31..81 z points at 30 m; a seeded 3-layer tilted-VTI medium
+    (vp 1.0..4.5 m/ms, vs = vp / 1.8, Gardner density, dip <= 30 deg per layer,
+    Thomsen TTI_THOMSEN); one Ricker vz force at a random surface point; a
+    line of 16 surface vz receivers."""
+    rng = np.random.default_rng(10_000 + seed)
+    nx = int(rng.choice(np.arange(61, 302, 30))) - 1
+    ny = int(rng.choice(np.arange(61, 302, 30))) - 1
+    nzc = int(rng.integers(31, 82)) - 1
+    grids = [((nx, ny, 30), 10.0), ((nx // 3, ny // 3, nzc), 30.0)]
+    depth = 30 * 10.0 + nzc * 30.0
+    tops = np.sort(rng.uniform(0.15, 0.85, 2)) * depth
+    vps = np.sort(rng.uniform(1.0, 4.5, 3))
+    dips = np.radians(rng.uniform(0, 30, 3))
+    azis = rng.uniform(-math.pi, math.pi, 3)
+    media = []
+    z0 = 0.0
+    for (n, h) in grids:
+        z = z0 + np.arange(n[2] + 1) * h
+        layer = np.searchsorted(tops, z)
+        shp = (n[2] + 1, n[1] + 1, n[0] + 1)
+        vp = np.broadcast_to(vps[layer][:, None, None], shp).astype(np.float32)
+        m = {"vp": vp, "vs": (vp / np.float32(1.8)).astype(np.float32),
+             "rho": (0.31 * (vp * 1000.0) ** 0.25).astype(np.float32),
+             "dip": np.broadcast_to(dips[layer][:, None, None], shp).astype(np.float32),
+             "azi": np.broadcast_to(azis[layer][:, None, None], shp).astype(np.float32)}
+        media.append({k: np.ascontiguousarray(v) for k, v in m.items()})
+        z0 += n[2] * h
+    h0 = grids[0][1]
+    vmax = float(vps.max()) * math.sqrt(1 + 2 * TTI_THOMSEN[0])
+    dt = h0 / vmax / math.sqrt(3) * cfl
+    lx, ly = nx * h0, ny * h0
+    src = (float(rng.uniform(0.1, 0.9)) * lx, float(rng.uniform(0.1, 0.9)) * ly, 0.0)
+    rec = np.stack([np.linspace(0.1, 0.9, 16) * lx, np.full(16, 0.5 * ly), np.zeros(16)], 1).astype(np.float32)
+    case = Case(name="batch_%d" % seed, grids=[{"n": n, "h": (h, h, h)} for (n, h) in grids], media=media,
+                medium="tti", dt=dt, nsteps=nsteps, radius=1, top_bc=1, imode=1,
+                src={"xyz": src, "trace": ricker(nsteps, dt * 1e-3, fpeak), "scale": 1.0, "comp": 2},
+                rec=rec, rec_comp=2)
+    case.thomsen = TTI_THOMSEN
+    return case

@@ -275,6 +275,34 @@ int ecsg_get_gradient(ecsg_sim *sim, int g, int which, double *dst);
  * the final forward state. */
 int ecsg_misfit_gradient(ecsg_sim *sim, int nsteps, const float *observed, int ckpt_every, double *loss);
 
+/* ---------------------------------------------------------------------------
+ * Batches (no counterpart in the reference).
+ * ------------------------------------------------------------------------- */
+/* A new instance with the grids and configuration of model whose medium IS
+ * the model's (one copy on the device; set the model's medium first, keep the
+ * model alive while shots exist; ecsg_set_medium_* on a shot fails).  Own
+ * fields, source, receivers, adjoint state. */
+int ecsg_create_shot(const ecsg_sim *model, ecsg_sim **out);
+/* Advance n instances (any sizes and media, one precision, one device) by
+ * nsteps steps starting at step n0 (source index and trace row 0): one CUDA
+ * graph holds one step of every instance, each on its own stream, and is
+ * launched once per step.  traces[b] (may be null) receives instance b's
+ * receiver traces (nsteps x n_rec); ms the device time of the steps. */
+int ecsg_batch_run(ecsg_sim *const *sims, int n, int n0, int nsteps, float *const *traces, double *ms);
+/* ecsg_misfit_gradient of n instances at once (one host thread and stream
+ * each, so their kernels overlap); observed[b] as for a single instance. */
+int ecsg_batch_misfit_gradient(ecsg_sim *const *sims, int n, int nsteps, const float *const *observed, int ckpt_every,
+                               double *losses);
+/* dst's gradients = the sum of the instances' gradients, accumulated in FP64
+ * (dst may be one of them; same geometry and precision). */
+int ecsg_sum_gradients(ecsg_sim *dst, ecsg_sim *const *srcs, int n);
+/* Autotuner: for each grid, time the FP32 velocity and stress sweeps over
+ * candidate z-march depths (chunks per column) on the simulation's own state
+ * (restored afterwards) and keep the fastest; reps timed repetitions each.
+ * ecsg_get_tuning returns the chosen chunk counts (0 = the built-in choice). */
+int ecsg_autotune(ecsg_sim *sim, int reps);
+int ecsg_get_tuning(const ecsg_sim *sim, int g, int chunks[2]);
+
 #ifdef __cplusplus
 }
 #endif

@@ -18,15 +18,13 @@
 //
 // Adjoint state of a grid: lambda of the 9 fields in the grid's box layout;
 // gradients: g_b at the nodes (buoyancy) and g_c[21] at the slot positions.
-// Work buffers (zero between operators): W[0..5] adjoints of the strain
-// increments e1..e6, W[6..8] of the link products Q45, Q46, Q56, W[9..11] of
-// P4, P5, P6.
+// The grid operators gather where the forward gathers (no atomics) except on
+// the free-surface plane; the velocity update scatters with atomics.
+// Work boxes of the stress adjoint: see the stage description below.
 #include "adjoint.cuh"
 #include "gen21_device.cuh"
 
 namespace ecsg {
-
-enum { W_E1 = 0, W_E2, W_E3, W_E4, W_E5, W_E6, W_Q45, W_Q46, W_Q56, W_P4, W_P5, W_P6 };
 
 // closure weights of a 2 x 2 neighbourhood (avg4 of gen21_device.cuh)
 template <typename T>
@@ -154,22 +152,38 @@ __global__ void rec_adj_kernel(const RecAdj<T> R)
 }
 
 // ---------------------------------------------------------------------------
-// 21-Cij stress update (stress21.cu), reverse mode in four stages.
-//   S1 per point: the sigma adjoints of N, L6, L4, L5 outputs -> gradients of
-//      the coefficients that multiply forward values, W[e] of own strains,
-//      scattered W[e] / W[Q] / W[P] of the averaged neighbours
-//   S2 per point: W[Q], W[P] -> gradients and own W[e]
-//   S3 free surface: the condensed e3 -> e1, e2, the averaged e4..e6
-//   S4 per point: W[e] -> lambda_v (transpose of the differences)
+// 21-Cij stress update (stress21.cu), reverse mode as gathers.
+// Work boxes: E[0..5] the forward strain increments e1..e6 (e3 condensed on a
+// free surface), S[0..2] at N the adjoints of the averages Abar4..6
+// (sum_i a_i C_i,4..6), W[0..5] the adjoints of e1..e6.  Every averaging
+// relation of the forward (an output point averages a 2 x 2 neighbourhood of
+// a source position with its own closure weights) is inverted: a point
+// gathers from the output points whose average contains it, with the weight
+// that output point gave it.
+//   G0 pointwise: E, S, the own-point part of W[N]; the surface mirrors of
+//      syz/sxz folded back (lambda at z = -1 added, negated, to z = 0)
+//   G1 gathers: the rest of W[N] (link products P4..6 read by L4, L5, L6),
+//      W[L4], W[L5], W[L6], and every coefficient gradient
+//   G2 free surface: the condensed e3's adjoint to e1, e2, Abar4..6 (atomics
+//      on the surface plane only)
+//   G3 gathers: W -> lambda_v (transpose of the differences)
+// Buffers are read only at positions valid for the grid, so values left by
+// other grids (the work boxes are shared) are never seen.
 // ---------------------------------------------------------------------------
-template <typename T>
-__device__ __forceinline__ T e3u_at(const GridDev<T> &G, const Ext &E, bool surf, int x, int y, int z, int p)
-{
-    return e3_used(G, E, surf, x, y, z, p, e1_at(G, p), e2_at(G, p));
-}
+enum { X_E = 0, X_S = 6, X_W = 9 };
 
 template <typename T>
-__global__ void stress21_adj_s1(GridDev<T> G, AdjDev<T> A, int flag)
+__device__ __forceinline__ T wgt(bool a0, bool a1, bool b0, bool b1, int i, int j)
+{
+    T wa0, wa1, wb0, wb1;
+    w2<T>(a0, a1, wa0, wa1);
+    w2<T>(b0, b1, wb0, wb1);
+    return mul_(i ? wa1 : wa0, j ? wb1 : wb0);
+}
+__device__ __forceinline__ bool in_(int v, int lo, int hi) { return v >= lo && v <= hi; }
+
+template <typename T>
+__global__ void stress21_adj_g0(GridDev<T> G, AdjDev<T> A, int flag)
 {
     const Geo &g = G.g;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
@@ -177,285 +191,282 @@ __global__ void stress21_adj_s1(GridDev<T> G, AdjDev<T> A, int flag)
     const int64_t n = (int64_t)(nx + 1) * (ny + 1) * (nz + 1);
     const int sz = g.px * g.py;
     const T *const *c = G.c;
-    T *const *W = A.w;
+    T *const *X = A.w;
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
         const int x = (int)(t % (nx + 1)), y = (int)((t / (nx + 1)) % (ny + 1)), z = (int)(t / ((int64_t)(nx + 1) * (ny + 1)));
         const int p = g.idx(x, y, z);
-        bool a_[2], b_[2];
-        T w[2][2];
         if (E.n(x, y, z)) {
             const bool surf = flag && z == 0;
+            const T e1 = e1_at(G, p), e2 = e2_at(G, p);
+            X[X_E + 0][p] = e1;
+            X[X_E + 1][p] = e2;
+            X[X_E + 2][p] = e3_used(G, E, surf, x, y, z, p, e1, e2);
             const T a[3] = {A.l[SXX][p], A.l[SYY][p], surf ? T(0) : A.l[SZZ][p]};
-            if (a[0] != T(0) || a[1] != T(0) || a[2] != T(0)) {
-                const T e[3] = {e1_at(G, p), e2_at(G, p), e3u_at(G, E, surf, x, y, z, p)};
-                const T ab[3] = {abar4_g(G, E, x, y, z), abar5_g(G, E, x, y, z), abar6_g(G, E, x, y, z)};
-                const int rowc[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
-                T le[3] = {T(0), T(0), T(0)}, lab[3] = {T(0), T(0), T(0)};
+            const int rowc[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+            for (int j = 0; j < 3; j++) {
+                T le = T(0), ls = T(0);
                 for (int i = 0; i < 3; i++) {
-                    for (int j = 0; j < 3; j++) {
-                        const int s = rowc[i][j];
-                        A.gc[s][p] = add_(A.gc[s][p], mul_(a[i], e[j]));
-                        le[j] = fma_(a[i], c[s][p], le[j]);
-                    }
-                    for (int j = 0; j < 3; j++) {
-                        const int s = 6 + 3 * i + j;
-                        A.gc[s][p] = add_(A.gc[s][p], mul_(a[i], ab[j]));
-                        lab[j] = fma_(a[i], c[s][p], lab[j]);
-                    }
+                    le = fma_(a[i], c[rowc[i][j]][p], le);
+                    ls = fma_(a[i], c[6 + 3 * i + j][p], ls);
                 }
-                W[W_E1][p] = add_(W[W_E1][p], le[0]);
-                W[W_E2][p] = add_(W[W_E2][p], le[1]);
-                W[W_E3][p] = add_(W[W_E3][p], le[2]);
-                // Abar4: L4 (x, y-1+i, z-1+j)
-                for (int i = 0; i < 2; i++) { a_[i] = (y - 1 + i) >= 0 && (y - 1 + i) <= ny - 1; b_[i] = (z - 1 + i) >= 0 && (z - 1 + i) <= nz - 1; }
-                weights4(a_, b_, w);
-                for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++)
-                    if (w[i][j] != T(0)) atom(W[W_E4] + g.idx(x, y - 1 + i, z - 1 + j), mul_(w[i][j], lab[0]));
-                // Abar5: L5 (x+i, y, z-1+j)
-                for (int i = 0; i < 2; i++) { a_[i] = (x + i) <= nx; b_[i] = (z - 1 + i) >= 0 && (z - 1 + i) <= nz - 1; }
-                weights4(a_, b_, w);
-                for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++)
-                    if (w[i][j] != T(0)) atom(W[W_E5] + g.idx(x + i, y, z - 1 + j), mul_(w[i][j], lab[1]));
-                // Abar6: L6 (x+i, y-1+j, z)
-                for (int i = 0; i < 2; i++) { a_[i] = (x + i) <= nx; b_[i] = (y - 1 + i) >= 0 && (y - 1 + i) <= ny - 1; }
-                weights4(a_, b_, w);
-                for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++)
-                    if (w[i][j] != T(0)) atom(W[W_E6] + g.idx(x + i, y - 1 + j, z), mul_(w[i][j], lab[2]));
-            }
-        }
-        if (E.l6(x, y, z)) {
-            const T a = A.l[SXY][p];
-            if (a != T(0)) {
-                A.gc[20][p] = add_(A.gc[20][p], mul_(a, e6_at(G, p)));
-                atom(W[W_E6] + p, mul_(c[20][p], a));
-                // Q46 over L4 (x-1+i, y, z-1+j)
-                for (int i = 0; i < 2; i++) { a_[i] = (x - 1 + i) >= 0 && (x - 1 + i) <= nx - 1; b_[i] = (z - 1 + i) >= 0 && (z - 1 + i) <= nz - 1; }
-                weights4(a_, b_, w);
-                for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++)
-                    if (w[i][j] != T(0)) atom(W[W_Q46] + g.idx(x - 1 + i, y, z - 1 + j), mul_(w[i][j], a));
-                // Q56 over L5 (x, y+i, z-1+j)
-                for (int i = 0; i < 2; i++) { a_[i] = (y + i) <= ny; b_[i] = (z - 1 + i) >= 0 && (z - 1 + i) <= nz - 1; }
-                weights4(a_, b_, w);
-                for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++)
-                    if (w[i][j] != T(0)) atom(W[W_Q56] + g.idx(x, y + i, z - 1 + j), mul_(w[i][j], a));
-                // P6 over N (x-1+i, y+j, z)
-                for (int i = 0; i < 2; i++) { a_[i] = (x - 1 + i) >= 0 && (x - 1 + i) <= nx - 1; b_[i] = (y + i) <= ny; }
-                weights4(a_, b_, w);
-                for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++)
-                    if (w[i][j] != T(0)) atom(W[W_P6] + g.idx(x - 1 + i, y + j, z), mul_(w[i][j], a));
+                X[X_W + j][p] = le;
+                X[X_S + j][p] = ls;
             }
         }
         if (E.l4(x, y, z)) {
-            T a = A.l[SYZ][p];
-            if (flag && z == 0) {   // surface mirror syz(-1) = -syz(0)
-                a = sub_(a, A.l[SYZ][p - sz]);
+            X[X_E + 3][p] = e4_at(G, p);
+            if (flag && z == 0) {   // syz(-1) = -syz(0)
+                A.l[SYZ][p] = sub_(A.l[SYZ][p], A.l[SYZ][p - sz]);
                 A.l[SYZ][p - sz] = T(0);
-                A.l[SYZ][p] = a;
-            }
-            if (a != T(0)) {
-                // e5 over L5 (x+i, y+j, z); e6 over L6 (x+i, y, z+j); P4 over N (x, y+i, z+j)
-                T v[2][2];
-                bool oa[2], ob[2];
-                for (int i = 0; i < 2; i++) { oa[i] = (x + i) <= nx; ob[i] = (y + i) <= ny; }
-                for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++)
-                    v[i][j] = (oa[i] && ob[j]) ? e5_at(G, g.idx(x + i, y + j, z)) : T(0);
-                const T t5 = avg4<T>(v, oa, ob);
-                weights4(oa, ob, w);
-                const T c45 = c[16][p], c46 = c[17][p];
-                for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++)
-                    if (w[i][j] != T(0)) atom(W[W_E5] + g.idx(x + i, y + j, z), mul_(w[i][j], mul_(c45, a)));
-                for (int i = 0; i < 2; i++) { oa[i] = (x + i) <= nx; ob[i] = (z + i) <= nz; }
-                for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++)
-                    v[i][j] = (oa[i] && ob[j]) ? e6_at(G, g.idx(x + i, y, z + j)) : T(0);
-                const T t6 = avg4<T>(v, oa, ob);
-                weights4(oa, ob, w);
-                for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++)
-                    if (w[i][j] != T(0)) atom(W[W_E6] + g.idx(x + i, y, z + j), mul_(w[i][j], mul_(c46, a)));
-                for (int i = 0; i < 2; i++) { oa[i] = (y + i) <= ny; ob[i] = (z + i) <= nz; }
-                weights4(oa, ob, w);
-                for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++)
-                    if (w[i][j] != T(0)) atom(W[W_P4] + g.idx(x, y + i, z + j), mul_(w[i][j], a));
-                A.gc[15][p] = add_(A.gc[15][p], mul_(a, e4_at(G, p)));
-                A.gc[16][p] = add_(A.gc[16][p], mul_(a, t5));
-                A.gc[17][p] = add_(A.gc[17][p], mul_(a, t6));
-                atom(W[W_E4] + p, mul_(c[15][p], a));
             }
         }
         if (E.l5(x, y, z)) {
-            T a = A.l[SXZ][p];
-            if (flag && z == 0 && x >= 1 && x <= nx - 1 && y >= 1 && y <= ny - 1) {   // surface mirror of sxz
-                a = sub_(a, A.l[SXZ][p - sz]);
+            X[X_E + 4][p] = e5_at(G, p);
+            if (flag && z == 0 && x >= 1 && x <= nx - 1 && y >= 1 && y <= ny - 1) {
+                A.l[SXZ][p] = sub_(A.l[SXZ][p], A.l[SXZ][p - sz]);
                 A.l[SXZ][p - sz] = T(0);
-                A.l[SXZ][p] = a;
-            }
-            if (a != T(0)) {
-                // e6 over L6 (x, y-1+i, z+j); Q45 over L4 (x-1+i, y-1+j, z); P5 over N (x-1+i, y, z+j)
-                T v[2][2];
-                bool oa[2], ob[2];
-                for (int i = 0; i < 2; i++) { oa[i] = (y - 1 + i) >= 0 && (y - 1 + i) <= ny - 1; ob[i] = (z + i) <= nz; }
-                for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++)
-                    v[i][j] = (oa[i] && ob[j]) ? e6_at(G, g.idx(x, y - 1 + i, z + j)) : T(0);
-                const T t6 = avg4<T>(v, oa, ob);
-                weights4(oa, ob, w);
-                const T c56 = c[19][p];
-                for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++)
-                    if (w[i][j] != T(0)) atom(W[W_E6] + g.idx(x, y - 1 + i, z + j), mul_(w[i][j], mul_(c56, a)));
-                for (int i = 0; i < 2; i++) { oa[i] = (x - 1 + i) >= 0 && (x - 1 + i) <= nx - 1; ob[i] = (y - 1 + i) >= 0 && (y - 1 + i) <= ny - 1; }
-                weights4(oa, ob, w);
-                for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++)
-                    if (w[i][j] != T(0)) atom(W[W_Q45] + g.idx(x - 1 + i, y - 1 + j, z), mul_(w[i][j], a));
-                for (int i = 0; i < 2; i++) { oa[i] = (x - 1 + i) >= 0 && (x - 1 + i) <= nx - 1; ob[i] = (z + i) <= nz; }
-                weights4(oa, ob, w);
-                for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++)
-                    if (w[i][j] != T(0)) atom(W[W_P5] + g.idx(x - 1 + i, y, z + j), mul_(w[i][j], a));
-                A.gc[18][p] = add_(A.gc[18][p], mul_(a, e5_at(G, p)));
-                A.gc[19][p] = add_(A.gc[19][p], mul_(a, t6));
-                atom(W[W_E5] + p, mul_(c[18][p], a));
             }
         }
+        if (E.l6(x, y, z)) X[X_E + 5][p] = e6_at(G, p);
     }
 }
 
 template <typename T>
-__global__ void stress21_adj_s2(GridDev<T> G, AdjDev<T> A, int flag)
+__global__ void stress21_adj_g1(GridDev<T> G, AdjDev<T> A, int flag)
 {
     const Geo &g = G.g;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     const Ext E{nx, ny, nz};
     const int64_t n = (int64_t)(nx + 1) * (ny + 1) * (nz + 1);
     const T *const *c = G.c;
-    T *const *W = A.w;
+    T *const *X = A.w;
+    const T *l4 = A.l[SYZ], *l5 = A.l[SXZ], *l6 = A.l[SXY];
+    auto I = [&](int x, int y, int z) { return g.idx(x, y, z); };
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
         const int x = (int)(t % (nx + 1)), y = (int)((t / (nx + 1)) % (ny + 1)), z = (int)(t / ((int64_t)(nx + 1) * (ny + 1)));
-        const int p = g.idx(x, y, z);
-        if (E.l4(x, y, z)) {
-            const T z45 = W[W_Q45][p], z46 = W[W_Q46][p];
-            if (z45 != T(0) || z46 != T(0)) {
-                const T e4 = e4_at(G, p);
-                A.gc[16][p] = add_(A.gc[16][p], mul_(z45, e4));
-                A.gc[17][p] = add_(A.gc[17][p], mul_(z46, e4));
-                W[W_E4][p] = add_(W[W_E4][p], add_(mul_(c[16][p], z45), mul_(c[17][p], z46)));
-                W[W_Q45][p] = T(0);
-                W[W_Q46][p] = T(0);
-            }
-        }
-        if (E.l5(x, y, z)) {
-            const T z56 = W[W_Q56][p];
-            if (z56 != T(0)) {
-                A.gc[19][p] = add_(A.gc[19][p], mul_(z56, e5_at(G, p)));
-                W[W_E5][p] = add_(W[W_E5][p], mul_(c[19][p], z56));
-                W[W_Q56][p] = T(0);
-            }
-        }
+        const int p = I(x, y, z);
+        T v[2][2];
+        bool oa[2], ob[2];
+        // ---- N: adjoints of P4..6 gathered from L4 / L5 / L6, forward averages, gradients
         if (E.n(x, y, z)) {
-            const T zp[3] = {W[W_P4][p], W[W_P5][p], W[W_P6][p]};
-            if (zp[0] != T(0) || zp[1] != T(0) || zp[2] != T(0)) {
-                const bool surf = flag && z == 0;
-                const T e[3] = {e1_at(G, p), e2_at(G, p), e3u_at(G, E, surf, x, y, z, p)};
-                T le[3] = {T(0), T(0), T(0)};
-                for (int k = 0; k < 3; k++)           // P(4+k) = C(1,4+k) e1 + C(2,4+k) e2 + C(3,4+k) e3
-                    for (int j = 0; j < 3; j++) {
-                        const int s = 6 + 3 * j + k;
-                        A.gc[s][p] = add_(A.gc[s][p], mul_(zp[k], e[j]));
-                        le[j] = fma_(c[s][p], zp[k], le[j]);
+            T zp[3] = {T(0), T(0), T(0)};
+            for (int i = 0; i < 2; i++)
+                for (int j = 0; j < 2; j++) {
+                    int qx = x, qy = y - i, qz = z - j;   // L4 tp over N (x, y..y+1, z..z+1)
+                    if (E.l4(qx, qy, qz))
+                        zp[0] = fma_(wgt<T>(qy <= ny, qy + 1 <= ny, qz <= nz, qz + 1 <= nz, i, j), l4[I(qx, qy, qz)], zp[0]);
+                    qx = x + 1 - i; qy = y; qz = z - j;   // L5 tp over N (x-1..x, y, z..z+1)
+                    if (E.l5(qx, qy, qz))
+                        zp[1] = fma_(wgt<T>(in_(qx - 1, 0, nx - 1), in_(qx, 0, nx - 1), qz <= nz, qz + 1 <= nz, i, j),
+                                     l5[I(qx, qy, qz)], zp[1]);
+                    qx = x + 1 - i; qy = y - j; qz = z;   // L6 P6 over N (x-1..x, y..y+1, z)
+                    if (E.l6(qx, qy, qz))
+                        zp[2] = fma_(wgt<T>(in_(qx - 1, 0, nx - 1), in_(qx, 0, nx - 1), qy <= ny, qy + 1 <= ny, i, j),
+                                     l6[I(qx, qy, qz)], zp[2]);
+                }
+            const T e[3] = {X[X_E + 0][p], X[X_E + 1][p], X[X_E + 2][p]};
+            T ab[3];
+            for (int i = 0; i < 2; i++) { oa[i] = in_(y - 1 + i, 0, ny - 1); ob[i] = in_(z - 1 + i, 0, nz - 1); }
+            for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++) v[i][j] = (oa[i] && ob[j]) ? X[X_E + 3][I(x, y - 1 + i, z - 1 + j)] : T(0);
+            ab[0] = avg4<T>(v, oa, ob);
+            for (int i = 0; i < 2; i++) { oa[i] = (x + i) <= nx; ob[i] = in_(z - 1 + i, 0, nz - 1); }
+            for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++) v[i][j] = (oa[i] && ob[j]) ? X[X_E + 4][I(x + i, y, z - 1 + j)] : T(0);
+            ab[1] = avg4<T>(v, oa, ob);
+            for (int i = 0; i < 2; i++) { oa[i] = (x + i) <= nx; ob[i] = in_(y - 1 + i, 0, ny - 1); }
+            for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++) v[i][j] = (oa[i] && ob[j]) ? X[X_E + 5][I(x + i, y - 1 + j, z)] : T(0);
+            ab[2] = avg4<T>(v, oa, ob);
+            const bool surf = flag && z == 0;
+            const T a[3] = {A.l[SXX][p], A.l[SYY][p], surf ? T(0) : A.l[SZZ][p]};
+            const int rowc[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+            for (int i = 0; i < 3; i++)
+                for (int j = 0; j < 3; j++) {
+                    A.gc[rowc[i][j]][p] = add_(A.gc[rowc[i][j]][p], mul_(a[i], e[j]));
+                    A.gc[6 + 3 * i + j][p] = add_(A.gc[6 + 3 * i + j][p], mul_(a[i], ab[j]));
+                }
+            T le[3] = {X[X_W + 0][p], X[X_W + 1][p], X[X_W + 2][p]};
+            for (int k = 0; k < 3; k++)
+                for (int j = 0; j < 3; j++) {
+                    const int s = 6 + 3 * j + k;   // P(4+k) = C(1,4+k) e1 + C(2,4+k) e2 + C(3,4+k) e3
+                    A.gc[s][p] = add_(A.gc[s][p], mul_(zp[k], e[j]));
+                    le[j] = fma_(c[s][p], zp[k], le[j]);
+                }
+            X[X_W + 0][p] = le[0];
+            X[X_W + 1][p] = le[1];
+            X[X_W + 2][p] = le[2];
+        }
+        // ---- L4 q: C44 a4 + C45 Z45 + C46 Z46 + Abar4 adjoints of N
+        if (E.l4(x, y, z)) {
+            const T a4 = l4[p], e4 = X[X_E + 3][p];
+            T z45 = T(0), z46 = T(0), sn = T(0);
+            for (int i = 0; i < 2; i++)
+                for (int j = 0; j < 2; j++) {
+                    int sx = x + 1 - i, sy = y + 1 - j, sz_ = z;   // L5 t45 over L4 (x-1..x, y-1..y, z)
+                    if (E.l5(sx, sy, sz_))
+                        z45 = fma_(wgt<T>(in_(sx - 1, 0, nx - 1), in_(sx, 0, nx - 1), in_(sy - 1, 0, ny - 1), in_(sy, 0, ny - 1), i, j),
+                                   l5[I(sx, sy, sz_)], z45);
+                    sx = x + 1 - i; sy = y; sz_ = z + 1 - j;       // L6 t46 over L4 (x-1..x, y, z-1..z)
+                    if (E.l6(sx, sy, sz_))
+                        z46 = fma_(wgt<T>(in_(sx - 1, 0, nx - 1), in_(sx, 0, nx - 1), in_(sz_ - 1, 0, nz - 1), in_(sz_, 0, nz - 1), i, j),
+                                   l6[I(sx, sy, sz_)], z46);
+                    sx = x; sy = y + 1 - i; sz_ = z + 1 - j;       // N Abar4 over L4 (x, y-1..y, z-1..z)
+                    if (E.n(sx, sy, sz_))
+                        sn = fma_(wgt<T>(in_(sy - 1, 0, ny - 1), in_(sy, 0, ny - 1), in_(sz_ - 1, 0, nz - 1), in_(sz_, 0, nz - 1), i, j),
+                                  X[X_S + 0][I(sx, sy, sz_)], sn);
+                }
+            // forward averages t5 (e5 over L5 (x..x+1, y..y+1, z)) and t6 (e6 over L6 (x..x+1, y, z..z+1))
+            for (int i = 0; i < 2; i++) { oa[i] = (x + i) <= nx; ob[i] = (y + i) <= ny; }
+            for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++) v[i][j] = (oa[i] && ob[j]) ? X[X_E + 4][I(x + i, y + j, z)] : T(0);
+            const T t5 = avg4<T>(v, oa, ob);
+            for (int i = 0; i < 2; i++) { oa[i] = (x + i) <= nx; ob[i] = (z + i) <= nz; }
+            for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++) v[i][j] = (oa[i] && ob[j]) ? X[X_E + 5][I(x + i, y, z + j)] : T(0);
+            const T t6 = avg4<T>(v, oa, ob);
+            A.gc[15][p] = add_(A.gc[15][p], mul_(a4, e4));
+            A.gc[16][p] = add_(A.gc[16][p], add_(mul_(a4, t5), mul_(z45, e4)));
+            A.gc[17][p] = add_(A.gc[17][p], add_(mul_(a4, t6), mul_(z46, e4)));
+            X[X_W + 3][p] = add_(fma_(c[15][p], a4, fma_(c[16][p], z45, mul_(c[17][p], z46))), sn);
+        }
+        // ---- L5 s: C55 a5 + C56 Z56 + Abar5 adjoints of N + C45 a4 from L4's t5
+        if (E.l5(x, y, z)) {
+            const T a5 = l5[p], e5 = X[X_E + 4][p];
+            T z56 = T(0), sn = T(0), s4 = T(0);
+            for (int i = 0; i < 2; i++)
+                for (int j = 0; j < 2; j++) {
+                    int qx = x, qy = y - i, qz = z + 1 - j;      // L6 t56 over L5 (x, y..y+1, z-1..z)
+                    if (E.l6(qx, qy, qz))
+                        z56 = fma_(wgt<T>(qy <= ny, qy + 1 <= ny, in_(qz - 1, 0, nz - 1), in_(qz, 0, nz - 1), i, j), l6[I(qx, qy, qz)], z56);
+                    qx = x - i; qy = y; qz = z + 1 - j;          // N Abar5 over L5 (x..x+1, y, z-1..z)
+                    if (E.n(qx, qy, qz))
+                        sn = fma_(wgt<T>(qx <= nx, qx + 1 <= nx, in_(qz - 1, 0, nz - 1), in_(qz, 0, nz - 1), i, j),
+                                  X[X_S + 1][I(qx, qy, qz)], sn);
+                    qx = x - i; qy = y - j; qz = z;              // L4 t5 over L5 (x..x+1, y..y+1, z)
+                    if (E.l4(qx, qy, qz)) {
+                        const int q = I(qx, qy, qz);
+                        s4 = fma_(wgt<T>(qx <= nx, qx + 1 <= nx, qy <= ny, qy + 1 <= ny, i, j), mul_(c[16][q], l4[q]), s4);
                     }
-                W[W_E1][p] = add_(W[W_E1][p], le[0]);
-                W[W_E2][p] = add_(W[W_E2][p], le[1]);
-                W[W_E3][p] = add_(W[W_E3][p], le[2]);
-                W[W_P4][p] = T(0); W[W_P5][p] = T(0); W[W_P6][p] = T(0);
-            }
+                }
+            // forward average t6 (e6 over L6 (x, y-1..y, z..z+1))
+            for (int i = 0; i < 2; i++) { oa[i] = in_(y - 1 + i, 0, ny - 1); ob[i] = (z + i) <= nz; }
+            for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++) v[i][j] = (oa[i] && ob[j]) ? X[X_E + 5][I(x, y - 1 + i, z + j)] : T(0);
+            const T t6 = avg4<T>(v, oa, ob);
+            A.gc[18][p] = add_(A.gc[18][p], mul_(a5, e5));
+            A.gc[19][p] = add_(A.gc[19][p], add_(mul_(a5, t6), mul_(z56, e5)));
+            X[X_W + 4][p] = add_(add_(fma_(c[18][p], a5, mul_(c[19][p], z56)), sn), s4);
+        }
+        // ---- L6 t: C66 a6 + Abar6 adjoints of N + C46 a4 (L4 t6) + C56 a5 (L5 t6)
+        if (E.l6(x, y, z)) {
+            const T a6 = l6[p];
+            T sn = T(0), s4 = T(0), s5 = T(0);
+            for (int i = 0; i < 2; i++)
+                for (int j = 0; j < 2; j++) {
+                    int qx = x - i, qy = y + 1 - j, qz = z;      // N Abar6 over L6 (x..x+1, y-1..y, z)
+                    if (E.n(qx, qy, qz))
+                        sn = fma_(wgt<T>(qx <= nx, qx + 1 <= nx, in_(qy - 1, 0, ny - 1), in_(qy, 0, ny - 1), i, j),
+                                  X[X_S + 2][I(qx, qy, qz)], sn);
+                    qx = x - i; qy = y; qz = z - j;              // L4 t6 over L6 (x..x+1, y, z..z+1)
+                    if (E.l4(qx, qy, qz)) {
+                        const int q = I(qx, qy, qz);
+                        s4 = fma_(wgt<T>(qx <= nx, qx + 1 <= nx, qz <= nz, qz + 1 <= nz, i, j), mul_(c[17][q], l4[q]), s4);
+                    }
+                    qx = x; qy = y + 1 - i; qz = z - j;          // L5 t6 over L6 (x, y-1..y, z..z+1)
+                    if (E.l5(qx, qy, qz)) {
+                        const int q = I(qx, qy, qz);
+                        s5 = fma_(wgt<T>(in_(qy - 1, 0, ny - 1), in_(qy, 0, ny - 1), qz <= nz, qz + 1 <= nz, i, j),
+                                  mul_(c[19][q], l5[q]), s5);
+                    }
+                }
+            A.gc[20][p] = add_(A.gc[20][p], mul_(a6, X[X_E + 5][p]));
+            X[X_W + 5][p] = add_(add_(fma_(c[20][p], a6, sn), s4), s5);
         }
     }
 }
 
 // free surface: e3 = -(C13 e1 + C23 e2 + C34 A4 + C35 A5 + C36 A6) / C33 at z = 0
 template <typename T>
-__global__ void stress21_adj_s3(GridDev<T> G, AdjDev<T> A)
+__global__ void stress21_adj_g2(GridDev<T> G, AdjDev<T> A)
 {
     const Geo &g = G.g;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
-    const Ext E{nx, ny, nz};
     const int n = nx * (ny + 1);
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
     const int x = t % nx, y = t / nx, z = 0;
     const int p = g.idx(x, y, z);
-    const T le3 = A.w[W_E3][p];
+    T *const *X = A.w;
+    const T le3 = X[X_W + 2][p];
     if (le3 == T(0)) return;
-    A.w[W_E3][p] = T(0);
+    X[X_W + 2][p] = T(0);
     const T *const *c = G.c;
     const T c33 = c[5][p];
-    const T e1 = e1_at(G, p), e2 = e2_at(G, p), e3 = e3u_at(G, E, true, x, y, z, p);
-    const T ab[3] = {abar4_g(G, E, x, y, z), abar5_g(G, E, x, y, z), abar6_g(G, E, x, y, z)};
+    const T e1 = X[X_E + 0][p], e2 = X[X_E + 1][p], e3 = X[X_E + 2][p];
+    T v[2][2], w[2][2];
+    bool oa[2], ob[2];
+    T ab[3];
+    int bx[3][2][2], by[3][2][2], bz[3][2][2];
+    T bw[3][2][2];
+    // Abar4: L4 (x, y-1+i, z-1+j); Abar5: L5 (x+i, y, z-1+j); Abar6: L6 (x+i, y-1+j, z)
+    for (int k = 0; k < 3; k++) {
+        for (int i = 0; i < 2; i++) {
+            if (k == 0) { oa[i] = in_(y - 1 + i, 0, ny - 1); ob[i] = in_(z - 1 + i, 0, nz - 1); }
+            else if (k == 1) { oa[i] = (x + i) <= nx; ob[i] = in_(z - 1 + i, 0, nz - 1); }
+            else { oa[i] = (x + i) <= nx; ob[i] = in_(y - 1 + i, 0, ny - 1); }
+        }
+        for (int i = 0; i < 2; i++)
+            for (int j = 0; j < 2; j++) {
+                bx[k][i][j] = k == 0 ? x : x + i;
+                by[k][i][j] = k == 0 ? y - 1 + i : (k == 1 ? y : y - 1 + j);
+                bz[k][i][j] = k == 2 ? z : z - 1 + j;
+                v[i][j] = (oa[i] && ob[j]) ? X[X_E + 3 + k][g.idx(bx[k][i][j], by[k][i][j], bz[k][i][j])] : T(0);
+            }
+        ab[k] = avg4<T>(v, oa, ob);
+        weights4(oa, ob, w);
+        for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++) bw[k][i][j] = w[i][j];
+    }
     const T u = -div_(le3, c33);   // d e3 / d(numerator term) = -1 / C33
-    A.w[W_E1][p] = fma_(u, c[2][p], A.w[W_E1][p]);
-    A.w[W_E2][p] = fma_(u, c[4][p], A.w[W_E2][p]);
+    X[X_W + 0][p] = fma_(u, c[2][p], X[X_W + 0][p]);
+    X[X_W + 1][p] = fma_(u, c[4][p], X[X_W + 1][p]);
     A.gc[2][p] = fma_(u, e1, A.gc[2][p]);
     A.gc[4][p] = fma_(u, e2, A.gc[4][p]);
     A.gc[5][p] = fma_(u, e3, A.gc[5][p]);   // d e3 / d C33 = -e3 / C33
-    for (int k = 0; k < 3; k++) A.gc[12 + k][p] = fma_(u, ab[k], A.gc[12 + k][p]);
-    bool a_[2], b_[2];
-    T w[2][2];
-    const T l4 = mul_(u, c[12][p]), l5 = mul_(u, c[13][p]), l6 = mul_(u, c[14][p]);
-    for (int i = 0; i < 2; i++) { a_[i] = (y - 1 + i) >= 0 && (y - 1 + i) <= ny - 1; b_[i] = (z - 1 + i) >= 0 && (z - 1 + i) <= nz - 1; }
-    weights4(a_, b_, w);
-    for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++)
-        if (w[i][j] != T(0)) atom(A.w[W_E4] + g.idx(x, y - 1 + i, z - 1 + j), mul_(w[i][j], l4));
-    for (int i = 0; i < 2; i++) { a_[i] = (x + i) <= nx; b_[i] = (z - 1 + i) >= 0 && (z - 1 + i) <= nz - 1; }
-    weights4(a_, b_, w);
-    for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++)
-        if (w[i][j] != T(0)) atom(A.w[W_E5] + g.idx(x + i, y, z - 1 + j), mul_(w[i][j], l5));
-    for (int i = 0; i < 2; i++) { a_[i] = (x + i) <= nx; b_[i] = (y - 1 + i) >= 0 && (y - 1 + i) <= ny - 1; }
-    weights4(a_, b_, w);
-    for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++)
-        if (w[i][j] != T(0)) atom(A.w[W_E6] + g.idx(x + i, y - 1 + j, z), mul_(w[i][j], l6));
+    for (int k = 0; k < 3; k++) {
+        A.gc[12 + k][p] = fma_(u, ab[k], A.gc[12 + k][p]);
+        const T lk = mul_(u, c[12 + k][p]);
+        for (int i = 0; i < 2; i++)
+            for (int j = 0; j < 2; j++)
+                if (bw[k][i][j] != T(0)) atom(X[X_W + 3 + k] + g.idx(bx[k][i][j], by[k][i][j], bz[k][i][j]), mul_(bw[k][i][j], lk));
+    }
 }
 
-// transpose of the strain differences: W[e] -> lambda_v; the buffers are cleared
+// transpose of the strain differences: every velocity entry gathers the W of
+// the strains that read it
 template <typename T>
-__global__ void stress21_adj_s4(GridDev<T> G, AdjDev<T> A)
+__global__ void stress21_adj_g3(GridDev<T> G, AdjDev<T> A)
 {
     const Geo &g = G.g;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     const Ext E{nx, ny, nz};
-    const int64_t n = (int64_t)(nx + 1) * (ny + 1) * (nz + 1);
-    const int sy = g.px, sz = g.px * g.py;
+    const int64_t n = (int64_t)(nx + 2) * (ny + 2) * (nz + 2);   // x, y, z in [-1, n]
     const T k0 = G.k[0], k1 = G.k[1], k2 = G.k[2];
-    T *lvx = A.l[VX], *lvy = A.l[VY], *lvz = A.l[VZ];
-    T *const *W = A.w;
+    T *const *X = A.w;
+    auto I = [&](int x, int y, int z) { return g.idx(x, y, z); };
+    auto W = [&](int k, bool ok, int x, int y, int z) -> T { return ok ? X[X_W + k][I(x, y, z)] : T(0); };
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
-        const int x = (int)(t % (nx + 1)), y = (int)((t / (nx + 1)) % (ny + 1)), z = (int)(t / ((int64_t)(nx + 1) * (ny + 1)));
-        const int p = g.idx(x, y, z);
-        if (E.n(x, y, z)) {
-            const T w1 = W[W_E1][p], w2_ = W[W_E2][p], w3 = W[W_E3][p];
-            if (w1 != T(0)) { const T u = mul_(k0, w1); atom(lvx + p + 1, u); atom(lvx + p, -u); W[W_E1][p] = T(0); }
-            if (w2_ != T(0)) { const T u = mul_(k1, w2_); atom(lvy + p, u); atom(lvy + p - sy, -u); W[W_E2][p] = T(0); }
-            if (w3 != T(0)) { const T u = mul_(k2, w3); atom(lvz + p, u); atom(lvz + p - sz, -u); W[W_E3][p] = T(0); }
-        }
-        if (E.l4(x, y, z)) {
-            const T w4 = W[W_E4][p];
-            if (w4 != T(0)) {
-                const T u2 = mul_(k2, w4), u1 = mul_(k1, w4);
-                atom(lvy + p + sz, u2); atom(lvy + p, -u2); atom(lvz + p + sy, u1); atom(lvz + p, -u1);
-                W[W_E4][p] = T(0);
-            }
-        }
-        if (E.l5(x, y, z)) {
-            const T w5 = W[W_E5][p];
-            if (w5 != T(0)) {
-                const T u2 = mul_(k2, w5), u0 = mul_(k0, w5);
-                atom(lvx + p + sz, u2); atom(lvx + p, -u2); atom(lvz + p, u0); atom(lvz + p - 1, -u0);
-                W[W_E5][p] = T(0);
-            }
-        }
-        if (E.l6(x, y, z)) {
-            const T w6 = W[W_E6][p];
-            if (w6 != T(0)) {
-                const T u1 = mul_(k1, w6), u0 = mul_(k0, w6);
-                atom(lvx + p + sy, u1); atom(lvx + p, -u1); atom(lvy + p, u0); atom(lvy + p - 1, -u0);
-                W[W_E6][p] = T(0);
-            }
-        }
+        const int x = (int)(t % (nx + 2)) - 1, y = (int)((t / (nx + 2)) % (ny + 2)) - 1, z = (int)(t / ((int64_t)(nx + 2) * (ny + 2))) - 1;
+        const int p = I(x, y, z);
+        // vx: e1(N x-1) - e1(N x), e5(L5 z-1) - e5(L5 z), e6(L6 y-1) - e6(L6 y)
+        const T gx = add_(add_(mul_(k0, sub_(W(0, E.n(x - 1, y, z), x - 1, y, z), W(0, E.n(x, y, z), x, y, z))),
+                               mul_(k2, sub_(W(4, E.l5(x, y, z - 1), x, y, z - 1), W(4, E.l5(x, y, z), x, y, z)))),
+                          mul_(k1, sub_(W(5, E.l6(x, y - 1, z), x, y - 1, z), W(5, E.l6(x, y, z), x, y, z))));
+        // vy: e2(N y) - e2(N y+1), e4(L4 z-1) - e4(L4 z), e6(L6 x) - e6(L6 x+1)
+        const T gy = add_(add_(mul_(k1, sub_(W(1, E.n(x, y, z), x, y, z), W(1, E.n(x, y + 1, z), x, y + 1, z))),
+                               mul_(k2, sub_(W(3, E.l4(x, y, z - 1), x, y, z - 1), W(3, E.l4(x, y, z), x, y, z)))),
+                          mul_(k0, sub_(W(5, E.l6(x, y, z), x, y, z), W(5, E.l6(x + 1, y, z), x + 1, y, z))));
+        // vz: e3(N z) - e3(N z+1), e4(L4 y-1) - e4(L4 y), e5(L5 x) - e5(L5 x+1)
+        const T gz = add_(add_(mul_(k2, sub_(W(2, E.n(x, y, z), x, y, z), W(2, E.n(x, y, z + 1), x, y, z + 1))),
+                               mul_(k1, sub_(W(3, E.l4(x, y - 1, z), x, y - 1, z), W(3, E.l4(x, y, z), x, y, z)))),
+                          mul_(k0, sub_(W(4, E.l5(x, y, z), x, y, z), W(4, E.l5(x + 1, y, z), x + 1, y, z))));
+        if (gx != T(0)) A.l[VX][p] = add_(A.l[VX][p], gx);
+        if (gy != T(0)) A.l[VY][p] = add_(A.l[VY][p], gy);
+        if (gz != T(0)) A.l[VZ][p] = add_(A.l[VZ][p], gz);
     }
 }
 
@@ -493,10 +504,10 @@ cudaError_t launch_stress21_adj(const GridDev<T> &G, const AdjDev<T> &A, int top
     const int flag = (top && top_bc) ? 1 : 0;
     const int64_t n = (int64_t)(g.nx + 1) * (g.ny + 1) * (g.nz + 1);
     const unsigned nb = blocks_for(n, sms);
-    stress21_adj_s1<T><<<nb, 256, 0, st>>>(G, A, flag);
-    stress21_adj_s2<T><<<nb, 256, 0, st>>>(G, A, flag);
-    if (flag) stress21_adj_s3<T><<<(g.nx * (g.ny + 1) + 255) / 256, 256, 0, st>>>(G, A);
-    stress21_adj_s4<T><<<nb, 256, 0, st>>>(G, A);
+    stress21_adj_g0<T><<<nb, 256, 0, st>>>(G, A, flag);
+    stress21_adj_g1<T><<<nb, 256, 0, st>>>(G, A, flag);
+    if (flag) stress21_adj_g2<T><<<(g.nx * (g.ny + 1) + 255) / 256, 256, 0, st>>>(G, A);
+    stress21_adj_g3<T><<<blocks_for((int64_t)(g.nx + 2) * (g.ny + 2) * (g.nz + 2), sms), 256, 0, st>>>(G, A);
     return cudaGetLastError();
 }
 

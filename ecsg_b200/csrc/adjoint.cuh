@@ -10,7 +10,7 @@ struct AdjDev {
     T *l[9];     // adjoint of the 9 fields, the grid's box layout
     T *gb;       // gradient w.r.t. the node buoyancy
     T *gc[21];   // gradient w.r.t. the 21 stiffness slots
-    T *w[12];    // work buffers, zero between operators
+    T *w[15];    // work boxes of the stress adjoint (strains, average adjoints, strain adjoints)
 };
 
 // Receiver adjoint sources of one step: lambda_{comp}[grid][off] += res[i].

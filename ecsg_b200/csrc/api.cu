@@ -1321,7 +1321,7 @@ static int adj_alloc(ecsg_sim *s)
         if ((rc = dmalloc(s, &s->gcblk[g], 21 * fb))) return rc;
     }
     s->wbox = maxbox;
-    if ((rc = dmalloc(s, &s->wblk, 12 * maxbox * s->tsize))) return rc;
+    if ((rc = dmalloc(s, &s->wblk, 15 * maxbox * s->tsize))) return rc;
     for (int i = 1; i < s->ng; i++) {
         const Geo &C = s->geo[i];
         const size_t m = (size_t)(C.ny - 1) * C.nx, nn = (size_t)(C.nx - 1) * (C.ny - 1), nxy = (size_t)(C.nx + 1) * (C.ny + 1);
@@ -1342,7 +1342,7 @@ static AdjDev<T> adj_dev(const ecsg_sim *s, int g)
     for (int k = 0; k < 9; k++) A.l[k] = (T *)s->lblk[g] + k * box;
     A.gb = (T *)s->gbblk[g];
     for (int k = 0; k < 21; k++) A.gc[k] = (T *)s->gcblk[g] + k * box;
-    for (int k = 0; k < 12; k++) A.w[k] = (T *)s->wblk + k * s->wbox;
+    for (int k = 0; k < 15; k++) A.w[k] = (T *)s->wblk + k * s->wbox;
     return A;
 }
 
@@ -1365,7 +1365,7 @@ static int adj_zero(ecsg_sim *s, bool fields, bool grads)
             CK(cudaMemsetAsync(s->gcblk[g], 0, 21 * fb, s->st));
         }
     }
-    CK(cudaMemsetAsync(s->wblk, 0, 12 * s->wbox * s->tsize, s->st));
+    CK(cudaMemsetAsync(s->wblk, 0, 15 * s->wbox * s->tsize, s->st));
     for (int i = 1; i < s->ng; i++) {
         const Geo &C = s->geo[i];
         CK(cudaMemsetAsync(s->adj_Y0[i], 0, sizeof(double) * (C.nx + 1) * (C.ny + 1), s->st));

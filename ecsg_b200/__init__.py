@@ -38,7 +38,7 @@ class Config(ctypes.Structure):
     _fields_ = [("num_grids", ctypes.c_int), ("radius", ctypes.c_int), ("dt", ctypes.c_double),
                 ("imode", ctypes.c_int), ("top_bc", ctypes.c_int), ("precision", ctypes.c_int),
                 ("medium", ctypes.c_int), ("energy", ctypes.c_int), ("jacobi_max_iter", ctypes.c_int),
-                ("device", ctypes.c_int), ("mirror_fix", ctypes.c_int)]
+                ("device", ctypes.c_int), ("mirror_fix", ctypes.c_int), ("ii_skip_end_column", ctypes.c_int)]
 
 
 class GridView(ctypes.Structure):
@@ -167,7 +167,8 @@ class Simulation:
                      top_bc=case.top_bc, precision=ECSG_F32 if precision == "f32" else ECSG_F64,
                      medium=_MEDIUM[case.medium],
                      energy=1 if energy else 0, jacobi_max_iter=jacobi_max_iter, device=device,
-                     mirror_fix=1 if getattr(case, "mirror_fix", False) else 0)
+                     mirror_fix=1 if getattr(case, "mirror_fix", False) else 0,
+                     ii_skip_end_column=1 if getattr(case, "ii_skip_end_column", False) else 0)
         h = ctypes.c_void_p()
         rc = L.ecsg_create(descs, ctypes.byref(cfg), ctypes.byref(h))
         if rc != ECSG_OK:

@@ -40,6 +40,8 @@ cudaError_t launch_ghost_vz(const GridDev<T> &, const GridDev<T> &, int, int, do
 template <typename T>
 cudaError_t launch_ghost_syz(const GridDev<T> &, const GridDev<T> &, int, cudaStream_t);
 template <typename T>
+cudaError_t launch_ghost_ii(int, const GridDev<T> &, const GridDev<T> &, cudaStream_t);
+template <typename T>
 cudaError_t launch_sxz_matrix(const GridDev<T> &, const GridDev<T> &, int, double *, cudaStream_t);
 template <typename T>
 int sxz_solve_blocks(int, int);
@@ -79,6 +81,9 @@ template <typename T>
 cudaError_t launch_ghost_syz_adj(const GridDev<T> &, const GridDev<T> &, const AdjDev<T> &, const AdjDev<T> &, int,
                                  cudaStream_t);
 template <typename T>
+cudaError_t launch_ghost_ii_adj(int, const GridDev<T> &, const GridDev<T> &, const AdjDev<T> &, const AdjDev<T> &,
+                                cudaStream_t);
+template <typename T>
 cudaError_t launch_ghost_sxz_adj(const GridDev<T> &, const GridDev<T> &, const AdjDev<T> &, const AdjDev<T> &, int,
                                  const SxzWork &, int, double *, cudaStream_t);
 // medium.cu
@@ -108,7 +113,7 @@ struct Iface {
 
 struct ecsg_sim {
     int ng = 0, R = 1, imode = 1, top_bc = 0, prec = ECSG_F32, medium = ECSG_MEDIUM_ISO, energy = 0;
-    int jacobi_max_iter = 10000, device = 0, sms = 148, mirror_fix = 0;
+    int jacobi_max_iter = 10000, device = 0, sms = 148, mirror_fix = 0, ii_skip_end = 0;
     bool scalar_stencils = false;   // FP32: use the scalar sweeps of stencil.cu (validation)
     double dt = 0;
     size_t tsize = 4;
@@ -257,7 +262,7 @@ static int create_impl(const ecsg_grid_desc *grids, const ecsg_config *cfg, ecsg
     if (cfg->num_grids < 1 || cfg->num_grids > kMaxGrids) { fail(s, ECSG_ERR_INVALID, "num_grids out of range"); return bail(ECSG_ERR_INVALID); }
     if (cfg->radius != 1) { fail(s, ECSG_ERR_INVALID, "radius %d: the device path implements radius 1", cfg->radius); return bail(ECSG_ERR_INVALID); }
     if (!(cfg->dt > 0)) { fail(s, ECSG_ERR_INVALID, "dt must be positive"); return bail(ECSG_ERR_INVALID); }
-    if (cfg->imode != ECSG_MODE_ECI) { fail(s, ECSG_ERR_INVALID, "imode %d not supported (energy-conserving mode 1 only)", cfg->imode); return bail(ECSG_ERR_INVALID); }
+    if (cfg->imode != ECSG_MODE_ECI && cfg->imode != ECSG_MODE_II) { fail(s, ECSG_ERR_INVALID, "imode %d: 0 (intuitive) or 1 (energy-conserving)", cfg->imode); return bail(ECSG_ERR_INVALID); }
     if (cfg->precision != ECSG_F32 && cfg->precision != ECSG_F64) { fail(s, ECSG_ERR_INVALID, "precision"); return bail(ECSG_ERR_INVALID); }
     if (cfg->medium != ECSG_MEDIUM_ISO && cfg->medium != ECSG_MEDIUM_ORTHO9 && cfg->medium != ECSG_MEDIUM_GEN21) { fail(s, ECSG_ERR_INVALID, "medium"); return bail(ECSG_ERR_INVALID); }
     s->ng = cfg->num_grids;
@@ -271,6 +276,7 @@ static int create_impl(const ecsg_grid_desc *grids, const ecsg_config *cfg, ecsg
     s->jacobi_max_iter = cfg->jacobi_max_iter > 0 ? cfg->jacobi_max_iter : 10000;
     s->device = cfg->device;
     s->mirror_fix = cfg->mirror_fix ? 1 : 0;
+    s->ii_skip_end = cfg->ii_skip_end_column ? 1 : 0;
     {
         const char *env = getenv("ECSG_SCALAR_STENCILS");
         s->scalar_stencils = env && env[0] == '1';
@@ -300,6 +306,7 @@ static int create_impl(const ecsg_grid_desc *grids, const ecsg_config *cfg, ecsg
         if (r < 2 || fabs(rx - r) > 1e-6 * r || fabs(s->h[i][1] / s->h[i - 1][1] - r) > 1e-6 * r) { fail(s, ECSG_ERR_INVALID, "interface %d: x/y refinement ratio must be an integer >= 2", i); return bail(ECSG_ERR_INVALID); }
         if (grids[i - 1].size[0] != r * grids[i].size[0] || grids[i - 1].size[1] != r * grids[i].size[1]) { fail(s, ECSG_ERR_INVALID, "interface %d: fine size must be ratio * coarse size in x and y", i); return bail(ECSG_ERR_INVALID); }
         if (grids[i].size[1] - 1 > 1024) { fail(s, ECSG_ERR_INVALID, "interface %d: coarse ny %d above the 1025 supported by the vz solve", i, grids[i].size[1]); return bail(ECSG_ERR_INVALID); }
+        if (cfg->imode == ECSG_MODE_II && r != 2) { fail(s, ECSG_ERR_INVALID, "interface %d: intuitive interpolation (imode 0) is defined for ratio 2 only", i); return bail(ECSG_ERR_INVALID); }
         s->itf[i].r = r;
     }
     int rc;
@@ -374,7 +381,8 @@ int ecsg_create_shot(const ecsg_sim *model, ecsg_sim **out)
         for (int d = 0; d < 3; d++) gd[g].step[d] = model->h[g][d];
     }
     ecsg_config cfg = {model->ng, model->R, model->dt, model->imode, model->top_bc, model->prec, model->medium,
-                       model->energy, model->jacobi_max_iter, model->device, model->mirror_fix};
+                       model->energy, model->jacobi_max_iter, model->device, model->mirror_fix,
+                       model->ii_skip_end};
     return create_impl(gd.data(), &cfg, out, model);
 }
 
@@ -703,6 +711,10 @@ static int stress_op(ecsg_sim *s, int g, int top = -1)
 template <typename T>
 static int vz_op(ecsg_sim *s, int i)
 {
+    if (s->imode == ECSG_MODE_II) {
+        CK(launch_ghost_ii<T>(s->ii_skip_end ? 3 : 0, dev<T>(s, i - 1), dev<T>(s, i), s->st));
+        return ECSG_OK;
+    }
     CK(launch_ghost_vz<T>(dev<T>(s, i - 1), dev<T>(s, i), med_kind(s), s->itf[i].r,
                           s->itf[i].vzc, s->st));
     return ECSG_OK;
@@ -711,6 +723,10 @@ static int vz_op(ecsg_sim *s, int i)
 template <typename T>
 static int syz_op(ecsg_sim *s, int i)
 {
+    if (s->imode == ECSG_MODE_II) {
+        CK(launch_ghost_ii<T>(2, dev<T>(s, i - 1), dev<T>(s, i), s->st));
+        return ECSG_OK;
+    }
     CK(launch_ghost_syz<T>(dev<T>(s, i - 1), dev<T>(s, i), s->itf[i].r, s->st));
     return ECSG_OK;
 }
@@ -719,6 +735,7 @@ template <typename T>
 static int sxz_prepare(ecsg_sim *s, int i)
 {
     Iface &I = s->itf[i];
+    if (s->imode == ECSG_MODE_II) return ECSG_OK;   // explicit: no system to assemble
     if (!I.A_ready) {
         CK(launch_sxz_matrix<T>(dev<T>(s, i - 1), dev<T>(s, i), I.r, I.A, s->st));
         I.A_ready = true;
@@ -729,6 +746,10 @@ static int sxz_prepare(ecsg_sim *s, int i)
 template <typename T>
 static int sxz_op(ecsg_sim *s, int i)
 {
+    if (s->imode == ECSG_MODE_II) {
+        CK(launch_ghost_ii<T>(1, dev<T>(s, i - 1), dev<T>(s, i), s->st));
+        return ECSG_OK;
+    }
     Iface &I = s->itf[i];
     SxzWork W;
     W.A = I.A;
@@ -1377,6 +1398,11 @@ template <typename T>
 static int adj_op_impl(ecsg_sim *s, int op, int i, const GridDev<T> *Gv)
 {
     // Gv: the forward fields of every grid the operator reads (its output state)
+    if (s->imode == ECSG_MODE_II && (op == ECSG_ADJ_GHOST_VZ || op == ECSG_ADJ_GHOST_SXZ || op == ECSG_ADJ_GHOST_SYZ)) {
+        const int which = op == ECSG_ADJ_GHOST_VZ ? (s->ii_skip_end ? 3 : 0) : (op == ECSG_ADJ_GHOST_SXZ ? 1 : 2);
+        CK(launch_ghost_ii_adj<T>(which, Gv[i - 1], Gv[i], adj_dev<T>(s, i - 1), adj_dev<T>(s, i), s->st));
+        return ECSG_OK;
+    }
     switch (op) {
     case ECSG_ADJ_VEL:
         CK(launch_vel_adj<T>(Gv[i], adj_dev<T>(s, i), i == 0, i == s->ng - 1, s->top_bc, s->mirror_fix, s->sms, s->st));

@@ -883,6 +883,306 @@ __global__ void sxz_adj_fine(GridDev<T> F, GridDev<T> C, AdjDev<T> AF, AdjDev<T>
 }
 
 // ---------------------------------------------------------------------------
+// Intuitive interpolation (imode 0, ratio 2): explicit ghosts
+// (update_ghost_vz.cpp:36-123, update_ghost_sxz.cpp:37-84,
+// update_ghost_syz.cpp:23-150).  One thread per fine ghost point of the
+// interface plane; the thread at fine (2 j0, 2 j1) also writes the coarse
+// ghost of (j0, j1).  Each op reads only fine planes nz1-2, nz1-1 and the
+// coarse plane 0 and writes only the ghost planes, so the threads are
+// independent.  Every formula adds its terms in the reference's order and
+// with the reference's types: with T = float the T-typed terms round in float
+// and the terms the reference writes with double literals (0.375 * x,
+// x * 2 / 3.0) in double, as in its float build; with T = double all of it is
+// double.  The file is compiled without FMA contraction.
+// ---------------------------------------------------------------------------
+
+// The element the reference's row-major Field (rows of len0 = extent + 2R)
+// reads at (x, y) of a z-plane when x runs past the end of the row: the same
+// linear offset, re-split into (x, y).  Identity for x inside the row.
+__device__ __forceinline__ void row_major_wrap(int x, int y, int len0, int R, int &xo, int &yo)
+{
+    const int l = (y + R) * len0 + (x + R);
+    yo = l / len0 - R;
+    xo = l % len0 - R;
+}
+
+// skip_end: leave the fine ghosts of the last x column as they are (the
+// revision of update_ghost_vz.cpp that produced the II golden traces)
+template <typename T>
+__global__ void ghost_vz_ii_kernel(GridDev<T> F, GridDev<T> C, int skip_end)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int nx2 = C.g.nx, ny2 = C.g.ny, nz1 = F.g.nz;
+    const int nx1 = 2 * nx2, ny1 = 2 * ny2;
+    if (x >= nx1 || y >= ny1) return;
+    T *vz1 = F.f[VZ];
+    T *vz2 = C.f[VZ];
+    const int sz1 = F.g.px * F.g.py;
+    const int pf = F.g.idx(x, y, nz1);
+    if (!(x & 1) && !(y & 1) && y > 0) {   // coarse ghost (x/2, y/2, -1), update_ghost_vz.cpp:46-50
+        const int q2 = pf - 2 * sz1, q1 = pf - sz1;
+        const T s = vz1[q2] + vz1[q2 + 1] + vz1[q1] + vz1[q1 + 1];
+        vz2[C.g.idx(x / 2, y / 2, -1)] = (T)(0.25 * (double)s);
+    }
+    if (skip_end && x == nx1 - 1) return;
+    const T own = vz1[pf - sz1];
+    const int j1 = y / 2, odd_y = y & 1;
+    T v;
+    if (x >= 1 && x <= nx1 - 2) {   // update_ghost_vz.cpp:57-81
+        const int j0 = (x - 1) / 2, second = (x - 1) & 1;
+        const int p0 = C.g.idx(j0, j1, 0);
+        const T c00 = vz2[p0], c10 = vz2[p0 + 1];
+        if (!odd_y) {
+            v = second ? own / (T)3 + c00 / (T)6 + c10 / (T)2 : own / (T)3 + c00 / (T)2 + c10 / (T)6;
+        } else {
+            const T c01 = vz2[p0 + C.g.px], c11 = vz2[p0 + C.g.px + 1];
+            v = second ? own / (T)3 + c00 / (T)12 + c10 / (T)4 + c01 / (T)12 + c11 / (T)4
+                       : own / (T)3 + c00 / (T)4 + c10 / (T)12 + c01 / (T)4 + c11 / (T)12;
+        }
+    } else {   // x = 0 or nx1-1: update_ghost_vz.cpp:87-110
+        const int xin = (x == 0) ? 1 : x - 1;
+        // the coarse x index is the fine x (nx1-1 at the far column): read where the
+        // reference's layout puts it (rows of nx2 + 2R elements for vz)
+        int cx0, cy0, cx1, cy1;
+        row_major_wrap(x, j1, nx2 + 2 * C.g.R, C.g.R, cx0, cy0);
+        row_major_wrap(x, j1 + 1, nx2 + 2 * C.g.R, C.g.R, cx1, cy1);
+        const T ca = vz2[C.g.idx(cx0, cy0, 0)];
+        if (!odd_y) {
+            v = own * (T)2 / (T)3 - vz1[F.g.idx(xin, y, nz1 - 1)] / (T)3 + ca * (T)2 / (T)3;
+        } else {
+            const T cb = vz2[C.g.idx(cx1, cy1, 0)];
+            v = own * (T)2 / (T)3 - vz1[F.g.idx(xin, y - 1, nz1 - 1)] / (T)3 + ca / (T)3 + cb / (T)3;
+        }
+    }
+    vz1[pf] = v;
+}
+
+template <typename T>
+__global__ void ghost_sxz_ii_kernel(GridDev<T> F, GridDev<T> C)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int nx2 = C.g.nx, ny2 = C.g.ny, nz1 = F.g.nz;
+    if (x >= 2 * nx2 || y >= 2 * ny2) return;
+    T *sxz1 = F.f[SXZ];
+    T *sxz2 = C.f[SXZ];
+    const int sz1 = F.g.px * F.g.py;
+    const int pf = F.g.idx(x, y, nz1);
+    const int j0 = x / 2, j1 = y / 2;
+    const int p0 = C.g.idx(j0, j1, 0), sy2 = C.g.px;
+    if (!(x & 1) && !(y & 1))   // update_ghost_sxz.cpp:46-49
+        sxz2[p0 - C.g.px * C.g.py] = (T)(0.5 * (double)(sxz1[pf - 2 * sz1] + sxz1[pf - sz1]));
+    const T own = sxz1[pf - sz1];
+    T v;
+    switch ((x & 1) | ((y & 1) << 1)) {   // update_ghost_sxz.cpp:55-81
+    case 0: v = (T)((double)(own / (T)3) + (double)(sxz2[p0] * (T)2) / 3.0); break;
+    case 1: v = own / (T)3 + sxz2[p0] / (T)3 + sxz2[p0 + 1] / (T)3; break;
+    case 2: v = own / (T)3 + sxz2[p0] / (T)3 + sxz2[p0 + sy2] / (T)3; break;
+    default:
+        v = own / (T)3 + sxz2[p0] / (T)6 + sxz2[p0 + sy2] / (T)6 + sxz2[p0 + 1] / (T)6 + sxz2[p0 + sy2 + 1] / (T)6;
+    }
+    sxz1[pf] = v;
+}
+
+template <typename T>
+__global__ void ghost_syz_ii_kernel(GridDev<T> F, GridDev<T> C)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int nx2 = C.g.nx, ny2 = C.g.ny, nz1 = F.g.nz;
+    const int X1 = 2 * nx2 - 1, Y1 = 2 * ny2 - 1;
+    if (x > X1 || y > Y1) return;
+    T *syz1 = F.f[SYZ];
+    T *syz2 = C.f[SYZ];
+    const int sy1 = F.g.px, sz1 = F.g.px * F.g.py, sy2 = C.g.px;
+    const int pf = F.g.idx(x, y, nz1);
+    if (!(x & 1) && !(y & 1)) {   // coarse ghost, update_ghost_syz.cpp:33-42
+        const int q2 = pf - 2 * sz1, q1 = pf - sz1;
+        const T s = syz1[q2] + syz1[q2 + 1] + syz1[q2 + sy1] + syz1[q2 + sy1 + 1]
+                  + syz1[q1] + syz1[q1 + 1] + syz1[q1 + sy1] + syz1[q1 + sy1 + 1];
+        syz2[C.g.idx(x / 2, y / 2, -1)] = (T)(0.125 * (double)s);
+    }
+    const int pb = pf - sz1;   // the fine plane below
+    const T own = syz1[pb];
+    T v;
+    if (x >= 1 && x <= X1 - 1 && y >= 1 && y <= Y1 - 1) {   // update_ghost_syz.cpp:49-74
+        const int j0 = (x - 1) / 2, j1 = (y - 1) / 2;
+        const int nr = ((x - 1) & 1) | (((y - 1) & 1) << 1);   // coarse corner nearest (x, y)
+        const int p0 = C.g.idx(j0, j1, 0);
+        const T c[4] = {syz2[p0], syz2[p0 + 1], syz2[p0 + sy2], syz2[p0 + sy2 + 1]};
+        // the far corner's term is x/24 (type T) and the near and adjacent ones
+        // are 0.375*x and 0.125*x (double); the sum starts in T only when the
+        // second term is the far corner's (fine point (2 j0 + 2, 2 j1 + 2))
+        double acc = nr == 3 ? (double)(own / (T)3 + c[0] / (T)24)
+                             : (double)(own / (T)3) + (nr == 0 ? 0.375 : 0.125) * (double)c[0];
+#pragma unroll
+        for (int k = 1; k < 4; k++) {
+            const int d = k ^ nr;
+            acc = acc + (d == 3 ? (double)(c[k] / (T)24) : (d == 0 ? 0.375 * (double)c[k] : 0.125 * (double)c[k]));
+        }
+        v = (T)acc;
+    } else {   // edges, update_ghost_syz.cpp:78-134
+        const T cc = syz2[C.g.idx(x / 2, y / 2, 0)] * (T)2 / (T)3;
+        if (y == 0 || y == Y1) {
+            const int yin = (y == 0) ? 1 : Y1 - 1;
+            const T in_y = syz1[F.g.idx(x, yin, nz1 - 1)];
+            if (x == 0 || x == X1) {
+                const int xin = (x == 0) ? 1 : X1 - 1;
+                v = own - syz1[F.g.idx(xin, y, nz1 - 1)] / (T)3 - in_y / (T)3 + cc;
+            } else {
+                v = own / (T)3 + syz1[F.g.idx(x - 1 + 2 * (x & 1), y, nz1 - 1)] / (T)3 - in_y / (T)3 + cc;
+            }
+        } else {
+            const int xin = (x == 0) ? 1 : X1 - 1;
+            v = own / (T)3 + syz1[F.g.idx(x, y - 1 + 2 * (y & 1), nz1 - 1)] / (T)3
+              - syz1[F.g.idx(xin, y, nz1 - 1)] / (T)3 + cc;
+        }
+    }
+    syz1[pf] = v;
+}
+
+// Transposes of the three imode-0 maps.  Each ghost value is overwritten from
+// values of other planes, so its adjoint is read, cleared and spread onto
+// those values with the forward weights; the sources are never ghosts, so one
+// launch with atomic adds is race free.  The thread layout is the forward's.
+template <typename T>
+__global__ void ghost_vz_ii_adj_kernel(GridDev<T> F, GridDev<T> C, AdjDev<T> AF, AdjDev<T> AC, int skip_end)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int nx2 = C.g.nx, ny2 = C.g.ny, nz1 = F.g.nz;
+    const int nx1 = 2 * nx2, ny1 = 2 * ny2;
+    if (x >= nx1 || y >= ny1) return;
+    T *l1 = AF.l[VZ], *l2 = AC.l[VZ];
+    const int sz1 = F.g.px * F.g.py;
+    const int pf = F.g.idx(x, y, nz1);
+    if (!(x & 1) && !(y & 1) && y > 0) {
+        const int pg = C.g.idx(x / 2, y / 2, -1);
+        const T a = (T)(0.25 * (double)l2[pg]);
+        l2[pg] = (T)0;
+        const int q2 = pf - 2 * sz1, q1 = pf - sz1;
+        atom(l1 + q2, a); atom(l1 + q2 + 1, a); atom(l1 + q1, a); atom(l1 + q1 + 1, a);
+    }
+    if (skip_end && x == nx1 - 1) return;   // identity there
+    const T a = l1[pf];
+    l1[pf] = (T)0;
+    const int j1 = y / 2, odd_y = y & 1;
+    if (x >= 1 && x <= nx1 - 2) {
+        const int j0 = (x - 1) / 2, second = (x - 1) & 1;
+        const int p0 = C.g.idx(j0, j1, 0);
+        atom(l1 + pf - sz1, a / (T)3);
+        if (!odd_y) {
+            atom(l2 + p0, a / (T)(second ? 6 : 2));
+            atom(l2 + p0 + 1, a / (T)(second ? 2 : 6));
+        } else {
+            const T wn = a / (T)4, wf = a / (T)12;
+            atom(l2 + p0, second ? wf : wn);
+            atom(l2 + p0 + 1, second ? wn : wf);
+            atom(l2 + p0 + C.g.px, second ? wf : wn);
+            atom(l2 + p0 + C.g.px + 1, second ? wn : wf);
+        }
+    } else {
+        const int xin = (x == 0) ? 1 : x - 1;
+        int cx0, cy0, cx1, cy1;
+        row_major_wrap(x, j1, nx2 + 2 * C.g.R, C.g.R, cx0, cy0);
+        row_major_wrap(x, j1 + 1, nx2 + 2 * C.g.R, C.g.R, cx1, cy1);
+        atom(l1 + pf - sz1, a * (T)2 / (T)3);
+        atom(l1 + F.g.idx(xin, odd_y ? y - 1 : y, nz1 - 1), -a / (T)3);
+        if (!odd_y) {
+            atom(l2 + C.g.idx(cx0, cy0, 0), a * (T)2 / (T)3);
+        } else {
+            atom(l2 + C.g.idx(cx0, cy0, 0), a / (T)3);
+            atom(l2 + C.g.idx(cx1, cy1, 0), a / (T)3);
+        }
+    }
+}
+
+template <typename T>
+__global__ void ghost_sxz_ii_adj_kernel(GridDev<T> F, GridDev<T> C, AdjDev<T> AF, AdjDev<T> AC)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x + 1;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y + 1;
+    const int nx2 = C.g.nx, ny2 = C.g.ny, nz1 = F.g.nz;
+    if (x >= 2 * nx2 || y >= 2 * ny2) return;
+    T *l1 = AF.l[SXZ], *l2 = AC.l[SXZ];
+    const int sz1 = F.g.px * F.g.py;
+    const int pf = F.g.idx(x, y, nz1);
+    const int p0 = C.g.idx(x / 2, y / 2, 0), sy2 = C.g.px;
+    if (!(x & 1) && !(y & 1)) {
+        const int pg = p0 - C.g.px * C.g.py;
+        const T b = (T)(0.5 * (double)l2[pg]);
+        l2[pg] = (T)0;
+        atom(l1 + pf - 2 * sz1, b);
+        atom(l1 + pf - sz1, b);
+    }
+    const T a = l1[pf];
+    l1[pf] = (T)0;
+    atom(l1 + pf - sz1, a / (T)3);
+    switch ((x & 1) | ((y & 1) << 1)) {
+    case 0: atom(l2 + p0, (T)((double)a * 2.0 / 3.0)); break;
+    case 1: atom(l2 + p0, a / (T)3); atom(l2 + p0 + 1, a / (T)3); break;
+    case 2: atom(l2 + p0, a / (T)3); atom(l2 + p0 + sy2, a / (T)3); break;
+    default: {
+        const T w = a / (T)6;
+        atom(l2 + p0, w); atom(l2 + p0 + sy2, w); atom(l2 + p0 + 1, w); atom(l2 + p0 + sy2 + 1, w);
+    }
+    }
+}
+
+template <typename T>
+__global__ void ghost_syz_ii_adj_kernel(GridDev<T> F, GridDev<T> C, AdjDev<T> AF, AdjDev<T> AC)
+{
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    const int nx2 = C.g.nx, ny2 = C.g.ny, nz1 = F.g.nz;
+    const int X1 = 2 * nx2 - 1, Y1 = 2 * ny2 - 1;
+    if (x > X1 || y > Y1) return;
+    T *l1 = AF.l[SYZ], *l2 = AC.l[SYZ];
+    const int sy1 = F.g.px, sz1 = F.g.px * F.g.py, sy2 = C.g.px;
+    const int pf = F.g.idx(x, y, nz1);
+    if (!(x & 1) && !(y & 1)) {
+        const int pg = C.g.idx(x / 2, y / 2, -1);
+        const T b = (T)(0.125 * (double)l2[pg]);
+        l2[pg] = (T)0;
+        for (int q = pf - 2 * sz1; q <= pf - sz1; q += sz1) {
+            atom(l1 + q, b); atom(l1 + q + 1, b); atom(l1 + q + sy1, b); atom(l1 + q + sy1 + 1, b);
+        }
+    }
+    const T a = l1[pf];
+    l1[pf] = (T)0;
+    const int pb = pf - sz1;
+    if (x >= 1 && x <= X1 - 1 && y >= 1 && y <= Y1 - 1) {
+        atom(l1 + pb, a / (T)3);
+        const int nr = ((x - 1) & 1) | (((y - 1) & 1) << 1);
+        const int p0 = C.g.idx((x - 1) / 2, (y - 1) / 2, 0);
+        const int pc[4] = {p0, p0 + 1, p0 + sy2, p0 + sy2 + 1};
+#pragma unroll
+        for (int k = 0; k < 4; k++) {
+            const int d = k ^ nr;
+            atom(l2 + pc[k], d == 3 ? a / (T)24 : (d == 0 ? (T)(0.375 * (double)a) : (T)(0.125 * (double)a)));
+        }
+    } else {
+        atom(l2 + C.g.idx(x / 2, y / 2, 0), a * (T)2 / (T)3);
+        if (y == 0 || y == Y1) {
+            const int yin = (y == 0) ? 1 : Y1 - 1;
+            atom(l1 + F.g.idx(x, yin, nz1 - 1), -a / (T)3);
+            if (x == 0 || x == X1) {
+                atom(l1 + pb, a);
+                atom(l1 + F.g.idx((x == 0) ? 1 : X1 - 1, y, nz1 - 1), -a / (T)3);
+            } else {
+                atom(l1 + pb, a / (T)3);
+                atom(l1 + F.g.idx(x - 1 + 2 * (x & 1), y, nz1 - 1), a / (T)3);
+            }
+        } else {
+            atom(l1 + pb, a / (T)3);
+            atom(l1 + F.g.idx(x, y - 1 + 2 * (y & 1), nz1 - 1), a / (T)3);
+            atom(l1 + F.g.idx((x == 0) ? 1 : X1 - 1, y, nz1 - 1), -a / (T)3);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Host launchers
 // ---------------------------------------------------------------------------
 template <typename T>
@@ -898,6 +1198,39 @@ cudaError_t launch_ghost_vz(const GridDev<T> &F, const GridDev<T> &C, int medium
     const int nx1 = r * C.g.nx, ny1 = r * C.g.ny;
     dim3 bs(128, 2), gs((nx1 + 127) / 128, (ny1 - 1 + 1) / 2);
     ghost_vz_scatter_kernel<T><<<gs, bs, 0, st>>>(F, C, r);
+    return cudaGetLastError();
+}
+
+// imode 0 (ratio 2): one launch per op over the fine interface plane;
+// op 0 vz, 1 sxz, 2 syz, 3 vz with the last fine x column left as it is
+template <typename T>
+cudaError_t launch_ghost_ii(int op, const GridDev<T> &F, const GridDev<T> &C, cudaStream_t st)
+{
+    const int nx1 = 2 * C.g.nx, ny1 = 2 * C.g.ny;
+    dim3 b(64, 4);
+    switch (op) {
+    case 0:
+    case 3: ghost_vz_ii_kernel<T><<<dim3((nx1 + 63) / 64, (ny1 + 3) / 4), b, 0, st>>>(F, C, op == 3); break;
+    case 1: ghost_sxz_ii_kernel<T><<<dim3((nx1 - 1 + 63) / 64, (ny1 - 1 + 3) / 4), b, 0, st>>>(F, C); break;
+    case 2: ghost_syz_ii_kernel<T><<<dim3((nx1 + 63) / 64, (ny1 + 3) / 4), b, 0, st>>>(F, C); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_ghost_ii_adj(int op, const GridDev<T> &F, const GridDev<T> &C, const AdjDev<T> &AF,
+                                const AdjDev<T> &AC, cudaStream_t st)
+{
+    const int nx1 = 2 * C.g.nx, ny1 = 2 * C.g.ny;
+    dim3 b(64, 4);
+    switch (op) {
+    case 0:
+    case 3: ghost_vz_ii_adj_kernel<T><<<dim3((nx1 + 63) / 64, (ny1 + 3) / 4), b, 0, st>>>(F, C, AF, AC, op == 3); break;
+    case 1: ghost_sxz_ii_adj_kernel<T><<<dim3((nx1 - 1 + 63) / 64, (ny1 - 1 + 3) / 4), b, 0, st>>>(F, C, AF, AC); break;
+    case 2: ghost_syz_ii_adj_kernel<T><<<dim3((nx1 + 63) / 64, (ny1 + 3) / 4), b, 0, st>>>(F, C, AF, AC); break;
+    default: return cudaErrorInvalidValue;
+    }
     return cudaGetLastError();
 }
 
@@ -1015,6 +1348,9 @@ cudaError_t launch_ghost_sxz_adj(const GridDev<T> &F, const GridDev<T> &C, const
                                                  cudaStream_t);                                                   \
     template cudaError_t launch_ghost_vz<T>(const GridDev<T> &, const GridDev<T> &, int, int, double *, cudaStream_t); \
     template cudaError_t launch_ghost_syz<T>(const GridDev<T> &, const GridDev<T> &, int, cudaStream_t);     \
+    template cudaError_t launch_ghost_ii<T>(int, const GridDev<T> &, const GridDev<T> &, cudaStream_t);     \
+    template cudaError_t launch_ghost_ii_adj<T>(int, const GridDev<T> &, const GridDev<T> &, const AdjDev<T> &,   \
+                                                const AdjDev<T> &, cudaStream_t);                               \
     template cudaError_t launch_sxz_matrix<T>(const GridDev<T> &, const GridDev<T> &, int, double *, cudaStream_t); \
     template int sxz_solve_blocks<T>(int, int);                                                          \
     template cudaError_t launch_sxz_solve<T>(const GridDev<T> &, const GridDev<T> &, int, const SxzWork &, int, cudaStream_t);

@@ -21,7 +21,7 @@
 // driver passes (buoyancy to UpdateVel / UpdateGhostSXZ / UpdateGhostSYZ,
 // stiffness to UpdateStress / UpdateGhostVZ); an operator only reads the part
 // it was given.  Errors abort with a message, as the reference does
-// (field.cpp:35-44).  Radius 1, ECI mode (imode 1) only.
+// (field.cpp:35-44).  Radius 1; both interface modes (imode 0 at ratio 2, imode 1).
 #include "sim_utils.hpp"
 #include "ecsg_b200.h"
 
@@ -78,7 +78,7 @@ struct SimRec {
 };
 
 std::map<const Field *, GridRec> g_grids;
-std::map<std::vector<const Field *>, SimRec> g_sims;
+std::map<std::pair<std::vector<const Field *>, int>, SimRec> g_sims;   // (members, imode)
 int g_top_bc = -1;
 
 GridRec &grid_of(const Field *sim)
@@ -99,9 +99,9 @@ void note_coeff(GridRec &G, real **coeff)
 }
 
 // the simulation of one grid or of one interface (fine, coarse)
-SimRec &sim_of(std::vector<const Field *> members)
+SimRec &sim_of(std::vector<const Field *> members, int imode = ECSG_MODE_ECI)
 {
-    SimRec &S = g_sims[members];
+    SimRec &S = g_sims[{members, imode}];
     if (!S.sim) {
         S.grids = members;
         S.version.assign(members.size(), -1);
@@ -116,7 +116,7 @@ SimRec &sim_of(std::vector<const Field *> members)
                 gd[i].step[d] = (double)(i == 0 ? 1 : r);   // coefficients are set below
             }
         }
-        ecsg_config cfg = {(int)members.size(), 1, 1.0, ECSG_MODE_ECI, g_top_bc < 0 ? 0 : g_top_bc, ECSG_F64,
+        ecsg_config cfg = {(int)members.size(), 1, 1.0, imode, g_top_bc < 0 ? 0 : g_top_bc, ECSG_F64,
                            ECSG_MEDIUM_ORTHO9, 1, 0, 0, 0};
         ck(ecsg_create(gd.data(), &cfg, &S.sim), "ecsg_create", S.sim);
     }
@@ -184,11 +184,12 @@ void learn_stiff(GridRec &G, Field *const *st)
     }
 }
 
-SimRec &interface_of(Field *sim1, Field *sim2)
+SimRec &interface_of(Field *sim1, Field *sim2, int mode = ECSG_MODE_ECI)
 {
+    if (mode != ECSG_MODE_ECI && mode != ECSG_MODE_II) die("interface mode must be 0 or 1");
     grid_of(sim1);
     grid_of(sim2);
-    return sim_of({sim1, sim2});
+    return sim_of({sim1, sim2}, mode);
 }
 
 } // namespace
@@ -223,13 +224,12 @@ void UpdateGhostVZ(Field sim1[9], Field sim2[9], Field *stiff1[9], Field *stiff2
                    Array &A, Array &B, int mode)
 {
     (void)A; (void)B;   // the reference's work arrays; the device has its own
-    if (mode != 1) die("UpdateGhostVZ: only the energy-conserving mode (imode 1) is implemented");
     GridRec &F = grid_of(sim1), &C = grid_of(sim2);
     note_coeff(F, coeff1);
     note_coeff(C, coeff2);
     learn_stiff(F, stiff1);
     learn_stiff(C, stiff2);
-    SimRec &S = interface_of(sim1, sim2);
+    SimRec &S = interface_of(sim1, sim2, mode);
     upload(S, 0, sim1);
     upload(S, 1, sim2);
     ck(ecsg_ghost_vz(S.sim, 1), "UpdateGhostVZ", S.sim);
@@ -241,15 +241,20 @@ void UpdateGhostSXZ(Field sim1[9], Field sim2[9], Field *buoy1, Field *buoy2, re
                     Array &g_sxz2, Array &A, Array &B, Array &g_tmp, int mode)
 {
     (void)A; (void)B; (void)g_tmp;
-    if (mode != 1) die("UpdateGhostSXZ: only the energy-conserving mode (imode 1) is implemented");
     GridRec &F = grid_of(sim1), &C = grid_of(sim2);
     note_coeff(F, coeff1);
     note_coeff(C, coeff2);
     learn_buoy(F, buoy1);
     learn_buoy(C, buoy2);
-    SimRec &S = interface_of(sim1, sim2);
+    SimRec &S = interface_of(sim1, sim2, mode);
     upload(S, 0, sim1);
     upload(S, 1, sim2);
+    if (mode == ECSG_MODE_II) {   // explicit interpolation: g_sxz2 is not used (update_ghost_sxz.cpp:37-84)
+        ck(ecsg_ghost_sxz(S.sim, 1), "UpdateGhostSXZ", S.sim);
+        download(S, 0, sim1, 7, 7);
+        download(S, 1, sim2, 7, 7);
+        return;
+    }
     // the Jacobi warm start lives in the caller's g_sxz2 ((nx2+1) x (ny2+1), x fastest)
     const size_t nxy = (size_t)(C.n[0] + 1) * (C.n[1] + 1);
     std::vector<double> X(nxy);
@@ -264,13 +269,12 @@ void UpdateGhostSXZ(Field sim1[9], Field sim2[9], Field *buoy1, Field *buoy2, re
 
 void UpdateGhostSYZ(Field sim1[9], Field sim2[9], Field *buoy1, Field *buoy2, real **coeff1, real **coeff2, int mode)
 {
-    if (mode != 1) die("UpdateGhostSYZ: only the energy-conserving mode (imode 1) is implemented");
     GridRec &F = grid_of(sim1), &C = grid_of(sim2);
     note_coeff(F, coeff1);
     note_coeff(C, coeff2);
     learn_buoy(F, buoy1);
     learn_buoy(C, buoy2);
-    SimRec &S = interface_of(sim1, sim2);
+    SimRec &S = interface_of(sim1, sim2, mode);
     upload(S, 0, sim1);
     upload(S, 1, sim2);
     ck(ecsg_ghost_syz(S.sim, 1), "UpdateGhostSYZ", S.sim);

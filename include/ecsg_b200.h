@@ -61,7 +61,7 @@ typedef struct ecsg_config {
     int num_grids;        /* num_grids */
     int radius;           /* stencil radius; 1 (the interface solves assume 1) */
     double dt;            /* time step */
-    int imode;            /* ECSG_MODE_ECI (1) */
+    int imode;            /* ECSG_MODE_ECI (1), or ECSG_MODE_II (0: ratio-2 interfaces only) */
     int top_bc;           /* 0 rigid, 1 free surface */
     int precision;        /* ECSG_F32 or ECSG_F64 */
     int medium;           /* ECSG_MEDIUM_ISO, ECSG_MEDIUM_ORTHO9 or ECSG_MEDIUM_GEN21 */
@@ -72,6 +72,11 @@ typedef struct ecsg_config {
                            * mirrors also cover the top-most updated plane of vy
                            * (update_vel.cpp:211-246 stop one plane short), which
                            * makes the composite energy exactly conserved */
+    int ii_skip_end_column; /* imode 0 only.  0: update_ghost_vz.cpp as it stands.
+                           * 1: leave the fine vz ghosts of the last x column
+                           * untouched, as the revision that produced the
+                           * reference's II golden traces did (its line 98
+                           * declared a new `int i1` instead of setting i0) */
 } ecsg_config;
 
 typedef struct ecsg_sim ecsg_sim;

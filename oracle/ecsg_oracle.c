@@ -660,6 +660,163 @@ void o_ghost_syz_eci(ogrid *g1, ogrid *g2, int r)
 }
 
 /* ------------------------------------------------------------------------- */
+/* Intuitive interpolation (imode = 0), ratio 2 only: explicit, second-order  */
+/* accurate ghosts that do not conserve the discrete energy.                  */
+/* update_ghost_vz.cpp:36-123, update_ghost_sxz.cpp:37-84,                    */
+/* update_ghost_syz.cpp:23-150.  Each function is written per fine ghost      */
+/* point; the terms of every formula are added in the reference's order with  */
+/* its constant forms (x/3, x*2/3, 0.375*x ...), so the results are bitwise    */
+/* those of the reference's FP64 build.                                       */
+/* ------------------------------------------------------------------------- */
+
+/* vz: coarse ghost vz2(j0, j1, -1), j0 in [0,nx2), j1 in [1,ny2): mean of the
+ * four fine vz above it (update_ghost_vz.cpp:46-50).  Fine ghost vz1(x, y, nz1)
+ * for x in [0,nx1), y in [0,ny1) (y = ny1 is left as it is):
+ *   interior x: 1/3 of the fine value below plus x-linear (and y-linear at odd
+ *   y) weights of the coarse plane, as fractions (update_ghost_vz.cpp:57-81);
+ *   x = 0 and x = nx1-1: one-sided extrapolation in x (:87-110).  The x = nx1-1
+ *   formulas index vz2 with the FINE x index nx1-1, which is past the end of
+ *   vz2's rows; the reference's row-major layout then reads the element that
+ *   many places further on (a later row).  AT() has the same layout, so this
+ *   reads the same element.  end_column = 0 leaves x = nx1-1 untouched, as the
+ *   revision of update_ghost_vz.cpp:98 that declared a shadowing `int i1`
+ *   instead of assigning i0 did (its stray write lands outside the field). */
+void o_ghost_vz_ii(ogrid *g1, ogrid *g2, int end_column)
+{
+    ofield *vz1 = &g1->f[2], *vz2 = &g2->f[2];
+    const int nx2 = vz2->end[0] + 1, ny2 = vz2->end[1];
+    const int nz1 = vz1->end[2] + 1;
+    const int nx1 = 2 * nx2, ny1 = 2 * ny2;
+
+    for (int j1 = 1; j1 < ny2; j1++)
+        for (int j0 = 0; j0 < nx2; j0++)
+            V(vz2, j0, j1, -1) = 0.25 * (V(vz1, 2 * j0, 2 * j1, nz1 - 2) + V(vz1, 2 * j0 + 1, 2 * j1, nz1 - 2)
+                                         + V(vz1, 2 * j0, 2 * j1, nz1 - 1) + V(vz1, 2 * j0 + 1, 2 * j1, nz1 - 1));
+
+#pragma omp parallel for
+    for (int y = 0; y < ny1; y++)
+        for (int x = 0; x < nx1; x++) {
+            const double own = V(vz1, x, y, nz1 - 1);
+            const int j1 = y / 2, odd_y = y & 1;
+            double v;
+            if (x >= 1 && x <= nx1 - 2) {
+                const int j0 = (x - 1) / 2, second = (x - 1) & 1;   /* x = 2 j0 + 1 + second */
+                /* divisors of c(j0), c(j0+1) on the coarse row j1 (even y), or of
+                 * c(j0,j1), c(j0+1,j1), c(j0,j1+1), c(j0+1,j1+1) (odd y) */
+                static const double dv[2][2][4] = {{{2, 6, 0, 0}, {6, 2, 0, 0}}, {{4, 12, 4, 12}, {12, 4, 12, 4}}};
+                const double *d = dv[odd_y][second];
+                v = own / 3 + V(vz2, j0, j1, 0) / d[0] + V(vz2, j0 + 1, j1, 0) / d[1];
+                if (odd_y) v = v + V(vz2, j0, j1 + 1, 0) / d[2] + V(vz2, j0 + 1, j1 + 1, 0) / d[3];
+            } else {
+                if (x == nx1 - 1 && !end_column) continue;
+                const int xin = (x == 0) ? 1 : x - 1;   /* x-neighbour one column in */
+                const int cx = x;                       /* coarse x index as the reference writes it */
+                if (!odd_y)
+                    v = own * 2 / 3 - V(vz1, xin, y, nz1 - 1) / 3 + V(vz2, cx, j1, 0) * 2 / 3;
+                else   /* the neighbour term reads the even row y-1 (update_ghost_vz.cpp:93,105) */
+                    v = own * 2 / 3 - V(vz1, xin, y - 1, nz1 - 1) / 3 + V(vz2, cx, j1, 0) / 3 + V(vz2, cx, j1 + 1, 0) / 3;
+            }
+            V(vz1, x, y, nz1) = v;
+        }
+}
+
+/* sxz: coarse ghost sxz2(j0, j1, -1) at the interior coarse nodes = mean of the
+ * two fine cells above (update_ghost_sxz.cpp:46-49); fine ghost at every
+ * interior fine node (x, y) = 1/3 of the fine value below plus 2/3 of the
+ * bilinear coarse interpolation, written per node parity (:55-81). */
+void o_ghost_sxz_ii(ogrid *g1, ogrid *g2)
+{
+    ofield *sxz1 = &g1->f[7], *sxz2 = &g2->f[7];
+    const int nx2 = g2->n[0], ny2 = g2->n[1], nz1 = g1->n[2];
+    const int nx1 = 2 * nx2, ny1 = 2 * ny2;
+
+    for (int j1 = 1; j1 < ny2; j1++)
+        for (int j0 = 1; j0 < nx2; j0++)
+            V(sxz2, j0, j1, -1) = 0.5 * (V(sxz1, 2 * j0, 2 * j1, nz1 - 2) + V(sxz1, 2 * j0, 2 * j1, nz1 - 1));
+
+#pragma omp parallel for
+    for (int y = 1; y < ny1; y++)
+        for (int x = 1; x < nx1; x++) {
+            const int j0 = x / 2, j1 = y / 2;
+            const double own = V(sxz1, x, y, nz1 - 1);
+            double v;
+            switch ((x & 1) | ((y & 1) << 1)) {
+            case 0: v = own / 3 + V(sxz2, j0, j1, 0) * 2 / 3.0; break;
+            case 1: v = own / 3 + V(sxz2, j0, j1, 0) / 3 + V(sxz2, j0 + 1, j1, 0) / 3; break;
+            case 2: v = own / 3 + V(sxz2, j0, j1, 0) / 3 + V(sxz2, j0, j1 + 1, 0) / 3; break;
+            default:
+                v = own / 3 + V(sxz2, j0, j1, 0) / 6 + V(sxz2, j0, j1 + 1, 0) / 6 + V(sxz2, j0 + 1, j1, 0) / 6
+                    + V(sxz2, j0 + 1, j1 + 1, 0) / 6;
+            }
+            V(sxz1, x, y, nz1) = v;
+        }
+}
+
+/* syz: coarse ghost syz2(j0, j1, -1) at every coarse cell = mean of the eight
+ * fine values in the two cell layers above (update_ghost_syz.cpp:33-42).  Fine
+ * ghost at every fine cell (x, y):
+ *   interior (x in [1,nx1-2], y in [1,ny1-2]): 1/3 of the fine value below plus
+ *   the bilinear coarse interpolation scaled by 2/3, weights 9/24 3/24 3/24 1/24
+ *   (:49-74);
+ *   edges: extrapolation from the fine plane below (:78-134): at the four
+ *   corners own - (x-neighbour)/3 - (inward y-neighbour)/3 + 2/3 coarse; along
+ *   an edge own/3 + (the other fine cell of the same coarse cell along the
+ *   edge)/3 - (inward neighbour)/3 + 2/3 coarse. */
+void o_ghost_syz_ii(ogrid *g1, ogrid *g2)
+{
+    ofield *syz1 = &g1->f[6], *syz2 = &g2->f[6];
+    const int nx2 = g2->n[0], ny2 = g2->n[1], nz1 = g1->n[2];
+    const int X1 = 2 * nx2 - 1, Y1 = 2 * ny2 - 1;   /* last fine cell */
+
+    for (int j1 = 0; j1 < ny2; j1++)
+        for (int j0 = 0; j0 < nx2; j0++) {
+            double s = 0.0;
+            int first = 1;
+            for (int dz = 2; dz >= 1; dz--)
+                for (int dy = 0; dy < 2; dy++)
+                    for (int dx = 0; dx < 2; dx++) {
+                        double t = V(syz1, 2 * j0 + dx, 2 * j1 + dy, nz1 - dz);
+                        s = first ? t : s + t;
+                        first = 0;
+                    }
+            V(syz2, j0, j1, -1) = 0.125 * s;
+        }
+
+#pragma omp parallel for
+    for (int y = 0; y <= Y1; y++)
+        for (int x = 0; x <= X1; x++) {
+            const double own = V(syz1, x, y, nz1 - 1);
+            double v;
+            if (x >= 1 && x <= X1 - 1 && y >= 1 && y <= Y1 - 1) {
+                const int j0 = (x - 1) / 2, j1 = (y - 1) / 2;
+                const int near = ((x - 1) & 1) | (((y - 1) & 1) << 1);   /* coarse corner nearest (x, y) */
+                const double c[4] = {V(syz2, j0, j1, 0), V(syz2, j0 + 1, j1, 0), V(syz2, j0, j1 + 1, 0),
+                                     V(syz2, j0 + 1, j1 + 1, 0)};
+                v = own / 3;
+                for (int k = 0; k < 4; k++) {
+                    const int far = (k ^ near) == 3, adj = __builtin_popcount(k ^ near) == 1;
+                    v = v + (far ? c[k] / 24 : (adj ? 0.125 * c[k] : 0.375 * c[k]));
+                }
+            } else {
+                const double cc = V(syz2, x / 2, y / 2, 0) * 2 / 3;
+                if (y == 0 || y == Y1) {
+                    const int yin = (y == 0) ? 1 : Y1 - 1;
+                    if (x == 0 || x == X1) {
+                        const int xin = (x == 0) ? 1 : X1 - 1;
+                        v = own - V(syz1, xin, y, nz1 - 1) / 3 - V(syz1, x, yin, nz1 - 1) / 3 + cc;
+                    } else {
+                        v = own / 3 + V(syz1, x - 1 + 2 * (x % 2), y, nz1 - 1) / 3 - V(syz1, x, yin, nz1 - 1) / 3 + cc;
+                    }
+                } else {
+                    const int xin = (x == 0) ? 1 : X1 - 1;
+                    v = own / 3 + V(syz1, x, y - 1 + 2 * (y % 2), nz1 - 1) / 3 - V(syz1, xin, y, nz1 - 1) / 3 + cc;
+                }
+            }
+            V(syz1, x, y, nz1) = v;
+        }
+}
+
+/* ------------------------------------------------------------------------- */
 /* Energy: compute_energy.cpp:34-54 with TriMulFields (field.cpp:482-518).    */
 /* dens[3]: density at vx, vy, vz positions; comp[9]: compliance in the       */
 /* stiffness order; all R = 0 fields at the matching staggered positions.     */

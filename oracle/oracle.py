@@ -46,6 +46,9 @@ def lib():
         L.o_ghost_sxz_eci.argtypes = [P(OGrid), P(OGrid), ctypes.c_int, c_dp, c_dp, c_dp, c_dp,
                                       ctypes.c_int, c_dp]
         L.o_ghost_sxz_eci.restype = ctypes.c_int
+        L.o_ghost_vz_ii.argtypes = [P(OGrid), P(OGrid), ctypes.c_int]
+        L.o_ghost_sxz_ii.argtypes = [P(OGrid), P(OGrid)]
+        L.o_ghost_syz_ii.argtypes = [P(OGrid), P(OGrid)]
         L.o_energy.argtypes = [P(OGrid), P(OField), P(OField), P(OField), c_dp]
         L.o_energy.restype = ctypes.c_double
         L.o_residues.argtypes = [P(OGrid), P(OGrid), ctypes.c_int, ctypes.c_int, c_dp]
@@ -173,9 +176,16 @@ class OracleRun:
     """Double-precision composite run on the C restatement."""
 
     def __init__(self, case, energy=False):
+        """case.ii_skip_end_column (imode 0 only) leaves the fine vz ghosts of
+        the last x column untouched, as the revision of update_ghost_vz.cpp that
+        produced the reference's II golden traces did."""
         self.case = case
         self.R = case.radius
         self.r = case.ratio
+        self.imode = case.imode
+        self.ii_end_column = not getattr(case, "ii_skip_end_column", False)
+        if self.imode == 0 and len(case.grids) > 1 and self.r != 2:
+            raise ValueError("intuitive interpolation (imode 0) is defined for ratio 2 only")
         self.energy_on = energy
         self.levels = []
         origins = []
@@ -266,16 +276,25 @@ class OracleRun:
             lib().o_update_stress(ctypes.byref(self.structs[g]), int(g == 0), int(g == ng - 1), self.case.top_bc)
 
     def ghost_vz(self, i):
-        if "c21" in self.levels[i]:
+        if self.imode == 0:
+            lib().o_ghost_vz_ii(ctypes.byref(self.structs[i - 1]), ctypes.byref(self.structs[i]),
+                                int(self.ii_end_column))
+        elif "c21" in self.levels[i]:
             lib().o_ghost_vz_eci21(ctypes.byref(self.structs[i - 1]), ctypes.byref(self.structs[i]), self.r,
                                    self.levels[i - 1]["_c21"], self.levels[i]["_c21"])
         else:
             lib().o_ghost_vz_eci(ctypes.byref(self.structs[i - 1]), ctypes.byref(self.structs[i]), self.r)
 
     def ghost_syz(self, i):
+        if self.imode == 0:
+            lib().o_ghost_syz_ii(ctypes.byref(self.structs[i - 1]), ctypes.byref(self.structs[i]))
+            return
         lib().o_ghost_syz_eci(ctypes.byref(self.structs[i - 1]), ctypes.byref(self.structs[i]), self.r)
 
     def ghost_sxz(self, i, max_iter=0):
+        if self.imode == 0:
+            lib().o_ghost_sxz_ii(ctypes.byref(self.structs[i - 1]), ctypes.byref(self.structs[i]))
+            return 0, 0.0
         w = self.X[i - 1]
         tol = ctypes.c_double(0)
         it = lib().o_ghost_sxz_eci(ctypes.byref(self.structs[i - 1]), ctypes.byref(self.structs[i]), self.r,

@@ -37,7 +37,7 @@ def _read_rsf(path):
     return hdr, np.frombuffer(raw[i + 3:], dtype="<f4")
 
 
-def _inputs(tmp, case, nsteps):
+def _inputs(tmp, case, nsteps, imode=1):
     args = []
     for gi, g in enumerate(case.grids):
         n, h = g["n"], g["h"]
@@ -54,7 +54,7 @@ def _inputs(tmp, case, nsteps):
     # nt = ceil(movie_dt * movie_nt / dt) + 1 steps (main.cpp:165)
     args += ["src=" + os.path.join(tmp, "src.rsf"), "rec_in=" + os.path.join(tmp, "rec.rsf"),
              "num_threads=4", "num_grids=%d" % len(case.grids), "radius=1", "dt=%r" % float(case.dt),
-             "imode=1", "top_bc=%d" % case.top_bc, "check_energy=y", "verb=y",
+             "imode=%d" % imode, "top_bc=%d" % case.top_bc, "check_energy=y", "verb=y",
              "movie_dt=%r" % float(case.dt), "movie_nt=%d" % (nsteps - 1)]
     return args
 
@@ -66,8 +66,8 @@ def _run(exe, args, tmp, tag):
     return {k: _read_rsf(v)[1] for k, v in outs.items()}
 
 
-@pytest.mark.parametrize("top_bc", [1, 0])
-def test_reference_driver_through_the_shim(tmp_path, top_bc):
+@pytest.mark.parametrize("top_bc,imode", [(1, 1), (0, 1), (1, 0)])
+def test_reference_driver_through_the_shim(tmp_path, top_bc, imode):
     if not (os.path.exists(REF_MAIN) and os.path.exists(SHIM_MAIN)):
         pytest.skip("reference driver builds absent (built from the reference sources by __graft_entry__.build)")
     case = random_case(71 + top_bc, ratio=2, nx2=14, ny2=12, nz=(10, 8), top_bc=top_bc)
@@ -78,7 +78,7 @@ def test_reference_driver_through_the_shim(tmp_path, top_bc):
     case.rec = np.array([[(n[0] // 2 + 3) * h[0], n[1] // 2 * h[1], 3 * h[2]],
                          [(n[0] // 3) * h[0], (n[1] // 3) * h[1], (n[2] - 1) * h[2]],
                          [(n[0] // 2) * h[0], (n[1] // 2) * h[1], (n[2] + 3) * h[2]]], dtype=np.float32)
-    args = _inputs(str(tmp_path), case, nsteps)
+    args = _inputs(str(tmp_path), case, nsteps, imode)
     ref = _run(REF_MAIN, args, str(tmp_path), "ref")
     got = _run(SHIM_MAIN, args, str(tmp_path), "shim")
     assert ref["rec_out"].size == 3 * nsteps and np.abs(ref["rec_out"]).max() > 0

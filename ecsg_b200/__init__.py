@@ -73,6 +73,10 @@ SIGNATURES = [
                                            ctypes.c_double, ctypes.c_double, ctypes.c_double]),
     ("ecsg_set_field", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, c_dp]),
     ("ecsg_get_field", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, c_dp]),
+    ("ecsg_domain_shape", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]),
+    ("ecsg_get_domain", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]),
+    ("ecsg_host_alloc", ctypes.c_int, [ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p)]),
+    ("ecsg_host_free", ctypes.c_int, [ctypes.c_void_p]),
     ("ecsg_field_elems", ctypes.c_longlong, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     ("ecsg_update_vel", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("ecsg_update_stress", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
@@ -273,6 +277,15 @@ class Simulation:
         n = self.case.grids[g]["n"]
         out = np.empty(field_shape(n, SIM_POS[k], self.R))
         self._ck(lib().ecsg_get_field(self.h, g, k, out.ctypes.data_as(c_dp)))
+        return out
+
+    def frame(self, g, k):
+        """Computational domain of field k of grid g as float32 (z, y, x), as a
+        movie frame holds it (no halo)."""
+        dims = (ctypes.c_int * 3)()
+        self._ck(lib().ecsg_domain_shape(self.h, g, k, dims))
+        out = np.empty((dims[2], dims[1], dims[0]), np.float32)
+        self._ck(lib().ecsg_get_domain(self.h, g, k, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float))))
         return out
 
     def set_field(self, g, k, arr):

@@ -77,6 +77,23 @@ def build_lib(verbose=False, force=False):
     return LIB
 
 
+CLI_DIR = os.path.join(HERE, "cli")
+CLI = os.path.join(OUT_DIR, "ecsg_main")
+
+
+def build_cli():
+    """ecsg_main: the reference's command-line driver on the library (host C++,
+    linked to libecsg_b200.so next to it)."""
+    srcs = [os.path.join(CLI_DIR, f) for f in ("ecsg_main.cpp", "rsf_io.cpp")]
+    deps = srcs + [os.path.join(CLI_DIR, "rsf_io.hpp"), os.path.join(ROOT, "include", "ecsg_b200.h"), LIB]
+    if _newer(CLI, deps):
+        return CLI
+    cmd = ["g++", "-O2", "-std=c++17", "-Wall", "-I", os.path.join(ROOT, "include"), "-o", CLI] + srcs + \
+          ["-L", OUT_DIR, "-lecsg_b200", "-Wl,-rpath,$ORIGIN", "-lpthread"]
+    subprocess.check_call(cmd)
+    return CLI
+
+
 def build_oracle():
     """Test-side checkers: the C restatement always; the reference build
     (oracle/_ref) only where the reference sources are mounted, including the
@@ -91,6 +108,7 @@ def build_oracle():
 
 if __name__ == "__main__":
     build_lib(verbose="-v" in sys.argv, force="--force" in sys.argv)
+    build_cli()
     if "--all" in sys.argv:
         build_oracle()
     print(LIB)

@@ -62,6 +62,8 @@ cudaError_t launch_pack(T *, const Geo &, const S *, int, int, int, int, cudaStr
 template <typename T>
 cudaError_t launch_unpack(double *, const Geo &, const T *, int, int, int, int, cudaStream_t);
 template <typename T>
+cudaError_t launch_snapshot(float *, const Geo &, const T *, int, int, int, cudaStream_t);
+template <typename T>
 cudaError_t launch_iso_medium(const Geo &, const double *, const double *, double *, T *const[5], cudaStream_t);
 // adjoint.cu and the interface adjoints of interface.cu
 template <typename T>
@@ -178,6 +180,8 @@ struct ecsg_sim {
     long long epoch = 0;           // bumped when anything a captured step refers to changes
     long long gx_epoch[2] = {-1, -1};
     int run_n0 = 0;                // pinned by the async copies at the start of a run
+    float *snap = nullptr;         // movie-frame staging (ecsg_get_domain)
+    size_t snap_cap = 0;
     long long bytes = 0;
     std::string err;
 };
@@ -403,7 +407,7 @@ int ecsg_destroy(ecsg_sim *s)
     }
     cudaFree(s->partial); cudaFree(s->ints); cudaFree(s->iters_total); cudaFree(s->dscal); cudaFree(s->bar);
     cudaFree(s->src_trace); cudaFree(s->rec_grid); cudaFree(s->rec_off); cudaFree(s->traces);
-    cudaFree(s->run_energy); cudaFree(s->run_res);
+    cudaFree(s->run_energy); cudaFree(s->run_res); cudaFree(s->snap);
     cudaFree(s->wblk); cudaFree(s->ckpt); cudaFree(s->seg); cudaFree(s->recT); cudaFree(s->obs);
     for (int v = 0; v < 2; v++)
         if (s->gx[v]) cudaGraphExecDestroy(s->gx[v]);
@@ -605,6 +609,53 @@ int ecsg_get_field(ecsg_sim *s, int g, int k, double *dst)
     CK(cudaMemcpyAsync(dst, stage, n * sizeof(double), cudaMemcpyDeviceToHost, s->st));
     CK(cudaStreamSynchronize(s->st));
     cudaFree(stage);
+    return ECSG_OK;
+}
+
+int ecsg_domain_shape(const ecsg_sim *s, int g, int k, int dims[3])
+{
+    if (!s || g < 0 || g >= s->ng || k < 0 || k > 8 || !dims) return ECSG_ERR_INVALID;
+    const int n[3] = {s->geo[g].nx, s->geo[g].ny, s->geo[g].nz};
+    for (int d = 0; d < 3; d++) dims[d] = kPos[k][d] ? n[d] : n[d] + 1;
+    return ECSG_OK;
+}
+
+int ecsg_get_domain(ecsg_sim *s, int g, int k, float *dst)
+{
+    int dims[3];
+    if (!dst || ecsg_domain_shape(s, g, k, dims) != ECSG_OK) return fail(s, ECSG_ERR_INVALID, "get_domain: bad arguments");
+    CK(cudaSetDevice(s->device));
+    const size_t n = (size_t)dims[0] * dims[1] * dims[2];
+    if (n > s->snap_cap) {
+        cudaFree(s->snap);
+        s->snap = nullptr;
+        s->snap_cap = 0;
+        CK(cudaMalloc(&s->snap, n * sizeof(float)));
+        s->snap_cap = n;
+    }
+    if (s->prec == ECSG_F32)
+        CK(launch_snapshot<float>(s->snap, s->geo[g], (const float *)s->f[g][k], dims[0], dims[1], dims[2], s->st));
+    else
+        CK(launch_snapshot<double>(s->snap, s->geo[g], (const double *)s->f[g][k], dims[0], dims[1], dims[2], s->st));
+    CK(cudaMemcpyAsync(dst, s->snap, n * sizeof(float), cudaMemcpyDeviceToHost, s->st));
+    CK(cudaStreamSynchronize(s->st));
+    return ECSG_OK;
+}
+
+int ecsg_host_alloc(size_t bytes, void **out)
+{
+    if (!out) return ECSG_ERR_INVALID;
+    *out = nullptr;
+    if (cudaHostAlloc(out, bytes ? bytes : 1, cudaHostAllocDefault) != cudaSuccess) {
+        *out = nullptr;
+        return ECSG_ERR_CUDA;
+    }
+    return ECSG_OK;
+}
+
+int ecsg_host_free(void *p)
+{
+    if (p && cudaFreeHost(p) != cudaSuccess) return ECSG_ERR_CUDA;
     return ECSG_OK;
 }
 

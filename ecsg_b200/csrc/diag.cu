@@ -287,6 +287,19 @@ __global__ void unpack_kernel(double *dst, Geo g, const T *src, int l0, int l1, 
     }
 }
 
+// One movie frame: the computational domain of a field (d0 x d1 x d2, x
+// fastest, no halo) as float32, in the order PrintFieldToRSF writes it
+// (print.cpp:89-104).  One thread per element, consecutive threads along x.
+template <typename T>
+__global__ void snapshot_kernel(float *dst, Geo g, const T *src, int d0, int d1, int d2)
+{
+    const int64_t n = (int64_t)d0 * d1 * d2;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+        const int i0 = (int)(t % d0), i1 = (int)((t / d0) % d1), i2 = (int)(t / ((int64_t)d0 * d1));
+        dst[t] = (float)src[g.idx(i0, i1, i2)];
+    }
+}
+
 // Isotropic medium from node values (init_del_par_field.cpp:99-149):
 // s44 = s11 - s13 at nodes, then ReshapeField to the stress positions:
 // c11, c13 at (1,0,0); c44 at (1,1,1); c55 at (0,0,1); c66 at (0,1,0).
@@ -385,6 +398,16 @@ cudaError_t launch_unpack(double *dst, const Geo &g, const T *src, int l0, int l
 }
 
 template <typename T>
+cudaError_t launch_snapshot(float *dst, const Geo &g, const T *src, int d0, int d1, int d2, cudaStream_t st)
+{
+    const int64_t n = (int64_t)d0 * d1 * d2;
+    int blocks = (int)((n + 255) / 256);
+    if (blocks > 8 * 148) blocks = 8 * 148;
+    snapshot_kernel<T><<<blocks, 256, 0, st>>>(dst, g, src, d0, d1, d2);
+    return cudaGetLastError();
+}
+
+template <typename T>
 cudaError_t launch_iso_medium(const Geo &g, const double *s11, const double *s13, double *s44, T *const c[5], cudaStream_t st)
 {
     const int64_t n = (int64_t)(g.nx + 1) * (g.ny + 1) * (g.nz + 1);
@@ -407,6 +430,7 @@ cudaError_t launch_iso_medium(const Geo &g, const double *s11, const double *s13
     template cudaError_t launch_pack<T, float>(T *, const Geo &, const float *, int, int, int, int, cudaStream_t); \
     template cudaError_t launch_pack<T, double>(T *, const Geo &, const double *, int, int, int, int, cudaStream_t); \
     template cudaError_t launch_unpack<T>(double *, const Geo &, const T *, int, int, int, int, cudaStream_t);    \
+    template cudaError_t launch_snapshot<T>(float *, const Geo &, const T *, int, int, int, cudaStream_t);      \
     template cudaError_t launch_iso_medium<T>(const Geo &, const double *, const double *, double *, T *const[5], \
                                               cudaStream_t);
 INST(float)

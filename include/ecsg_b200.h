@@ -182,6 +182,17 @@ int ecsg_locate(const ecsg_sim *sim, const double xyz[3], int loc4[4]);
 int ecsg_run(ecsg_sim *sim, int n0, int nsteps, float *traces, double *energy, int energy_every, double *residues,
              int use_graph);
 
+/* Movie frames (InitMovie/PrintMovie, init_del_movie.cpp:5-95, print.cpp:89-104):
+ * the computational domain of field k of grid g (no halo), dims[0] x dims[1]
+ * x dims[2] with x fastest, as float32, packed on the device and copied to
+ * dst (pinned memory from ecsg_host_alloc makes the copy asynchronous-rate);
+ * returns once dst holds the frame. */
+int ecsg_domain_shape(const ecsg_sim *sim, int g, int k, int dims[3]);
+int ecsg_get_domain(ecsg_sim *sim, int g, int k, float *dst);
+/* Page-locked host memory for frame and trace buffers. */
+int ecsg_host_alloc(size_t bytes, void **out);
+int ecsg_host_free(void *p);
+
 /* Device time (CUDA events around the step loop) of the last ecsg_run and the
  * number of kernels it launched. */
 int ecsg_last_run(ecsg_sim *sim, double *device_ms, long long *launches);

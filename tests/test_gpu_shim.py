@@ -9,61 +9,14 @@ the driver writes them) agree to one float rounding, the energy to 1e-10 and
 the interface residues to the float precision of their traces.
 """
 import os
-import subprocess
 
 import numpy as np
 import pytest
 
 from ecsg_b200.workloads import random_case, ricker
+from rsf_util import REF_MAIN, SHIM_MAIN, run_driver, write_inputs
 
 pytestmark = pytest.mark.gpu
-ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF_MAIN = os.path.join(ROOT, "oracle", "_ref", "ecsg_ref_main")
-SHIM_MAIN = os.path.join(ROOT, "oracle", "_ref", "ecsg_shim_main")
-
-
-def _write_rsf(path, data, **hdr):
-    with open(path, "wb") as fh:
-        for k, v in hdr.items():
-            fh.write(("%s=%s\n" % (k, repr(v) if isinstance(v, float) else v)).encode())
-        fh.write(b"\x0c\x0c\x04")
-        fh.write(np.ascontiguousarray(data, dtype="<f4").tobytes())
-
-
-def _read_rsf(path):
-    raw = open(path, "rb").read()
-    i = raw.index(b"\x0c\x0c\x04")
-    hdr = dict(l.strip().split("=", 1) for l in raw[:i].decode().splitlines() if "=" in l)
-    return hdr, np.frombuffer(raw[i + 3:], dtype="<f4")
-
-
-def _inputs(tmp, case, nsteps, imode=1):
-    args = []
-    for gi, g in enumerate(case.grids):
-        n, h = g["n"], g["h"]
-        for key in ("buoy", "s11", "s13"):
-            p = os.path.join(tmp, "%s_%d.rsf" % (key, gi + 1))
-            _write_rsf(p, case.media[gi][key], n1=n[0] + 1, n2=n[1] + 1, n3=n[2] + 1,
-                       d1=float(h[0]), d2=float(h[1]), d3=float(h[2]))
-            args.append("%s_%d=%s" % (key, gi + 1, p))
-    x, y, z = case.src["xyz"]
-    tr = np.asarray(case.src["trace"], np.float32)
-    _write_rsf(os.path.join(tmp, "src.rsf"), tr, n1=tr.size, d1=float(case.dt) / 1000.0,
-               o2=float(x), o3=float(y), o4=float(z))
-    _write_rsf(os.path.join(tmp, "rec.rsf"), case.rec, n1=3, n2=len(case.rec))
-    # nt = ceil(movie_dt * movie_nt / dt) + 1 steps (main.cpp:165)
-    args += ["src=" + os.path.join(tmp, "src.rsf"), "rec_in=" + os.path.join(tmp, "rec.rsf"),
-             "num_threads=4", "num_grids=%d" % len(case.grids), "radius=1", "dt=%r" % float(case.dt),
-             "imode=%d" % imode, "top_bc=%d" % case.top_bc, "check_energy=y", "verb=y",
-             "movie_dt=%r" % float(case.dt), "movie_nt=%d" % (nsteps - 1)]
-    return args
-
-
-def _run(exe, args, tmp, tag):
-    outs = {k: os.path.join(tmp, "%s_%s.rsf" % (tag, k)) for k in ("rec_out", "energy_trace", "res_trace")}
-    cmd = [exe] + args + ["%s=%s" % (k, v) for k, v in outs.items()]
-    subprocess.run(cmd, check=True, cwd=tmp, stdout=subprocess.DEVNULL, timeout=600)
-    return {k: _read_rsf(v)[1] for k, v in outs.items()}
 
 
 @pytest.mark.parametrize("top_bc,imode", [(1, 1), (0, 1), (1, 0)])
@@ -78,9 +31,9 @@ def test_reference_driver_through_the_shim(tmp_path, top_bc, imode):
     case.rec = np.array([[(n[0] // 2 + 3) * h[0], n[1] // 2 * h[1], 3 * h[2]],
                          [(n[0] // 3) * h[0], (n[1] // 3) * h[1], (n[2] - 1) * h[2]],
                          [(n[0] // 2) * h[0], (n[1] // 2) * h[1], (n[2] + 3) * h[2]]], dtype=np.float32)
-    args = _inputs(str(tmp_path), case, nsteps, imode)
-    ref = _run(REF_MAIN, args, str(tmp_path), "ref")
-    got = _run(SHIM_MAIN, args, str(tmp_path), "shim")
+    args = write_inputs(str(tmp_path), case, nsteps, imode)
+    ref = {k: v[1] for k, v in run_driver(REF_MAIN, args, str(tmp_path), "ref")[0].items()}
+    got = {k: v[1] for k, v in run_driver(SHIM_MAIN, args, str(tmp_path), "shim")[0].items()}
     assert ref["rec_out"].size == 3 * nsteps and np.abs(ref["rec_out"]).max() > 0
     assert np.abs(got["rec_out"] - ref["rec_out"]).max() <= 1e-6 * np.abs(ref["rec_out"]).max()
     assert np.abs(got["energy_trace"] - ref["energy_trace"]).max() <= 1e-10 * np.abs(ref["energy_trace"]).max() + 1e-30

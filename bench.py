@@ -150,7 +150,8 @@ def shot_gradients(args, local, world, max_over_ranks, barrier):
     every 50 steps; observed data from the same model with a 3 % vs blob.
     One shot per GPU; device time (CUDA events on the library's stream)
     around ecsg_misfit_gradient (forward with checkpoints, recomputation and
-    adjoint)."""
+    adjoint) and, on several GPUs, the FP64 all-reduce of the gradient volumes
+    (NCCL, on the same stream)."""
     import ecsg_b200
     from ecsg_b200.workloads import two_grid_adjoint_case
     n = args.grad_steps
@@ -160,15 +161,21 @@ def shot_gradients(args, local, world, max_over_ranks, barrier):
     case = two_grid_adjoint_case(0, shot, n, blob=False)
     with ecsg_b200.Simulation(case, precision="f32", device=local) as s:
         s.misfit_gradient(obs[: min(n, 60)], ckpt_every=50)   # warm-up (allocations, tensor maps)
+        if world > 1:
+            from ecsg_b200.distributed import allreduce_gradients
+            allreduce_gradients(s)   # warm-up of the collective
         barrier()
         s.timer_start()
         loss = s.misfit_gradient(obs, ckpt_every=50)
+        if world > 1:
+            allreduce_gradients(s)
         ms = s.timer_stop()
         gmax = float(np.abs(s.gradient(0, 0)).max())
         status = s.status()
     ms = max_over_ranks(ms)
     return {"metric": "shot-gradients/s", "value": world / (ms * 1e-3), "unit": "shot-gradients/s",
-            "mode": "plain (one shot per GPU at a time)", "ms_per_shot_gradient": ms, "steps": n,
+            "mode": "plain (one shot per GPU at a time)" + (", FP64 NCCL all-reduce of the gradients" if world > 1 else ""),
+            "ms_per_shot_gradient": ms, "steps": n,
             "ckpt_every": 50, "points": case.points(), "receivers": len(case.rec), "dtype": "f32",
             "loss": loss, "finite": bool(np.isfinite(loss) and np.isfinite(gmax)), "status": status,
             "workload": "two-grid 361x361x61@10m / 121x121x81@30m, smooth orthorhombic, shot %d of 4x4" % shot}

@@ -77,6 +77,10 @@ SIGNATURES = [
     ("ecsg_get_domain", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_float)]),
     ("ecsg_host_alloc", ctypes.c_int, [ctypes.c_size_t, ctypes.POINTER(ctypes.c_void_p)]),
     ("ecsg_host_free", ctypes.c_int, [ctypes.c_void_p]),
+    ("ecsg_gradient_elems", ctypes.c_longlong, [ctypes.c_void_p, ctypes.c_int]),
+    ("ecsg_pack_gradient", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
+    ("ecsg_unpack_gradient", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
+    ("ecsg_stream", ctypes.c_void_p, [ctypes.c_void_p]),
     ("ecsg_field_elems", ctypes.c_longlong, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     ("ecsg_update_vel", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("ecsg_update_stress", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
@@ -163,6 +167,7 @@ class Simulation:
         self.R = case.radius
         self.precision = precision
         self.energy_on = bool(energy)
+        self.device = device
         descs = (GridDesc * self.ng)()
         for i, g in enumerate(case.grids):
             descs[i].size[:] = list(g["n"])
@@ -278,6 +283,21 @@ class Simulation:
         out = np.empty(field_shape(n, SIM_POS[k], self.R))
         self._ck(lib().ecsg_get_field(self.h, g, k, out.ctypes.data_as(c_dp)))
         return out
+
+    def gradient_elems(self, g):
+        return int(lib().ecsg_gradient_elems(self.h, g))
+
+    def pack_gradient(self, g, dst_ptr):
+        """Enqueue the FP64 pack of grid g's 22 gradient volumes into device
+        memory at dst_ptr (gradient_elems(g) doubles) on the library stream."""
+        self._ck(lib().ecsg_pack_gradient(self.h, g, ctypes.c_void_p(dst_ptr)))
+
+    def unpack_gradient(self, g, src_ptr):
+        self._ck(lib().ecsg_unpack_gradient(self.h, g, ctypes.c_void_p(src_ptr)))
+
+    def stream(self):
+        """The library's cudaStream_t for this simulation (an integer handle)."""
+        return lib().ecsg_stream(self.h)
 
     def frame(self, g, k):
         """Computational domain of field k of grid g as float32 (z, y, x), as a

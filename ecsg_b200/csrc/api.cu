@@ -1567,6 +1567,51 @@ int ecsg_get_gradient(ecsg_sim *s, int g, int which, double *dst)
                    G.ny + 1 - kCij21Pos[k][1], G.nz + 1 - kCij21Pos[k][2], 0, dst);
 }
 
+long long ecsg_gradient_elems(const ecsg_sim *s, int g)
+{
+    if (!s || g < 0 || g >= s->ng) return -1;
+    const Geo &G = s->geo[g];
+    long long n = (long long)(G.nx + 1) * (G.ny + 1) * (G.nz + 1);
+    for (int k = 0; k < 21; k++)
+        n += (long long)(G.nx + 1 - kCij21Pos[k][0]) * (G.ny + 1 - kCij21Pos[k][1]) * (G.nz + 1 - kCij21Pos[k][2]);
+    return n;
+}
+
+// the 22 gradient volumes of grid g, each without halo, x fastest: node
+// buoyancy, then the 21 slots at their positions
+template <typename T>
+static int gradient_move(ecsg_sim *s, int g, double *packed, bool to_packed)
+{
+    const Geo &G = s->geo[g];
+    const size_t box = (size_t)G.size();
+    size_t off = 0;
+    for (int w = 0; w < 22; w++) {
+        T *vol = w == 0 ? (T *)s->gbblk[g] : (T *)s->gcblk[g] + (size_t)(w - 1) * box;
+        const int *p = w == 0 ? nullptr : kCij21Pos[w - 1];
+        const int l0 = G.nx + 1 - (p ? p[0] : 0), l1 = G.ny + 1 - (p ? p[1] : 0), l2 = G.nz + 1 - (p ? p[2] : 0);
+        if (to_packed) CK(launch_unpack<T>(packed + off, G, vol, l0, l1, l2, 0, s->st));
+        else CK((launch_pack<T, double>(vol, G, packed + off, l0, l1, l2, 0, s->st)));
+        off += (size_t)l0 * l1 * l2;
+    }
+    return ECSG_OK;
+}
+
+int ecsg_pack_gradient(ecsg_sim *s, int g, double *dst)
+{
+    if (!s || g < 0 || g >= s->ng || !dst) return fail(s, ECSG_ERR_INVALID, "pack_gradient: bad arguments");
+    if (int rc = adj_check(s)) return rc;
+    return DISPATCH(gradient_move)(s, g, dst, true);
+}
+
+int ecsg_unpack_gradient(ecsg_sim *s, int g, const double *src)
+{
+    if (!s || g < 0 || g >= s->ng || !src) return fail(s, ECSG_ERR_INVALID, "unpack_gradient: bad arguments");
+    if (int rc = adj_check(s)) return rc;
+    return DISPATCH(gradient_move)(s, g, const_cast<double *>(src), false);
+}
+
+void *ecsg_stream(const ecsg_sim *s) { return s ? (void *)s->st : nullptr; }
+
 int ecsg_adjoint_op(ecsg_sim *s, int op, int index)
 {
     if (!s) return ECSG_ERR_INVALID;

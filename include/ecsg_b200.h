@@ -282,6 +282,18 @@ int ecsg_adjoint_op(ecsg_sim *sim, int op, int index);
  * x fastest), which = 1 + k the stiffness slot k of ecsg_set_medium_cij21 in
  * that slot's R = 0 layout. */
 int ecsg_get_gradient(ecsg_sim *sim, int g, int which, double *dst);
+/* The 22 gradient volumes of grid g in one FP64 DEVICE buffer of
+ * ecsg_gradient_elems(sim, g) doubles (the layouts of ecsg_get_gradient, which
+ * = 0 .. 21 back to back), for a sum over processes (e.g. an NCCL all-reduce
+ * of the shots' gradients; no reference counterpart).  Both are enqueued on
+ * the simulation's stream (ecsg_stream) and return before they complete;
+ * unpack overwrites the gradient with the buffer, converted to the
+ * simulation's precision. */
+long long ecsg_gradient_elems(const ecsg_sim *sim, int g);
+int ecsg_pack_gradient(ecsg_sim *sim, int g, double *dst_device);
+int ecsg_unpack_gradient(ecsg_sim *sim, int g, const double *src_device);
+/* The CUDA stream (cudaStream_t) the simulation's work runs on. */
+void *ecsg_stream(const ecsg_sim *sim);
 /* Misfit L = 1/2 sum_n sum_r (v_r(n) - observed[n * n_rec + r])^2 over nsteps
  * steps from rest (receivers as set by ecsg_set_receivers, sampled as the
  * traces), and its gradient with respect to the medium: the forward run keeps

@@ -23,6 +23,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = {
     "stencil.cu": [],
     "stencil_v4.cu": [],
+    "stencil_r.cu": ["-fmad=false"],
     "stress21.cu": ["-fmad=false"],
     "stress21_tma.cu": ["-fmad=false"],
     "medium.cu": [],

@@ -63,6 +63,11 @@ template <typename T>
 cudaError_t launch_unpack(double *, const Geo &, const T *, int, int, int, int, cudaStream_t);
 template <typename T>
 cudaError_t launch_snapshot(float *, const Geo &, const T *, int, int, int, cudaStream_t);
+bool fd_coefficients(int R, double dt, const double h[3], double k[3][6]);
+template <typename T>
+cudaError_t launch_vel_r(const GridDev<T> &, const double[3][6], int, int, int, int, int, T *const[3], cudaStream_t);
+template <typename T>
+cudaError_t launch_stress_r(const GridDev<T> &, const double[3][6], int, int, int, int, int, cudaStream_t);
 template <typename T>
 cudaError_t launch_iso_medium(const Geo &, const double *, const double *, double *, T *const[5], cudaStream_t);
 // adjoint.cu and the interface adjoints of interface.cu
@@ -264,7 +269,9 @@ static int create_impl(const ecsg_grid_desc *grids, const ecsg_config *cfg, ecsg
         return ECSG_ERR_NO_DEVICE;
     }
     if (cfg->num_grids < 1 || cfg->num_grids > kMaxGrids) { fail(s, ECSG_ERR_INVALID, "num_grids out of range"); return bail(ECSG_ERR_INVALID); }
-    if (cfg->radius != 1) { fail(s, ECSG_ERR_INVALID, "radius %d: the device path implements radius 1", cfg->radius); return bail(ECSG_ERR_INVALID); }
+    if (cfg->radius < 1 || cfg->radius > 6) { fail(s, ECSG_ERR_INVALID, "radius %d: FD coefficients exist for radius 1..6 (init_del_fdcoeff.cpp:38-85)", cfg->radius); return bail(ECSG_ERR_INVALID); }
+    if (cfg->radius > 1 && cfg->num_grids > 1) { fail(s, ECSG_ERR_INVALID, "radius %d: the interface conditions are derived for radius 1; composites need radius 1", cfg->radius); return bail(ECSG_ERR_INVALID); }
+    if (cfg->radius > 1 && cfg->medium == ECSG_MEDIUM_GEN21) { fail(s, ECSG_ERR_INVALID, "radius %d: the 21-Cij update is radius 1", cfg->radius); return bail(ECSG_ERR_INVALID); }
     if (!(cfg->dt > 0)) { fail(s, ECSG_ERR_INVALID, "dt must be positive"); return bail(ECSG_ERR_INVALID); }
     if (cfg->imode != ECSG_MODE_ECI && cfg->imode != ECSG_MODE_II) { fail(s, ECSG_ERR_INVALID, "imode %d: 0 (intuitive) or 1 (energy-conserving)", cfg->imode); return bail(ECSG_ERR_INVALID); }
     if (cfg->precision != ECSG_F32 && cfg->precision != ECSG_F64) { fail(s, ECSG_ERR_INVALID, "precision"); return bail(ECSG_ERR_INVALID); }
@@ -679,6 +686,12 @@ static int vel_kernel_op(ecsg_sim *s, int g, bool with_copy, int top = -1, int b
 {
     T *vc[3] = {(T *)s->vc[g][0], (T *)s->vc[g][1], (T *)s->vc[g][2]};
     const int tp = top_of(s, g, top), bt = bottom_of(s, g, bottom);
+    if (s->R > 1) {   // radius 2..6: sweep and its halo mirrors (stencil_r.cu)
+        double k[3][6];
+        fd_coefficients(s->R, s->dt, s->h[g], k);
+        CK(launch_vel_r<T>(dev<T>(s, g), k, s->R, tp, bt, s->top_bc, s->mirror_fix, with_copy ? vc : nullptr, s->st));
+        return ECSG_OK;
+    }
     if constexpr (std::is_same<T, float>::value) {
         if (!s->scalar_stencils) {
             CK(launch_vel_v4(dev<float>(s, g), tp, bt, s->top_bc, with_copy ? vc : nullptr, s->sms, s->st, s->ztune[g][0]));
@@ -692,6 +705,7 @@ static int vel_kernel_op(ecsg_sim *s, int g, bool with_copy, int top = -1, int b
 template <typename T>
 static int vel_mirror_op(ecsg_sim *s, int g, int top = -1, int bottom = -1)
 {
+    if (s->R > 1) return ECSG_OK;   // launch_vel_r ran them with the sweep
     CK(launch_vel_mirror<T>(dev<T>(s, g), top_of(s, g, top), bottom_of(s, g, bottom), s->top_bc, s->mirror_fix, s->st));
     return ECSG_OK;
 }
@@ -731,10 +745,16 @@ static int stress_prepare(ecsg_sim *s)
 }
 
 template <typename T>
-static int stress_op(ecsg_sim *s, int g, int top = -1)
+static int stress_op(ecsg_sim *s, int g, int top = -1, int bottom = -1)
 {
     const int med = med_kind(s);
     const int tp = top_of(s, g, top);
+    if (s->R > 1) {   // radius 2..6 (stencil_r.cu); its bottom mirrors need the bottom role
+        double k[3][6];
+        fd_coefficients(s->R, s->dt, s->h[g], k);
+        CK(launch_stress_r<T>(dev<T>(s, g), k, s->R, med, tp, bottom_of(s, g, bottom), s->top_bc, s->st));
+        return ECSG_OK;
+    }
     if (med == MED_GEN21) {
         T *eps[6];
         for (int k = 0; k < 6; k++) eps[k] = (T *)s->eps[g][k];
@@ -844,10 +864,11 @@ int ecsg_update_vel_ex(ecsg_sim *s, int g, int top, int bottom)
 
 int ecsg_update_stress_ex(ecsg_sim *s, int g, int top, int bottom)
 {
-    (void)bottom;   // the stress update has no bottom-boundary case (update_stress.cpp:4-311)
+    // bottom matters for radius > 1 only (the bottom mirrors of update_stress.cpp:293-309 are empty at radius 1)
     if (!s || g < 0 || g >= s->ng) return fail(s, ECSG_ERR_INVALID, "update_stress_ex: bad grid");
     if (int rc = check_ready(s)) return rc;
-    int rc = s->prec == ECSG_F32 ? stress_op<float>(s, g, top ? 1 : 0) : stress_op<double>(s, g, top ? 1 : 0);
+    int rc = s->prec == ECSG_F32 ? stress_op<float>(s, g, top ? 1 : 0, bottom ? 1 : 0)
+                                 : stress_op<double>(s, g, top ? 1 : 0, bottom ? 1 : 0);
     if (rc) return rc;
     CK(cudaStreamSynchronize(s->st));
     return ECSG_OK;
@@ -856,6 +877,7 @@ int ecsg_update_stress_ex(ecsg_sim *s, int g, int top, int bottom)
 int ecsg_set_coefficients(ecsg_sim *s, int g, const double k[3])
 {
     if (!s || g < 0 || g >= s->ng || !k) return fail(s, ECSG_ERR_INVALID, "set_coefficients: bad arguments");
+    if (s->R != 1) return fail(s, ECSG_ERR_INVALID, "set_coefficients: radius-1 coefficients only");
     for (int d = 0; d < 3; d++) {
         if (!(k[d] > 0)) return fail(s, ECSG_ERR_INVALID, "set_coefficients: coefficients must be positive");
         s->kover[g][d] = k[d];
@@ -871,7 +893,7 @@ int ecsg_update_stress(ecsg_sim *s, int g)
 {
     if (!s || g < 0 || g >= s->ng) return fail(s, ECSG_ERR_INVALID, "update_stress: bad grid");
     if (int rc = check_ready(s)) return rc;
-    int rc = DISPATCH(stress_op)(s, g, -1);
+    int rc = DISPATCH(stress_op)(s, g, -1, -1);
     if (rc) return rc;
     CK(cudaStreamSynchronize(s->st));
     return ECSG_OK;
@@ -1420,6 +1442,7 @@ static AdjDev<T> adj_dev(const ecsg_sim *s, int g)
 
 static int adj_check(ecsg_sim *s)
 {
+    if (s->R != 1) return fail(s, ECSG_ERR_STATE, "adjoint: radius 1 only");
     if (s->medium != ECSG_MEDIUM_GEN21) return fail(s, ECSG_ERR_STATE, "adjoint: the simulation must use ECSG_MEDIUM_GEN21");
     if (int rc = check_ready(s)) return rc;
     CK(cudaSetDevice(s->device));

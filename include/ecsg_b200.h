@@ -59,7 +59,9 @@ typedef struct ecsg_grid_desc {
 /* Run parameters: the key=value parameters of main.cpp:36-67. */
 typedef struct ecsg_config {
     int num_grids;        /* num_grids */
-    int radius;           /* stencil radius; 1 (the interface solves assume 1) */
+    int radius;           /* stencil radius 1..6 (init_del_fdcoeff.cpp:38-85); composites
+                           * and 21-Cij media need 1 (the interface conditions are
+                           * derived for radius 1) */
     double dt;            /* time step */
     int imode;            /* ECSG_MODE_ECI (1), or ECSG_MODE_II (0: ratio-2 interfaces only) */
     int top_bc;           /* 0 rigid, 1 free surface */

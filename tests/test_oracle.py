@@ -88,10 +88,11 @@ def test_operators_match_reference(seed, top_bc):
 
 
 @needs_ref
-@pytest.mark.parametrize("radius", [2, 3])
-def test_high_order_stencils_match_reference(radius):
+@pytest.mark.parametrize("top_bc", [1, 0])
+@pytest.mark.parametrize("radius", [2, 3, 4, 5, 6])
+def test_high_order_stencils_match_reference(radius, top_bc):
     from oracle.ref import RefRun
-    case = random_case(7, ratio=2, nx2=8, ny2=7, nz=(9,), num_grids=1, radius=radius, top_bc=1)
+    case = random_case(7, ratio=2, nx2=8, ny2=7, nz=(9,), num_grids=1, radius=radius, top_bc=top_bc)
     o = OracleRun(case)
     r = RefRun(case, threads=2)
     try:

@@ -4,17 +4,20 @@
 // the results are bitwise equal to its FP32 instantiation), organised for
 // bandwidth: a CTA owns a 32 x 8 tile of
 // (x, y) points and marches z.  One producer thread streams, per plane,
-//   * the 12 coefficient slots read around the tile (c6..c14, c16, c17, c19)
-//     and the three velocities as 40 x 10 boxes (tile, one-point halo, the x
+//   * the three velocities as 40 x 10 boxes (tile, one-point halo, the x
 //     start rounded down to a 16-byte boundary),
+//   * the 12 coefficient slots read around the tile (c6..c14, c16, c17, c19)
+//     as 36 x 9 boxes, each with the one-sided halo its products need: slots
+//     c6..c14 at x-1 and y+1 (normal products), c16, c17 at x-1 and y-1 (L4
+//     links), c19 at x+1 and y+1 (the L5 link),
 //   * the other 9 coefficient slots, the 6 stresses and (energy runs) the 6
 //     strain accumulators as 32 x 8 boxes,
 // into shared-memory rings with cp.async.bulk.tensor (no multicast),
 // completion tracked by mbarriers.  Each group of fields (velocities, the 12
 // haloed slots, the 9 other slots, stresses, strains) is one allocation with
 // its fields at a fixed stride, so one 4-D tensor map (x, y, z, field) moves
-// a whole group: 5 copies per plane instead of 36 (small boxes from many
-// descriptors kept the copy engine, not HBM, the limit).  Eight consumer warps compute
+// a whole group or sub-group: 7 copies per plane instead of 36 (small boxes
+// from many descriptors kept the copy engine, not HBM, the limit).  Eight consumer warps compute
 // every strain / link product of their own point plus one halo row or column
 // of one kind per warp (each kind needs a one-sided halo only), exchange them
 // through a two-plane ring, and update the stresses.  Velocities stay resident
@@ -39,11 +42,16 @@ constexpr int NQ = 9;
 constexpr int NSP = 3, NSV = 5;               // ring depths: plane data, velocities
 constexpr int HBOX = BW * BH * 4;             // 1600 bytes
 constexpr int IBOX = TX * TY * 4;             // 1024 bytes
+constexpr int CW = 36, CHH = 9, CBOX = CW * CHH * 4;   // one-sided coefficient box: 1296 bytes
 constexpr int NCH = 12, NCI = 9;
-constexpr int P_CH = 0, P_CI = NCH * HBOX, P_SG = P_CI + NCI * IBOX, P_EP = P_SG + 6 * IBOX;
-constexpr int PSLOT = P_EP + 6 * IBOX;        // 40704, a multiple of 128
+constexpr int NCA = 9, NCB = 2;               // c6..c14 | c16, c17 | c19
+__host__ __device__ constexpr int up128(int b) { return (b + 127) / 128 * 128; }
+constexpr int P_CHA = 0, P_CHB = up128(NCA * CBOX), P_CHC = up128(P_CHB + NCB * CBOX);
+constexpr int P_CI = up128(P_CHC + CBOX), P_SG = P_CI + NCI * IBOX, P_EP = P_SG + 6 * IBOX;
+constexpr int PSLOT = P_EP + 6 * IBOX;        // 37376, a multiple of 128
 constexpr int VSLOT = (3 * HBOX + 127) / 128 * 128;   // 4864
-static_assert(P_CI % 128 == 0 && P_SG % 128 == 0 && P_EP % 128 == 0 && PSLOT % 128 == 0, "128-byte aligned boxes");
+static_assert(P_CHB % 128 == 0 && P_CHC % 128 == 0 && P_CI % 128 == 0 && P_SG % 128 == 0 && P_EP % 128 == 0 &&
+                  PSLOT % 128 == 0, "128-byte aligned boxes");
 constexpr int OFF_V = NSP * PSLOT;
 constexpr int OFF_IM = OFF_V + NSV * VSLOT;
 constexpr int OFF_BAR = OFF_IM + 2 * NQ * HP * 4;
@@ -58,7 +66,9 @@ __host__ __device__ constexpr int ci_slot(int k) { return k < 6 ? k : (k == 6 ? 
 
 struct S21Maps {
     CUtensorMap v;    // vx vy vz: haloed boxes
-    CUtensorMap ch;   // c6..c14, c16, c17, c19: haloed boxes
+    CUtensorMap cha;  // c6..c14: boxes x-4 .. x+31, y .. y+8
+    CUtensorMap chb;  // c16, c17: boxes x-4 .. x+31, y-1 .. y+7
+    CUtensorMap chc;  // c19: box x .. x+35, y .. y+8
     CUtensorMap ci;   // c0..c5, c15, c18, c20: interior boxes
     CUtensorMap sg;   // sxx syy szz syz sxz sxy: interior boxes
     CUtensorMap ep;   // strain accumulators: interior boxes
@@ -159,9 +169,11 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
                 const int q = qstart + i;
                 const bool inner = q >= z0 && q <= z1;
                 const unsigned dst = smem_u32(sm + s * PSLOT);
-                mbar_expect_tx(fullP(s), NCH * HBOX + (inner ? (NCI + 6 + (ACC ? 6 : 0)) * IBOX : 0));
+                mbar_expect_tx(fullP(s), NCH * CBOX + (inner ? (NCI + 6 + (ACC ? 6 : 0)) * IBOX : 0));
                 const int zc = g.R + q;
-                tma_load4(dst + P_CH, &maps.ch, hx0, hy0, zc, fullP(s));
+                tma_load4(dst + P_CHA, &maps.cha, hx0, iy0, zc, fullP(s));
+                tma_load4(dst + P_CHB, &maps.chb, hx0, hy0, zc, fullP(s));
+                tma_load4(dst + P_CHC, &maps.chc, ix0, iy0, zc, fullP(s));
                 if (inner) {
                     tma_load4(dst + P_CI, &maps.ci, ix0, iy0, zc, fullP(s));
                     tma_load4(dst + P_SG, &maps.sg, ix0, iy0, zc, fullP(s));
@@ -210,6 +222,11 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
         }
         const bool hact = warp < 4 || lane < 9;
         const int hvb = (hyp - y0 + 1) * BW + (hxp - x0 + 4), hhb = (hyp - y0 + 1) * HX + (hxp - x0 + 1);
+        // coefficient boxes: own point and halo point in each (the halo index is
+        // used only with the sub-group that covers this warp's halo kind)
+        const int ia = ty * CW + tx + 4, ibb = (ty + 1) * CW + tx + 4, ic = ty * CW + tx;
+        const int ha = (hyp - y0) * CW + (hxp - x0) + 4, hb = (hyp - y0 + 1) * CW + (hxp - x0) + 4,
+                  hc = (hyp - y0) * CW + (hxp - x0);
         // Tiles whose points and halos all lie strictly inside the grid (x, y in
         // 1 .. n-1): on their planes 1 .. nz-1 every extent test passes and every
         // closure weight is 1/4, so the fast variant drops the tests.
@@ -231,7 +248,9 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
             consumedP = i + 1;
             consumedV = i + 3;
             const unsigned char *PS = sm + (i % NSP) * PSLOT;
-            const float *CH = (const float *)(PS + P_CH);
+            const float *CHA = (const float *)(PS + P_CHA);
+            const float *CHB = (const float *)(PS + P_CHB);
+            const float *CHC = (const float *)(PS + P_CHC);
             const float *CI = (const float *)(PS + P_CI);
             const float *SG = (const float *)(PS + P_SG);
             const float *EP = (const float *)(PS + P_EP);
@@ -247,7 +266,10 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
             const bool inner = p >= z0 && p <= z1;
             const int pm = p - 1;
             const bool outer_pm = pm >= z0 && pm <= z1;
-            auto chv = [&](int k, int b) { return CH[k * HS + b]; };
+            constexpr int CS = CBOX / 4;   // floats between the coefficient boxes of a sub-group
+            // coefficient slot k (0..11 of ch_slot) at this thread's point or at its halo point
+            auto cho = [&](int k) { return k < NCA ? CHA[k * CS + ia] : (k < NCA + NCB ? CHB[(k - NCA) * CS + ibb] : CHC[ic]); };
+            auto chh = [&](int k) { return k < NCA ? CHA[k * CS + ha] : (k < NCA + NCB ? CHB[(k - NCA) * CS + hb] : CHC[hc]); };
 
             auto body = [&](auto fast_tag) {
                 constexpr bool FAST = decltype(fast_tag)::value;
@@ -267,12 +289,12 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
                     float e4 = 0.f, q45 = 0.f, q46 = 0.f, e5 = 0.f, q56 = 0.f, e6 = 0.f, p4 = 0.f, p5 = 0.f, p6 = 0.f;
                     if (FAST || E.l4(ox, oy, p)) {
                         e4 = fma_(k1, sub_(Vp[2 * HS + vb + BW], Vp[2 * HS + vb]), mul_(k2, sub_(Vn[HS + vb], Vp[HS + vb])));
-                        q45 = mul_(chv(9, vb), e4);
-                        q46 = mul_(chv(10, vb), e4);
+                        q45 = mul_(cho(9), e4);
+                        q46 = mul_(cho(10), e4);
                     }
                     if (FAST || E.l5(ox, oy, p)) {
                         e5 = fma_(k0, sub_(Vp[2 * HS + vb], Vp[2 * HS + vb - 1]), mul_(k2, sub_(Vn[vb], Vp[vb])));
-                        q56 = mul_(chv(11, vb), e5);
+                        q56 = mul_(cho(11), e5);
                     }
                     if (FAST || E.l6(ox, oy, p)) e6 = fma_(k0, sub_(Vp[HS + vb], Vp[HS + vb - 1]), mul_(k1, sub_(Vp[vb + BW], Vp[vb])));
                     if (FAST || E.n(ox, oy, p)) {
@@ -282,9 +304,9 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
                             e3 = e3_used(G, E, true, ox, oy, p, pbase + p * sz, e1, e2);
                         else
                             e3 = mul_(k2, sub_(Vp[2 * HS + vb], Vm[2 * HS + vb]));
-                        p4 = fma_(chv(6, vb), e3, fma_(chv(3, vb), e2, mul_(chv(0, vb), e1)));
-                        p5 = fma_(chv(7, vb), e3, fma_(chv(4, vb), e2, mul_(chv(1, vb), e1)));
-                        p6 = fma_(chv(8, vb), e3, fma_(chv(5, vb), e2, mul_(chv(2, vb), e1)));
+                        p4 = fma_(cho(6), e3, fma_(cho(3), e2, mul_(cho(0), e1)));
+                        p5 = fma_(cho(7), e3, fma_(cho(4), e2, mul_(cho(1), e1)));
+                        p6 = fma_(cho(8), e3, fma_(cho(5), e2, mul_(cho(2), e1)));
                     }
                     const int hb = hy * HX + hx;
                     IMs[0 * HP + hb] = e4; IMs[1 * HP + hb] = q45; IMs[2 * HP + hb] = q46;
@@ -297,15 +319,15 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
                         float e4 = 0.f, q45 = 0.f, q46 = 0.f;
                         if (FAST || E.l4(x, y, p)) {
                             e4 = fma_(k1, sub_(Vp[2 * HS + b + BW], Vp[2 * HS + b]), mul_(k2, sub_(Vn[HS + b], Vp[HS + b])));
-                            q45 = mul_(chv(9, b), e4);
-                            q46 = mul_(chv(10, b), e4);
+                            q45 = mul_(chh(9), e4);
+                            q46 = mul_(chh(10), e4);
                         }
                         IMs[0 * HP + hhb] = e4; IMs[1 * HP + hhb] = q45; IMs[2 * HP + hhb] = q46;
                     } else if (hk == 1) {
                         float e5 = 0.f, q56 = 0.f;
                         if (FAST || E.l5(x, y, p)) {
                             e5 = fma_(k0, sub_(Vp[2 * HS + b], Vp[2 * HS + b - 1]), mul_(k2, sub_(Vn[b], Vp[b])));
-                            q56 = mul_(chv(11, b), e5);
+                            q56 = mul_(chh(11), e5);
                         }
                         IMs[3 * HP + hhb] = e5; IMs[4 * HP + hhb] = q56;
                     } else if (hk == 2) {
@@ -319,9 +341,9 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
                             const float f2 = mul_(k1, sub_(Vp[HS + b], Vp[HS + b - BW]));
                             const float f3 = (!FAST && surf) ? e3_used(G, E, true, x, y, p, g.idx(x, y, p), f1, f2)
                                                              : mul_(k2, sub_(Vp[2 * HS + b], Vm[2 * HS + b]));
-                            p4 = fma_(chv(6, b), f3, fma_(chv(3, b), f2, mul_(chv(0, b), f1)));
-                            p5 = fma_(chv(7, b), f3, fma_(chv(4, b), f2, mul_(chv(1, b), f1)));
-                            p6 = fma_(chv(8, b), f3, fma_(chv(5, b), f2, mul_(chv(2, b), f1)));
+                            p4 = fma_(chh(6), f3, fma_(chh(3), f2, mul_(chh(0), f1)));
+                            p5 = fma_(chh(7), f3, fma_(chh(4), f2, mul_(chh(1), f1)));
+                            p6 = fma_(chh(8), f3, fma_(chh(5), f2, mul_(chh(2), f1)));
                         }
                         IMs[6 * HP + hhb] = p4; IMs[7 * HP + hhb] = p5; IMs[8 * HP + hhb] = p6;
                     }
@@ -347,9 +369,9 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
                         float d[3];
 #pragma unroll
                         for (int r = 0; r < 3; r++)
-                            d[r] = fma_(chv(2 + 3 * r, vb), a6,
-                                        fma_(chv(1 + 3 * r, vb), a5,
-                                             fma_(chv(3 * r, vb), a4,
+                            d[r] = fma_(cho(2 + 3 * r), a6,
+                                        fma_(cho(1 + 3 * r), a5,
+                                             fma_(cho(3 * r), a4,
                                                   fma_(CI[rowc[r][2] * IS + ib], e3,
                                                        fma_(CI[rowc[r][1] * IS + ib], e2, mul_(CI[rowc[r][0] * IS + ib], e1))))));
                         sxx[pp] = add_(SG[0 * IS + ib], d[0]);
@@ -430,7 +452,7 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
 
             if (inner) {
                 c15p = CI[6 * IS + ib]; c18p = CI[7 * IS + ib];
-                c16p = chv(9, vb); c17p = chv(10, vb); c19p = chv(11, vb);
+                c16p = cho(9); c17p = cho(10); c19p = cho(11);
                 s3p = SG[3 * IS + ib]; s4p = SG[4 * IS + ib];
                 if (ACC) { ep3p = EP[3 * IS + ib]; ep4p = EP[4 * IS + ib]; }
             }
@@ -515,7 +537,8 @@ bool s21_encode_maps(void *out, const GridDev<float> &G, float *const eps[6])
               strided(g, NCH, [&](int k) { return G.c[ch_slot(k)]; }) &&
               strided(g, NCI, [&](int k) { return G.c[ci_slot(k)]; }) &&
               strided(g, 6, [&](int k) { return (const float *)G.f[SXX + k]; });
-    ok = ok && encode(&M.v, g, G.f[0], 3, BW, BH) && encode(&M.ch, g, G.c[ch_slot(0)], NCH, BW, BH) &&
+    ok = ok && encode(&M.v, g, G.f[0], 3, BW, BH) && encode(&M.cha, g, G.c[ch_slot(0)], NCA, CW, CHH) &&
+         encode(&M.chb, g, G.c[ch_slot(NCA)], NCB, CW, CHH) && encode(&M.chc, g, G.c[ch_slot(NCA + NCB)], 1, CW, CHH) &&
          encode(&M.ci, g, G.c[ci_slot(0)], NCI, TX, TY) && encode(&M.sg, g, G.f[SXX], 6, TX, TY);
     if (ok && eps && eps[0])
         ok = strided(g, 6, [&](int k) { return (const float *)eps[k]; }) && encode(&M.ep, g, eps[0], 6, TX, TY);

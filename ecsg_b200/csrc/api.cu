@@ -353,7 +353,7 @@ static int create_impl(const ecsg_grid_desc *grids, const ecsg_config *cfg, ecsg
     if ((rc = dmalloc(s, (void **)&s->ints, sizeof(int) * 4))) return bail(rc);
     if ((rc = dmalloc(s, (void **)&s->iters_total, sizeof(long long) * kMaxGrids))) return bail(rc);
     if ((rc = dmalloc(s, (void **)&s->dscal, sizeof(double) * 64))) return bail(rc);
-    if ((rc = dmalloc(s, (void **)&s->bar, sizeof(unsigned) * 2 * kMaxGrids))) return bail(rc);
+    if ((rc = dmalloc(s, (void **)&s->bar, sizeof(unsigned) * kBarWords * kMaxGrids))) return bail(rc);
     for (int i = 1; i < s->ng; i++) {
         Iface &I = s->itf[i];
         const Geo &C = s->geo[i];
@@ -365,7 +365,8 @@ static int create_impl(const ecsg_grid_desc *grids, const ecsg_config *cfg, ecsg
         if ((rc = dmalloc(s, (void **)&I.X0, sizeof(double) * nxy))) return bail(rc);
         if ((rc = dmalloc(s, (void **)&I.X1, sizeof(double) * nxy))) return bail(rc);
         I.nblocks = s->prec == ECSG_F32 ? sxz_solve_blocks<float>((int)nn, s->sms) : sxz_solve_blocks<double>((int)nn, s->sms);
-        if ((rc = dmalloc(s, (void **)&I.partial, sizeof(double) * (size_t)I.nblocks))) return bail(rc);
+        // two halves: the solve's reduction rounds alternate between them
+        if ((rc = dmalloc(s, (void **)&I.partial, sizeof(double) * 2 * (size_t)I.nblocks))) return bail(rc);
     }
     if (cudaStreamSynchronize(s->st) != cudaSuccess) return bail(fail(s, ECSG_ERR_CUDA, "initial clear"));
     s->share = share;
@@ -829,7 +830,7 @@ static int sxz_op(ecsg_sim *s, int i)
     W.X1 = I.X1;
     W.partial = I.partial;
     W.total = s->dscal + 1;
-    W.bar = s->bar + 2 * i;
+    W.bar = s->bar + kBarWords * i;
     W.status = s->ints;
     W.iters = s->ints + 2;
     W.iters_total = s->iters_total + i;
@@ -1501,7 +1502,7 @@ static int adj_op_impl(ecsg_sim *s, int op, int i, const GridDev<T> *Gv)
         W.X1 = s->adj_Y1[i];
         W.partial = I.partial;
         W.total = s->dscal + 1;
-        W.bar = s->bar + 2 * i;
+        W.bar = s->bar + kBarWords * i;
         W.status = s->ints;
         W.iters = s->ints + 2;
         W.iters_total = s->iters_total + i;

@@ -88,14 +88,18 @@ enum : int {
     ST_PIPE_TIMEOUT = 8,      // a TMA pipeline wait gave up (the CTA stopped early)
 };
 
+// Barrier words of one grid-wide solve: [0] generation, [32] arrival count
+// (separate 128-byte lines).
+constexpr int kBarWords = 64;
+
 // Work space of one sxz interface solve (interface.cu).
 struct SxzWork {
     const double *A;          // 9 diagonals, [k][j1-1][j0-1]
     double *B;
     double *X0, *X1;          // (nx2+1)*(ny2+1), zero border; X0 holds the warm start
-    double *partial;          // one double per CTA of the solve
-    double *total;            // 1 double
-    unsigned *bar;            // [0] arrival count, [1] generation
+    double *partial;          // two doubles per CTA of the solve (alternating halves)
+    double *total;            // spare word (the total is formed in every CTA)
+    unsigned *bar;            // kBarWords words: generation, arrival count (grid_arrive)
     int *status;
     int *iters;               // sweeps of the last solve
     long long *iters_total;   // running sum of sweeps

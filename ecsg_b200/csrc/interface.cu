@@ -309,51 +309,76 @@ __device__ __forceinline__ double block_sum(double v, double *red)
     return s;   // valid in thread 0
 }
 
-// Grid-wide deterministic sum.  Each CTA publishes its partial; the last CTA
-// to arrive sums all partials with all its threads (fixed strided split, then
-// a fixed tree), publishes the total and releases the others by advancing the
-// generation word.  Every CTA returns the same value.  Waiting is bounded: on
-// timeout the status bit is set, ok becomes false and the caller stops.
-__device__ double grid_sum(double v, const SxzWork &W, double *red, bool &ok)
+// Grid-wide deterministic sum.  Each CTA writes its partial into the half of
+// W.partial that belongs to this round (rounds alternate between two halves of
+// gridDim.x doubles, so a CTA that has already left round k cannot overwrite a
+// partial of round k that a slower CTA is still reading: to write into the same
+// half again it must pass round k+1, which the slower CTA has not reached),
+// then arrives at a barrier: one master thread per CTA releases the CTA's
+// writes with a fence and adds to the arrival count; the last to arrive resets
+// the count and advances the generation word, the others spin on it.  After
+// the barrier every CTA sums all partials in the same fixed order (strided
+// split, then a fixed tree), so every CTA gets the same total with no second
+// publication round.  Waiting is bounded: on timeout the status bit is set, ok
+// becomes false and the caller stops.
+// Publish this CTA's partial of round `round` and wait for every CTA (the
+// barrier half of grid_sum).  One master thread per CTA releases the CTA's
+// writes with a fence and adds to the arrival count; the last to arrive
+// resets the count and advances the generation word, on which the others
+// wait.  The count and the polled generation sit on separate 128-byte lines.
+__device__ void grid_arrive(double v, const SxzWork &W, double *red, bool &ok, int &round)
 {
-    __threadfence();
-    const double bs = block_sum(v, red);   // valid in thread 0
-    __shared__ double s_total;
-    __shared__ int s_last, s_ok;
-    __shared__ unsigned s_gen;
+    const double bs = block_sum(v, red);   // valid in thread 0; ends with a CTA barrier
+    __shared__ int s_ok;
+    double *part = W.partial + (size_t)(round & 1) * gridDim.x;
+    round++;
     if (threadIdx.x == 0) {
-        s_gen = *(volatile unsigned *)(W.bar + 1);   // generation of this round, read before arriving
-        W.partial[blockIdx.x] = bs;
+        unsigned *gen_w = W.bar, *cnt_w = W.bar + 32;
+        const unsigned gen = *(volatile unsigned *)gen_w;   // generation of this round, read before arriving
+        __stcg(part + blockIdx.x, bs);
         __threadfence();
-        const unsigned prev = atomicAdd(W.bar, 1u);
-        s_last = (prev == gridDim.x - 1);
-        s_ok = 1;
-    }
-    __syncthreads();
-    if (s_last) {
-        __threadfence();
-        double t = 0.0;
-        for (unsigned i = threadIdx.x; i < gridDim.x; i += blockDim.x) t += __ldcg(W.partial + i);
-        const double tot = block_sum(t, red);
-        if (threadIdx.x == 0) {
-            __stcg(W.total, tot);
-            W.bar[0] = 0;
+        int okv = 1;
+        if (atomicAdd(cnt_w, 1u) == gridDim.x - 1) {
+            *cnt_w = 0;
             __threadfence();
-            atomicAdd(W.bar + 1, 1u);
-            s_total = tot;
-        }
-    } else if (threadIdx.x == 0) {
-        long long spin = 0;
-        while (*(volatile unsigned *)(W.bar + 1) == s_gen) {
-            if (++spin > kSpinLimit) { atomicOr(W.status, ST_BARRIER_TIMEOUT); s_ok = 0; break; }
-            __nanosleep(32);
+            atomicAdd(gen_w, 1u);
+        } else {
+            long long spin = 0;
+            while (*(volatile unsigned *)gen_w == gen) {
+                if (++spin > kSpinLimit) { atomicOr(W.status, ST_BARRIER_TIMEOUT); okv = 0; break; }
+                __nanosleep(32);
+            }
         }
         __threadfence();
-        s_total = __ldcg(W.total);
+        s_ok = okv;
     }
     __syncthreads();
     ok = s_ok != 0;
+}
+
+// This thread's share of the partials of a finished round (fixed strided split)
+__device__ __forceinline__ double partial_share(const SxzWork &W, int finished_round)
+{
+    const double *part = W.partial + (size_t)(finished_round & 1) * gridDim.x;
+    double t = 0.0;
+    for (unsigned i = threadIdx.x; i < gridDim.x; i += blockDim.x) t += __ldcg(part + i);
+    return t;
+}
+
+// The total of a share over the CTA (fixed tree), returned to every thread
+__device__ __forceinline__ double share_total(double t, double *red)
+{
+    __shared__ double s_total;
+    const double tot = block_sum(t, red);
+    if (threadIdx.x == 0) s_total = tot;
+    __syncthreads();
     return s_total;
+}
+
+__device__ double grid_sum(double v, const SxzWork &W, double *red, bool &ok, int &round)
+{
+    grid_arrive(v, W, red, ok, round);
+    return share_total(partial_share(W, round - 1), red);
 }
 
 template <typename T>
@@ -366,6 +391,7 @@ __global__ void __launch_bounds__(256) sxz_solve_kernel(GridDev<T> F, GridDev<T>
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x;
     const int gstride = gridDim.x * blockDim.x;
     bool ok = true;
+    int round = 0;   // grid_sum rounds (alternating halves of W.partial)
 
     // B and avg|B| (Array::AvgAbs, array.cpp:172-210)
     double sab = 0.0;
@@ -374,32 +400,51 @@ __global__ void __launch_bounds__(256) sxz_solve_kernel(GridDev<T> F, GridDev<T>
         W.B[q] = bq;
         sab += fabs(bq);
     }
-    const double sumabs = grid_sum(sab, W, red, ok);
+    const double sumabs = grid_sum(sab, W, red, ok, round);
     double tol = 1e-5 * (sumabs / (double)nn);
     if (tol > 1e-12) tol = 1e-12;
 
     // Jacobi2D (update_ghost_sxz.cpp:314-350), ping-pong instead of copy
     double *Xc = W.X0, *Xn = W.X1;
+    // the row of A and the entry of B of this thread's first unknown stay in
+    // registers for the whole solve (further unknowns, on grids with more
+    // unknowns than threads, are read from memory)
+    double a0[9] = {0, 0, 0, 0, 1, 0, 0, 0, 0}, b0 = 0.0;
+    if (gtid < nn) {
+#pragma unroll
+        for (int k = 0; k < 9; k++) a0[k] = W.A[(size_t)k * nn + gtid];
+        b0 = W.B[gtid];
+    }
+    auto update = [&](const double *Xo, double *Xw, int q, const double (&a)[9], double bq) {
+        const int i0 = q % n0 + 1, i1 = q / n0 + 1;
+        const double xn = (bq
+                           - a[0] * __ldcg(Xo + (i1 - 1) * ld + (i0 - 1))
+                           - a[1] * __ldcg(Xo + (i1) * ld + (i0 - 1))
+                           - a[2] * __ldcg(Xo + (i1 + 1) * ld + (i0 - 1))
+                           - a[3] * __ldcg(Xo + (i1 - 1) * ld + (i0))
+                           - a[5] * __ldcg(Xo + (i1 + 1) * ld + (i0))
+                           - a[6] * __ldcg(Xo + (i1 - 1) * ld + (i0 + 1))
+                           - a[7] * __ldcg(Xo + (i1) * ld + (i0 + 1))
+                           - a[8] * __ldcg(Xo + (i1 + 1) * ld + (i0 + 1))) / a[4];
+        const double d = xn - __ldcg(Xo + i1 * ld + i0);
+        __stcg(Xw + i1 * ld + i0, xn);
+        return d * d;
+    };
+    auto sweep = [&](const double *Xo, double *Xw) {
+        double s = 0.0;
+        if (gtid < nn) s += update(Xo, Xw, gtid, a0, b0);
+        for (int q = gtid + gstride; q < nn; q += gstride) {
+            double a[9];
+#pragma unroll
+            for (int k = 0; k < 9; k++) a[k] = W.A[(size_t)k * nn + q];
+            s += update(Xo, Xw, q, a, W.B[q]);
+        }
+        return s;
+    };
     int it = 0;
     while (ok) {
-        double s = 0.0;
-        for (int q = gtid; q < nn; q += gstride) {
-            const int i0 = q % n0 + 1, i1 = q / n0 + 1;
-            const double *a = W.A + q;
-            const double xn = (W.B[q]
-                               - a[0 * nn] * __ldcg(Xc + (i1 - 1) * ld + (i0 - 1))
-                               - a[1 * nn] * __ldcg(Xc + (i1) * ld + (i0 - 1))
-                               - a[2 * nn] * __ldcg(Xc + (i1 + 1) * ld + (i0 - 1))
-                               - a[3 * nn] * __ldcg(Xc + (i1 - 1) * ld + (i0))
-                               - a[5 * nn] * __ldcg(Xc + (i1 + 1) * ld + (i0))
-                               - a[6 * nn] * __ldcg(Xc + (i1 - 1) * ld + (i0 + 1))
-                               - a[7 * nn] * __ldcg(Xc + (i1) * ld + (i0 + 1))
-                               - a[8 * nn] * __ldcg(Xc + (i1 + 1) * ld + (i0 + 1))) / a[4 * nn];
-            const double d = xn - __ldcg(Xc + i1 * ld + i0);
-            __stcg(Xn + i1 * ld + i0, xn);
-            s += d * d;
-        }
-        const double tot = grid_sum(s, W, red, ok);
+        const double s = sweep(Xc, Xn);
+        const double tot = grid_sum(s, W, red, ok, round);
         double *tmp = Xc; Xc = Xn; Xn = tmp;
         it++;
         if (!(sqrt(tot) > tol)) break;
@@ -770,9 +815,10 @@ __global__ void __launch_bounds__(256) sxz_adj_solve_kernel(int nx2, int ny2, Sx
     const int n0 = nx2 - 1, n1 = ny2 - 1, ld = nx2 + 1, nn = n0 * n1;
     const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gstride = gridDim.x * blockDim.x;
     bool ok = true;
+    int round = 0;   // grid_sum rounds (alternating halves of W.partial)
     double sab = 0.0;
     for (int q = gtid; q < nn; q += gstride) sab += fabs(lx[q]);
-    const double sum = grid_sum(sab, W, red, ok);
+    const double sum = grid_sum(sab, W, red, ok, round);
     if (!(sum > 0.0)) {   // no adjoint at this interface yet: y = 0
         for (int q = gtid; q < nn; q += gstride) W.X0[(q / n0 + 1) * ld + q % n0 + 1] = 0.0;
         if (gtid == 0) *W.iters = 0;
@@ -799,7 +845,7 @@ __global__ void __launch_bounds__(256) sxz_adj_solve_kernel(int nx2, int ny2, Sx
             __stcg(Xn + i1 * ld + i0, xn);
             s += d * d;
         }
-        const double tot = grid_sum(s, W, red, ok);
+        const double tot = grid_sum(s, W, red, ok, round);
         double *tmp = Xc; Xc = Xn; Xn = tmp;
         it++;
         if (!(sqrt(tot) > tol)) break;

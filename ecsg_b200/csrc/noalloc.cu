@@ -49,9 +49,11 @@ constexpr size_t kOffB = kOffA + align256(9 * kMaxUnknowns * sizeof(double));
 constexpr size_t kOffX1 = kOffB + align256(kMaxUnknowns * sizeof(double));
 constexpr size_t kOffPartial = kOffX1 + align256(kMaxNodes * sizeof(double));
 constexpr size_t kOffWords = kOffPartial + align256(kMaxBlocks * sizeof(double));
-// words: double total, double tol, long long iters_total, unsigned bar[2], int status, int iters
+// words: double total, double tol, long long iters_total, (spare), int status, int iters
 constexpr size_t kWordsBytes = 64;
-constexpr size_t kScratchBytes = kOffWords + align256(kWordsBytes);
+constexpr size_t kOffBar = kOffWords + align256(kWordsBytes);   // grid-barrier words
+constexpr size_t kBarBytes = kBarWords * sizeof(unsigned);
+constexpr size_t kScratchBytes = kOffBar + align256(kBarBytes);
 static_assert(kScratchBytes < (16u << 20), "scratch must stay modest");
 
 constexpr int kMaxDevices = 64;
@@ -117,11 +119,12 @@ static int solve(const ecsg_grid_view *fine, const ecsg_grid_view *coarse, int r
         return report(errbuf, errlen, ECSG_ERR_CUDA, "cannot query the SM count");
     const int nn = (coarse->size[0] - 1) * (coarse->size[1] - 1);
     const int nblocks = sxz_solve_blocks<T>(nn, sms);
-    if ((size_t)nblocks > kMaxBlocks) return report(errbuf, errlen, ECSG_ERR_INVALID, "too many SMs for the static partial sums");
+    if (2 * (size_t)nblocks > kMaxBlocks)   // two halves of partial sums (alternating reduction rounds)
+        return report(errbuf, errlen, ECSG_ERR_INVALID, "too many SMs for the static partial sums");
     const size_t nodes = (size_t)(coarse->size[0] + 1) * (coarse->size[1] + 1);
     // zero the second iterate (its border must be zero) and the barrier/status words
     if ((e = cudaMemsetAsync(base + kOffX1, 0, nodes * sizeof(double), st)) != cudaSuccess ||
-        (e = cudaMemsetAsync(base + kOffWords, 0, kWordsBytes, st)) != cudaSuccess)
+        (e = cudaMemsetAsync(base + kOffWords, 0, kOffBar - kOffWords + kBarBytes, st)) != cudaSuccess)
         return report(errbuf, errlen, ECSG_ERR_CUDA, cudaGetErrorString(e));
     const GridDev<T> F = view_dev<T>(fine, dt), C = view_dev<T>(coarse, dt);
     double *A = (double *)(base + kOffA);
@@ -136,7 +139,7 @@ static int solve(const ecsg_grid_view *fine, const ecsg_grid_view *coarse, int r
     W.total = (double *)(w + 0);
     W.tol_out = (double *)(w + 8);
     W.iters_total = (long long *)(w + 16);
-    W.bar = (unsigned *)(w + 24);
+    W.bar = (unsigned *)(base + kOffBar);
     W.status = (int *)(w + 32);
     W.iters = (int *)(w + 36);
     W.max_iter = max_iter > 0 ? max_iter : 10000;

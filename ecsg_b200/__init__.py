@@ -81,6 +81,9 @@ SIGNATURES = [
     ("ecsg_pack_gradient", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
     ("ecsg_unpack_gradient", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p]),
     ("ecsg_stream", ctypes.c_void_p, [ctypes.c_void_p]),
+    ("ecsg_state_bytes", ctypes.c_longlong, [ctypes.c_void_p]),
+    ("ecsg_save_state", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
+    ("ecsg_load_state", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p]),
     ("ecsg_field_elems", ctypes.c_longlong, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     ("ecsg_update_vel", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("ecsg_update_stress", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
@@ -283,6 +286,22 @@ class Simulation:
         out = np.empty(field_shape(n, SIM_POS[k], self.R))
         self._ck(lib().ecsg_get_field(self.h, g, k, out.ctypes.data_as(c_dp)))
         return out
+
+    def save_state(self):
+        """The run state (fields, sxz warm starts, strain accumulators) as bytes."""
+        buf = np.empty(int(lib().ecsg_state_bytes(self.h)), np.uint8)
+        self._ck(lib().ecsg_save_state(self.h, buf.ctypes.data_as(ctypes.c_void_p)))
+        return buf
+
+    def load_state(self, buf, step_index=None):
+        """Restore a save_state() of a simulation with the same set-up; runs
+        continue from step_index (the next step of the saved run)."""
+        buf = np.ascontiguousarray(buf, dtype=np.uint8)
+        if buf.size != int(lib().ecsg_state_bytes(self.h)):
+            raise ValueError("state size does not match this simulation")
+        self._ck(lib().ecsg_load_state(self.h, buf.ctypes.data_as(ctypes.c_void_p)))
+        if step_index is not None:
+            self.step_index = int(step_index)
 
     def gradient_elems(self, g):
         return int(lib().ecsg_gradient_elems(self.h, g))

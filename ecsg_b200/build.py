@@ -26,6 +26,7 @@ SOURCES = {
     "stencil_r.cu": ["-fmad=false"],
     "stress21.cu": ["-fmad=false"],
     "stress21_tma.cu": ["-fmad=false"],
+    "vel_tma.cu": [],
     "medium.cu": [],
     "adjoint.cu": ["-fmad=false"],
     "interface.cu": ["-fmad=false"],

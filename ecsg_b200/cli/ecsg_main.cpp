@@ -17,7 +17,11 @@
 // the reference's double build to its rounding), device=0, graph=y,
 // src_comp=0, rec_comp=0, mirror_fix=n, ii_skip_end_column=n, datapath= (write
 // samples to separate files there instead of after the header), dryrun=y
-// (read the inputs, print the set-up, run nothing).
+// (read the inputs, print the set-up, run nothing), checkpoint=path with
+// checkpoint_every=K (write the run state after every K completed steps) and
+// stop_after=M (stop after M steps, writing the checkpoint), resume=path
+// (continue a checkpointed run: the outputs are those of an uninterrupted run;
+// movies cannot be continued).
 //
 // The loop is main.cpp:165-261: niter = 0 .. ceil(movie_dt*movie_nt/dt).  It
 // runs on the device in segments that end at the steps where main.cpp prints
@@ -33,6 +37,7 @@
 #include <condition_variable>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <deque>
 #include <memory>
 #include <mutex>
@@ -194,6 +199,67 @@ private:
     std::string error_;
 };
 
+// Checkpoint file: an RSF-style header (the set-up it belongs to, the number
+// of completed steps, the sizes of the parts), then 0x0c 0x0c 0x04, the
+// library's run state (ecsg_save_state), the receiver samples, energies and
+// residues of the completed steps.
+void write_checkpoint(const std::string &path, const std::string &setup, int done, long long state_bytes,
+                      ecsg_sim *sim, const std::vector<float> &rec, const std::vector<double> &energy,
+                      const std::vector<double> &res)
+{
+    const std::string tmp = path + ".partial";
+    FILE *fp = std::fopen(tmp.c_str(), "wb");
+    if (!fp) die("cannot create " + tmp);
+    std::vector<unsigned char> state((size_t)state_bytes);
+    ck(ecsg_save_state(sim, state.data()), "ecsg_save_state", sim);
+    std::fprintf(fp, "ecsg_checkpoint=1 %s done=%d state_bytes=%lld\n", setup.c_str(), done, state_bytes);
+    std::fputc(0x0c, fp);
+    std::fputc(0x0c, fp);
+    std::fputc(0x04, fp);
+    bool ok = std::fwrite(state.data(), 1, state.size(), fp) == state.size();
+    // histories: the whole arrays (steps after `done` are unset and ignored on resume)
+    ok = ok && std::fwrite(rec.data(), sizeof(float), rec.size(), fp) == rec.size();
+    ok = ok && std::fwrite(energy.data(), sizeof(double), energy.size(), fp) == energy.size();
+    ok = ok && std::fwrite(res.data(), sizeof(double), res.size(), fp) == res.size();
+    ok = (std::fclose(fp) == 0) && ok;
+    if (!ok || std::rename(tmp.c_str(), path.c_str()) != 0) die("cannot write checkpoint " + path);
+}
+
+int read_checkpoint(const std::string &path, const std::string &setup, long long state_bytes, ecsg_sim *sim,
+                    std::vector<float> &rec, std::vector<double> &energy, std::vector<double> &res)
+{
+    FILE *fp = std::fopen(path.c_str(), "rb");
+    if (!fp) die("cannot open checkpoint " + path);
+    std::string text;
+    int c, p1 = -1, p2 = -1;
+    bool marker = false;
+    while ((c = std::fgetc(fp)) != EOF) {
+        if (p2 == 0x0c && p1 == 0x0c && c == 0x04) { marker = true; text.resize(text.size() - 2); break; }
+        text.push_back((char)c);
+        p2 = p1;
+        p1 = c;
+    }
+    if (!marker) die(path + ": not a checkpoint");
+    std::map<std::string, std::string> kv, want;
+    ecsg_cli::parse_pairs(text, kv);
+    ecsg_cli::parse_pairs(setup, want);
+    if (kv["ecsg_checkpoint"] != "1") die(path + ": not a checkpoint");
+    for (auto &w : want)
+        if (kv[w.first] != w.second)
+            die(path + ": written for " + w.first + "=" + kv[w.first] + ", this run has " + w.second);
+    if (std::strtoll(kv["state_bytes"].c_str(), nullptr, 10) != state_bytes) die(path + ": state size differs");
+    const int done = (int)std::strtol(kv["done"].c_str(), nullptr, 10);
+    std::vector<unsigned char> state((size_t)state_bytes);
+    bool ok = std::fread(state.data(), 1, state.size(), fp) == state.size();
+    ok = ok && std::fread(rec.data(), sizeof(float), rec.size(), fp) == rec.size();
+    ok = ok && std::fread(energy.data(), sizeof(double), energy.size(), fp) == energy.size();
+    ok = ok && std::fread(res.data(), sizeof(double), res.size(), fp) == res.size();
+    std::fclose(fp);
+    if (!ok || done <= 0) die(path + ": truncated checkpoint");
+    ck(ecsg_load_state(sim, state.data()), "ecsg_load_state", sim);
+    return done;
+}
+
 int run(const Params &P)
 {
     const bool check_energy = P.b("check_energy", false);
@@ -339,17 +405,45 @@ int run(const Params &P)
     std::unique_ptr<FrameWriter> writer;
     if (!movies.empty()) writer = std::make_unique<FrameWriter>(max_frame, 2 * (int)movies.size());
 
-    // the loop, in segments ending at frame steps
+    // the loop, in segments ending at frame steps and checkpoint steps
     const bool residues = verb && num_grids > 1;
     std::vector<float> rec((size_t)nsteps * n_rec);
     std::vector<double> energy(check_energy ? nsteps : 0);
     std::vector<double> res(residues ? (size_t)nsteps * (num_grids - 1) * 9 : 0);
     const int use_graph = P.b("graph", true) ? 1 : 0;
+    const std::string ckpt_path = P.str("checkpoint", "");
+    const int ckpt_every = P.i("checkpoint_every", 0);
+    const int stop_after = P.i("stop_after", 0);
+    // the set-up a checkpoint must match (key=value, compared as text on resume)
+    std::string setup = "num_grids=" + std::to_string(num_grids) + " radius=" + std::to_string(radius) +
+                        " imode=" + std::to_string(imode) + " top_bc=" + std::to_string(top_bc) + " precision=" +
+                        precision + " check_energy=" + std::to_string((int)check_energy) +
+                        " residues=" + std::to_string((int)residues) + " n_rec=" + std::to_string(n_rec) +
+                        " nsteps=" + std::to_string(nsteps);
+    for (int g = 0; g < num_grids; g++)
+        setup += " grid_" + std::to_string(g + 1) + "=" + std::to_string(grids[g].size[0]) + "x" +
+                 std::to_string(grids[g].size[1]) + "x" + std::to_string(grids[g].size[2]);
+    {
+        char buf[64];
+        std::snprintf(buf, sizeof buf, " dt=%.17g", dt);
+        setup += buf;
+    }
+    const long long state_bytes = ecsg_state_bytes(sim);
+    int start = 0;
+    if (P.has("resume")) {
+        if (!movies.empty()) die("resume: movies cannot be continued; run without movie flags");
+        start = read_checkpoint(P.str("resume"), setup, state_bytes, sim, rec, energy, res);
+        std::printf("== Resumed after step %d of %d\n", start - 1, nsteps - 1);
+    }
+    const int stop = stop_after > 0 && stop_after < nsteps ? stop_after : nsteps;
     const auto t0 = std::chrono::steady_clock::now();
     double device_ms = 0.0;
     size_t next_frame = 0;
-    for (int n0 = 0; n0 < nsteps;) {
-        const int end = next_frame < frame_steps.size() ? frame_steps[next_frame] + 1 : nsteps;
+    while (next_frame < frame_steps.size() && frame_steps[next_frame] < start) next_frame++;
+    for (int n0 = start; n0 < stop;) {
+        int end = next_frame < frame_steps.size() ? frame_steps[next_frame] + 1 : stop;
+        if (ckpt_every > 0) end = std::min(end, (n0 / ckpt_every + 1) * ckpt_every);
+        end = std::min(end, stop);
         const int len = end - n0;
         ck(ecsg_run(sim, n0, len, n_rec ? &rec[(size_t)n0 * n_rec] : nullptr, check_energy ? &energy[n0] : nullptr,
                     1, residues ? &res[(size_t)n0 * (num_grids - 1) * 9] : nullptr, use_graph),
@@ -369,7 +463,18 @@ int run(const Params &P)
             }
             next_frame++;
         }
+        if (!ckpt_path.empty() && ((ckpt_every > 0 && end % ckpt_every == 0) || end == stop) && end < nsteps)
+            write_checkpoint(ckpt_path, setup, end, state_bytes, sim, rec, energy, res);
         n0 = end;
+    }
+    if (stop < nsteps) {
+        if (writer) writer->drain();
+        std::printf("== Stopped after step %d of %d%s\n", stop - 1, nsteps - 1,
+                    ckpt_path.empty() ? "" : (", checkpoint " + ckpt_path).c_str());
+        movies.clear();
+        writer.reset();
+        ecsg_destroy(sim);
+        return 0;
     }
     if (writer) writer->drain();
     int status = 0;

@@ -3,6 +3,8 @@
 //
 // One ecsg_sim owns one CUDA stream and all device memory of a composite run.
 // There is no host fallback: without a usable device every entry point fails.
+#include <nvtx3/nvToolsExt.h>
+#include <optional>
 #include "ecsg_device.cuh"
 #include "adjoint.cuh"
 #include "../../include/ecsg_b200.h"
@@ -34,6 +36,10 @@ size_t s21_maps_bytes();
 bool s21_encode_maps(void *, const GridDev<float> &, float *const[6]);
 cudaError_t s21_set_attributes();
 cudaError_t launch_stress21_tma(const void *, const GridDev<float> &, int, int, float *const[6], int *, int, cudaStream_t, int);
+size_t vel_maps_bytes();
+bool vel_encode_maps(void *, const GridDev<float> &);
+cudaError_t vel_tma_set_attributes();
+cudaError_t launch_vel_tma(const void *, const GridDev<float> &, int, int, int, float *const[3], int *, int, cudaStream_t, int);
 // interface.cu
 template <typename T>
 cudaError_t launch_ghost_vz(const GridDev<T> &, const GridDev<T> &, int, int, double *, cudaStream_t);
@@ -142,6 +148,9 @@ struct ecsg_sim {
     void *eps[kMaxGrids][6] = {};   // 21-Cij media with energy: accumulated strains at the stress positions
     std::vector<unsigned char> s21maps[kMaxGrids];   // TMA tensor maps of the FP32 21-Cij sweep, per grid
     bool s21_ready = false;
+    std::vector<unsigned char> velmaps[kMaxGrids];   // TMA tensor maps of the FP32 velocity sweep, per grid
+    bool vel_ready = false;
+    bool vel_tma = true;             // FP32 velocity sweep: TMA-staged (false: the float4 sweep)
     // adjoint state (allocated on first use): adjoint fields, gradients, work boxes
     bool adj = false;
     void *lblk[kMaxGrids] = {}, *gbblk[kMaxGrids] = {}, *gcblk[kMaxGrids] = {};
@@ -189,6 +198,15 @@ struct ecsg_sim {
     size_t snap_cap = 0;
     long long bytes = 0;
     std::string err;
+};
+
+// NVTX range for the duration of a scope (visible in Nsight timelines; no cost
+// without a tool attached)
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
 };
 
 static int fail(ecsg_sim *s, int code, const char *fmt, ...)
@@ -291,6 +309,10 @@ static int create_impl(const ecsg_grid_desc *grids, const ecsg_config *cfg, ecsg
     {
         const char *env = getenv("ECSG_SCALAR_STENCILS");
         s->scalar_stencils = env && env[0] == '1';
+    }
+    {
+        const char *env = getenv("ECSG_VEL_TMA");   // "0": the float4 velocity sweep (validation)
+        s->vel_tma = !(env && env[0] == '0');
     }
     s->tsize = s->prec == ECSG_F32 ? 4 : 8;
     s->nc = s->medium == ECSG_MEDIUM_ISO ? 5 : (s->medium == ECSG_MEDIUM_ORTHO9 ? 9 : 21);
@@ -682,6 +704,9 @@ static int check_ready(ecsg_sim *s)
 static int top_of(const ecsg_sim *s, int g, int top) { return top < 0 ? (g == 0) : top; }
 static int bottom_of(const ecsg_sim *s, int g, int bottom) { return bottom < 0 ? (g == s->ng - 1) : bottom; }
 
+static bool use_vel_tma(const ecsg_sim *s);
+static int stress_prepare(ecsg_sim *s);
+
 template <typename T>
 static int vel_kernel_op(ecsg_sim *s, int g, bool with_copy, int top = -1, int bottom = -1)
 {
@@ -694,6 +719,12 @@ static int vel_kernel_op(ecsg_sim *s, int g, bool with_copy, int top = -1, int b
         return ECSG_OK;
     }
     if constexpr (std::is_same<T, float>::value) {
+        if (use_vel_tma(s)) {
+            if (int rc = stress_prepare(s)) return rc;
+            CK(launch_vel_tma(s->velmaps[g].data(), dev<float>(s, g), tp, bt, s->top_bc, with_copy ? vc : nullptr, s->ints,
+                              s->sms, s->st, s->ztune[g][0]));
+            return ECSG_OK;
+        }
         if (!s->scalar_stencils) {
             CK(launch_vel_v4(dev<float>(s, g), tp, bt, s->top_bc, with_copy ? vc : nullptr, s->sms, s->st, s->ztune[g][0]));
             return ECSG_OK;
@@ -723,15 +754,29 @@ static int med_kind(const ecsg_sim *s)
     return s->medium == ECSG_MEDIUM_ISO ? MED_ISO5 : (s->medium == ECSG_MEDIUM_ORTHO9 ? MED_ORTHO9 : MED_GEN21);
 }
 
+static bool use_vel_tma(const ecsg_sim *s)
+{
+    return s->prec == ECSG_F32 && !s->scalar_stencils && s->vel_tma && s->R == 1;
+}
+
 static bool use_s21_tma(const ecsg_sim *s)
 {
     return s->medium == ECSG_MEDIUM_GEN21 && s->prec == ECSG_F32 && !s->scalar_stencils;
 }
 
-// Tensor maps and kernel attributes of the TMA-staged 21-Cij sweep; host work
-// only, done once before any capture.
+// Tensor maps and kernel attributes of the TMA-staged sweeps (velocity, and
+// 21-Cij stress); host work only, done once before any capture.
 static int stress_prepare(ecsg_sim *s)
 {
+    if (use_vel_tma(s) && !s->vel_ready) {
+        for (int g = 0; g < s->ng; g++) {
+            s->velmaps[g].assign(vel_maps_bytes(), 0);
+            if (!vel_encode_maps(s->velmaps[g].data(), dev<float>(s, g)))
+                return fail(s, ECSG_ERR_CUDA, "grid %d: TMA tensor maps of the velocity sweep could not be encoded", g);
+        }
+        CK(vel_tma_set_attributes());
+        s->vel_ready = true;
+    }
     if (!use_s21_tma(s) || s->s21_ready) return ECSG_OK;
     for (int g = 0; g < s->ng; g++) {
         float *eps[6];
@@ -1290,6 +1335,7 @@ static int run_op(ecsg_sim *s, int n0, int nsteps, float *traces, double *energy
 int ecsg_run(ecsg_sim *s, int n0, int nsteps, float *traces, double *energy, int energy_every, double *residues,
              int use_graph)
 {
+    NvtxRange range("ecsg_run");
     if (!s || nsteps < 0) return fail(s, ECSG_ERR_INVALID, "run: bad arguments");
     if (energy && !s->energy) return fail(s, ECSG_ERR_STATE, "run: energy requested but simulation created without it");
     if (int rc = check_ready(s)) return rc;
@@ -1663,12 +1709,12 @@ static int save_state(ecsg_sim *s, char *dst)
 {
     for (int g = 0; g < s->ng; g++) {
         const size_t b = 9 * (size_t)s->geo[g].size() * s->tsize;
-        CK(cudaMemcpyAsync(dst, s->fblk[g], b, cudaMemcpyDeviceToDevice, s->st));
+        CK(cudaMemcpyAsync(dst, s->fblk[g], b, cudaMemcpyDefault, s->st));
         dst += b;
     }
     for (int i = 1; i < s->ng; i++) {
         const size_t b = sizeof(double) * (size_t)(s->geo[i].nx + 1) * (s->geo[i].ny + 1);
-        CK(cudaMemcpyAsync(dst, s->itf[i].X0, b, cudaMemcpyDeviceToDevice, s->st));
+        CK(cudaMemcpyAsync(dst, s->itf[i].X0, b, cudaMemcpyDefault, s->st));
         dst += b;
     }
     return ECSG_OK;
@@ -1678,14 +1724,57 @@ static int load_state(ecsg_sim *s, const char *src)
 {
     for (int g = 0; g < s->ng; g++) {
         const size_t b = 9 * (size_t)s->geo[g].size() * s->tsize;
-        CK(cudaMemcpyAsync(s->fblk[g], src, b, cudaMemcpyDeviceToDevice, s->st));
+        CK(cudaMemcpyAsync(s->fblk[g], src, b, cudaMemcpyDefault, s->st));
         src += b;
     }
     for (int i = 1; i < s->ng; i++) {
         const size_t b = sizeof(double) * (size_t)(s->geo[i].nx + 1) * (s->geo[i].ny + 1);
-        CK(cudaMemcpyAsync(s->itf[i].X0, src, b, cudaMemcpyDeviceToDevice, s->st));
+        CK(cudaMemcpyAsync(s->itf[i].X0, src, b, cudaMemcpyDefault, s->st));
         src += b;
     }
+    return ECSG_OK;
+}
+
+// The whole run state: save_state's part, then the strain accumulators of the
+// grids that keep them.  buf may be device or host memory.
+static size_t run_state_bytes(const ecsg_sim *s)
+{
+    size_t b = state_bytes(s);
+    for (int g = 0; g < s->ng; g++)
+        if (s->epsblk[g]) b += 6 * (size_t)s->geo[g].size() * s->tsize;
+    return b;
+}
+
+static int move_run_state(ecsg_sim *s, char *buf, bool save)
+{
+    if (int rc = save ? save_state(s, buf) : load_state(s, buf)) return rc;
+    char *p = buf + state_bytes(s);
+    for (int g = 0; g < s->ng; g++)
+        if (s->epsblk[g]) {
+            const size_t b = 6 * (size_t)s->geo[g].size() * s->tsize;
+            CK(cudaMemcpyAsync(save ? p : s->epsblk[g], save ? s->epsblk[g] : p, b, cudaMemcpyDefault, s->st));
+            p += b;
+        }
+    return ECSG_OK;
+}
+
+long long ecsg_state_bytes(const ecsg_sim *s) { return s ? (long long)run_state_bytes(s) : -1; }
+
+int ecsg_save_state(ecsg_sim *s, void *dst)
+{
+    if (!s || !dst) return fail(s, ECSG_ERR_INVALID, "save_state: bad arguments");
+    CK(cudaSetDevice(s->device));
+    if (int rc = move_run_state(s, (char *)dst, true)) return rc;
+    CK(cudaStreamSynchronize(s->st));
+    return ECSG_OK;
+}
+
+int ecsg_load_state(ecsg_sim *s, const void *src)
+{
+    if (!s || !src) return fail(s, ECSG_ERR_INVALID, "load_state: bad arguments");
+    CK(cudaSetDevice(s->device));
+    if (int rc = move_run_state(s, (char *)src, false)) return rc;
+    CK(cudaStreamSynchronize(s->st));
     return ECSG_OK;
 }
 
@@ -1734,6 +1823,8 @@ static int misfit_gradient_op(ecsg_sim *s, int nsteps, const float *observed, in
     if ((rc = stress_prepare(s))) return rc;
     if ((rc = adj_zero(s, true, true))) return rc;
     // forward from rest with checkpoints every k steps
+    std::optional<NvtxRange> forward_range;
+    forward_range.emplace("misfit forward");
     for (int g = 0; g < s->ng; g++) CK(cudaMemsetAsync(s->fblk[g], 0, 9 * (size_t)s->geo[g].size() * s->tsize, s->st));
     for (int i = 1; i < s->ng; i++)
         CK(cudaMemsetAsync(s->itf[i].X0, 0, sizeof(double) * (s->geo[i].nx + 1) * (s->geo[i].ny + 1), s->st));
@@ -1744,6 +1835,8 @@ static int misfit_gradient_op(ecsg_sim *s, int nsteps, const float *observed, in
         if ((rc = step_op<T>(s, false, nullptr, nullptr, nrec ? rec + (size_t)n * nrec : nullptr))) return rc;
     }
     if ((rc = save_state(s, s->ckpt + (size_t)ncp * sb))) return rc;
+    forward_range.reset();
+    NvtxRange backward_range("misfit backward");
     CK(cudaMemsetAsync(s->dscal + 8, 0, sizeof(double), s->st));
     CK(launch_residual<T>(rec, s->obs, (int64_t)nobs, s->dscal + 8, s->st));
     // backward, segment by segment: recompute the segment's states, then reverse its steps
@@ -1906,6 +1999,7 @@ static int batch_check(ecsg_sim *const *sims, int n)
 
 int ecsg_batch_run(ecsg_sim *const *sims, int n, int n0, int nsteps, float *const *traces, double *ms)
 {
+    NvtxRange range("ecsg_batch_run");
     if (int rc = batch_check(sims, n)) return rc;
     if (nsteps < 1) return ECSG_OK;
     return sims[0]->prec == ECSG_F32 ? batch_run_op<float>(sims, n, n0, nsteps, traces, ms)
@@ -1980,6 +2074,7 @@ int ecsg_sum_gradients(ecsg_sim *dst, ecsg_sim *const *srcs, int n)
 // ---------------------------------------------------------------------------
 int ecsg_autotune(ecsg_sim *s, int reps)
 {
+    NvtxRange range("ecsg_autotune");
     if (!s) return ECSG_ERR_INVALID;
     if (int rc = check_ready(s)) return rc;
     CK(cudaSetDevice(s->device));
@@ -1988,22 +2083,9 @@ int ecsg_autotune(ecsg_sim *s, int reps)
     int rc;
     if ((rc = stress_prepare(s))) return rc;
     // the trial sweeps change the fields (and strain accumulators): keep and restore them
-    const size_t sb = state_bytes(s);
-    size_t eb = 0;
-    for (int g = 0; g < s->ng; g++)
-        if (s->epsblk[g]) eb += 6 * (size_t)s->geo[g].size() * s->tsize;
     char *save = nullptr;
-    CK(cudaMalloc(&save, sb + eb + 1));
-    if ((rc = save_state(s, save))) { cudaFree(save); return rc; }
-    {
-        char *p = save + sb;
-        for (int g = 0; g < s->ng; g++)
-            if (s->epsblk[g]) {
-                const size_t b = 6 * (size_t)s->geo[g].size() * s->tsize;
-                CK(cudaMemcpyAsync(p, s->epsblk[g], b, cudaMemcpyDeviceToDevice, s->st));
-                p += b;
-            }
-    }
+    CK(cudaMalloc(&save, run_state_bytes(s) + 1));
+    if ((rc = move_run_state(s, save, true))) { cudaFree(save); return rc; }
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
@@ -2032,16 +2114,7 @@ int ecsg_autotune(ecsg_sim *s, int reps)
         }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    rc = load_state(s, save);
-    {
-        char *p = save + sb;
-        for (int g = 0; g < s->ng; g++)
-            if (s->epsblk[g]) {
-                const size_t b = 6 * (size_t)s->geo[g].size() * s->tsize;
-                CK(cudaMemcpyAsync(s->epsblk[g], p, b, cudaMemcpyDeviceToDevice, s->st));
-                p += b;
-            }
-    }
+    rc = move_run_state(s, save, false);
     CK(cudaStreamSynchronize(s->st));
     cudaFree(save);
     s->epoch++;   // the cached step graphs hold the old launch shapes

@@ -184,6 +184,17 @@ int ecsg_locate(const ecsg_sim *sim, const double xyz[3], int loc4[4]);
 int ecsg_run(ecsg_sim *sim, int n0, int nsteps, float *traces, double *energy, int energy_every, double *residues,
              int use_graph);
 
+/* Run state for checkpoint / resume (no reference counterpart): the fields of
+ * every grid in the library's own layout and precision, the sxz warm starts
+ * and, when the simulation keeps them, the strain accumulators of 21-Cij
+ * media, as one opaque buffer of ecsg_state_bytes(sim) bytes (host or device
+ * memory).  Loading it into a simulation created with the same grids,
+ * configuration and medium continues the run bit for bit: pass the next step
+ * index as n0 of ecsg_run. */
+long long ecsg_state_bytes(const ecsg_sim *sim);
+int ecsg_save_state(ecsg_sim *sim, void *dst);
+int ecsg_load_state(ecsg_sim *sim, const void *src);
+
 /* Movie frames (InitMovie/PrintMovie, init_del_movie.cpp:5-95, print.cpp:89-104):
  * the computational domain of field k of grid g (no halo), dims[0] x dims[1]
  * x dims[2] with x fastest, as float32, packed on the device and copied to

@@ -101,3 +101,55 @@ def test_frame_is_the_field_domain(precision):
                 want = f[R:R + fr.shape[0], R:R + fr.shape[1], R:R + fr.shape[2]].astype(np.float32)
                 assert fr.shape == tuple(d - 2 * R for d in f.shape)
                 assert np.array_equal(fr, want), (g, k)
+
+
+@pytest.mark.parametrize("precision", ["f32", "f64"])
+def test_checkpoint_and_resume_match_an_uninterrupted_run(tmp_path, precision):
+    """stop_after + checkpoint, then resume: rec_out, energy_trace and
+    res_trace bitwise equal to one uninterrupted run; a checkpoint from a
+    different set-up is refused."""
+    if not os.path.exists(ECSG_MAIN):
+        pytest.skip("ecsg_main absent")
+    import subprocess
+    tmp = str(tmp_path)
+    case = _case(1, 41)
+    args = write_inputs(tmp, case, 41)
+    extra = ["precision=" + precision]
+    full, _ = run_driver(ECSG_MAIN, args, tmp, "full", extra=extra)
+    ck = os.path.join(tmp, "state.ckpt")
+    _, out1 = run_driver(ECSG_MAIN, args, tmp, "part", extra=extra + ["checkpoint=" + ck, "checkpoint_every=7",
+                                                                       "stop_after=17"])
+    assert "Stopped after step 16" in out1 and os.path.exists(ck)
+    resumed, out2 = run_driver(ECSG_MAIN, args, tmp, "res", extra=extra + ["resume=" + ck])
+    assert "Resumed after step 16" in out2
+    for key in ("rec_out", "energy_trace", "res_trace"):
+        assert np.array_equal(full[key][1], resumed[key][1]), key
+    # another precision is another set-up
+    other = "f64" if precision == "f32" else "f32"
+    cmd = [ECSG_MAIN] + args + ["rec_out=" + os.path.join(tmp, "x.rsf"), "precision=" + other, "resume=" + ck]
+    p = subprocess.run(cmd, cwd=tmp, stdout=subprocess.PIPE, stderr=subprocess.PIPE, timeout=300)
+    assert p.returncode != 0 and b"precision" in p.stderr
+
+
+@pytest.mark.parametrize("medium", ["iso", "gen21"])
+def test_save_and_load_state_continue_bit_for_bit(medium):
+    from ecsg_b200 import Simulation
+    from ecsg_b200.workloads import random_case_gen21
+    if medium == "iso":
+        case = _case(1, 30)
+    else:
+        case = random_case_gen21(8, ratio=2, nx2=10, ny2=9, nz=(8, 6), aniso=0.3)
+        n, h = case.grids[0]["n"], case.grids[0]["h"]
+        case.src = {"xyz": (n[0] // 2 * h[0], n[1] // 2 * h[1], 2 * h[2]), "trace": ricker(30, case.dt * 1e-3, 15.0),
+                    "scale": 1000.0, "comp": 0}
+        case.rec = np.array([[(n[0] // 2 + 2) * h[0], n[1] // 2 * h[1], 2 * h[2]]], dtype=np.float32)
+    with Simulation(case, precision="f32", energy=True) as s:
+        whole = s.run(30, energy_every=5)
+    with Simulation(case, precision="f32", energy=True) as s:
+        first = s.run(12, energy_every=5)
+        state = s.save_state()
+    with Simulation(case, precision="f32", energy=True) as s:
+        s.load_state(state, step_index=12)
+        second = s.run(18, energy_every=5)
+    assert np.array_equal(whole["rec"], np.concatenate([first["rec"], second["rec"]], axis=1))
+    assert np.array_equal(whole["energy"][12:], second["energy"], equal_nan=True)

@@ -217,3 +217,43 @@ def test_tma_sweep_equals_scalar_sweep(monkeypatch, ratio, top_bc, nx2, ny2, nz,
         assert np.array_equal(ra["energy"], rb["energy"], equal_nan=True)
     for a, b in zip(fa, fb):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("medium", ["tti", "iso"])
+@pytest.mark.parametrize("ratio,top_bc,nx2,ny2,nz", [(3, 1, 45, 11, (60, 30)), (2, 0, 67, 9, (20, 50)),
+                                                    (2, 1, 33, 16, (49, 24))])
+def test_tma_velocity_sweep_equals_float4_sweep(monkeypatch, ratio, top_bc, nx2, ny2, nz, medium):
+    """The FP32 TMA-staged velocity sweep (vel_tma.cu) against the float4 sweep
+    (stencil_v4.cu, selected by ECSG_VEL_TMA=0): bitwise equal fields after one
+    operator on random fields, and bitwise equal traces, energies and fields
+    after 30 steps (energy copies every 3rd step), on tiles that do not divide
+    the grid in x or y and with several z-chunks."""
+    from ecsg_b200 import SIM_POS, field_shape
+    from ecsg_b200.workloads import random_case
+    if medium == "tti":
+        case = random_case_tti(80 + ratio + top_bc, ratio=ratio, nx2=nx2, ny2=ny2, nz=nz, top_bc=top_bc)
+    else:
+        case = random_case(80 + ratio + top_bc, ratio=ratio, nx2=nx2, ny2=ny2, nz=nz, top_bc=top_bc)
+    case = _with_src_rec(case)
+    ops, outs = [], []
+    for tma in ("0", "1"):
+        monkeypatch.setenv("ECSG_VEL_TMA", tma)
+        rng = np.random.default_rng(nx2 + ny2)
+        with Simulation(case, precision="f32", energy=True) as s:
+            for g in range(2):
+                for k in range(9):
+                    s.set_field(g, k, rng.standard_normal(field_shape(case.grids[g]["n"], SIM_POS[k], 1)))
+            for g in range(2):
+                s.update_vel(g)
+            ops.append([s.field(g, k) for g in range(2) for k in range(3)])
+        with Simulation(case, precision="f32", energy=True) as s:
+            r = s.run(30, energy_every=3, graph=True)
+            outs.append((r, [s.field(g, k) for g in range(2) for k in range(9)], s.status()))
+    for a, b in zip(*ops):
+        assert np.array_equal(a, b)
+    (ra, fa, sa), (rb, fb, sb) = outs
+    assert sa == 0 and sb == 0
+    assert np.array_equal(ra["rec"], rb["rec"])
+    assert np.array_equal(ra["energy"], rb["energy"], equal_nan=True)
+    for a, b in zip(fa, fb):
+        assert np.array_equal(a, b)

@@ -317,7 +317,7 @@ def main():
         kname = "stress21_tma_kernel<%s>" % ("true" if acc else "false") if medium == "tti" else "stress_kernel_v4<ISO5>"
         dom, dom_ms, dom_bytes = kname + " (grid 0)", st_ms, (STRESS_BYTES[medium] + acc) * cells0
     else:
-        dom, dom_ms, dom_bytes = "vel_kernel_v4 (grid 0)", ve_ms, VEL_BYTES * cells0
+        dom, dom_ms, dom_bytes = "vel_tma_kernel (grid 0)", ve_ms, VEL_BYTES * cells0
     achieved = dom_bytes / (dom_ms * 1e-3) / 1e9
     step_ms = run_ms / args.steps
     step_gbs = (BYTES_PER_CELL[medium] + acc) * pts / (step_ms * 1e-3) / 1e9

@@ -35,7 +35,7 @@ sys.path.insert(0, ROOT)
 BYTES_PER_CELL = {"iso": 132, "ortho9": 148, "tti": 196}    # compulsory FP32 traffic per cell-update
 STRESS_BYTES = {"iso": 80, "ortho9": 96, "tti": 144}        # stress kernel: 3v + 6 sigma (rmw) + N_C words
 VEL_BYTES = 52                                              # velocity kernel: 6 sigma + 3 v (rmw) + buoyancy
-EPS_BYTES = 48                                              # 21-Cij energy: 6 strain accumulators (rmw)
+DISP_BYTES = 24                                             # 21-Cij energy: 3 displacement sums (rmw)
 
 
 def measured_peak():
@@ -258,8 +258,8 @@ def main():
     pts = case.points()
     ev = args.energy_every
     sim = ecsg_b200.Simulation(case, precision="f32", energy=ev > 0, device=local)
-    # 21-Cij energy needs the strain accumulators, updated by every stress sweep
-    acc = EPS_BYTES if (medium == "tti" and ev > 0) else 0
+    # 21-Cij energy needs the displacement sums, updated by every stress sweep
+    acc = DISP_BYTES if (medium == "tti" and ev > 0) else 0
 
     def barrier():
         if pg is not None:
@@ -327,7 +327,10 @@ def main():
     tpath = os.path.join(ROOT, "profiles", "traffic.json")
     if os.path.exists(tpath):
         try:
-            per_cell = json.load(open(tpath)).get(dom.split(" ")[0], {}).get("dram_bytes_per_cell")
+            entry = json.load(open(tpath)).get(dom.split(" ")[0], {})
+            # only a capture of the same kernel variant (same algorithmic bytes)
+            same = entry.get("algorithmic_bytes_per_cell") == dom_bytes / cells0
+            per_cell = entry.get("dram_bytes_per_cell") if same else None
             traffic = per_cell * cells0 if per_cell else None
         except Exception:
             traffic = None

@@ -288,7 +288,7 @@ class Simulation:
         return out
 
     def save_state(self):
-        """The run state (fields, sxz warm starts, strain accumulators) as bytes."""
+        """The run state (fields, sxz warm starts, displacement sums) as bytes."""
         buf = np.empty(int(lib().ecsg_state_bytes(self.h)), np.uint8)
         self._ck(lib().ecsg_save_state(self.h, buf.ctypes.data_as(ctypes.c_void_p)))
         return buf

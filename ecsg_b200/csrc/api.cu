@@ -30,12 +30,12 @@ cudaError_t launch_vel_v4(const GridDev<float> &, int, int, int, float *const[3]
 cudaError_t launch_stress_v4(const GridDev<float> &, int, int, int, int, cudaStream_t, int);
 // stress21.cu (21-Cij media)
 template <typename T>
-cudaError_t launch_stress21(const GridDev<T> &, int, int, T *const[6], int, cudaStream_t);
+cudaError_t launch_stress21(const GridDev<T> &, int, int, T *const[3], int, cudaStream_t);
 // stress21_tma.cu (FP32 21-Cij sweeps, TMA-staged)
 size_t s21_maps_bytes();
-bool s21_encode_maps(void *, const GridDev<float> &, float *const[6]);
+bool s21_encode_maps(void *, const GridDev<float> &, float *const[3]);
 cudaError_t s21_set_attributes();
-cudaError_t launch_stress21_tma(const void *, const GridDev<float> &, int, int, float *const[6], int *, int, cudaStream_t, int);
+cudaError_t launch_stress21_tma(const void *, const GridDev<float> &, int, int, float *const[3], int *, int, cudaStream_t, int);
 size_t vel_maps_bytes();
 bool vel_encode_maps(void *, const GridDev<float> &);
 cudaError_t vel_tma_set_attributes();
@@ -55,7 +55,7 @@ template <typename T>
 cudaError_t launch_sxz_solve(const GridDev<T> &, const GridDev<T> &, int, const SxzWork &, int, cudaStream_t);
 // diag.cu
 template <typename T>
-cudaError_t launch_energy(const GridDev<T> &, int, T *const[3], T *const[6], double *, int, double, double, double,
+cudaError_t launch_energy(const GridDev<T> &, int, T *const[3], T *const[3], int, double *, int, double, double, double,
                           double *, const int *, const int *, int, int *, cudaStream_t);
 template <typename T>
 cudaError_t launch_residue(const GridDev<T> &, const GridDev<T> &, int, double, double *, int, double *, cudaStream_t);
@@ -136,16 +136,16 @@ struct ecsg_sim {
     const ecsg_sim *share = nullptr;     // medium owner when this instance shares its medium (ecsg_create_shot)
     bool kset[kMaxGrids] = {};           // FD coefficients given by the caller (ecsg_set_coefficients)
     double kover[kMaxGrids][3] = {};
-    // Per grid, the 9 fields, the stiffness slots and the strain accumulators
+    // Per grid, the 9 fields, the stiffness slots and the displacement sums
     // each live in one allocation (fields of a group at a fixed stride), so
     // that one tensor map can address a whole group.
-    void *fblk[kMaxGrids] = {}, *cblk[kMaxGrids] = {}, *epsblk[kMaxGrids] = {};
+    void *fblk[kMaxGrids] = {}, *cblk[kMaxGrids] = {}, *dispblk[kMaxGrids] = {};
     void *f[kMaxGrids][9] = {};
     void *b[kMaxGrids] = {};
     void *c[kMaxGrids][21] = {};
     int nc = 5;
     void *vc[kMaxGrids][3] = {};
-    void *eps[kMaxGrids][6] = {};   // 21-Cij media with energy: accumulated strains at the stress positions
+    void *disp[kMaxGrids][3] = {};  // 21-Cij media with energy: velocities summed over the stress updates (stress21.cu)
     std::vector<unsigned char> s21maps[kMaxGrids];   // TMA tensor maps of the FP32 21-Cij sweep, per grid
     bool s21_ready = false;
     std::vector<unsigned char> velmaps[kMaxGrids];   // TMA tensor maps of the FP32 velocity sweep, per grid
@@ -366,8 +366,8 @@ static int create_impl(const ecsg_grid_desc *grids, const ecsg_config *cfg, ecsg
             for (int k = 0; k < 3; k++)
                 if ((rc = dmalloc(s, &s->vc[g][k], fb))) return bail(rc);
         if (s->energy && s->medium == ECSG_MEDIUM_GEN21) {
-            if ((rc = dmalloc(s, &s->epsblk[g], 6 * fb))) return bail(rc);
-            for (int k = 0; k < 6; k++) s->eps[g][k] = (char *)s->epsblk[g] + k * fb;
+            if ((rc = dmalloc(s, &s->dispblk[g], 3 * fb))) return bail(rc);
+            for (int k = 0; k < 3; k++) s->disp[g][k] = (char *)s->dispblk[g] + k * fb;
         }
     }
     s->red_blocks = 4 * s->sms;
@@ -429,7 +429,7 @@ int ecsg_destroy(ecsg_sim *s)
         if (!s->share) cudaFree(s->b[g]);
         cudaFree(s->cblk[g]);
         for (int k = 0; k < 3; k++) cudaFree(s->vc[g][k]);
-        cudaFree(s->epsblk[g]);
+        cudaFree(s->dispblk[g]);
         cudaFree(s->lblk[g]); cudaFree(s->gbblk[g]); cudaFree(s->gcblk[g]);
         cudaFree(s->adj_lx[g]); cudaFree(s->adj_y[g]); cudaFree(s->adj_Y0[g]); cudaFree(s->adj_Y1[g]);
         Iface &I = s->itf[g];
@@ -779,10 +779,10 @@ static int stress_prepare(ecsg_sim *s)
     }
     if (!use_s21_tma(s) || s->s21_ready) return ECSG_OK;
     for (int g = 0; g < s->ng; g++) {
-        float *eps[6];
-        for (int k = 0; k < 6; k++) eps[k] = (float *)s->eps[g][k];
+        float *disp[3];
+        for (int k = 0; k < 3; k++) disp[k] = (float *)s->disp[g][k];
         s->s21maps[g].assign(s21_maps_bytes(), 0);
-        if (!s21_encode_maps(s->s21maps[g].data(), dev<float>(s, g), eps))
+        if (!s21_encode_maps(s->s21maps[g].data(), dev<float>(s, g), disp))
             return fail(s, ECSG_ERR_CUDA, "grid %d: TMA tensor maps of the 21-Cij sweep could not be encoded", g);
     }
     CK(s21_set_attributes());
@@ -802,17 +802,17 @@ static int stress_op(ecsg_sim *s, int g, int top = -1, int bottom = -1)
         return ECSG_OK;
     }
     if (med == MED_GEN21) {
-        T *eps[6];
-        for (int k = 0; k < 6; k++) eps[k] = (T *)s->eps[g][k];
+        T *disp[3];
+        for (int k = 0; k < 3; k++) disp[k] = (T *)s->disp[g][k];
         if constexpr (std::is_same<T, float>::value) {
             if (use_s21_tma(s)) {
                 if (int rc = stress_prepare(s)) return rc;
-                CK(launch_stress21_tma(s->s21maps[g].data(), dev<float>(s, g), tp, s->top_bc, eps, s->ints, s->sms, s->st,
+                CK(launch_stress21_tma(s->s21maps[g].data(), dev<float>(s, g), tp, s->top_bc, disp, s->ints, s->sms, s->st,
                                        s->ztune[g][1]));
                 return ECSG_OK;
             }
         }
-        CK(launch_stress21<T>(dev<T>(s, g), tp, s->top_bc, eps, s->sms, s->st));
+        CK(launch_stress21<T>(dev<T>(s, g), tp, s->top_bc, disp, s->sms, s->st));
         return ECSG_OK;
     }
     if constexpr (std::is_same<T, float>::value) {
@@ -1023,9 +1023,10 @@ static int energy_op(ecsg_sim *s, double *out, const int *step, const int *step0
 {
     for (int g = 0; g < s->ng; g++) {
         T *vc[3] = {(T *)s->vc[g][0], (T *)s->vc[g][1], (T *)s->vc[g][2]};
-        T *eps[6];
-        for (int k = 0; k < 6; k++) eps[k] = (T *)s->eps[g][k];
-        CK(launch_energy<T>(dev<T>(s, g), med_kind(s), vc, eps, s->partial,
+        T *disp[3];
+        for (int k = 0; k < 3; k++) disp[k] = (T *)s->disp[g][k];
+        const int flag = (top_of(s, g, -1) && s->top_bc) ? 1 : 0;
+        CK(launch_energy<T>(dev<T>(s, g), med_kind(s), vc, disp, flag, s->partial,
                             s->red_blocks, s->h[g][0], s->h[g][1], s->h[g][2], out, step, step0, g == 0, s->ints, s->st));
     }
     return ECSG_OK;
@@ -1735,13 +1736,13 @@ static int load_state(ecsg_sim *s, const char *src)
     return ECSG_OK;
 }
 
-// The whole run state: save_state's part, then the strain accumulators of the
+// The whole run state: save_state's part, then the displacement sums of the
 // grids that keep them.  buf may be device or host memory.
 static size_t run_state_bytes(const ecsg_sim *s)
 {
     size_t b = state_bytes(s);
     for (int g = 0; g < s->ng; g++)
-        if (s->epsblk[g]) b += 6 * (size_t)s->geo[g].size() * s->tsize;
+        if (s->dispblk[g]) b += 3 * (size_t)s->geo[g].size() * s->tsize;
     return b;
 }
 
@@ -1750,9 +1751,9 @@ static int move_run_state(ecsg_sim *s, char *buf, bool save)
     if (int rc = save ? save_state(s, buf) : load_state(s, buf)) return rc;
     char *p = buf + state_bytes(s);
     for (int g = 0; g < s->ng; g++)
-        if (s->epsblk[g]) {
-            const size_t b = 6 * (size_t)s->geo[g].size() * s->tsize;
-            CK(cudaMemcpyAsync(save ? p : s->epsblk[g], save ? s->epsblk[g] : p, b, cudaMemcpyDefault, s->st));
+        if (s->dispblk[g]) {
+            const size_t b = 3 * (size_t)s->geo[g].size() * s->tsize;
+            CK(cudaMemcpyAsync(save ? p : s->dispblk[g], save ? s->dispblk[g] : p, b, cudaMemcpyDefault, s->st));
             p += b;
         }
     return ECSG_OK;
@@ -2082,7 +2083,7 @@ int ecsg_autotune(ecsg_sim *s, int reps)
     if (reps < 1) reps = 3;
     int rc;
     if ((rc = stress_prepare(s))) return rc;
-    // the trial sweeps change the fields (and strain accumulators): keep and restore them
+    // the trial sweeps change the fields (and displacement sums): keep and restore them
     char *save = nullptr;
     CK(cudaMalloc(&save, run_state_bytes(s) + 1));
     if ((rc = move_run_state(s, save, true))) { cudaFree(save); return rc; }

@@ -5,6 +5,7 @@
 // fixed tree and writes one partial per term; a single-CTA finalize sums the
 // partials in CTA order.  Accumulation is in double precision.
 #include "ecsg_device.cuh"
+#include "gen21_device.cuh"
 
 namespace ecsg {
 
@@ -35,14 +36,13 @@ __device__ __forceinline__ void block_sums(double (&v)[N], double *partial, int 
 // the reference's operation order (InvertParameters, init_del_par_field.cpp:224-283;
 // ReshapeField, field.cpp:465-472).  12 term partials per CTA.
 // ---------------------------------------------------------------------------
-template <typename T>
-struct Eps6 {
-    const T *e[6];
-};
-
+// 21-Cij media: the potential energy 1/2 (eps, sigma) takes the accumulated
+// strains as the strain differences of the displacement sums U (stress21.cu),
+// evaluated by the stress update's own strain functions on a copy of the grid
+// whose velocities are U (GU), e3 condensed on a free surface (flag).
 template <typename T>
 __global__ void __launch_bounds__(RED_THREADS) energy_kernel(GridDev<T> G, int medium, const T *vc0, const T *vc1,
-                                                            const T *vc2, Eps6<T> eps, double *partial)
+                                                            const T *vc2, GridDev<T> GU, int flag, double *partial)
 {
     const Geo &g = G.g;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
@@ -74,16 +74,18 @@ __global__ void __launch_bounds__(RED_THREADS) energy_kernel(GridDev<T> G, int m
             acc[2] += my * (1.0 / rb) * (double)G.f[VZ][p] * (double)vc2[p];
         }
         if (medium == MED_GEN21) {
-            // 21-Cij media: potential energy (eps, sigma) from the accumulated
-            // strains, terms 3..8 in stress order, trapezoid weights per position
+            // terms 3..8 in stress order, trapezoid weights per position
             if (xs) {
                 const double w = mz * my;
-#pragma unroll
-                for (int k = 0; k < 3; k++) acc[3 + k] += w * (double)eps.e[k][p] * (double)G.f[SXX + k][p];
+                const T e1 = e1_at(GU, p), e2 = e2_at(GU, p);
+                const T e3 = e3_used(GU, Ext{nx, ny, nz}, flag && z == 0, x, y, z, p, e1, e2);
+                acc[3] += w * (double)e1 * (double)G.f[SXX][p];
+                acc[4] += w * (double)e2 * (double)G.f[SYY][p];
+                acc[5] += w * (double)e3 * (double)G.f[SZZ][p];
             }
-            if (xs && ys && zs) acc[6] += (double)eps.e[3][p] * (double)G.f[SYZ][p];
-            if (zs) acc[7] += my * mx * (double)eps.e[4][p] * (double)G.f[SXZ][p];
-            if (ys) acc[8] += mz * mx * (double)eps.e[5][p] * (double)G.f[SXY][p];
+            if (xs && ys && zs) acc[6] += (double)e4_at(GU, p) * (double)G.f[SYZ][p];
+            if (zs) acc[7] += my * mx * (double)e5_at(GU, p) * (double)G.f[SXZ][p];
+            if (ys) acc[8] += mz * mx * (double)e6_at(GU, p) * (double)G.f[SXY][p];
             continue;
         }
         if (xs) {         // normal stresses at (1,0,0)
@@ -338,14 +340,14 @@ __global__ void iso_medium_kernel(Geo g, const double *s11, const double *s13, d
 // Host launchers
 // ---------------------------------------------------------------------------
 template <typename T>
-cudaError_t launch_energy(const GridDev<T> &G, int medium, T *const vc[3], T *const eps[6], double *partial, int nblocks,
-                          double h0, double h1, double h2, double *out, const int *step, const int *step0, int first,
-                          int *status, cudaStream_t st)
+cudaError_t launch_energy(const GridDev<T> &G, int medium, T *const vc[3], T *const disp[3], int flag, double *partial,
+                          int nblocks, double h0, double h1, double h2, double *out, const int *step, const int *step0,
+                          int first, int *status, cudaStream_t st)
 {
-    Eps6<T> E;
-    for (int k = 0; k < 6; k++) E.e[k] = eps ? eps[k] : nullptr;
-    if (medium == MED_GEN21 && !E.e[0]) return cudaErrorInvalidValue;
-    energy_kernel<T><<<nblocks, RED_THREADS, 0, st>>>(G, medium, vc[0], vc[1], vc[2], E, partial);
+    GridDev<T> GU = G;
+    for (int k = 0; k < 3; k++) GU.f[VX + k] = disp ? disp[k] : nullptr;
+    if (medium == MED_GEN21 && !GU.f[VX]) return cudaErrorInvalidValue;
+    energy_kernel<T><<<nblocks, RED_THREADS, 0, st>>>(G, medium, vc[0], vc[1], vc[2], GU, flag, partial);
     energy_finalize_kernel<<<1, 32, 0, st>>>(partial, nblocks, h0, h1, h2, out, step, step0, first, status,
                                              medium == MED_GEN21);
     return cudaGetLastError();
@@ -419,7 +421,7 @@ cudaError_t launch_iso_medium(const Geo &g, const double *s11, const double *s13
 }
 
 #define INST(T)                                                                                               \
-    template cudaError_t launch_energy<T>(const GridDev<T> &, int, T *const[3], T *const[6], double *, int,      \
+    template cudaError_t launch_energy<T>(const GridDev<T> &, int, T *const[3], T *const[3], int, double *, int, \
                                           double, double, double, double *, const int *, const int *, int, int *, \
                                           cudaStream_t);                                                       \
     template cudaError_t launch_residue<T>(const GridDev<T> &, const GridDev<T> &, int, double, double *, int,   \

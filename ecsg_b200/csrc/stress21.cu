@@ -26,8 +26,14 @@
 // velocity and stiffness word comes from HBM once per sweep; the halo points'
 // recomputation reads L1/L2.
 //
-// Optional strain accumulators eps[6] (same positions as the stresses) make
-// the energy computable without inverting the stiffness operator.
+// Optional displacement sums U[3] (the velocities summed over the stress
+// updates, at the velocity positions) make the energy computable without
+// inverting the stiffness operator: the strains are linear in the
+// velocities, so the accumulated strain at every stress position is the
+// strain difference of U (gen21_device.cuh), three fields where strain
+// accumulators would take six.  Each update adds the velocities it reads on
+// U's support: x in [0, nx], y in [0, ny], z in [0, nz] plus the faces
+// x = -1, y = -1 and z = -1 that the strain differences reach into.
 #include "gen21_device.cuh"
 
 namespace ecsg {
@@ -41,9 +47,29 @@ struct S21 {
 };
 enum { Q_E4 = 0, Q_Q45, Q_Q46, Q_E5, Q_Q56, Q_E6, Q_P4, Q_P5, Q_P6 };
 
+// U += v on the support of the displacement sums owned by the output point
+// (x, y) of plane z: the point itself (x <= nx, y <= ny), its x = -1 / y = -1
+// face neighbours when x / y is 0, and the z = -1 point below when lower.
+template <typename T>
+__device__ __forceinline__ void add_velocities(const GridDev<T> &G, T *u0, T *u1, T *u2, int x, int y, int z, bool lower)
+{
+    const Geo &g = G.g;
+    if (x > g.nx || y > g.ny) return;
+    T *const u[3] = {u0, u1, u2};
+    const int p = g.idx(x, y, z);
+    const int sy = g.px, sz = g.px * g.py;
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        const T *v = G.f[VX + c];
+        u[c][p] = add_(u[c][p], v[p]);
+        if (x == 0) u[c][p - 1] = add_(u[c][p - 1], v[p - 1]);
+        if (y == 0) u[c][p - sy] = add_(u[c][p - sy], v[p - sy]);
+        if (lower) u[c][p - sz] = add_(u[c][p - sz], v[p - sz]);
+    }
+}
+
 template <typename T, bool ACC>
-__global__ void __launch_bounds__(S21<T>::TX *S21<T>::TY) stress21_kernel(GridDev<T> G, int flag, int zchunk, T *eps0, T *eps1,
-                                                                         T *eps2, T *eps3, T *eps4, T *eps5)
+__global__ void __launch_bounds__(S21<T>::TX *S21<T>::TY) stress21_kernel(GridDev<T> G, int flag, int zchunk, T *u0, T *u1, T *u2)
 {
     using C = S21<T>;
     __shared__ T ring[2][C::NQ][C::HP];
@@ -138,11 +164,6 @@ __global__ void __launch_bounds__(S21<T>::TX *S21<T>::TY) stress21_kernel(GridDe
                 sxx[pp] = add_(sxx[pp], d[0]);
                 syy[pp] = add_(syy[pp], d[1]);
                 if (!surf) szz[pp] = add_(szz[pp], d[2]);
-                if (ACC) {
-                    eps0[pp] = add_(eps0[pp], e1);
-                    eps1[pp] = add_(eps1[pp], e2);
-                    eps2[pp] = add_(eps2[pp], e3);
-                }
             }
             if (E.l6(ox, oy, p)) {
                 const int pp = g.idx(ox, oy, p);
@@ -163,9 +184,9 @@ __global__ void __launch_bounds__(S21<T>::TX *S21<T>::TY) stress21_kernel(GridDe
                 const T e6 = R(s, Q_E6, hx, hy);
                 const T dd = add_(add_(fma_(c[20][pp], e6, t46), t56), t6);
                 sxy[pp] = add_(sxy[pp], dd);
-                if (ACC) eps5[pp] = add_(eps5[pp], e6);
             }
         }
+        if (ACC && p >= z0 && p <= z1) add_velocities(G, u0, u1, u2, ox, oy, p, z0 == 0 && p == 0);
         const int pm = p - 1;
         if (pm >= z0 && pm <= z1) {
             if (E.l4(ox, oy, pm)) {
@@ -189,7 +210,6 @@ __global__ void __launch_bounds__(S21<T>::TX *S21<T>::TY) stress21_kernel(GridDe
                 const T nv = add_(syz[pp], dd);
                 syz[pp] = nv;
                 if (flag && pm == 0) syz[pp - sz] = -nv;
-                if (ACC) eps3[pp] = add_(eps3[pp], e4);
             }
             if (E.l5(ox, oy, pm)) {
                 const int pp = g.idx(ox, oy, pm);
@@ -212,7 +232,6 @@ __global__ void __launch_bounds__(S21<T>::TX *S21<T>::TY) stress21_kernel(GridDe
                 const T nv = add_(sxz[pp], dd);
                 sxz[pp] = nv;
                 if (flag && pm == 0 && ox >= 1 && ox <= nx - 1 && oy >= 1 && oy <= ny - 1) sxz[pp - sz] = -nv;
-                if (ACC) eps4[pp] = add_(eps4[pp], e5);
             }
         }
         __syncthreads();
@@ -220,7 +239,7 @@ __global__ void __launch_bounds__(S21<T>::TX *S21<T>::TY) stress21_kernel(GridDe
 }
 
 template <typename T>
-cudaError_t launch_stress21(const GridDev<T> &G, int top, int top_bc, T *const eps[6], int sms, cudaStream_t st)
+cudaError_t launch_stress21(const GridDev<T> &G, int top, int top_bc, T *const disp[3], int sms, cudaStream_t st)
 {
     using C = S21<T>;
     const Geo &g = G.g;
@@ -232,14 +251,14 @@ cudaError_t launch_stress21(const GridDev<T> &G, int top, int top_bc, T *const e
     if (nchunk > (g.nz + 1) / 8 + 1) nchunk = (g.nz + 1) / 8 + 1;   // keep >= ~8 planes per CTA (2 recomputed)
     const int zc = (g.nz + 1 + nchunk - 1) / nchunk;
     dim3 blk(C::TX, C::TY), grd(bx, by, (g.nz + 1 + zc - 1) / zc);
-    if (eps && eps[0])
-        stress21_kernel<T, true><<<grd, blk, 0, st>>>(G, flag, zc, eps[0], eps[1], eps[2], eps[3], eps[4], eps[5]);
+    if (disp && disp[0])
+        stress21_kernel<T, true><<<grd, blk, 0, st>>>(G, flag, zc, disp[0], disp[1], disp[2]);
     else
-        stress21_kernel<T, false><<<grd, blk, 0, st>>>(G, flag, zc, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
+        stress21_kernel<T, false><<<grd, blk, 0, st>>>(G, flag, zc, nullptr, nullptr, nullptr);
     return cudaGetLastError();
 }
 
-template cudaError_t launch_stress21<float>(const GridDev<float> &, int, int, float *const[6], int, cudaStream_t);
-template cudaError_t launch_stress21<double>(const GridDev<double> &, int, int, double *const[6], int, cudaStream_t);
+template cudaError_t launch_stress21<float>(const GridDev<float> &, int, int, float *const[3], int, cudaStream_t);
+template cudaError_t launch_stress21<double>(const GridDev<double> &, int, int, double *const[3], int, cudaStream_t);
 
 } // namespace ecsg

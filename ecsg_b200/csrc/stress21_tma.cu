@@ -10,11 +10,11 @@
 //     as 36 x 9 boxes, each with the one-sided halo its products need: slots
 //     c6..c14 at x-1 and y+1 (normal products), c16, c17 at x-1 and y-1 (L4
 //     links), c19 at x+1 and y+1 (the L5 link),
-//   * the other 9 coefficient slots, the 6 stresses and (energy runs) the 6
-//     strain accumulators as 32 x 8 boxes,
+//   * the other 9 coefficient slots, the 6 stresses and (energy runs) the 3
+//     displacement sums (stress21.cu) as 32 x 8 boxes,
 // into shared-memory rings with cp.async.bulk.tensor (no multicast),
 // completion tracked by mbarriers.  Each group of fields (velocities, the 12
-// haloed slots, the 9 other slots, stresses, strains) is one allocation with
+// haloed slots, the 9 other slots, stresses, displacement sums) is one allocation with
 // its fields at a fixed stride, so one 4-D tensor map (x, y, z, field) moves
 // a whole group or sub-group: 7 copies per plane instead of 36 (small boxes
 // from many descriptors kept the copy engine, not HBM, the limit).  Eight consumer warps compute
@@ -49,10 +49,14 @@ constexpr int NCA = 9, NCB = 2;               // c6..c14 | c16, c17 | c19
 __host__ __device__ constexpr int up128(int b) { return (b + 127) / 128 * 128; }
 constexpr int P_CHA = 0, P_CHB = up128(NCA * CBOX), P_CHC = up128(P_CHB + NCB * CBOX);
 constexpr int P_CI = up128(P_CHC + CBOX), P_SG = P_CI + NCI * IBOX, P_EP = P_SG + 6 * IBOX;
-constexpr int PSLOT = P_EP + 6 * IBOX;        // 37376, a multiple of 128
+// low-face boxes of the displacement sums (tiles at x0 = 0 / y0 = 0): x = -4..-1
+// beside the tile's 8 rows, and row y = -1 under its 32 columns
+constexpr int XFW = 4, XFBOX = XFW * TY * 4, YFBOX = TX * 4;   // 128 bytes each per field
+constexpr int P_EX = P_EP + 3 * IBOX, P_EY = P_EX + 3 * XFBOX;
+constexpr int PSLOT = P_EY + 3 * YFBOX;       // 35072, a multiple of 128
 constexpr int VSLOT = (3 * HBOX + 127) / 128 * 128;   // 4864
 static_assert(P_CHB % 128 == 0 && P_CHC % 128 == 0 && P_CI % 128 == 0 && P_SG % 128 == 0 && P_EP % 128 == 0 &&
-                  PSLOT % 128 == 0, "128-byte aligned boxes");
+                  P_EX % 128 == 0 && P_EY % 128 == 0 && PSLOT % 128 == 0, "128-byte aligned boxes");
 constexpr int OFF_V = NSP * PSLOT;
 constexpr int OFF_IM = OFF_V + NSV * VSLOT;
 constexpr int OFF_BAR = OFF_IM + 2 * NQ * HP * 4;
@@ -71,15 +75,17 @@ struct S21Maps {
     CUtensorMap chc;  // c19: box x .. x+35, y .. y+8
     CUtensorMap ci;   // c0..c5, c15, c18, c20: interior boxes
     CUtensorMap sg;   // sxx syy szz syz sxz sxy: interior boxes
-    CUtensorMap ep;   // strain accumulators: interior boxes
+    CUtensorMap ep;   // displacement sums: interior boxes
+    CUtensorMap epx;  // displacement sums: x = -4..-1 face boxes (tiles at x0 = 0)
+    CUtensorMap epy;  // displacement sums: y = -1 face rows (tiles at y0 = 0)
 };
 
 __device__ __forceinline__ void consumer_sync() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
 
 template <bool ACC>
 __global__ void __launch_bounds__(s21t::NTHREADS, 1)
-    stress21_tma_kernel(const __grid_constant__ S21Maps maps, GridDev<float> G, int flag, int zchunk, float *eps0,
-                        float *eps1, float *eps2, float *eps3, float *eps4, float *eps5, int *status)
+    stress21_tma_kernel(const __grid_constant__ S21Maps maps, GridDev<float> G, int flag, int zchunk, float *u0,
+                        float *u1, float *u2, int *status)
 {
     using namespace s21t;
     extern __shared__ __align__(128) unsigned char sm[];
@@ -129,8 +135,13 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
                 if (i >= NSP && !mbar_wait(emptyP(s), ((i / NSP) - 1) & 1)) return false;
                 const int q = qstart + i;
                 const bool inner = q >= z0 && q <= z1;
+                // displacement sums: interior box on inner planes and on plane -1,
+                // face boxes on the inner planes of low-face tiles
+                const bool uin = ACC && (inner || q == -1);
+                const bool ux = ACC && inner && x0 == 0, uy = ACC && inner && y0 == 0;
                 const unsigned dst = smem_u32(sm + s * PSLOT);
-                mbar_expect_tx(fullP(s), NCH * CBOX + (inner ? (NCI + 6 + (ACC ? 6 : 0)) * IBOX : 0));
+                mbar_expect_tx(fullP(s), NCH * CBOX + (inner ? (NCI + 6) * IBOX : 0) + (uin ? 3 * IBOX : 0) +
+                                             (ux ? 3 * XFBOX : 0) + (uy ? 3 * YFBOX : 0));
                 const int zc = g.R + q;
                 tma_load4(dst + P_CHA, &maps.cha, hx0, iy0, zc, fullP(s));
                 tma_load4(dst + P_CHB, &maps.chb, hx0, hy0, zc, fullP(s));
@@ -138,8 +149,10 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
                 if (inner) {
                     tma_load4(dst + P_CI, &maps.ci, ix0, iy0, zc, fullP(s));
                     tma_load4(dst + P_SG, &maps.sg, ix0, iy0, zc, fullP(s));
-                    if (ACC) tma_load4(dst + P_EP, &maps.ep, ix0, iy0, zc, fullP(s));
                 }
+                if (uin) tma_load4(dst + P_EP, &maps.ep, ix0, iy0, zc, fullP(s));
+                if (ux) tma_load4(dst + P_EX, &maps.epx, XOFF - XFW, iy0, zc, fullP(s));
+                if (uy) tma_load4(dst + P_EY, &maps.epy, ix0, g.R - 1, zc, fullP(s));
                 return true;
             };
             bool ok = true;
@@ -167,7 +180,7 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
         const float k0 = G.k[0], k1 = G.k[1], k2 = G.k[2];
         float *sxx = G.f[SXX], *syy = G.f[SYY], *szz = G.f[SZZ], *syz = G.f[SYZ], *sxz = G.f[SXZ], *sxy = G.f[SXY];
         // carries from plane pm = p-1 for the syz / sxz outputs
-        float c15p = 0.f, c16p = 0.f, c17p = 0.f, c18p = 0.f, c19p = 0.f, s3p = 0.f, s4p = 0.f, ep3p = 0.f, ep4p = 0.f;
+        float c15p = 0.f, c16p = 0.f, c17p = 0.f, c18p = 0.f, c19p = 0.f, s3p = 0.f, s4p = 0.f;
         // the halo job of this warp: kind (0 L4, 1 L5, 2 L6, 3 N) and point
         int hk, hxp, hyp;
         {
@@ -338,11 +351,6 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
                         sxx[pp] = add_(SG[0 * IS + ib], d[0]);
                         syy[pp] = add_(SG[1 * IS + ib], d[1]);
                         if (FAST || !surf) szz[pp] = add_(SG[2 * IS + ib], d[2]);
-                        if (ACC) {
-                            eps0[pp] = add_(EP[0 * IS + ib], e1);
-                            eps1[pp] = add_(EP[1 * IS + ib], e2);
-                            eps2[pp] = add_(EP[2 * IS + ib], e3);
-                        }
                     }
                     if (FAST || E.l6(ox, oy, p)) {
                         float v[2][2];
@@ -359,7 +367,6 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
                         const float e6 = RR(1, 5, hx, hy);
                         const float dd = add_(add_(fma_(CI[8 * IS + ib], e6, t46), t56), t6);
                         sxy[pp] = add_(SG[5 * IS + ib], dd);
-                        if (ACC) eps5[pp] = add_(EP[5 * IS + ib], e6);
                     }
                 }
                 if (outer_pm) {
@@ -381,7 +388,6 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
                         const float nv = add_(s3p, dd);
                         syz[pp] = nv;
                         if (flag && pm == 0) syz[pp - sz] = -nv;
-                        if (ACC) eps3[pp] = add_(ep3p, e4);
                     }
                     if (FAST || E.l5(ox, oy, pm)) {
                         float v[2][2];
@@ -400,7 +406,6 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
                         const float nv = add_(s4p, dd);
                         sxz[pp] = nv;
                         if (flag && pm == 0 && (FAST || (ox >= 1 && ox <= nx - 1 && oy >= 1 && oy <= ny - 1))) sxz[pp - sz] = -nv;
-                        if (ACC) eps4[pp] = add_(ep4p, e5);
                     }
                 }
             };
@@ -411,11 +416,33 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
             else
                 body(std::false_type{});
 
+            // displacement sums: U += v at this thread's point (x <= nx, y <= ny)
+            // of an inner plane, the x = -1 / y = -1 face points beside it, and
+            // the z = -1 point below it on the first plane of the grid
+            if (ACC && (inner || p == -1) && ox <= nx && oy <= ny) {
+                const int pp = pbase + p * sz;
+                u0[pp] = add_(EP[0 * IS + ib], Vp[0 * HS + vb]);
+                u1[pp] = add_(EP[1 * IS + ib], Vp[1 * HS + vb]);
+                u2[pp] = add_(EP[2 * IS + ib], Vp[2 * HS + vb]);
+                if (inner && x0 == 0 && tx == 0) {
+                    const float *EX = (const float *)(PS + P_EX);
+                    constexpr int XS = XFBOX / 4;
+                    u0[pp - 1] = add_(EX[0 * XS + ty * XFW + XFW - 1], Vp[0 * HS + vb - 1]);
+                    u1[pp - 1] = add_(EX[1 * XS + ty * XFW + XFW - 1], Vp[1 * HS + vb - 1]);
+                    u2[pp - 1] = add_(EX[2 * XS + ty * XFW + XFW - 1], Vp[2 * HS + vb - 1]);
+                }
+                if (inner && y0 == 0 && ty == 0) {
+                    const float *EY = (const float *)(PS + P_EY);
+                    constexpr int YS = YFBOX / 4;
+                    u0[pp - g.px] = add_(EY[0 * YS + tx], Vp[0 * HS + vb - BW]);
+                    u1[pp - g.px] = add_(EY[1 * YS + tx], Vp[1 * HS + vb - BW]);
+                    u2[pp - g.px] = add_(EY[2 * YS + tx], Vp[2 * HS + vb - BW]);
+                }
+            }
             if (inner) {
                 c15p = CI[6 * IS + ib]; c18p = CI[7 * IS + ib];
                 c16p = cho(9); c17p = cho(10); c19p = cho(11);
                 s3p = SG[3 * IS + ib]; s4p = SG[4 * IS + ib];
-                if (ACC) { ep3p = EP[3 * IS + ib]; ep4p = EP[4 * IS + ib]; }
             }
             consumer_sync();
             if (tid == 0) {
@@ -455,7 +482,7 @@ size_t s21_maps_bytes() { return sizeof(S21Maps); }
 // Fills the maps of one grid; false if the driver entry point is missing, a
 // group is not laid out at a fixed stride, or an address / pitch is not
 // encodable.
-bool s21_encode_maps(void *out, const GridDev<float> &G, float *const eps[6])
+bool s21_encode_maps(void *out, const GridDev<float> &G, float *const disp[3])
 {
     using namespace s21t;
     S21Maps M;
@@ -469,8 +496,9 @@ bool s21_encode_maps(void *out, const GridDev<float> &G, float *const eps[6])
     ok = ok && encode(&M.v, g, G.f[0], 3, BW, BH) && encode(&M.cha, g, G.c[ch_slot(0)], NCA, CW, CHH) &&
          encode(&M.chb, g, G.c[ch_slot(NCA)], NCB, CW, CHH) && encode(&M.chc, g, G.c[ch_slot(NCA + NCB)], 1, CW, CHH) &&
          encode(&M.ci, g, G.c[ci_slot(0)], NCI, TX, TY) && encode(&M.sg, g, G.f[SXX], 6, TX, TY);
-    if (ok && eps && eps[0])
-        ok = strided(g, 6, [&](int k) { return (const float *)eps[k]; }) && encode(&M.ep, g, eps[0], 6, TX, TY);
+    if (ok && disp && disp[0])
+        ok = strided(g, 3, [&](int k) { return (const float *)disp[k]; }) && encode(&M.ep, g, disp[0], 3, TX, TY) &&
+             encode(&M.epx, g, disp[0], 3, XFW, TY) && encode(&M.epy, g, disp[0], 3, TX, 1);
     if (ok) memcpy(out, &M, sizeof M);
     return ok;
 }
@@ -484,7 +512,7 @@ cudaError_t s21_set_attributes()
     return e;
 }
 
-cudaError_t launch_stress21_tma(const void *maps, const GridDev<float> &G, int top, int top_bc, float *const eps[6],
+cudaError_t launch_stress21_tma(const void *maps, const GridDev<float> &G, int top, int top_bc, float *const disp[3],
                                 int *status, int sms, cudaStream_t st, int nchunk_req)
 {
     using namespace s21t;
@@ -501,10 +529,10 @@ cudaError_t launch_stress21_tma(const void *maps, const GridDev<float> &G, int t
     const int zc = (g.nz + 1 + nchunk - 1) / nchunk;
     dim3 grd(bx, by, (g.nz + 1 + zc - 1) / zc);
     const S21Maps &M = *(const S21Maps *)maps;
-    if (eps && eps[0]) {
-        stress21_tma_kernel<true><<<grd, NTHREADS, SMEM, st>>>(M, G, flag, zc, eps[0], eps[1], eps[2], eps[3], eps[4], eps[5], status);
+    if (disp && disp[0]) {
+        stress21_tma_kernel<true><<<grd, NTHREADS, SMEM, st>>>(M, G, flag, zc, disp[0], disp[1], disp[2], status);
     } else {
-        stress21_tma_kernel<false><<<grd, NTHREADS, SMEM, st>>>(M, G, flag, zc, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, status);
+        stress21_tma_kernel<false><<<grd, NTHREADS, SMEM, st>>>(M, G, flag, zc, nullptr, nullptr, nullptr, status);
     }
     return cudaGetLastError();
 }

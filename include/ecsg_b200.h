@@ -112,8 +112,9 @@ int ecsg_set_medium_ortho9(ecsg_sim *sim, int g, const double *buoy, const doubl
  * = C55 C56 at the sxz position (0,0,1); 20 = C66 at the sxy position (0,1,0).
  * With the 12 off-block slots zero this is the orthorhombic update with
  * C44 = c44/2 etc. of ecsg_set_medium_ortho9.  With cfg.energy the stress
- * update also accumulates strains so that ecsg_energy can return
- * 1/2 (rho v, v') + 1/2 (eps, sigma). */
+ * update also sums the velocities it reads (three displacement sums U, the
+ * strains being linear in the velocities) so that ecsg_energy can return
+ * 1/2 (rho v, v') + 1/2 (eps, sigma) with eps the strain differences of U. */
 int ecsg_set_medium_cij21(ecsg_sim *sim, int g, const double *buoy, const double *const c[21]);
 /* Tilted transversely isotropic medium built on the device into the 21-Cij
  * slots (no counterpart in the reference).  Node-layout float arrays (R = 0,
@@ -186,7 +187,7 @@ int ecsg_run(ecsg_sim *sim, int n0, int nsteps, float *traces, double *energy, i
 
 /* Run state for checkpoint / resume (no reference counterpart): the fields of
  * every grid in the library's own layout and precision, the sxz warm starts
- * and, when the simulation keeps them, the strain accumulators of 21-Cij
+ * and, when the simulation keeps them, the displacement sums of 21-Cij
  * media, as one opaque buffer of ecsg_state_bytes(sim) bytes (host or device
  * memory).  Loading it into a simulation created with the same grids,
  * configuration and medium continues the run bit for bit: pass the next step

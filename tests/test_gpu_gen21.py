@@ -63,7 +63,7 @@ def test_stress21_and_vz_f64(ratio, top_bc, nz):
             o.update_stress(g)
             s.update_stress(g)
         assert _err(o, s) == 0.0
-        # a second update adds onto the strain accumulators of the first
+        # a second update adds onto the displacement sums of the first
         _randomize(o, s, rng, "f64")
         for g in range(2):
             o.update_stress(g)
@@ -191,7 +191,7 @@ def test_tma_sweep_equals_scalar_sweep(monkeypatch, ratio, top_bc, nx2, ny2, nz,
     (stress21.cu, selected by ECSG_SCALAR_STENCILS=1): bitwise equal fields,
     traces and energies, on ragged tiles (x not a multiple of 32, y not of 8),
     several z-chunks per column, with and without the free surface and the
-    strain accumulators."""
+    displacement sums."""
     case = _with_src_rec(random_case_tti(70 + ratio + top_bc, ratio=ratio, nx2=nx2, ny2=ny2, nz=nz, top_bc=top_bc))
     from ecsg_b200 import SIM_POS, field_shape
     outs, ops = [], []
@@ -257,3 +257,4 @@ def test_tma_velocity_sweep_equals_float4_sweep(monkeypatch, ratio, top_bc, nx2,
     assert np.array_equal(ra["energy"], rb["energy"], equal_nan=True)
     for a, b in zip(fa, fb):
         assert np.array_equal(a, b)
+

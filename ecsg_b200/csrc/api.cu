@@ -151,6 +151,13 @@ struct ecsg_sim {
     std::vector<unsigned char> velmaps[kMaxGrids];   // TMA tensor maps of the FP32 velocity sweep, per grid
     bool vel_ready = false;
     bool vel_tma = true;             // FP32 velocity sweep: TMA-staged (false: the float4 sweep)
+    // Side streams of the coarse grids' sweeps (multi-grid runs): the grids'
+    // velocity sweeps are independent of each other, and so are their stress
+    // sweeps, so the coarse grids' sweeps run beside the fine grid's and fill
+    // the SMs its last wave leaves idle.
+    bool side_grids = true;
+    cudaStream_t side[kMaxGrids] = {};
+    cudaEvent_t fork_ev = nullptr, join_ev[kMaxGrids] = {};
     // adjoint state (allocated on first use): adjoint fields, gradients, work boxes
     bool adj = false;
     void *lblk[kMaxGrids] = {}, *gbblk[kMaxGrids] = {}, *gcblk[kMaxGrids] = {};
@@ -314,6 +321,10 @@ static int create_impl(const ecsg_grid_desc *grids, const ecsg_config *cfg, ecsg
         const char *env = getenv("ECSG_VEL_TMA");   // "0": the float4 velocity sweep (validation)
         s->vel_tma = !(env && env[0] == '0');
     }
+    {
+        const char *env = getenv("ECSG_SIDE_GRIDS");   // "0": every sweep on the one stream
+        s->side_grids = !(env && env[0] == '0');
+    }
     s->tsize = s->prec == ECSG_F32 ? 4 : 8;
     s->nc = s->medium == ECSG_MEDIUM_ISO ? 5 : (s->medium == ECSG_MEDIUM_ORTHO9 ? 9 : 21);
     if (cudaSetDevice(s->device) != cudaSuccess) { fail(s, ECSG_ERR_NO_DEVICE, "cudaSetDevice(%d) failed", s->device); return bail(ECSG_ERR_NO_DEVICE); }
@@ -324,6 +335,16 @@ static int create_impl(const ecsg_grid_desc *grids, const ecsg_config *cfg, ecsg
     if (cudaStreamCreateWithFlags(&s->st, cudaStreamNonBlocking) != cudaSuccess) return bail(fail(s, ECSG_ERR_CUDA, "stream"));
     for (int e = 0; e < 4; e++)
         if (cudaEventCreate(&s->ev[e]) != cudaSuccess) return bail(fail(s, ECSG_ERR_CUDA, "event"));
+    if (s->ng > 1 && s->side_grids) {
+        int lo = 0, hi = 0;   // side streams at the lowest priority: the fine grid's CTAs go first
+        cudaDeviceGetStreamPriorityRange(&lo, &hi);
+        if (cudaEventCreateWithFlags(&s->fork_ev, cudaEventDisableTiming) != cudaSuccess)
+            return bail(fail(s, ECSG_ERR_CUDA, "event"));
+        for (int g = 1; g < s->ng; g++)
+            if (cudaStreamCreateWithPriority(&s->side[g], cudaStreamNonBlocking, lo) != cudaSuccess ||
+                cudaEventCreateWithFlags(&s->join_ev[g], cudaEventDisableTiming) != cudaSuccess)
+                return bail(fail(s, ECSG_ERR_CUDA, "side stream"));
+    }
 
     for (int g = 0; g < s->ng; g++) {
         for (int d = 0; d < 3; d++) {
@@ -443,6 +464,11 @@ int ecsg_destroy(ecsg_sim *s)
         if (s->gx[v]) cudaGraphExecDestroy(s->gx[v]);
     for (int e = 0; e < 4; e++)
         if (s->ev[e]) cudaEventDestroy(s->ev[e]);
+    for (int g = 0; g < kMaxGrids; g++) {
+        if (s->side[g]) cudaStreamDestroy(s->side[g]);
+        if (s->join_ev[g]) cudaEventDestroy(s->join_ev[g]);
+    }
+    if (s->fork_ev) cudaEventDestroy(s->fork_ev);
     if (s->st) cudaStreamDestroy(s->st);
     delete s;
     return ECSG_OK;
@@ -1193,12 +1219,38 @@ static SrcRec make_srcrec(ecsg_sim *s, int mode)
 }
 
 // One iteration of main.cpp:165-261 (movies excluded).
+// op(g) for every grid: grid 0 on the library stream, the coarse grids on
+// their side streams (forked from and joined back into the library stream,
+// so a graph capture sees parallel branches), or all on the library stream.
+template <typename Op>
+static int each_grid(ecsg_sim *s, Op op)
+{
+    int rc;
+    if (s->ng == 1 || !s->side[1]) {
+        for (int g = 0; g < s->ng; g++)
+            if ((rc = op(g))) return rc;
+        return ECSG_OK;
+    }
+    cudaStream_t lib_stream = s->st;
+    CK(cudaEventRecord(s->fork_ev, lib_stream));
+    for (int g = 1; g < s->ng; g++) CK(cudaStreamWaitEvent(s->side[g], s->fork_ev, 0));
+    if ((rc = op(0))) return rc;
+    for (int g = 1; g < s->ng; g++) {
+        s->st = s->side[g];
+        rc = op(g);
+        s->st = lib_stream;
+        if (rc) return rc;
+        CK(cudaEventRecord(s->join_ev[g], s->side[g]));
+        CK(cudaStreamWaitEvent(lib_stream, s->join_ev[g], 0));
+    }
+    return ECSG_OK;
+}
+
 template <typename T>
 static int step_op(ecsg_sim *s, bool energy, double *energy_buf, double *res_row, T *sample_row = nullptr)
 {
     int rc;
-    for (int g = 0; g < s->ng; g++)
-        if ((rc = vel_op<T>(s, g, energy))) return rc;
+    if ((rc = each_grid(s, [&](int g) { return vel_op<T>(s, g, energy); }))) return rc;
     if (sample_row) CK(launch_rec_sample<T>(make_srcrec(s, 0), sample_row, s->st));
     if (res_row) {
         CK(launch_src_rec<T>(make_srcrec(s, 1), s->st));
@@ -1215,8 +1267,7 @@ static int step_op(ecsg_sim *s, bool energy, double *energy_buf, double *res_row
             if ((rc = residue_op<T>(s, i, 4, res_row + 12 * (i - 1)))) return rc;
     if (energy)
         if ((rc = energy_op<T>(s, energy_buf, s->ints + 1, s->ints + 3))) return rc;
-    for (int g = 0; g < s->ng; g++)
-        if ((rc = stress_op<T>(s, g))) return rc;
+    if ((rc = each_grid(s, [&](int g) { return stress_op<T>(s, g); }))) return rc;
     for (int i = 1; i < s->ng; i++) {
         if ((rc = sxz_op<T>(s, i))) return rc;
         if ((rc = syz_op<T>(s, i))) return rc;

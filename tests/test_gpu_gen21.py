@@ -258,3 +258,27 @@ def test_tma_velocity_sweep_equals_float4_sweep(monkeypatch, ratio, top_bc, nx2,
     for a, b in zip(fa, fb):
         assert np.array_equal(a, b)
 
+
+@pytest.mark.parametrize("medium", ["tti", "iso"])
+@pytest.mark.parametrize("graph", [False, True])
+def test_side_stream_grids_equal_one_stream(monkeypatch, medium, graph):
+    """The coarse grids' velocity and stress sweeps on side streams (the
+    default for multi-grid runs) against every sweep on the library stream
+    (ECSG_SIDE_GRIDS=0): bitwise equal traces, energies and fields on a
+    three-grid ratio-3 composite, eager and as a CUDA graph."""
+    from ecsg_b200.workloads import three_grid_case
+    case = three_grid_case(seed=4, grids=[((72, 54, 12), 5.0), ((24, 18, 10), 15.0), ((8, 6, 8), 45.0)],
+                           nsteps=40, medium=medium)
+    outs = []
+    for side in ("0", "1"):
+        monkeypatch.setenv("ECSG_SIDE_GRIDS", side)
+        with Simulation(case, precision="f32", energy=True) as s:
+            r = s.run(40, energy_every=4, graph=graph)
+            outs.append((r, [s.field(g, k) for g in range(3) for k in range(9)], s.status()))
+    (ra, fa, sa), (rb, fb, sb) = outs
+    assert sa == 0 and sb == 0
+    assert np.abs(ra["rec"]).max() > 0
+    assert np.array_equal(ra["rec"], rb["rec"])
+    assert np.array_equal(ra["energy"], rb["energy"], equal_nan=True)
+    for a, b in zip(fa, fb):
+        assert np.array_equal(a, b)

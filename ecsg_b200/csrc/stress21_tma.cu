@@ -59,7 +59,7 @@ static_assert(P_CHB % 128 == 0 && P_CHC % 128 == 0 && P_CI % 128 == 0 && P_SG % 
                   P_EX % 128 == 0 && P_EY % 128 == 0 && PSLOT % 128 == 0, "128-byte aligned boxes");
 constexpr int OFF_V = NSP * PSLOT;
 constexpr int OFF_IM = OFF_V + NSV * VSLOT;
-constexpr int OFF_BAR = OFF_IM + 2 * NQ * HP * 4;
+constexpr int OFF_BAR = OFF_IM + 3 * NQ * HP * 4;   // three-plane ring of intermediates
 constexpr int NBAR = 2 * NSP + 2 * NSV;
 constexpr int OFF_FLAG = OFF_BAR + NBAR * 8;
 constexpr int SMEM = OFF_FLAG + 64;
@@ -102,16 +102,19 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
     auto emptyP = [&](int s) { return bar0 + 8u * (NSP + s); };
     auto fullV = [&](int s) { return bar0 + 8u * (2 * NSP + s); };
     auto emptyV = [&](int s) { return bar0 + 8u * (2 * NSP + NSV + s); };
-    // [0] producer gave up, [1] P stages consumed, [2] V stages consumed, [3] consumers gave up.
-    // [3] is written only by consumers before a consumer barrier and read between
-    // that barrier and the next, so every consumer takes the same branch.
+    // [0] producer gave up, [1] P stages consumed, [2] V stages consumed, [3 + (i & 1)]
+    // consumers gave up on plane stage i.  A consumer sets it before the plane's
+    // one consumer barrier and every consumer reads it right after that barrier;
+    // no consumer can reach stage i + 2 (same word) before all have passed the
+    // barrier of stage i + 1, so every consumer takes the same branch.
     volatile int *flags = (volatile int *)(sm + OFF_FLAG);
     float *IM = (float *)(sm + OFF_IM);
 
     if (tid == 0) {
-        for (int s = 0; s < NSP; s++) { mbar_init(fullP(s), 1); mbar_init(emptyP(s), 1); }
-        for (int s = 0; s < NSV; s++) { mbar_init(fullV(s), 1); mbar_init(emptyV(s), 1); }
-        flags[0] = 0; flags[1] = 0; flags[2] = 0; flags[3] = 0;
+        // a slot is free again once each of the 8 consumer warps has arrived
+        for (int s = 0; s < NSP; s++) { mbar_init(fullP(s), 1); mbar_init(emptyP(s), NT / 32); }
+        for (int s = 0; s < NSV; s++) { mbar_init(fullV(s), 1); mbar_init(emptyV(s), NT / 32); }
+        flags[0] = 0; flags[1] = 0; flags[2] = 0; flags[3] = 0; flags[4] = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
@@ -165,7 +168,7 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
                     ok = issueP(i);
                     if (ok) issuedP++;
                 }
-                if (flags[3]) break;
+                if (flags[3] || flags[4]) break;
             }
             if (!ok) {
                 flags[0] = 1;
@@ -216,11 +219,7 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
             }
             ok = ok && mbar_wait(fullV((i + 2) % NSV), ((i + 2) / NSV) & 1);
             ok = ok && mbar_wait(fullP(i % NSP), (i / NSP) & 1);
-            if (!ok) flags[3] = 1;
-            consumer_sync();
-            if (flags[3]) break;
-            consumedP = i + 1;
-            consumedV = i + 3;
+            if (!ok) flags[3 + (i & 1)] = 1;
             const unsigned char *PS = sm + (i % NSP) * PSLOT;
             const float *CHA = (const float *)(PS + P_CHA);
             const float *CHB = (const float *)(PS + P_CHB);
@@ -233,9 +232,12 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
             const float *Vn = (const float *)(sm + OFF_V + ((i + 2) % NSV) * VSLOT);
             constexpr int HS = HBOX / 4;   // floats between the haloed boxes of a group
             constexpr int IS = IBOX / 4;
-            float *IMs = IM + (p & 1) * NQ * HP;
-            const float *Rs = IM + (p & 1) * NQ * HP;          // plane p
-            const float *Rp = IM + ((p - 1) & 1) * NQ * HP;    // plane p-1
+            // three-plane ring: stage i + 1 writes the slot that stage i - 1 read,
+            // so no barrier is needed between a stage's outputs and the next
+            // stage's intermediates
+            float *IMs = IM + (i % 3) * NQ * HP;
+            const float *Rs = IMs;                               // plane p
+            const float *Rp = IM + ((i + 2) % 3) * NQ * HP;      // plane p-1
             const bool surf = flag && p == 0;
             const bool inner = p >= z0 && p <= z1;
             const int pm = p - 1;
@@ -323,6 +325,7 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
                     }
                 }
                 consumer_sync();
+                if (flags[3 + (i & 1)]) return false;
 
                 // ---- outputs: sigma_N, sigma_6 at plane p; sigma_4, sigma_5 at plane p-1
                 if (inner) {
@@ -408,13 +411,14 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
                         if (flag && pm == 0 && (FAST || (ox >= 1 && ox <= nx - 1 && oy >= 1 && oy <= ny - 1))) sxz[pp - sz] = -nv;
                     }
                 }
+                return true;
             };
             // fast planes: interior tile, 1 <= p <= nz-1 (not the free surface,
             // every closure weight 1/4 for the outputs at p and p-1)
-            if (tile_in && p >= 1 && p <= nz - 1)
-                body(std::true_type{});
-            else
-                body(std::false_type{});
+            const bool go = (tile_in && p >= 1 && p <= nz - 1) ? body(std::true_type{}) : body(std::false_type{});
+            if (!go) break;
+            consumedP = i + 1;
+            consumedV = i + 3;
 
             // displacement sums: U += v at this thread's point (x <= nx, y <= ny)
             // of an inner plane, the x = -1 / y = -1 face points beside it, and
@@ -444,8 +448,9 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
                 c16p = cho(9); c17p = cho(10); c19p = cho(11);
                 s3p = SG[3 * IS + ib]; s4p = SG[4 * IS + ib];
             }
-            consumer_sync();
-            if (tid == 0) {
+            // this warp is done with plane stage i's slots
+            __syncwarp();
+            if (lane == 0) {
                 mbar_arrive(emptyP(i % NSP));
                 mbar_arrive(emptyV(i % NSV));
             }
@@ -453,7 +458,7 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
         if (tid == 0) {
             flags[1] = consumedP;
             flags[2] = consumedV;
-            if (flags[3]) atomicOr(status, ST_PIPE_TIMEOUT);
+            if (flags[3] || flags[4]) atomicOr(status, ST_PIPE_TIMEOUT);
         }
     }
     __syncthreads();

@@ -40,7 +40,7 @@ constexpr int TX = 32, TY = 8, NT = TX * TY, NTHREADS = NT + 32;
 constexpr int BW = 40, BH = 10;              // haloed box: x0-4 .. x0+35, y0-1 .. y0+8
 constexpr int HX = 34, HYI = 10, HP = HX * HYI;   // intermediates: x0-1 .. x0+32, y0-1 .. y0+8
 constexpr int NQ = 9;
-constexpr int NSP = 3, NSV = 5;               // ring depths: plane data, velocities
+constexpr int NSP = 4, NSV = 6;               // ring depths: plane data, velocities (206 KB of shared memory)
 constexpr int HBOX = BW * BH * 4;             // 1600 bytes
 constexpr int IBOX = TX * TY * 4;             // 1024 bytes
 constexpr int CW = 36, CHH = 9, CBOX = CW * CHH * 4;   // one-sided coefficient box: 1296 bytes

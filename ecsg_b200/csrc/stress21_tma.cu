@@ -80,6 +80,9 @@ struct S21Maps {
     CUtensorMap epy;  // displacement sums: y = -1 face rows (tiles at y0 = 0)
 };
 
+// the two closure weights of a neighbour pair (w2 of gen21_device.cuh)
+__device__ __forceinline__ void closure_w2(bool a, bool b, float (&w)[2]) { w2<float>(a, b, w[0], w[1]); }
+
 __device__ __forceinline__ void consumer_sync() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
 
 template <bool ACC>
@@ -208,6 +211,13 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
         // 1 .. n-1): on their planes 1 .. nz-1 every extent test passes and every
         // closure weight is 1/4, so the fast variant drops the tests.
         const bool tile_in = x0 >= 1 && x0 + TX <= nx && y0 >= 1 && y0 + TY <= ny;
+        // closure weights of this point's x and y neighbour pairs: xA {x, x+1}
+        // (extent 0..nx), xB {x-1, x} (0..nx-1), yA {y-1, y} (0..ny-1), yB {y, y+1} (0..ny)
+        float wxA[2], wxB[2], wyA[2], wyB[2];
+        closure_w2(ox <= nx, ox + 1 <= nx, wxA);
+        closure_w2(ox - 1 >= 0 && ox - 1 <= nx - 1, ox <= nx - 1, wxB);
+        closure_w2(oy - 1 >= 0 && oy - 1 <= ny - 1, oy <= ny - 1, wyA);
+        closure_w2(oy <= ny, oy + 1 <= ny, wyB);
         const int pbase = g.idx(ox, oy, 0);
         int consumedP = 0, consumedV = 0;
         for (int i = 0; i < n; i++) {
@@ -247,16 +257,31 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
             auto cho = [&](int k) { return k < NCA ? CHA[k * CS + ia] : (k < NCA + NCB ? CHB[(k - NCA) * CS + ibb] : CHC[ic]); };
             auto chh = [&](int k) { return k < NCA ? CHA[k * CS + ha] : (k < NCA + NCB ? CHB[(k - NCA) * CS + hb] : CHC[hc]); };
 
+            // closure weights of the z pairs: zA {p-1, p} (extent 0..nz-1) for the
+            // outputs at p, zB {pm, pm+1} (extent 0..nz) for the outputs at pm
+            float wzA[2], wzB[2];
+            closure_w2(p - 1 >= 0 && p - 1 <= nz - 1, p >= 0 && p <= nz - 1, wzA);
+            closure_w2(pm <= nz, pm + 1 <= nz, wzB);
             auto body = [&](auto fast_tag) {
                 constexpr bool FAST = decltype(fast_tag)::value;
                 auto RR = [&](int plane_is_p, int q, int hx_, int hy_) { return (plane_is_p ? Rs : Rp)[q * HP + hy_ * HX + hx_]; };
-                // closure-weighted mean of four neighbours (avg4); 1/4 each on the fast path
-                auto av = [&](const float (&v)[2][2], const bool (&a)[2], const bool (&b)[2]) -> float {
+                // closure-weighted mean of four neighbours: 1/4 each on the fast
+                // path, else the per-dimension closure weights w0 (first index of
+                // v) and w1 (second).  avg4's order; its skipped zero-weight terms
+                // are included here, which leaves the sum bitwise unchanged (the
+                // sum starts at +0, so it is never -0, and adding a signed zero to
+                // it changes nothing; the neighbours outside an extent hold 0).
+                auto av = [&](const float (&v)[2][2], const float (&w0)[2], const float (&w1)[2]) -> float {
                     if (FAST) {
                         const float w = 0.25f;
                         return fma_(w, v[1][1], fma_(w, v[1][0], fma_(w, v[0][1], fma_(w, v[0][0], 0.f))));
                     }
-                    return avg4<float>(v, a, b);
+                    float acc = 0.f;
+#pragma unroll
+                    for (int a = 0; a < 2; a++)
+#pragma unroll
+                        for (int b = 0; b < 2; b++) acc = fma_(mul_(w0[a], w1[b]), v[a][b], acc);
+                    return acc;
                 };
 
                 // ---- intermediates of plane p: own point (all kinds), then the halo job
@@ -332,16 +357,12 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
                     const int pp = pbase + p * sz;
                     if (FAST || E.n(ox, oy, p)) {
                         float v[2][2];
-                        bool a[2], b[2];
-                        for (int k = 0; k < 2; k++) { a[k] = (oy - 1 + k) >= 0 && (oy - 1 + k) <= ny - 1; b[k] = (p - 1 + k) >= 0 && (p - 1 + k) <= nz - 1; }
                         for (int k = 0; k < 2; k++) for (int j = 0; j < 2; j++) v[k][j] = RR(j, 0, hx, hy - 1 + k);
-                        const float a4 = av(v, a, b);
-                        for (int k = 0; k < 2; k++) { a[k] = (ox + k) <= nx; b[k] = (p - 1 + k) >= 0 && (p - 1 + k) <= nz - 1; }
+                        const float a4 = av(v, wyA, wzA);
                         for (int k = 0; k < 2; k++) for (int j = 0; j < 2; j++) v[k][j] = RR(j, 3, hx + k, hy);
-                        const float a5 = av(v, a, b);
-                        for (int k = 0; k < 2; k++) { a[k] = (ox + k) <= nx; b[k] = (oy - 1 + k) >= 0 && (oy - 1 + k) <= ny - 1; }
+                        const float a5 = av(v, wxA, wzA);
                         for (int k = 0; k < 2; k++) for (int j = 0; j < 2; j++) v[k][j] = RR(1, 5, hx + k, hy - 1 + j);
-                        const float a6 = av(v, a, b);
+                        const float a6 = av(v, wxA, wyA);
                         const int rowc[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
                         float d[3];
 #pragma unroll
@@ -357,16 +378,12 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
                     }
                     if (FAST || E.l6(ox, oy, p)) {
                         float v[2][2];
-                        bool a[2], b[2];
-                        for (int k = 0; k < 2; k++) { a[k] = (ox - 1 + k) >= 0 && (ox - 1 + k) <= nx - 1; b[k] = (p - 1 + k) >= 0 && (p - 1 + k) <= nz - 1; }
                         for (int k = 0; k < 2; k++) for (int j = 0; j < 2; j++) v[k][j] = RR(j, 2, hx - 1 + k, hy);
-                        const float t46 = av(v, a, b);
-                        for (int k = 0; k < 2; k++) { a[k] = (oy + k) <= ny; b[k] = (p - 1 + k) >= 0 && (p - 1 + k) <= nz - 1; }
+                        const float t46 = av(v, wxB, wzA);
                         for (int k = 0; k < 2; k++) for (int j = 0; j < 2; j++) v[k][j] = RR(j, 4, hx, hy + k);
-                        const float t56 = av(v, a, b);
-                        for (int k = 0; k < 2; k++) { a[k] = (ox - 1 + k) >= 0 && (ox - 1 + k) <= nx - 1; b[k] = (oy + k) <= ny; }
+                        const float t56 = av(v, wyB, wzA);
                         for (int k = 0; k < 2; k++) for (int j = 0; j < 2; j++) v[k][j] = RR(1, 8, hx - 1 + k, hy + j);
-                        const float t6 = av(v, a, b);
+                        const float t6 = av(v, wxB, wyB);
                         const float e6 = RR(1, 5, hx, hy);
                         const float dd = add_(add_(fma_(CI[8 * IS + ib], e6, t46), t56), t6);
                         sxy[pp] = add_(SG[5 * IS + ib], dd);
@@ -376,16 +393,12 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
                     const int pp = pbase + pm * sz;
                     if (FAST || E.l4(ox, oy, pm)) {
                         float v[2][2];
-                        bool a[2], b[2];
-                        for (int k = 0; k < 2; k++) { a[k] = (ox + k) <= nx; b[k] = (oy + k) <= ny; }
                         for (int k = 0; k < 2; k++) for (int j = 0; j < 2; j++) v[k][j] = RR(0, 3, hx + k, hy + j);
-                        const float t5 = av(v, a, b);
-                        for (int k = 0; k < 2; k++) { a[k] = (ox + k) <= nx; b[k] = (pm + k) <= nz; }
+                        const float t5 = av(v, wxA, wyB);
                         for (int k = 0; k < 2; k++) for (int j = 0; j < 2; j++) v[k][j] = RR(j, 5, hx + k, hy);
-                        const float t6 = av(v, a, b);
-                        for (int k = 0; k < 2; k++) { a[k] = (oy + k) <= ny; b[k] = (pm + k) <= nz; }
+                        const float t6 = av(v, wxA, wzB);
                         for (int k = 0; k < 2; k++) for (int j = 0; j < 2; j++) v[k][j] = RR(j, 6, hx, hy + k);
-                        const float tp = av(v, a, b);
+                        const float tp = av(v, wyB, wzB);
                         const float e4 = RR(0, 0, hx, hy);
                         const float dd = add_(fma_(c17p, t6, fma_(c16p, t5, mul_(c15p, e4))), tp);
                         const float nv = add_(s3p, dd);
@@ -394,16 +407,12 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
                     }
                     if (FAST || E.l5(ox, oy, pm)) {
                         float v[2][2];
-                        bool a[2], b[2];
-                        for (int k = 0; k < 2; k++) { a[k] = (oy - 1 + k) >= 0 && (oy - 1 + k) <= ny - 1; b[k] = (pm + k) <= nz; }
                         for (int k = 0; k < 2; k++) for (int j = 0; j < 2; j++) v[k][j] = RR(j, 5, hx, hy - 1 + k);
-                        const float t6 = av(v, a, b);
-                        for (int k = 0; k < 2; k++) { a[k] = (ox - 1 + k) >= 0 && (ox - 1 + k) <= nx - 1; b[k] = (oy - 1 + k) >= 0 && (oy - 1 + k) <= ny - 1; }
+                        const float t6 = av(v, wyA, wzB);
                         for (int k = 0; k < 2; k++) for (int j = 0; j < 2; j++) v[k][j] = RR(0, 1, hx - 1 + k, hy - 1 + j);
-                        const float t45 = av(v, a, b);
-                        for (int k = 0; k < 2; k++) { a[k] = (ox - 1 + k) >= 0 && (ox - 1 + k) <= nx - 1; b[k] = (pm + k) <= nz; }
+                        const float t45 = av(v, wxB, wyA);
                         for (int k = 0; k < 2; k++) for (int j = 0; j < 2; j++) v[k][j] = RR(j, 7, hx - 1 + k, hy);
-                        const float tp = av(v, a, b);
+                        const float tp = av(v, wxB, wzB);
                         const float e5 = RR(0, 3, hx, hy);
                         const float dd = add_(add_(fma_(c19p, t6, mul_(c18p, e5)), t45), tp);
                         const float nv = add_(s4p, dd);

@@ -195,39 +195,54 @@ __global__ void stress21_adj_g0(GridDev<T> G, AdjDev<T> A, int flag)
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
         const int x = (int)(t % (nx + 1)), y = (int)((t / (nx + 1)) % (ny + 1)), z = (int)(t / ((int64_t)(nx + 1) * (ny + 1)));
         const int p = g.idx(x, y, z);
-        if (E.n(x, y, z)) {
+        // all loads and arithmetic of the point first, then its stores (the
+        // pointers may alias as far as the compiler knows: a load after a
+        // store could not be moved ahead of it and would wait for memory)
+        const bool in_n = E.n(x, y, z), in_4 = E.l4(x, y, z), in_5 = E.l5(x, y, z), in_6 = E.l6(x, y, z);
+        T en[3] = {}, le[3] = {}, ls[3] = {}, e4 = T(0), e5 = T(0), e6 = T(0);
+        if (in_n) {
             const bool surf = flag && z == 0;
-            const T e1 = e1_at(G, p), e2 = e2_at(G, p);
-            X[X_E + 0][p] = e1;
-            X[X_E + 1][p] = e2;
-            X[X_E + 2][p] = e3_used(G, E, surf, x, y, z, p, e1, e2);
+            en[0] = e1_at(G, p);
+            en[1] = e2_at(G, p);
+            en[2] = e3_used(G, E, surf, x, y, z, p, en[0], en[1]);
             const T a[3] = {A.l[SXX][p], A.l[SYY][p], surf ? T(0) : A.l[SZZ][p]};
             const int rowc[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
-            for (int j = 0; j < 3; j++) {
-                T le = T(0), ls = T(0);
+#pragma unroll
+            for (int j = 0; j < 3; j++)
+#pragma unroll
                 for (int i = 0; i < 3; i++) {
-                    le = fma_(a[i], c[rowc[i][j]][p], le);
-                    ls = fma_(a[i], c[6 + 3 * i + j][p], ls);
+                    le[j] = fma_(a[i], c[rowc[i][j]][p], le[j]);
+                    ls[j] = fma_(a[i], c[6 + 3 * i + j][p], ls[j]);
                 }
-                X[X_W + j][p] = le;
-                X[X_S + j][p] = ls;
+        }
+        // the surface mirrors of syz / sxz folded back: lambda(0) - lambda(-1)
+        const bool fold4 = in_4 && flag && z == 0;   // syz(-1) = -syz(0)
+        const bool fold5 = in_5 && flag && z == 0 && x >= 1 && x <= nx - 1 && y >= 1 && y <= ny - 1;
+        T f4 = T(0), f5 = T(0);
+        if (in_4) e4 = e4_at(G, p);
+        if (fold4) f4 = sub_(A.l[SYZ][p], A.l[SYZ][p - sz]);
+        if (in_5) e5 = e5_at(G, p);
+        if (fold5) f5 = sub_(A.l[SXZ][p], A.l[SXZ][p - sz]);
+        if (in_6) e6 = e6_at(G, p);
+        if (in_n) {
+#pragma unroll
+            for (int j = 0; j < 3; j++) {
+                X[X_E + j][p] = en[j];
+                X[X_W + j][p] = le[j];
+                X[X_S + j][p] = ls[j];
             }
         }
-        if (E.l4(x, y, z)) {
-            X[X_E + 3][p] = e4_at(G, p);
-            if (flag && z == 0) {   // syz(-1) = -syz(0)
-                A.l[SYZ][p] = sub_(A.l[SYZ][p], A.l[SYZ][p - sz]);
-                A.l[SYZ][p - sz] = T(0);
-            }
+        if (in_4) X[X_E + 3][p] = e4;
+        if (fold4) {
+            A.l[SYZ][p] = f4;
+            A.l[SYZ][p - sz] = T(0);
         }
-        if (E.l5(x, y, z)) {
-            X[X_E + 4][p] = e5_at(G, p);
-            if (flag && z == 0 && x >= 1 && x <= nx - 1 && y >= 1 && y <= ny - 1) {
-                A.l[SXZ][p] = sub_(A.l[SXZ][p], A.l[SXZ][p - sz]);
-                A.l[SXZ][p - sz] = T(0);
-            }
+        if (in_5) X[X_E + 4][p] = e5;
+        if (fold5) {
+            A.l[SXZ][p] = f5;
+            A.l[SXZ][p - sz] = T(0);
         }
-        if (E.l6(x, y, z)) X[X_E + 5][p] = e6_at(G, p);
+        if (in_6) X[X_E + 5][p] = e6;
     }
 }
 
@@ -277,19 +292,33 @@ __global__ void stress21_adj_g1(GridDev<T> G, AdjDev<T> A, int flag)
             ab[2] = avg4<T>(v, oa, ob);
             const bool surf = flag && z == 0;
             const T a[3] = {A.l[SXX][p], A.l[SYY][p], surf ? T(0) : A.l[SZZ][p]};
-            const int rowc[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
-            for (int i = 0; i < 3; i++)
-                for (int j = 0; j < 3; j++) {
-                    A.gc[rowc[i][j]][p] = add_(A.gc[rowc[i][j]][p], mul_(a[i], e[j]));
-                    A.gc[6 + 3 * i + j][p] = add_(A.gc[6 + 3 * i + j][p], mul_(a[i], ab[j]));
-                }
+            // every load of the block before its first store (the pointers may
+            // alias as far as the compiler knows, so loads after a store would
+            // each wait for memory in turn); same updates in the same order
+            T gk[15], cs[9];
+#pragma unroll
+            for (int k = 0; k < 15; k++) gk[k] = A.gc[k][p];
+#pragma unroll
+            for (int k = 0; k < 9; k++) cs[k] = c[6 + k][p];
             T le[3] = {X[X_W + 0][p], X[X_W + 1][p], X[X_W + 2][p]};
+            const int rowc[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+#pragma unroll
+            for (int i = 0; i < 3; i++)
+#pragma unroll
+                for (int j = 0; j < 3; j++) {
+                    gk[rowc[i][j]] = add_(gk[rowc[i][j]], mul_(a[i], e[j]));
+                    gk[6 + 3 * i + j] = add_(gk[6 + 3 * i + j], mul_(a[i], ab[j]));
+                }
+#pragma unroll
             for (int k = 0; k < 3; k++)
+#pragma unroll
                 for (int j = 0; j < 3; j++) {
                     const int s = 6 + 3 * j + k;   // P(4+k) = C(1,4+k) e1 + C(2,4+k) e2 + C(3,4+k) e3
-                    A.gc[s][p] = add_(A.gc[s][p], mul_(zp[k], e[j]));
-                    le[j] = fma_(c[s][p], zp[k], le[j]);
+                    gk[s] = add_(gk[s], mul_(zp[k], e[j]));
+                    le[j] = fma_(cs[s - 6], zp[k], le[j]);
                 }
+#pragma unroll
+            for (int k = 0; k < 15; k++) A.gc[k][p] = gk[k];
             X[X_W + 0][p] = le[0];
             X[X_W + 1][p] = le[1];
             X[X_W + 2][p] = le[2];
@@ -320,10 +349,12 @@ __global__ void stress21_adj_g1(GridDev<T> G, AdjDev<T> A, int flag)
             for (int i = 0; i < 2; i++) { oa[i] = (x + i) <= nx; ob[i] = (z + i) <= nz; }
             for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++) v[i][j] = (oa[i] && ob[j]) ? X[X_E + 5][I(x + i, y, z + j)] : T(0);
             const T t6 = avg4<T>(v, oa, ob);
-            A.gc[15][p] = add_(A.gc[15][p], mul_(a4, e4));
-            A.gc[16][p] = add_(A.gc[16][p], add_(mul_(a4, t5), mul_(z45, e4)));
-            A.gc[17][p] = add_(A.gc[17][p], add_(mul_(a4, t6), mul_(z46, e4)));
-            X[X_W + 3][p] = add_(fma_(c[15][p], a4, fma_(c[16][p], z45, mul_(c[17][p], z46))), sn);
+            const T g15 = A.gc[15][p], g16 = A.gc[16][p], g17 = A.gc[17][p];
+            const T c15 = c[15][p], c16 = c[16][p], c17 = c[17][p];
+            A.gc[15][p] = add_(g15, mul_(a4, e4));
+            A.gc[16][p] = add_(g16, add_(mul_(a4, t5), mul_(z45, e4)));
+            A.gc[17][p] = add_(g17, add_(mul_(a4, t6), mul_(z46, e4)));
+            X[X_W + 3][p] = add_(fma_(c15, a4, fma_(c16, z45, mul_(c17, z46))), sn);
         }
         // ---- L5 s: C55 a5 + C56 Z56 + Abar5 adjoints of N + C45 a4 from L4's t5
         if (E.l5(x, y, z)) {
@@ -348,9 +379,10 @@ __global__ void stress21_adj_g1(GridDev<T> G, AdjDev<T> A, int flag)
             for (int i = 0; i < 2; i++) { oa[i] = in_(y - 1 + i, 0, ny - 1); ob[i] = (z + i) <= nz; }
             for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++) v[i][j] = (oa[i] && ob[j]) ? X[X_E + 5][I(x, y - 1 + i, z + j)] : T(0);
             const T t6 = avg4<T>(v, oa, ob);
-            A.gc[18][p] = add_(A.gc[18][p], mul_(a5, e5));
-            A.gc[19][p] = add_(A.gc[19][p], add_(mul_(a5, t6), mul_(z56, e5)));
-            X[X_W + 4][p] = add_(add_(fma_(c[18][p], a5, mul_(c[19][p], z56)), sn), s4);
+            const T g18 = A.gc[18][p], g19 = A.gc[19][p], c18 = c[18][p], c19 = c[19][p];
+            A.gc[18][p] = add_(g18, mul_(a5, e5));
+            A.gc[19][p] = add_(g19, add_(mul_(a5, t6), mul_(z56, e5)));
+            X[X_W + 4][p] = add_(add_(fma_(c18, a5, mul_(c19, z56)), sn), s4);
         }
         // ---- L6 t: C66 a6 + Abar6 adjoints of N + C46 a4 (L4 t6) + C56 a5 (L5 t6)
         if (E.l6(x, y, z)) {
@@ -374,8 +406,9 @@ __global__ void stress21_adj_g1(GridDev<T> G, AdjDev<T> A, int flag)
                                   mul_(c[19][q], l5[q]), s5);
                     }
                 }
-            A.gc[20][p] = add_(A.gc[20][p], mul_(a6, X[X_E + 5][p]));
-            X[X_W + 5][p] = add_(add_(fma_(c[20][p], a6, sn), s4), s5);
+            const T g20 = A.gc[20][p], e6 = X[X_E + 5][p], c20 = c[20][p];
+            A.gc[20][p] = add_(g20, mul_(a6, e6));
+            X[X_W + 5][p] = add_(add_(fma_(c20, a6, sn), s4), s5);
         }
     }
 }
@@ -464,9 +497,12 @@ __global__ void stress21_adj_g3(GridDev<T> G, AdjDev<T> A)
         const T gz = add_(add_(mul_(k2, sub_(W(2, E.n(x, y, z), x, y, z), W(2, E.n(x, y, z + 1), x, y, z + 1))),
                                mul_(k1, sub_(W(3, E.l4(x, y - 1, z), x, y - 1, z), W(3, E.l4(x, y, z), x, y, z)))),
                           mul_(k0, sub_(W(4, E.l5(x, y, z), x, y, z), W(4, E.l5(x + 1, y, z), x + 1, y, z))));
-        if (gx != T(0)) A.l[VX][p] = add_(A.l[VX][p], gx);
-        if (gy != T(0)) A.l[VY][p] = add_(A.l[VY][p], gy);
-        if (gz != T(0)) A.l[VZ][p] = add_(A.l[VZ][p], gz);
+        // the three loads before the first store (they are in the box for every
+        // x, y, z in [-1, n])
+        const T lx = A.l[VX][p], ly = A.l[VY][p], lz = A.l[VZ][p];
+        if (gx != T(0)) A.l[VX][p] = add_(lx, gx);
+        if (gy != T(0)) A.l[VY][p] = add_(ly, gy);
+        if (gz != T(0)) A.l[VZ][p] = add_(lz, gz);
     }
 }
 

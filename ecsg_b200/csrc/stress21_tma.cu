@@ -40,7 +40,7 @@ constexpr int TX = 32, TY = 8, NT = TX * TY, NTHREADS = NT + 32;
 constexpr int BW = 40, BH = 10;              // haloed box: x0-4 .. x0+35, y0-1 .. y0+8
 constexpr int HX = 34, HYI = 10, HP = HX * HYI;   // intermediates: x0-1 .. x0+32, y0-1 .. y0+8
 constexpr int NQ = 9;
-constexpr int NSP = 4, NSV = 6;               // ring depths: plane data, velocities (206 KB of shared memory)
+constexpr int NSP = 2, NSV = 4;               // ring depths: plane data, velocities (112 KB in all: 2 CTAs per SM)
 constexpr int HBOX = BW * BH * 4;             // 1600 bytes
 constexpr int IBOX = TX * TY * 4;             // 1024 bytes
 constexpr int CW = 36, CHH = 9, CBOX = CW * CHH * 4;   // one-sided coefficient box: 1296 bytes
@@ -59,10 +59,11 @@ static_assert(P_CHB % 128 == 0 && P_CHC % 128 == 0 && P_CI % 128 == 0 && P_SG % 
                   P_EX % 128 == 0 && P_EY % 128 == 0 && PSLOT % 128 == 0, "128-byte aligned boxes");
 constexpr int OFF_V = NSP * PSLOT;
 constexpr int OFF_IM = OFF_V + NSV * VSLOT;
-constexpr int OFF_BAR = OFF_IM + 3 * NQ * HP * 4;   // three-plane ring of intermediates
+constexpr int OFF_BAR = OFF_IM + 2 * NQ * HP * 4;   // two-plane ring of intermediates
 constexpr int NBAR = 2 * NSP + 2 * NSV;
 constexpr int OFF_FLAG = OFF_BAR + NBAR * 8;
 constexpr int SMEM = OFF_FLAG + 64;
+static_assert(2 * (SMEM + 1024) <= 233472, "two CTAs per SM (228 KB of shared memory, 1 KB reserved per CTA)");
 // coefficient slot of each staged box
 __host__ __device__ constexpr int ch_slot(int k) { return k < 9 ? 6 + k : (k == 9 ? 16 : (k == 10 ? 17 : 19)); }
 __host__ __device__ constexpr int ci_slot(int k) { return k < 6 ? k : (k == 6 ? 15 : (k == 7 ? 18 : 20)); }
@@ -86,7 +87,7 @@ __device__ __forceinline__ void closure_w2(bool a, bool b, float (&w)[2]) { w2<f
 __device__ __forceinline__ void consumer_sync() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
 
 template <bool ACC>
-__global__ void __launch_bounds__(s21t::NTHREADS, 1)
+__global__ void __launch_bounds__(s21t::NTHREADS, 2)
     stress21_tma_kernel(const __grid_constant__ S21Maps maps, GridDev<float> G, int flag, int zchunk, float *u0,
                         float *u1, float *u2, int *status)
 {
@@ -242,12 +243,11 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
             const float *Vn = (const float *)(sm + OFF_V + ((i + 2) % NSV) * VSLOT);
             constexpr int HS = HBOX / 4;   // floats between the haloed boxes of a group
             constexpr int IS = IBOX / 4;
-            // three-plane ring: stage i + 1 writes the slot that stage i - 1 read,
-            // so no barrier is needed between a stage's outputs and the next
-            // stage's intermediates
-            float *IMs = IM + (i % 3) * NQ * HP;
+            // two-plane ring: stage i + 1 writes the slot stage i reads as plane
+            // p-1, hence the consumer barrier at the end of every stage
+            float *IMs = IM + (i & 1) * NQ * HP;
             const float *Rs = IMs;                               // plane p
-            const float *Rp = IM + ((i + 2) % 3) * NQ * HP;      // plane p-1
+            const float *Rp = IM + ((i + 1) & 1) * NQ * HP;      // plane p-1
             const bool surf = flag && p == 0;
             const bool inner = p >= z0 && p <= z1;
             const int pm = p - 1;
@@ -457,8 +457,8 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 1)
                 c16p = cho(9); c17p = cho(10); c19p = cho(11);
                 s3p = SG[3 * IS + ib]; s4p = SG[4 * IS + ib];
             }
-            // this warp is done with plane stage i's slots
-            __syncwarp();
+            // every consumer is done with plane stage i's intermediates and slots
+            consumer_sync();
             if (lane == 0) {
                 mbar_arrive(emptyP(i % NSP));
                 mbar_arrive(emptyV(i % NSV));

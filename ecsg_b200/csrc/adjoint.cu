@@ -246,8 +246,9 @@ __global__ void stress21_adj_g0(GridDev<T> G, AdjDev<T> A, int flag)
     }
 }
 
+// FP32: 4 CTAs per SM (64 registers, no spills) for latency hiding
 template <typename T>
-__global__ void stress21_adj_g1(GridDev<T> G, AdjDev<T> A, int flag)
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) stress21_adj_g1(GridDev<T> G, AdjDev<T> A, int flag)
 {
     const Geo &g = G.g;
     const int nx = g.nx, ny = g.ny, nz = g.nz;

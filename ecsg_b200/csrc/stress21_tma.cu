@@ -23,8 +23,12 @@
 // through a two-plane ring, and update the stresses.  Velocities stay resident
 // for three planes (p-1, p, p+1), coefficients and stresses for one; the
 // values the z-staggered outputs (syz, sxz at plane p-1) need from plane p-1
-// are carried in registers.  All waits are bounded: on a timeout the CTA sets
-// ST_PIPE_TIMEOUT, stops, and drains its own copies before returning.
+// are carried in registers.  The rings are sized for two CTAs per SM (two
+// plane stages, four velocity stages, 112 KB; 96 registers): the second CTA,
+// not a deeper ring, hides the copy and dependency latency.  Tiles on the
+// domain edges take the same arithmetic with per-thread closure weights.
+// All waits are bounded: on a timeout the CTA sets ST_PIPE_TIMEOUT, stops,
+// and drains its own copies before returning.
 #include "ecsg_device.cuh"
 #include "gen21_device.cuh"
 #include "tma_util.cuh"

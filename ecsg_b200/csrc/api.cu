@@ -1246,6 +1246,38 @@ static int each_grid(ecsg_sim *s, Op op)
     return ECSG_OK;
 }
 
+// The vz ghost solves of every interface: interface 1 on the library stream,
+// the others on side streams, when every middle grid is thick enough (nz >= 8)
+// that the planes its two interfaces touch (its top, its bottom) are apart.
+// Each interface has its own scratch; these are ordinary (not cooperative)
+// launches that wait on nothing.
+template <typename T>
+static int each_vz_ghost(ecsg_sim *s)
+{
+    int rc;
+    bool side = s->ng > 2 && s->side[1];
+    for (int g = 1; g < s->ng - 1 && side; g++)
+        if (s->geo[g].nz < 8) side = false;
+    if (!side) {
+        for (int i = 1; i < s->ng; i++)
+            if ((rc = vz_op<T>(s, i))) return rc;
+        return ECSG_OK;
+    }
+    cudaStream_t lib_stream = s->st;
+    CK(cudaEventRecord(s->fork_ev, lib_stream));
+    for (int i = 2; i < s->ng; i++) CK(cudaStreamWaitEvent(s->side[i], s->fork_ev, 0));
+    if ((rc = vz_op<T>(s, 1))) return rc;
+    for (int i = 2; i < s->ng; i++) {
+        s->st = s->side[i];
+        rc = vz_op<T>(s, i);
+        s->st = lib_stream;
+        if (rc) return rc;
+        CK(cudaEventRecord(s->join_ev[i], s->side[i]));
+        CK(cudaStreamWaitEvent(lib_stream, s->join_ev[i], 0));
+    }
+    return ECSG_OK;
+}
+
 template <typename T>
 static int step_op(ecsg_sim *s, bool energy, double *energy_buf, double *res_row, T *sample_row = nullptr)
 {
@@ -1260,8 +1292,7 @@ static int step_op(ecsg_sim *s, bool energy, double *energy_buf, double *res_row
     } else {
         CK(launch_src_rec<T>(make_srcrec(s, 3), s->st));
     }
-    for (int i = 1; i < s->ng; i++)
-        if ((rc = vz_op<T>(s, i))) return rc;
+    if ((rc = each_vz_ghost<T>(s))) return rc;
     if (res_row)
         for (int i = 1; i < s->ng; i++)
             if ((rc = residue_op<T>(s, i, 4, res_row + 12 * (i - 1)))) return rc;

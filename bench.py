@@ -151,7 +151,12 @@ def shot_gradients(args, local, world, max_over_ranks, barrier):
     One shot per GPU; device time (CUDA events on the library's stream)
     around ecsg_misfit_gradient (forward with checkpoints, recomputation and
     adjoint) and, on several GPUs, the FP64 all-reduce of the gradient volumes
-    (NCCL, on the same stream)."""
+    (NCCL, on the same stream).
+
+    Batched leg (--grad-batch B > 1): B shots of the same model sharing one
+    medium allocation (ecsg_create_shot) run at once (ecsg_batch_misfit_gradient,
+    one stream per shot); host wall clock around that synchronous call against
+    the same clock around one plain ecsg_misfit_gradient call."""
     import ecsg_b200
     from ecsg_b200.workloads import two_grid_adjoint_case
     n = args.grad_steps
@@ -172,13 +177,44 @@ def shot_gradients(args, local, world, max_over_ranks, barrier):
         ms = s.timer_stop()
         gmax = float(np.abs(s.gradient(0, 0)).max())
         status = s.status()
+        t0 = time.perf_counter()
+        s.misfit_gradient(obs, ckpt_every=50)
+        plain_wall = time.perf_counter() - t0
     ms = max_over_ranks(ms)
+    batched = None
+    nb = args.grad_batch
+    if nb > 1:
+        shots = [(local * nb + k) % 16 for k in range(nb)]
+        obs_b = []
+        for k in shots:
+            with ecsg_b200.Simulation(two_grid_adjoint_case(0, k, n, blob=True), precision="f32", device=local) as s:
+                obs_b.append(s.run(n)["rec"].T.copy())
+        model = ecsg_b200.Simulation(two_grid_adjoint_case(0, shots[0], n, blob=False), precision="f32", device=local)
+        sims = [model] + [ecsg_b200.Simulation.shot(model, two_grid_adjoint_case(0, k, n, blob=False)) for k in shots[1:]]
+        try:
+            ecsg_b200.batch_misfit_gradient(sims, [o[: min(n, 60)] for o in obs_b], ckpt_every=50)   # warm-up
+            barrier()
+            t0 = time.perf_counter()
+            losses = ecsg_b200.batch_misfit_gradient(sims, obs_b, ckpt_every=50)
+            wall = time.perf_counter() - t0
+            bstatus = max(x.status() for x in sims)
+        finally:
+            for x in sims[1:]:
+                x.close()
+            model.close()
+        wall = max_over_ranks(wall)
+        plain_wall = max_over_ranks(plain_wall)
+        batched = {"shots": nb, "value": world * nb / wall, "plain_value_wall_clock": world / plain_wall,
+                   "speedup_vs_plain": (nb / wall) / (1.0 / plain_wall), "s_per_batch": wall,
+                   "finite": bool(np.isfinite(losses).all()), "status": bstatus,
+                   "timing": "host wall clock around the synchronous calls (batched and one plain call)"}
     return {"metric": "shot-gradients/s", "value": world / (ms * 1e-3), "unit": "shot-gradients/s",
             "mode": "plain (one shot per GPU at a time)" + (", FP64 NCCL all-reduce of the gradients" if world > 1 else ""),
             "ms_per_shot_gradient": ms, "steps": n,
             "ckpt_every": 50, "points": case.points(), "receivers": len(case.rec), "dtype": "f32",
             "loss": loss, "finite": bool(np.isfinite(loss) and np.isfinite(gmax)), "status": status,
-            "workload": "two-grid 361x361x61@10m / 121x121x81@30m, smooth orthorhombic, shot %d of 4x4" % shot}
+            "workload": "two-grid 361x361x61@10m / 121x121x81@30m, smooth orthorhombic, shot %d of 4x4" % shot,
+            "batched": batched}
 
 
 def batched_forward(args, local, world, max_over_ranks, barrier):
@@ -227,6 +263,8 @@ def main():
     ap.add_argument("--energy-every", type=int, default=100)
     ap.add_argument("--medium", default="tti", choices=["tti", "iso"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--grad-batch", type=int, default=4,
+                    help="shots per batched shot-gradient run (0 or 1: no batched leg)")
     ap.add_argument("--grad-steps", type=int, default=1500,
                     help="steps of the shot-gradient measurement (0: skip it)")
     ap.add_argument("--batch-steps", type=int, default=200,

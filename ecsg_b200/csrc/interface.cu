@@ -35,6 +35,22 @@ __device__ __forceinline__ double pw_node(int i, int j, int r, int n2)
     if (d <= -r || d >= r) return 0.0;
     return 1.0 - (double)abs(d) / (double)r;
 }
+// pw_node for a ratio known at compile time (RR = 2 or 3; 0: the runtime r):
+// the weights 1 - |d|/r come from constants the compiler folds with the same
+// correctly rounded IEEE arithmetic, so they equal pw_node's bit for bit
+// without a division per call
+template <int RR>
+__device__ __forceinline__ double pw_node_r(int i, int j, int r_, int n2)
+{
+    const int r = RR ? RR : r_;
+    if (j <= 0 || j >= n2) return 0.0;
+    const int d = i - r * j;
+    if (d <= -r || d >= r) return 0.0;
+    const int a = abs(d);
+    if (RR == 2) return a == 0 ? 1.0 : 1.0 - 1.0 / 2.0;
+    if (RR == 3) return a == 0 ? 1.0 : (a == 1 ? 1.0 - 1.0 / 3.0 : 1.0 - 2.0 / 3.0);
+    return 1.0 - (double)a / (double)r;
+}
 __device__ __forceinline__ double pw_node_all(int i, int j, int r)
 {
     int d = i - r * j;
@@ -253,9 +269,12 @@ __global__ void sxz_matrix_kernel(GridDev<T> F, GridDev<T> C, int r, double *A)
     for (int k = 0; k < 9; k++) A[(int64_t)k * n0 * n1 + q] = a9[k];
 }
 
-template <typename T>
-__device__ double sxz_rhs(const GridDev<T> &F, const GridDev<T> &C, int r, int j0, int j1)
+// RR: the refinement ratio when it is known at compile time (2 or 3), so the
+// loops over the (2r-1)^2 fine points unroll and their loads overlap; 0: r.
+template <typename T, int RR>
+__device__ double sxz_rhs(const GridDev<T> &F, const GridDev<T> &C, int r_, int j0, int j1)
 {
+    const int r = RR ? RR : r_;
     const int nx2 = C.g.nx, ny2 = C.g.ny, nz1 = F.g.nz;
     const T *vx1 = F.f[VX], *sxx1 = F.f[SXX], *sxz1 = F.f[SXZ], *sxy1 = F.f[SXY], *b1 = F.b;
     const T *vx2 = C.f[VX], *sxx2 = C.f[SXX], *sxz2 = C.f[SXZ], *sxy2 = C.f[SXY], *b2 = C.b;
@@ -264,18 +283,22 @@ __device__ double sxz_rhs(const GridDev<T> &F, const GridDev<T> &C, int r, int j
     const double rr = (double)r, r2 = rr * rr, r4 = r2 * r2;
     const int sy1 = F.g.px, sz1 = F.g.px * F.g.py, sy2 = C.g.px;
     double fsum = 0.0;
-    for (int i1 = r * j1 - r + 1; i1 <= r * j1 + r - 1; i1++) {
-        const double wy = pw_node(i1, j1, r, ny2);
+#pragma unroll
+    for (int a1 = 0; a1 < 2 * r - 1; a1++) {
+        const int i1 = r * j1 - r + 1 + a1;
+        const double wy = pw_node_r<RR>(i1, j1, r, ny2);
         const int jy = i1 / r;
-        for (int i0 = r * j0 - r + 1; i0 <= r * j0 + r - 1; i0++) {
-            const double w = pw_node(i0, j0, r, nx2) * wy;
+#pragma unroll
+        for (int a0 = 0; a0 < 2 * r - 1; a0++) {
+            const int i0 = r * j0 - r + 1 + a0;
+            const double w = pw_node_r<RR>(i0, j0, r, nx2) * wy;
             const int jx = i0 / r;
             double ps0 = 0.0;
             for (int ey = 0; ey < 2; ey++)
                 for (int ex = 0; ex < 2; ex++) {
                     const int cx = jx + ex, cy = jy + ey;
                     if (cx > nx2 || cy > ny2) continue;
-                    const double ww = pw_node(i0, cx, r, nx2) * pw_node(i1, cy, r, ny2);
+                    const double ww = pw_node_r<RR>(i0, cx, r, nx2) * pw_node_r<RR>(i1, cy, r, ny2);
                     if (ww != 0.0) ps0 += ww * (double)sxz2[C.g.idx(cx, cy, 0)];
                 }
             const int pf = F.g.idx(i0, i1, nz1);
@@ -381,8 +404,8 @@ __device__ double grid_sum(double v, const SxzWork &W, double *red, bool &ok, in
     return share_total(partial_share(W, round - 1), red);
 }
 
-template <typename T>
-__global__ void __launch_bounds__(256) sxz_solve_kernel(GridDev<T> F, GridDev<T> C, int r, SxzWork W)
+template <typename T, int RR>
+__global__ void __launch_bounds__(256, 4) sxz_solve_kernel(GridDev<T> F, GridDev<T> C, int r, SxzWork W)
 {
     __shared__ double red[32];
     const int nx2 = C.g.nx, ny2 = C.g.ny, nz1 = F.g.nz;
@@ -396,7 +419,7 @@ __global__ void __launch_bounds__(256) sxz_solve_kernel(GridDev<T> F, GridDev<T>
     // B and avg|B| (Array::AvgAbs, array.cpp:172-210)
     double sab = 0.0;
     for (int q = gtid; q < nn; q += gstride) {
-        const double bq = sxz_rhs(F, C, r, q % n0 + 1, q / n0 + 1);
+        const double bq = sxz_rhs<T, RR>(F, C, r, q % n0 + 1, q / n0 + 1);
         W.B[q] = bq;
         sab += fabs(bq);
     }
@@ -470,22 +493,37 @@ __global__ void __launch_bounds__(256) sxz_solve_kernel(GridDev<T> F, GridDev<T>
     }
     const int nx1 = r * nx2, ny1 = r * ny2;
     const int nf = (nx1 - 1) * (ny1 - 1);
-    for (int q = gtid; q < nf; q += gstride) {
-        const int i0 = q % (nx1 - 1) + 1, i1 = q / (nx1 - 1) + 1;
-        const int jx = i0 / r, jy = i1 / r;
-        double acc = 0.0;
-        for (int ey = 0; ey < 2; ey++)
-            for (int ex = 0; ex < 2; ex++) {
-                const int cx = jx + ex, cy = jy + ey;
-                if (cx > nx2 || cy > ny2) continue;
-                const double ww = pw_node(i0, cx, r, nx2) * pw_node(i1, cy, r, ny2);
-                if (ww != 0.0) {
-                    const double xg = (double)(T)__ldcg(Xc + cy * ld + cx);
-                    acc += ww * (xg + (double)sxz2[C.g.idx(cx, cy, 0)]);
+    // the same points per thread (q = gtid + k gstride) in batches of NB: every
+    // load of a batch before its stores, so the loads of a batch overlap
+    constexpr int NB = 4;
+    for (int q0 = gtid; q0 < nf; q0 += NB * gstride) {
+        double val[NB];
+        int pfs[NB];
+#pragma unroll
+        for (int b = 0; b < NB; b++) {
+            const int q = q0 + b * gstride;
+            pfs[b] = -1;
+            val[b] = 0.0;
+            if (q >= nf) continue;
+            const int i0 = q % (nx1 - 1) + 1, i1 = q / (nx1 - 1) + 1;
+            const int jx = i0 / r, jy = i1 / r;
+            double acc = 0.0;
+            for (int ey = 0; ey < 2; ey++)
+                for (int ex = 0; ex < 2; ex++) {
+                    const int cx = jx + ex, cy = jy + ey;
+                    if (cx > nx2 || cy > ny2) continue;
+                    const double ww = pw_node_r<RR>(i0, cx, r, nx2) * pw_node_r<RR>(i1, cy, r, ny2);
+                    if (ww != 0.0) {
+                        const double xg = (double)(T)__ldcg(Xc + cy * ld + cx);
+                        acc += ww * (xg + (double)sxz2[C.g.idx(cx, cy, 0)]);
+                    }
                 }
-            }
-        const int pf = F.g.idx(i0, i1, nz1);
-        sxz1[pf] = (T)(-(double)sxz1[pf - fsz] + acc);
+            pfs[b] = F.g.idx(i0, i1, nz1);
+            val[b] = -(double)sxz1[pfs[b] - fsz] + acc;
+        }
+#pragma unroll
+        for (int b = 0; b < NB; b++)
+            if (pfs[b] >= 0) sxz1[pfs[b]] = (T)val[b];
     }
 }
 
@@ -1300,9 +1338,15 @@ cudaError_t launch_sxz_matrix(const GridDev<T> &F, const GridDev<T> &C, int r, d
 template <typename T>
 int sxz_solve_blocks(int nn, int sms)
 {
-    int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sxz_solve_kernel<T>, 256, 0) != cudaSuccess || per_sm < 1)
+    // the fewest resident CTAs per SM of the three instantiations (any ratio)
+    int per_sm = 0, p2 = 0, p3 = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sxz_solve_kernel<T, 0>, 256, 0) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p2, sxz_solve_kernel<T, 2>, 256, 0) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p3, sxz_solve_kernel<T, 3>, 256, 0) != cudaSuccess)
         per_sm = 1;
+    per_sm = per_sm < p2 ? per_sm : p2;
+    per_sm = per_sm < p3 ? per_sm : p3;
+    if (per_sm < 1) per_sm = 1;
     int want = (nn + 255) / 256;
     int cap = per_sm * sms;
     if (want > cap) want = cap;
@@ -1324,7 +1368,9 @@ cudaError_t launch_sxz_solve(const GridDev<T> &F, const GridDev<T> &C, int r, co
     attr[0].val.cooperative = 1;
     cfg.attrs = attr;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, sxz_solve_kernel<T>, F, C, r, W);
+    if (r == 2) return cudaLaunchKernelEx(&cfg, sxz_solve_kernel<T, 2>, F, C, r, W);
+    if (r == 3) return cudaLaunchKernelEx(&cfg, sxz_solve_kernel<T, 3>, F, C, r, W);
+    return cudaLaunchKernelEx(&cfg, sxz_solve_kernel<T, 0>, F, C, r, W);
 }
 
 

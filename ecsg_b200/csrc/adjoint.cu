@@ -574,7 +574,8 @@ namespace ecsg {
 template <typename T>
 __global__ void rec_sample_kernel(SrcRec S, T *out)
 {
-    for (int i = threadIdx.x; i < S.nrec; i += blockDim.x) out[i] = ((const T *)S.rec_base[S.rec_grid[i]])[S.rec_off[i]];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < S.nrec; i += gridDim.x * blockDim.x)
+        out[i] = ((const T *)S.rec_base[S.rec_grid[i]])[S.rec_off[i]];
 }
 
 // residual = sample - observed (in place), loss += 1/2 sum residual^2 (FP64)
@@ -602,7 +603,8 @@ template <typename T>
 cudaError_t launch_rec_sample(const SrcRec &S, T *out, cudaStream_t st)
 {
     if (S.nrec <= 0) return cudaSuccess;
-    rec_sample_kernel<T><<<1, 256, 0, st>>>(S, out);
+    const int blocks = (S.nrec + 255) / 256 < 1024 ? (S.nrec + 255) / 256 : 1024;
+    rec_sample_kernel<T><<<blocks, 256, 0, st>>>(S, out);
     return cudaGetLastError();
 }
 

@@ -63,6 +63,7 @@ template <typename T>
 cudaError_t launch_avgabs(const GridDev<T> &, int, const int[3], double *, int, double *, cudaStream_t);
 template <typename T>
 cudaError_t launch_src_rec(const SrcRec &, cudaStream_t);
+int src_rec_kernels(int nrec, int mode);
 template <typename T, typename S>
 cudaError_t launch_pack(T *, const Geo &, const S *, int, int, int, int, cudaStream_t);
 template <typename T>
@@ -1371,11 +1372,12 @@ static int run_op(ecsg_sim *s, int n0, int nsteps, float *traces, double *energy
     CK(cudaEventRecord(s->ev[0], s->st));
     long long launches = 0;
     // per step: velocity kernel + 2 mirror kernels and the stress kernel per grid,
-    // the receiver/source kernel, 3 vz + 1 sxz + 1 syz kernels per interface
-    const long long per_step = 4LL * s->ng + 1 + 5LL * (s->ng - 1);
+    // the receiver/source kernel(s), 3 vz + 1 sxz + 1 syz kernels per interface
+    const int srk = src_rec_kernels(s->nrec, 3);
+    const long long per_step = 4LL * s->ng + srk + 5LL * (s->ng - 1);
     for (int n = n0; n < n0 + nsteps; n++) {
         const bool e_step = energy && ((n % every) == 0);
-        launches += per_step + (e_step ? 2LL * s->ng : 0) + (residues ? 1 + 18LL * (s->ng - 1) : 0);
+        launches += per_step + (e_step ? 2LL * s->ng : 0) + (residues ? (2 - srk) + 18LL * (s->ng - 1) : 0);
         if (graphs) {
             cudaError_t e = cudaGraphLaunch(s->gx[e_step ? 1 : 0], s->st);
             if (e != cudaSuccess) { rc = fail(s, ECSG_ERR_CUDA, "graph launch: %s", cudaGetErrorString(e)); break; }
@@ -2060,7 +2062,7 @@ static int batch_run_op(ecsg_sim *const *sims, int n, int n0, int nsteps, float 
     for (int b = 0; b < n; b++) {
         ecsg_sim *x = sims[b];
         x->last_run_ms = ms;
-        x->launches = (long long)nsteps * (4LL * x->ng + 1 + 5LL * (x->ng - 1));
+        x->launches = (long long)nsteps * (4LL * x->ng + src_rec_kernels(x->nrec, 3) + 5LL * (x->ng - 1));
         if (traces && traces[b] && x->nrec > 0)
             CK(cudaMemcpy(traces[b], x->traces, sizeof(float) * (size_t)nsteps * x->nrec, cudaMemcpyDeviceToHost));
     }

@@ -243,6 +243,18 @@ __global__ void sum_partials_kernel(const double *partial, int nblocks, int nter
 // that a captured step replays unchanged; this kernel advances it.
 // ---------------------------------------------------------------------------
 
+// receiver samples of the step (mode 1 part of src_rec_kernel), one thread per receiver
+template <typename T>
+__global__ void rec_trace_kernel(SrcRec S)
+{
+    const int row = *S.step - *S.step0;
+    if (row < 0 || row >= S.trace_cap) return;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < S.nrec; i += gridDim.x * blockDim.x) {
+        const T *base = (const T *)S.rec_base[S.rec_grid[i]];
+        S.traces[(int64_t)row * S.nrec + i] = (float)base[S.rec_off[i]];
+    }
+}
+
 template <typename T>
 __global__ void src_rec_kernel(SrcRec S)
 {
@@ -372,10 +384,25 @@ cudaError_t launch_avgabs(const GridDev<T> &G, int comp, const int pos[3], doubl
     return cudaGetLastError();
 }
 
+// Kernels launched by launch_src_rec for nrec receivers and mode: more than one
+// CTA's worth of receivers are sampled by their own multi-CTA launch, the
+// injection (after the samples: main.cpp samples before it injects) by a second.
+int src_rec_kernels(int nrec, int mode) { return ((mode & 1) && nrec > 256 && (mode & 2)) ? 2 : 1; }
+
 template <typename T>
 cudaError_t launch_src_rec(const SrcRec &S, cudaStream_t st)
 {
-    src_rec_kernel<T><<<1, 256, 0, st>>>(S);
+    if ((S.mode & 1) && S.nrec > 256) {
+        const int blocks = (S.nrec + 255) / 256 < 1024 ? (S.nrec + 255) / 256 : 1024;
+        rec_trace_kernel<T><<<blocks, 256, 0, st>>>(S);
+        if (S.mode & 2) {
+            SrcRec inj = S;
+            inj.mode = 2;
+            src_rec_kernel<T><<<1, 32, 0, st>>>(inj);
+        }
+    } else {
+        src_rec_kernel<T><<<1, 256, 0, st>>>(S);
+    }
     return cudaGetLastError();
 }
 

@@ -578,9 +578,11 @@ __global__ void rec_sample_kernel(SrcRec S, T *out)
         out[i] = ((const T *)S.rec_base[S.rec_grid[i]])[S.rec_off[i]];
 }
 
-// residual = sample - observed (in place), loss += 1/2 sum residual^2 (FP64)
+// residual = sample - observed (in place); each CTA's share of 1/2 sum
+// residual^2 (FP64) into partial[blockIdx.x], summed in CTA order by
+// loss_sum_kernel, so the loss is the same on every run
 template <typename T>
-__global__ void residual_kernel(T *rec, const float *obs, int64_t n, double *loss)
+__global__ void residual_kernel(T *rec, const float *obs, int64_t n, double *partial)
 {
     __shared__ double red[8];
     double s = 0.0;
@@ -595,8 +597,15 @@ __global__ void residual_kernel(T *rec, const float *obs, int64_t n, double *los
     if (threadIdx.x == 0) {
         double t = 0.0;
         for (int w = 0; w < (int)(blockDim.x >> 5); w++) t += red[w];
-        atomicAdd(loss, t);
+        partial[blockIdx.x] = t;
     }
+}
+
+__global__ void loss_sum_kernel(const double *partial, int nblocks, double *loss)
+{
+    double t = 0.0;
+    for (int b = 0; b < nblocks; b++) t += partial[b];
+    *loss = t;
 }
 
 template <typename T>
@@ -609,18 +618,20 @@ cudaError_t launch_rec_sample(const SrcRec &S, T *out, cudaStream_t st)
 }
 
 template <typename T>
-cudaError_t launch_residual(T *rec, const float *obs, int64_t n, double *loss, cudaStream_t st)
+cudaError_t launch_residual(T *rec, const float *obs, int64_t n, double *loss, double *partial, int max_blocks,
+                            cudaStream_t st)
 {
     if (n <= 0) return cudaSuccess;
     int64_t b = (n + 255) / 256;
-    if (b > 1024) b = 1024;
-    residual_kernel<T><<<(unsigned)b, 256, 0, st>>>(rec, obs, n, loss);
+    if (b > max_blocks) b = max_blocks;
+    residual_kernel<T><<<(unsigned)b, 256, 0, st>>>(rec, obs, n, partial);
+    loss_sum_kernel<<<1, 1, 0, st>>>(partial, (int)b, loss);
     return cudaGetLastError();
 }
 
 template cudaError_t launch_rec_sample<float>(const SrcRec &, float *, cudaStream_t);
 template cudaError_t launch_rec_sample<double>(const SrcRec &, double *, cudaStream_t);
-template cudaError_t launch_residual<float>(float *, const float *, int64_t, double *, cudaStream_t);
-template cudaError_t launch_residual<double>(double *, const float *, int64_t, double *, cudaStream_t);
+template cudaError_t launch_residual<float>(float *, const float *, int64_t, double *, double *, int, cudaStream_t);
+template cudaError_t launch_residual<double>(double *, const float *, int64_t, double *, double *, int, cudaStream_t);
 
 } // namespace ecsg

@@ -87,7 +87,7 @@ cudaError_t launch_rec_adj(const RecAdj<T> &, cudaStream_t);
 template <typename T>
 cudaError_t launch_rec_sample(const SrcRec &, T *, cudaStream_t);
 template <typename T>
-cudaError_t launch_residual(T *, const float *, int64_t, double *, cudaStream_t);
+cudaError_t launch_residual(T *, const float *, int64_t, double *, double *, int, cudaStream_t);
 template <typename T>
 cudaError_t launch_ghost_vz_adj(const GridDev<T> &, const GridDev<T> &, const AdjDev<T> &, const AdjDev<T> &, int,
                                 double *, double *, double *, cudaStream_t);
@@ -1923,7 +1923,7 @@ static int misfit_gradient_op(ecsg_sim *s, int nsteps, const float *observed, in
     forward_range.reset();
     NvtxRange backward_range("misfit backward");
     CK(cudaMemsetAsync(s->dscal + 8, 0, sizeof(double), s->st));
-    CK(launch_residual<T>(rec, s->obs, (int64_t)nobs, s->dscal + 8, s->st));
+    CK(launch_residual<T>(rec, s->obs, (int64_t)nobs, s->dscal + 8, s->partial, 12 * s->red_blocks, s->st));
     // backward, segment by segment: recompute the segment's states, then reverse its steps
     GridDev<T> Ga[kMaxGrids], Gb[kMaxGrids];
     RecAdj<T> R;

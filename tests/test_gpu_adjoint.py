@@ -211,3 +211,25 @@ def test_torch_autograd_function_returns_the_device_gradient():
         for w in range(22):
             got = medium[g][w].grad.numpy()
             assert np.abs(got - want[g][w]).max() <= 1e-10 * max(np.abs(want[g][w]).max(), 1e-300)
+
+
+def test_misfit_loss_is_the_same_on_every_run():
+    """The loss over many receiver samples (blocks of the residual kernel
+    summed in a fixed order): identical on repeated runs, and equal to the sum
+    of the squared device residuals to round-off."""
+    nsteps = 40
+    case = _loop_case(13, 2, 1, nsteps)
+    h, n = case.grids[0]["h"], case.grids[0]["n"]
+    xs, ys = np.meshgrid(np.arange(1, n[0] - 1), np.arange(1, n[1] - 1), indexing="ij")
+    case.rec = np.stack([xs.ravel() * h[0], ys.ravel() * h[1], np.full(xs.size, 1 * h[2])], axis=1).astype(np.float32)
+    obs = (1e-3 * np.random.default_rng(5).standard_normal((nsteps, len(case.rec)))).astype(np.float32)
+    assert obs.size > 256 * 8
+    losses = []
+    for _ in range(3):
+        with Simulation(case, precision="f32") as sim:
+            losses.append(sim.misfit_gradient(obs, ckpt_every=10))
+    assert losses[0] == losses[1] == losses[2], losses
+    with Simulation(case, precision="f32") as sim:
+        rec = sim.run(nsteps)["rec"].astype(np.float64)
+    want = 0.5 * float(np.sum((rec.T - obs.astype(np.float64)) ** 2))
+    assert abs(losses[0] - want) <= 1e-5 * abs(want), (losses[0], want)

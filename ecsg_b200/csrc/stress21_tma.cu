@@ -111,8 +111,8 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 2)
     auto fullV = [&](int s) { return bar0 + 8u * (2 * NSP + s); };
     auto emptyV = [&](int s) { return bar0 + 8u * (2 * NSP + NSV + s); };
     // [0] producer gave up, [1] P stages consumed, [2] V stages consumed, [3 + (i & 1)]
-    // consumers gave up on plane stage i.  A consumer sets it before the plane's
-    // one consumer barrier and every consumer reads it right after that barrier;
+    // consumers gave up on plane stage i.  A consumer sets it before the stage's
+    // first consumer barrier and every consumer reads it right after that barrier;
     // no consumer can reach stage i + 2 (same word) before all have passed the
     // barrier of stage i + 1, so every consumer takes the same branch.
     volatile int *flags = (volatile int *)(sm + OFF_FLAG);
@@ -434,8 +434,8 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 2)
             consumedV = i + 3;
 
             // displacement sums: U += v at this thread's point (x <= nx, y <= ny)
-            // of an inner plane, the x = -1 / y = -1 face points beside it, and
-            // the z = -1 point below it on the first plane of the grid
+            // of an inner plane and of plane -1 (the grid's first stage), and
+            // on inner planes the x = -1 / y = -1 face points beside it
             if (ACC && (inner || p == -1) && ox <= nx && oy <= ny) {
                 const int pp = pbase + p * sz;
                 u0[pp] = add_(EP[0 * IS + ib], Vp[0 * HS + vb]);

@@ -41,7 +41,7 @@ __device__ __forceinline__ void block_sums(double (&v)[N], double *partial, int 
 // evaluated by the stress update's own strain functions on a copy of the grid
 // whose velocities are U (GU), e3 condensed on a free surface (flag).
 template <typename T>
-__global__ void __launch_bounds__(RED_THREADS) energy_kernel(GridDev<T> G, int medium, const T *vc0, const T *vc1,
+__global__ void __launch_bounds__(RED_THREADS, 3) energy_kernel(GridDev<T> G, int medium, const T *vc0, const T *vc1,
                                                             const T *vc2, GridDev<T> GU, int flag, double *partial)
 {
     const Geo &g = G.g;
@@ -359,8 +359,13 @@ cudaError_t launch_energy(const GridDev<T> &G, int medium, T *const vc[3], T *co
     GridDev<T> GU = G;
     for (int k = 0; k < 3; k++) GU.f[VX + k] = disp ? disp[k] : nullptr;
     if (medium == MED_GEN21 && !GU.f[VX]) return cudaErrorInvalidValue;
-    energy_kernel<T><<<nblocks, RED_THREADS, 0, st>>>(G, medium, vc[0], vc[1], vc[2], GU, flag, partial);
-    energy_finalize_kernel<<<1, 32, 0, st>>>(partial, nblocks, h0, h1, h2, out, step, step0, first, status,
+    // one wave: three CTAs per SM (the kernel's launch bounds), at most nblocks
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int eb = (sms > 0 && 3 * sms < nblocks) ? 3 * sms : nblocks;
+    energy_kernel<T><<<eb, RED_THREADS, 0, st>>>(G, medium, vc[0], vc[1], vc[2], GU, flag, partial);
+    energy_finalize_kernel<<<1, 32, 0, st>>>(partial, eb, h0, h1, h2, out, step, step0, first, status,
                                              medium == MED_GEN21);
     return cudaGetLastError();
 }

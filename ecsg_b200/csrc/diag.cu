@@ -51,10 +51,22 @@ __global__ void __launch_bounds__(RED_THREADS, 3) energy_kernel(GridDev<T> G, in
     double acc[12];
 #pragma unroll
     for (int k = 0; k < 12; k++) acc[k] = 0.0;
+    // point index -> (x, y, z) with two 32-bit divisions when the grid has
+    // fewer than 2^32 points (64-bit ones are long instruction sequences)
+    const bool idx32 = npts <= 0xffffffffLL;
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < npts; t += (int64_t)gridDim.x * blockDim.x) {
-        const int x = (int)(t % (nx + 1));
-        const int y = (int)((t / (nx + 1)) % (ny + 1));
-        const int z = (int)(t / ((int64_t)(nx + 1) * (ny + 1)));
+        int x, y, z;
+        if (idx32) {
+            const unsigned u = (unsigned)t, a = (unsigned)(nx + 1), b = (unsigned)(ny + 1);
+            const unsigned qa = u / a, qb = qa / b;
+            x = (int)(u - qa * a);
+            y = (int)(qa - qb * b);
+            z = (int)qb;
+        } else {
+            x = (int)(t % (nx + 1));
+            y = (int)((t / (nx + 1)) % (ny + 1));
+            z = (int)(t / ((int64_t)(nx + 1) * (ny + 1)));
+        }
         const int p = g.idx(x, y, z);
         const double mx = (x == 0 || x == nx) ? 0.5 : 1.0;
         const double my = (y == 0 || y == ny) ? 0.5 : 1.0;

@@ -108,6 +108,7 @@ SIGNATURES = [
     ("ecsg_ghost_sxz_noalloc", ctypes.c_int, [ctypes.POINTER(GridView), ctypes.POINTER(GridView), ctypes.c_double,
                                               ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, c_ip,
                                               ctypes.c_char_p, ctypes.c_size_t]),
+    ("ecsg_ghost_sxz_noalloc_status", ctypes.c_int, [ctypes.c_void_p, c_ip, ctypes.c_int]),
     ("ecsg_synchronize", ctypes.c_int, [ctypes.c_void_p]),
     ("ecsg_get_status", ctypes.c_int, [ctypes.c_void_p, c_ip, ctypes.c_int]),
     ("ecsg_device_bytes", ctypes.c_longlong, [ctypes.c_void_p]),

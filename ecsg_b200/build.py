@@ -98,14 +98,25 @@ def build_cli():
 
 def build_oracle():
     """Test-side checkers: the C restatement always; the reference build
-    (oracle/_ref) only where the reference sources are mounted, including the
-    reference driver linked through ecsg_b200/shim (build_lib first)."""
+    (oracle/_ref) only where the reference sources are found (reference_dir),
+    including the reference driver linked through ecsg_b200/shim (build_lib
+    first)."""
     mk = os.path.join(ROOT, "oracle")
     subprocess.check_call(["make", "-s", "-C", mk, "oracle"])
-    if os.path.isdir("/root/reference"):
-        subprocess.check_call(["make", "-s", "-C", mk, "ref"])
+    ref = reference_dir()
+    if ref:
+        subprocess.check_call(["make", "-s", "-C", mk, "ref", "REF=" + ref])
         # the reference driver linked against the shim and the library (needs LIB)
-        subprocess.check_call(["make", "-s", "-C", mk, "shim"])
+        subprocess.check_call(["make", "-s", "-C", mk, "shim", "REF=" + ref])
+
+
+def reference_dir():
+    """The reference checkout: $ECSG_REFERENCE, else a checkout named
+    "reference" beside this repository; None when neither exists."""
+    for d in (os.environ.get("ECSG_REFERENCE"), os.path.join(os.path.dirname(ROOT), "reference")):
+        if d and os.path.isfile(os.path.join(d, "main.cpp")):
+            return os.path.abspath(d)
+    return None
 
 
 if __name__ == "__main__":

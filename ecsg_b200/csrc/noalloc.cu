@@ -16,12 +16,19 @@
 //
 // Calls share the array and it keeps the last call's contents.  Each call
 // clears the parts that must start at zero (the second iterate, whose border
-// must be zero, and the barrier and status words) before it launches; the
-// matrix and right-hand side are rebuilt every call.  Calls that overlap on
+// must be zero, and the barrier and per-call status words) before it launches;
+// the matrix and right-hand side are rebuilt every call.  Calls that overlap on
 // the GPU (from two streams, or two host threads) race on the array.
+//
+// A call that does not wait (iters == NULL) cannot return the solve's outcome.
+// So every call also ORs its per-call status bits into a sticky word of the
+// array, which no call clears; ecsg_ghost_sxz_noalloc_status reads it (and
+// clears it on request) once the caller's stream has drained.
 #include "ecsg_device.cuh"
 #include "../../include/ecsg_b200.h"
 
+#include <climits>
+#include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <mutex>
@@ -53,13 +60,23 @@ constexpr size_t kOffWords = kOffPartial + align256(kMaxBlocks * sizeof(double))
 constexpr size_t kWordsBytes = 64;
 constexpr size_t kOffBar = kOffWords + align256(kWordsBytes);   // grid-barrier words
 constexpr size_t kBarBytes = kBarWords * sizeof(unsigned);
-constexpr size_t kScratchBytes = kOffBar + align256(kBarBytes);
+// sticky status: the OR of every call's status bits since the last clear
+constexpr size_t kOffSticky = kOffBar + align256(kBarBytes);
+constexpr size_t kScratchBytes = kOffSticky + 256;
 static_assert(kScratchBytes < (16u << 20), "scratch must stay modest");
 
 constexpr int kMaxDevices = 64;
 } // namespace
 
 static __device__ __align__(256) unsigned char g_sxz_scratch[kScratchBytes];
+
+// One thread: sticky |= this call's status (device code names the array itself).
+__global__ void latch_status_kernel()
+{
+    int *sticky = (int *)(g_sxz_scratch + kOffSticky);
+    const int st = *(const int *)(g_sxz_scratch + kOffWords + 32);
+    if (st) *sticky |= st;
+}
 
 static void *scratch_address(int device, cudaError_t *err)
 {
@@ -81,6 +98,27 @@ static int report(char *errbuf, size_t errlen, int code, const char *msg)
     if (errbuf && errlen) snprintf(errbuf, errlen, "%s", msg);
     fprintf(stderr, "ecsg_ghost_sxz_noalloc: %s\n", msg);
     return code;
+}
+
+// The layout of a view must hold every element the kernels may index: x, y, z
+// in [-radius, size + radius] inside the box the pitches span, with 32-bit
+// indices (the kernels' index type).  Returns why not, or NULL.
+static const char *check_view(const ecsg_grid_view *v)
+{
+    const long long R = v->radius;
+    for (int d = 0; d < 3; d++) {
+        if (v->size[d] < 1 || !(v->step[d] > 0)) return "grid view: size must be >= 1 and step > 0";
+        if ((long long)v->pitch[d] < v->size[d] + 1 + 2 * R) return "grid view: pitch[d] must be >= size[d] + 1 + 2 * radius";
+    }
+    for (int k = 0; k < 9; k++)
+        if (!v->field[k]) return "grid view: null field pointer";
+    if (!v->buoy) return "grid view: null buoyancy pointer";
+    const long long px = v->pitch[0], py = v->pitch[1], pz = v->pitch[2];
+    const long long lo = v->origin - R * (px * py + px + 1);
+    const long long hi = v->origin + ((v->size[2] + R) * py + v->size[1] + R) * px + v->size[0] + R;
+    if (lo < 0 || hi >= px * py * pz) return "grid view: origin puts the halo outside the box of the pitches";
+    if (px * py * pz > (long long)INT_MAX) return "grid view: box larger than 32-bit indexing";
+    return nullptr;
 }
 
 template <typename T>
@@ -144,6 +182,8 @@ static int solve(const ecsg_grid_view *fine, const ecsg_grid_view *coarse, int r
     W.iters = (int *)(w + 36);
     W.max_iter = max_iter > 0 ? max_iter : 10000;
     if ((e = launch_sxz_solve<T>(F, C, r, W, nblocks, st)) != cudaSuccess) return report(errbuf, errlen, ECSG_ERR_CUDA, cudaGetErrorString(e));
+    latch_status_kernel<<<1, 1, 0, st>>>();
+    if ((e = cudaGetLastError()) != cudaSuccess) return report(errbuf, errlen, ECSG_ERR_CUDA, cudaGetErrorString(e));
     if (iters) {
         int hv[2] = {0, 0};
         if ((e = cudaMemcpyAsync(hv, W.status, sizeof hv, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
@@ -162,9 +202,14 @@ int ecsg_ghost_sxz_noalloc(const ecsg_grid_view *fine, const ecsg_grid_view *coa
     if (!fine || !coarse || !X || !(dt > 0)) return report(errbuf, errlen, ECSG_ERR_INVALID, "null argument or dt <= 0");
     if (precision != ECSG_F32 && precision != ECSG_F64) return report(errbuf, errlen, ECSG_ERR_INVALID, "precision");
     if (fine->radius != 1 || coarse->radius != 1) return report(errbuf, errlen, ECSG_ERR_INVALID, "radius must be 1");
+    for (const ecsg_grid_view *v : {fine, coarse})
+        if (const char *why = check_view(v)) return report(errbuf, errlen, ECSG_ERR_INVALID, why);
+    // the same ratio rules as ecsg_create: an integer >= 2, equal in x and y
     const double rx = coarse->step[0] / fine->step[0];
-    const int r = (int)(rx + 0.5);
-    if (r < 2 || fine->size[0] != r * coarse->size[0] || fine->size[1] != r * coarse->size[1])
+    const int r = (int)std::lround(rx);
+    if (r < 2 || fabs(rx - r) > 1e-6 * r || fabs(coarse->step[1] / fine->step[1] - r) > 1e-6 * r)
+        return report(errbuf, errlen, ECSG_ERR_INVALID, "x/y refinement ratio must be an integer >= 2");
+    if (fine->size[0] != r * coarse->size[0] || fine->size[1] != r * coarse->size[1])
         return report(errbuf, errlen, ECSG_ERR_INVALID, "fine size must be ratio * coarse size in x and y");
     const size_t nn = (size_t)(coarse->size[0] - 1) * (coarse->size[1] - 1);
     const size_t nodes = (size_t)(coarse->size[0] + 1) * (coarse->size[1] + 1);
@@ -179,4 +224,22 @@ int ecsg_ghost_sxz_noalloc(const ecsg_grid_view *fine, const ecsg_grid_view *coa
     cudaStream_t st = (cudaStream_t)stream;
     return precision == ECSG_F32 ? solve<float>(fine, coarse, r, dt, X, max_iter, st, iters, errbuf, errlen)
                                  : solve<double>(fine, coarse, r, dt, X, max_iter, st, iters, errbuf, errlen);
+}
+
+int ecsg_ghost_sxz_noalloc_status(void *stream, int *status, int clear)
+{
+    if (!status) return report(nullptr, 0, ECSG_ERR_INVALID, "status: null pointer");
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) return report(nullptr, 0, ECSG_ERR_NO_DEVICE, "no current CUDA device");
+    unsigned char *base = (unsigned char *)scratch_address(dev, &e);
+    if (!base) return report(nullptr, 0, ECSG_ERR_CUDA, cudaGetErrorString(e));
+    cudaStream_t st = (cudaStream_t)stream;
+    int v = 0;
+    if ((e = cudaMemcpyAsync(&v, base + kOffSticky, sizeof v, cudaMemcpyDeviceToHost, st)) != cudaSuccess ||
+        (clear && (e = cudaMemsetAsync(base + kOffSticky, 0, sizeof(int), st)) != cudaSuccess) ||
+        (e = cudaStreamSynchronize(st)) != cudaSuccess)
+        return report(nullptr, 0, ECSG_ERR_CUDA, cudaGetErrorString(e));
+    *status = v;
+    return ECSG_OK;
 }

@@ -246,7 +246,19 @@ int ecsg_time_kernels(ecsg_sim *sim, int nsteps, double *ms);
  * cudaStream_t (NULL: the legacy default stream); the call is asynchronous
  * unless iters is non-null, in which case it waits for the solve and returns
  * ECSG_ERR_NOT_CONVERGED when the sweep cap was hit.  errbuf (may be NULL)
- * receives the message of a failure.
+ * receives the message of a failure.  The views are checked before anything
+ * runs: the x and y step ratios must be the same integer >= 2 (as in
+ * ecsg_create), fine sizes ratio * coarse sizes in x and y, pitches at least
+ * size + 1 + 2 * radius, and the halo of every component inside the box the
+ * pitches span with 32-bit indices; a view that fails is ECSG_ERR_INVALID.
+ *
+ * An asynchronous call (iters == NULL) cannot return the solve's outcome, so
+ * every call ORs its device status bits (ECSG_ST_JACOBI_CAP: the sweep cap
+ * was hit and X holds the last iterate; ECSG_ST_BARRIER_TIMEOUT: a grid
+ * barrier gave up) into a sticky word of the static array that no solve
+ * clears.  ecsg_ghost_sxz_noalloc_status waits for stream, returns that word
+ * of the current device in *status and, when clear is non-zero, resets it.
+ * It allocates nothing either.
  * ------------------------------------------------------------------------- */
 #define ECSG_NOALLOC_MAX_UNKNOWNS 131072
 #define ECSG_NOALLOC_MAX_NODES 132496
@@ -265,6 +277,7 @@ typedef struct ecsg_grid_view {
 
 int ecsg_ghost_sxz_noalloc(const ecsg_grid_view *fine, const ecsg_grid_view *coarse, double dt, int precision,
                            double *X, int max_iter, void *stream, int *iters, char *errbuf, size_t errlen);
+int ecsg_ghost_sxz_noalloc_status(void *stream, int *status, int clear);
 
 int ecsg_synchronize(ecsg_sim *sim);
 /* Device status bits accumulated since the last clear (ECSG_ST_*). */

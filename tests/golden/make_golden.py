@@ -5,8 +5,9 @@ The reference keeps its experiment results only in its SVN working-copy store:
 holds the bytes.  The *.hh files are RSF "header + data" files: a text header of
 key=value lines, the separator bytes 0x0c 0x0c 0x04, then little-endian float32.
 
-Run once in a container where the reference is mounted:
-    python tests/golden/make_golden.py /root/reference
+Run once where the reference checkout is available:
+    python tests/golden/make_golden.py <reference checkout>
+(or with $ECSG_REFERENCE naming the checkout).
 Writes tests/golden/<name>.npy (float32, shape (n2, n1): one row per receiver)
 and tests/golden/golden_index.json (headers and provenance).
 """
@@ -62,4 +63,7 @@ def main(ref_root):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("ECSG_REFERENCE")
+    if not ref:
+        sys.exit("usage: make_golden.py <reference checkout>  (or set ECSG_REFERENCE)")
+    main(ref)

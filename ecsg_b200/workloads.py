@@ -115,6 +115,39 @@ def eci_test_case(test=1, imode=1, nsteps=None):
                 rec=rec, rec_comp=0)
 
 
+def config1_case(ratio=3, nsteps=1500, fpeak=10.0, cfl=0.9):
+    """The plain two-grid composite of the benchmark's accuracy configuration:
+    fine top grid 91 x 91 x 31 points at 10 m (depth 0-300 m) over a coarse
+    grid at 10 * ratio m reaching 1500 m (ratio 3: 31 x 31 x 41 points; the
+    ratio-2 twin: 46 x 46 x 61), domain 900 x 900 m.  Isotropic media: top
+    vp 1000, vs 500 m/s, rho 1800 kg/m^3; bottom vp 3000, vs 1700, rho 2300
+    (in the reference tests' units m, ms, m/ms, g/cm^3: eci/SConstruct:34-40,
+    buoy = 1/rho, s11 = rho vp^2, s13 = s11 - 2 rho vs^2).  Free surface,
+    rigid sides and bottom.  A 10 Hz Ricker vz point force at (450, 450,
+    150 m); dt = cfl * h / vmax / sqrt(3); 91 vz receivers on the surface
+    line y = 450 m, x = 0, 10, ..., 900 m."""
+    top = {"rho": 1.8, "cs": 0.5, "cp": 1.0}
+    bot = {"rho": 2.3, "cs": 1.7, "cp": 3.0}
+    for L in (top, bot):
+        L["buoy"] = 1.0 / L["rho"]
+        L["s11"] = L["rho"] * L["cp"] ** 2
+        L["s13"] = L["s11"] - 2 * L["rho"] * L["cs"] ** 2
+    h1, h2 = 10.0, 10.0 * ratio
+    g1 = {"n": (90, 90, 30), "h": (h1,) * 3}
+    g2 = {"n": (90 // ratio, 90 // ratio, int(round(1200.0 / h2))), "h": (h2,) * 3}
+    media = []
+    for g, L in ((g1, top), (g2, bot)):
+        n = g["n"]
+        media.append({k: np.full((n[2] + 1, n[1] + 1, n[0] + 1), np.float32(L[k]), dtype=np.float32)
+                      for k in ("buoy", "s11", "s13")})
+    dt = cfl * h1 / bot["cp"] / math.sqrt(3)
+    rec = np.array([[10.0 * i, 450.0, 0.0] for i in range(91)], dtype=np.float32)
+    return Case(name="config1_r%d" % ratio, grids=[g1, g2], media=media, medium="iso", dt=dt, nsteps=nsteps,
+                radius=1, top_bc=1, imode=1,
+                src={"xyz": (450.0, 450.0, 150.0), "trace": ricker(nsteps, dt * 1e-3, fpeak), "scale": 1.0, "comp": 2},
+                rec=rec, rec_comp=2)
+
+
 def random_case(seed, ratio=2, nx2=6, ny2=5, nz=(5, 4), radius=1, top_bc=1, num_grids=2, h1=10.0):
     """Small heterogeneous isotropic composite with random fields, for operator tests."""
     rng = np.random.default_rng(seed)
@@ -440,13 +473,16 @@ def random_case_tti(seed, ratio=2, nx2=6, ny2=5, nz=(5, 4), top_bc=1, num_grids=
 ADJOINT_GRIDS = [((360, 360, 60), 10.0), ((120, 120, 80), 30.0)]
 
 
-def two_grid_adjoint_case(seed=0, shot=0, nsteps=1500, blob=False, grids=None, fpeak=10.0, cfl=0.9):
+def two_grid_adjoint_case(seed=0, shot=0, nsteps=1500, blob=False, grids=None, fpeak=10.0, cfl=0.9,
+                          blob_depth=500.0, blob_radius=150.0):
     """Two grids at ratio 3 (default 361x361x61 @ 10 m over 121x121x81 @ 30 m,
     9,135,502 points), the smooth seeded model of three_grid_model made
     orthorhombic (VTI with a vertical axis: Thomsen TTI_THOMSEN, dip 0), free
     surface, one of 16 shots on a 4 x 4 surface grid (Ricker vz force), vz
-    receivers on a 121 x 121 surface grid.  blob: the observed-data model, vs
-    raised by a 3 % Gaussian (radius 150 m) centred at 500 m depth."""
+    receivers on a surface grid of every third fine node (121 x 121 by
+    default).  blob: the observed-data model, vs raised by a 3 % Gaussian
+    (radius blob_radius, default 150 m) centred at blob_depth (500 m) below
+    the middle of the surface."""
     grids = grids or ADJOINT_GRIDS
     model = three_grid_model(seed, grids)
     n0, h0 = grids[0]
@@ -459,9 +495,9 @@ def two_grid_adjoint_case(seed=0, shot=0, nsteps=1500, blob=False, grids=None, f
         if blob:
             x = np.arange(n[0] + 1) * h - lx / 2
             y = np.arange(n[1] + 1) * h - ly / 2
-            z = z0 + np.arange(n[2] + 1) * h - 500.0
+            z = z0 + np.arange(n[2] + 1) * h - blob_depth
             r2 = z[:, None, None] ** 2 + y[None, :, None] ** 2 + x[None, None, :] ** 2
-            vs = (vs * (1 + 0.03 * np.exp(-r2 / (2 * 150.0 ** 2)))).astype(np.float32)
+            vs = (vs * (1 + 0.03 * np.exp(-r2 / (2 * blob_radius ** 2)))).astype(np.float32)
         zero = np.zeros_like(m["vp"])
         media.append({"vp": m["vp"], "vs": vs, "rho": m["rho"], "dip": zero, "azi": zero})
         vmax = max(vmax, float(m["vp"].max()) * math.sqrt(1 + 2 * TTI_THOMSEN[0]))

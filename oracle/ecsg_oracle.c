@@ -535,6 +535,12 @@ static void sxz_assemble(ogrid *g1, ogrid *g2, int r, double *A, double *B)
         }
 }
 
+/* Sweeps every solve takes at least (0: the reference rule alone).  The
+ * differentiated oracle (adjoint_ad.cpp) sets it so that each solve converges
+ * to rounding and its derivative is that of X = A^-1 B, not of a truncated
+ * iteration from the warm start. */
+int o_jacobi_min_sweeps = 0;
+
 int o_jacobi2d(double *X, const double *A, const double *B, int n0, int n1,
                double tol, double *Xt, int max_iter)
 {
@@ -570,7 +576,7 @@ int o_jacobi2d(double *X, const double *A, const double *B, int n0, int n1,
             }
         nrm = sqrt(s);
         it++;
-    } while (nrm > tol && (max_iter <= 0 || it < max_iter));
+    } while ((nrm > tol || it < o_jacobi_min_sweeps) && (max_iter <= 0 || it < max_iter));
     return it;
 }
 

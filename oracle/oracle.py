@@ -360,7 +360,8 @@ class OracleRun:
             self.copy_vel()
         for g in range(ng):
             self.update_vel(g)
-        rec = np.array([self.levels[g]["f"][0][iz + self.R, iy + self.R, ix + self.R]
+        rc = getattr(self.case, "rec_comp", 0)   # the sampled component (main.cpp:182-184 samples vx)
+        rec = np.array([self.levels[g]["f"][rc][iz + self.R, iy + self.R, ix + self.R]
                         for (g, ix, iy, iz) in self.rec])
         if residues:
             for i in range(1, ng):

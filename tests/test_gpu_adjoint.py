@@ -14,6 +14,17 @@
   device forward (FP64) and of the FP64 CPU oracle along random medium
   directions (1e-5 relative), independent of the checkpoint interval, and the
   FP32 gradient within 2e-3 of the FP64 one.
+* Against the FP64 CPU adjoint (oracle/adjoint_ad.cpp, reverse-mode
+  differentiation of the oracle's own loop): the device FP64 gradient equals
+  it element by element to 1e-10 of the gradient's scale, on random 21-Cij
+  composites (ratio 2 and 3, free surface and rigid top) and on a reduced
+  copy of the shot-gradient workload (10 m over 30 m at ratio 3, smooth
+  orthorhombic model, vz source and surface vz receivers, observed data from
+  the same model with a 3 % vs blob).
+* Central differences along 20 seeded random directions of the buoyancy and
+  all 21 slots: the FP64 device gradient within 1e-6, the FP32 device
+  gradient within 1e-3 (both relative to the difference quotient, which is
+  taken on the FP64 forward).
 """
 import copy
 import zlib
@@ -22,7 +33,8 @@ import numpy as np
 import pytest
 
 from ecsg_b200 import SIM_POS, Simulation, field_shape
-from ecsg_b200.workloads import CIJ21_POS, random_case_gen21, ricker
+from ecsg_b200.workloads import CIJ21_POS, random_case_gen21, ricker, tti_as_gen21, two_grid_adjoint_case
+from oracle.adjoint import misfit_gradient as cpu_adjoint
 from oracle.oracle import OracleRun
 
 pytestmark = pytest.mark.gpu
@@ -233,3 +245,82 @@ def test_misfit_loss_is_the_same_on_every_run():
         rec = sim.run(nsteps)["rec"].astype(np.float64)
     want = 0.5 * float(np.sum((rec.T - obs.astype(np.float64)) ** 2))
     assert abs(losses[0] - want) <= 1e-5 * abs(want), (losses[0], want)
+
+
+def _assert_equal_to_cpu_adjoint(g_dev, g_cpu, tol=1e-10):
+    """Element by element, relative to the largest gradient entry of the grid
+    (the slots' gradients differ by orders of magnitude between positions)."""
+    for g in range(len(g_cpu)):
+        scale = max(float(np.abs(a).max()) for a in g_cpu[g])
+        assert scale > 0
+        for w in range(22):
+            err = float(np.abs(g_dev[g][w] - g_cpu[g][w]).max())
+            assert err <= tol * scale, (g, w, err / scale)
+
+
+@pytest.mark.parametrize("ratio,top_bc", [(2, 1), (3, 0), (3, 1)])
+def test_device_gradient_equals_fp64_cpu_adjoint(ratio, top_bc):
+    nsteps = 30
+    case = _loop_case(21 + ratio, ratio, top_bc, nsteps)
+    rng = np.random.default_rng(100 + ratio)
+    obs = (0.1 * rng.standard_normal((nsteps, len(case.rec)))).astype(np.float32)
+    loss_cpu, g_cpu, _ = cpu_adjoint(case, obs)
+    with Simulation(case, precision="f64") as sim:
+        loss = sim.misfit_gradient(obs, ckpt_every=7)
+        g_dev = [[sim.gradient(g, w) for w in range(22)] for g in range(2)]
+    assert abs(loss - loss_cpu) <= 1e-12 * loss
+    _assert_equal_to_cpu_adjoint(g_dev, g_cpu)
+
+
+def _reduced_shot_case(nsteps):
+    """The shot-gradient workload's set-up at a reduced size: 19 x 19 x 11
+    points at 10 m over 7 x 7 x 9 at 30 m (ratio 3), the smooth orthorhombic
+    model, shot 5 of the 4 x 4 grid (vz force), surface vz receivers every
+    third fine node; observed data from the blob model with the blob scaled
+    into this volume (3 % vs, radius 40 m at 60 m depth)."""
+    grids = [((18, 18, 10), 10.0), ((6, 6, 8), 30.0)]
+    kw = dict(grids=grids, fpeak=40.0)
+    case = tti_as_gen21(two_grid_adjoint_case(0, 5, nsteps, blob=False, **kw))
+    truth = tti_as_gen21(two_grid_adjoint_case(0, 5, nsteps, blob=True, blob_depth=60.0, blob_radius=40.0, **kw))
+    with Simulation(truth, precision="f64") as sim:
+        obs = sim.run(nsteps, graph=False)["rec"].T.copy()
+    return case, obs
+
+
+def test_reduced_shot_workload_gradient_equals_cpu_adjoint():
+    nsteps = 40
+    case, obs = _reduced_shot_case(nsteps)
+    loss_cpu, g_cpu, _ = cpu_adjoint(case, obs)
+    assert loss_cpu > 0
+    with Simulation(case, precision="f64") as sim:
+        loss = sim.misfit_gradient(obs, ckpt_every=10)
+        g_dev = [[sim.gradient(g, w) for w in range(22)] for g in range(2)]
+    assert abs(loss - loss_cpu) <= 1e-12 * loss
+    _assert_equal_to_cpu_adjoint(g_dev, g_cpu)
+
+
+@pytest.mark.parametrize("which", ["random", "reduced_shot"])
+def test_gradients_on_twenty_directions(which):
+    """FP64 within 1e-6 and FP32 within 1e-3 of central differences of the
+    FP64 device forward, on 20 seeded directions."""
+    nsteps = 30 if which == "random" else 40
+    if which == "random":
+        case = _loop_case(41, 3, 1, nsteps)
+        obs = (0.1 * np.random.default_rng(41).standard_normal((nsteps, len(case.rec)))).astype(np.float32)
+    else:
+        case, obs = _reduced_shot_case(nsteps)
+    grads = {}
+    for prec in ("f64", "f32"):
+        with Simulation(case, precision=prec) as sim:
+            sim.misfit_gradient(obs, ckpt_every=10)
+            grads[prec] = [[sim.gradient(g, w) for w in range(22)] for g in range(2)]
+    rng = np.random.default_rng(2024)
+    worst = {"f64": 0.0, "f32": 0.0}
+    for trial in range(20):
+        dirs = _directions(case, rng)
+        eps = 1e-4
+        fd = (_loss(_perturbed(case, dirs, eps), obs) - _loss(_perturbed(case, dirs, -eps), obs)) / (2 * eps)
+        for prec in ("f64", "f32"):
+            worst[prec] = max(worst[prec], abs(_gdot(grads[prec], dirs) - fd) / abs(fd))
+    assert worst["f64"] <= 1e-6, worst
+    assert worst["f32"] <= 1e-3, worst

@@ -53,6 +53,10 @@ template <typename T>
 int sxz_solve_blocks(int, int);
 template <typename T>
 cudaError_t launch_sxz_solve(const GridDev<T> &, const GridDev<T> &, int, const SxzWork &, int, cudaStream_t);
+template <typename T>
+int sxz_multi_capacity(int);
+template <typename T>
+cudaError_t launch_sxz_solve_multi(const SxzSysList<T> &, cudaStream_t);
 // diag.cu
 template <typename T>
 cudaError_t launch_energy(const GridDev<T> &, int, T *const[3], T *const[3], int, double *, int, double, double, double,
@@ -157,6 +161,11 @@ struct ecsg_sim {
     // sweeps, so the coarse grids' sweeps run beside the fine grid's and fill
     // the SMs its last wave leaves idle.
     bool side_grids = true;
+    // The sxz solves of all interfaces of a step in one cooperative launch
+    // (each interface bitwise as in its own launch), when their CTAs fit
+    // co-resident (sxz_cap); otherwise one launch per interface.
+    bool sxz_fused = true;
+    int sxz_cap = 0;
     cudaStream_t side[kMaxGrids] = {};
     cudaEvent_t fork_ev = nullptr, join_ev[kMaxGrids] = {};
     // adjoint state (allocated on first use): adjoint fields, gradients, work boxes
@@ -326,6 +335,10 @@ static int create_impl(const ecsg_grid_desc *grids, const ecsg_config *cfg, ecsg
         const char *env = getenv("ECSG_SIDE_GRIDS");   // "0": every sweep on the one stream
         s->side_grids = !(env && env[0] == '0');
     }
+    {
+        const char *env = getenv("ECSG_SXZ_FUSED");    // "0": one sxz launch per interface
+        s->sxz_fused = !(env && env[0] == '0');
+    }
     s->tsize = s->prec == ECSG_F32 ? 4 : 8;
     s->nc = s->medium == ECSG_MEDIUM_ISO ? 5 : (s->medium == ECSG_MEDIUM_ORTHO9 ? 9 : 21);
     if (cudaSetDevice(s->device) != cudaSuccess) { fail(s, ECSG_ERR_NO_DEVICE, "cudaSetDevice(%d) failed", s->device); return bail(ECSG_ERR_NO_DEVICE); }
@@ -409,6 +422,8 @@ static int create_impl(const ecsg_grid_desc *grids, const ecsg_config *cfg, ecsg
         if ((rc = dmalloc(s, (void **)&I.X0, sizeof(double) * nxy))) return bail(rc);
         if ((rc = dmalloc(s, (void **)&I.X1, sizeof(double) * nxy))) return bail(rc);
         I.nblocks = s->prec == ECSG_F32 ? sxz_solve_blocks<float>((int)nn, s->sms) : sxz_solve_blocks<double>((int)nn, s->sms);
+        if (i == 1)
+            s->sxz_cap = s->prec == ECSG_F32 ? sxz_multi_capacity<float>(s->sms) : sxz_multi_capacity<double>(s->sms);
         // two halves: the solve's reduction rounds alternate between them
         if ((rc = dmalloc(s, (void **)&I.partial, sizeof(double) * 2 * (size_t)I.nblocks))) return bail(rc);
     }
@@ -887,6 +902,71 @@ static int sxz_prepare(ecsg_sim *s, int i)
     return ECSG_OK;
 }
 
+static SxzWork sxz_work(ecsg_sim *s, int i)
+{
+    Iface &I = s->itf[i];
+    SxzWork W;
+    W.A = I.A;
+    W.B = I.B;
+    W.X0 = I.X0;
+    W.X1 = I.X1;
+    W.partial = I.partial;
+    W.total = s->dscal + 1;
+    W.bar = s->bar + kBarWords * i;
+    W.status = s->ints;
+    W.iters = s->ints + 2;
+    W.iters_total = s->iters_total + i;
+    W.tol_out = s->dscal + 2 + i;
+    W.max_iter = s->jacobi_max_iter;
+    return W;
+}
+
+// The sxz solves of every interface: one cooperative launch over all of them
+// when there are several of one ratio whose CTAs fit co-resident (barrier
+// words: the spare slot 0 of s->bar), else one launch per interface.  The
+// interfaces' systems are independent (each reads and writes only the planes
+// at its own interface), and each is solved bitwise as in its own launch.
+template <typename T>
+static int sxz_op(ecsg_sim *s, int i);
+static bool sxz_fuses(const ecsg_sim *s)
+{
+    bool fuse = s->sxz_fused && s->imode != ECSG_MODE_II && s->ng > 2 && s->ng - 1 <= kMaxSxzSys;
+    int total = 0;
+    for (int i = 1; fuse && i < s->ng; i++) {
+        fuse = s->itf[i].r == s->itf[1].r && s->geo[i - 1].nz >= 2;
+        total += s->itf[i].nblocks;
+    }
+    return fuse && total <= s->sxz_cap;
+}
+
+template <typename T>
+static int sxz_all_op(ecsg_sim *s)
+{
+    if (!sxz_fuses(s)) {
+        for (int i = 1; i < s->ng; i++)
+            if (int rc = sxz_op<T>(s, i)) return rc;
+        return ECSG_OK;
+    }
+    SxzSysList<T> L;
+    memset(&L, 0, sizeof L);
+    L.n = s->ng - 1;
+    L.r = s->itf[1].r;
+    L.bar = s->bar;
+    L.status = s->ints;
+    int cta = 0;
+    for (int i = 1; i < s->ng; i++) {
+        SxzSys<T> &Y = L.s[i - 1];
+        Y.F = dev<T>(s, i - 1);
+        Y.C = dev<T>(s, i);
+        Y.W = sxz_work(s, i);
+        Y.cta0 = cta;
+        Y.ncta = s->itf[i].nblocks;
+        cta += Y.ncta;
+    }
+    CK(launch_sxz_solve_multi<T>(L, s->st));
+    return ECSG_OK;
+}
+
 template <typename T>
 static int sxz_op(ecsg_sim *s, int i)
 {
@@ -1300,10 +1380,9 @@ static int step_op(ecsg_sim *s, bool energy, double *energy_buf, double *res_row
     if (energy)
         if ((rc = energy_op<T>(s, energy_buf, s->ints + 1, s->ints + 3))) return rc;
     if ((rc = each_grid(s, [&](int g) { return stress_op<T>(s, g); }))) return rc;
-    for (int i = 1; i < s->ng; i++) {
-        if ((rc = sxz_op<T>(s, i))) return rc;
+    if ((rc = sxz_all_op<T>(s))) return rc;
+    for (int i = 1; i < s->ng; i++)
         if ((rc = syz_op<T>(s, i))) return rc;
-    }
     return ECSG_OK;
 }
 
@@ -1373,8 +1452,9 @@ static int run_op(ecsg_sim *s, int n0, int nsteps, float *traces, double *energy
     long long launches = 0;
     // per step: velocity kernel + 2 mirror kernels and the stress kernel per grid,
     // the receiver/source kernel(s), 3 vz + 1 sxz + 1 syz kernels per interface
+    // (one sxz kernel for all interfaces when they are fused)
     const int srk = src_rec_kernels(s->nrec, 3);
-    const long long per_step = 4LL * s->ng + srk + 5LL * (s->ng - 1);
+    const long long per_step = 4LL * s->ng + srk + 5LL * (s->ng - 1) - (sxz_fuses(s) ? s->ng - 2 : 0);
     for (int n = n0; n < n0 + nsteps; n++) {
         const bool e_step = energy && ((n % every) == 0);
         launches += per_step + (e_step ? 2LL * s->ng : 0) + (residues ? (2 - srk) + 18LL * (s->ng - 1) : 0);

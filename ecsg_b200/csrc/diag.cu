@@ -40,110 +40,122 @@ __device__ __forceinline__ void block_sums(double (&v)[N], double *partial, int 
 // strains as the strain differences of the displacement sums U (stress21.cu),
 // evaluated by the stress update's own strain functions on a copy of the grid
 // whose velocities are U (GU), e3 condensed on a free surface (flag).
-template <typename T>
-__global__ void __launch_bounds__(RED_THREADS, 3) energy_kernel(GridDev<T> G, int medium, const T *vc0, const T *vc1,
-                                                            const T *vc2, GridDev<T> GU, int flag, double *partial)
+//
+// Work is split into tiles of 32 x 8 (x, y) columns by ENERGY_ZC planes; a
+// CTA takes tiles blockIdx.x, blockIdx.x + gridDim.x, ... and each thread
+// marches z down its column (no per-point index division; neighbours in
+// x and y come from the same or an adjacent column, in z from the plane
+// before or after, all cached).  The medium kind is a template parameter so
+// each kernel holds only its own arithmetic.  The accumulation order is
+// fixed by the launch shape, so the result is the same on every run.
+constexpr int ENERGY_TX = 32, ENERGY_TY = 8, ENERGY_ZC = 16;
+
+template <typename T, int MED>
+__device__ __forceinline__ void energy_point(const GridDev<T> &G, const GridDev<T> &GU, const T *vc0, const T *vc1,
+                                             const T *vc2, int flag, int x, int y, int z, int p, double (&acc)[12])
 {
     const Geo &g = G.g;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
-    const int64_t npts = (int64_t)(nx + 1) * (ny + 1) * (nz + 1);
     const int sy = g.px, sz = g.px * g.py;
+    const double mx = (x == 0 || x == nx) ? 0.5 : 1.0;
+    const double my = (y == 0 || y == ny) ? 0.5 : 1.0;
+    const double mz = (z == 0 || z == nz) ? 0.5 : 1.0;
+    const bool xs = x < nx, ys = y < ny, zs = z < nz;
+    const double b000 = (double)G.b[p];
+    // vx at (0,0,0)
+    acc[0] += mz * my * mx * (1.0 / b000) * (double)G.f[VX][p] * (double)vc0[p];
+    if (xs && ys) {   // vy at (1,1,0)
+        const double b100 = (double)G.b[p + 1], b010 = (double)G.b[p + sy], b110 = (double)G.b[p + sy + 1];
+        const double rb = (b000 + b000 + b010 + b010 + b100 + b100 + b110 + b110) / 8;
+        acc[1] += mz * (1.0 / rb) * (double)G.f[VY][p] * (double)vc1[p];
+    }
+    if (xs && zs) {   // vz at (1,0,1)
+        const double b001 = (double)G.b[p + sz], b100 = (double)G.b[p + 1], b101 = (double)G.b[p + sz + 1];
+        const double rb = (b000 + b001 + b000 + b001 + b100 + b101 + b100 + b101) / 8;
+        acc[2] += my * (1.0 / rb) * (double)G.f[VZ][p] * (double)vc2[p];
+    }
+    if (MED == MED_GEN21) {
+        // terms 3..8 in stress order, trapezoid weights per position
+        if (xs) {
+            const double w = mz * my;
+            const T e1 = e1_at(GU, p), e2 = e2_at(GU, p);
+            const T e3 = (flag && z == 0) ? e3_used(GU, Ext{nx, ny, nz}, true, x, y, z, p, e1, e2) : e3_at(GU, p);
+            acc[3] += w * (double)e1 * (double)G.f[SXX][p];
+            acc[4] += w * (double)e2 * (double)G.f[SYY][p];
+            acc[5] += w * (double)e3 * (double)G.f[SZZ][p];
+        }
+        if (xs && ys && zs) acc[6] += (double)e4_at(GU, p) * (double)G.f[SYZ][p];
+        if (zs) acc[7] += my * mx * (double)e5_at(GU, p) * (double)G.f[SXZ][p];
+        if (ys) acc[8] += mz * mx * (double)e6_at(GU, p) * (double)G.f[SXY][p];
+        return;
+    }
+    if (xs) {         // normal stresses at (1,0,0)
+        double k11, k22, k33, k23, k13, k12;
+        if (MED == MED_ISO5) {
+            const double s11 = (double)G.c[0][p], s13 = (double)G.c[1][p];
+            double base = s11 * s13 * s13 * 3 - s13 * s13 * s13 * 2 - s11 * s11 * s11;
+            base = 1.0 / base;
+            k11 = k22 = k33 = (s13 * s13 - s11 * s11) * base;
+            k23 = k13 = k12 = (s13 * s11 - s13 * s13) * base;
+        } else {
+            const double a = (double)G.c[0][p], e = (double)G.c[1][p], i = (double)G.c[2][p];
+            const double f = (double)G.c[3][p], c = (double)G.c[4][p], bb = (double)G.c[5][p];
+            // inverse of [[a,bb,c],[bb,e,f],[c,f,i]]
+            const double A = e * i - f * f, Bq = -(bb * i - f * c), Cq = bb * f - e * c;
+            const double det = a * A + bb * Bq + c * Cq;
+            const double id = 1.0 / det;
+            k11 = A * id;
+            k12 = Bq * id;
+            k13 = Cq * id;
+            k22 = (a * i - c * c) * id;
+            k23 = -(a * f - bb * c) * id;
+            k33 = (a * e - bb * bb) * id;
+        }
+        const double w = mz * my;
+        const double sxx = (double)G.f[SXX][p], syy = (double)G.f[SYY][p], szz = (double)G.f[SZZ][p];
+        acc[3] += w * k11 * sxx * sxx;
+        acc[4] += w * k22 * syy * syy;
+        acc[5] += w * k33 * szz * szz;
+        acc[6] += w * k23 * syy * szz;
+        acc[7] += w * k13 * sxx * szz;
+        acc[8] += w * k12 * sxx * syy;
+    }
+    constexpr int s44 = MED == MED_ISO5 ? 2 : 6;
+    if (xs && ys && zs) {   // syz at (1,1,1)
+        const double s = (double)G.f[SYZ][p];
+        acc[9] += (1.0 / (double)G.c[s44][p]) * s * s;
+    }
+    if (zs) {               // sxz at (0,0,1)
+        const double s = (double)G.f[SXZ][p];
+        acc[10] += my * mx * (1.0 / (double)G.c[s44 + 1][p]) * s * s;
+    }
+    if (ys) {               // sxy at (0,1,0)
+        const double s = (double)G.f[SXY][p];
+        acc[11] += mz * mx * (1.0 / (double)G.c[s44 + 2][p]) * s * s;
+    }
+}
+
+template <typename T, int MED>
+__global__ void __launch_bounds__(RED_THREADS, 3) energy_kernel(GridDev<T> G, const T *vc0, const T *vc1, const T *vc2,
+                                                            GridDev<T> GU, int flag, double *partial)
+{
+    const Geo &g = G.g;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const int sz = g.px * g.py;
+    const int ntx = (nx + ENERGY_TX) / ENERGY_TX, nty = (ny + ENERGY_TY) / ENERGY_TY;
+    const int ntz = (nz + ENERGY_ZC) / ENERGY_ZC;
+    const int ntiles = ntx * nty * ntz;
+    const int lx = threadIdx.x % ENERGY_TX, ly = threadIdx.x / ENERGY_TX;
     double acc[12];
 #pragma unroll
     for (int k = 0; k < 12; k++) acc[k] = 0.0;
-    // point index -> (x, y, z) with two 32-bit divisions when the grid has
-    // fewer than 2^32 points (64-bit ones are long instruction sequences)
-    const bool idx32 = npts <= 0xffffffffLL;
-    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < npts; t += (int64_t)gridDim.x * blockDim.x) {
-        int x, y, z;
-        if (idx32) {
-            const unsigned u = (unsigned)t, a = (unsigned)(nx + 1), b = (unsigned)(ny + 1);
-            const unsigned qa = u / a, qb = qa / b;
-            x = (int)(u - qa * a);
-            y = (int)(qa - qb * b);
-            z = (int)qb;
-        } else {
-            x = (int)(t % (nx + 1));
-            y = (int)((t / (nx + 1)) % (ny + 1));
-            z = (int)(t / ((int64_t)(nx + 1) * (ny + 1)));
-        }
-        const int p = g.idx(x, y, z);
-        const double mx = (x == 0 || x == nx) ? 0.5 : 1.0;
-        const double my = (y == 0 || y == ny) ? 0.5 : 1.0;
-        const double mz = (z == 0 || z == nz) ? 0.5 : 1.0;
-        const bool xs = x < nx, ys = y < ny, zs = z < nz;
-        const double b000 = (double)G.b[p];
-        // vx at (0,0,0)
-        acc[0] += mz * my * mx * (1.0 / b000) * (double)G.f[VX][p] * (double)vc0[p];
-        if (xs && ys) {   // vy at (1,1,0)
-            const double b100 = (double)G.b[p + 1], b010 = (double)G.b[p + sy], b110 = (double)G.b[p + sy + 1];
-            const double rb = (b000 + b000 + b010 + b010 + b100 + b100 + b110 + b110) / 8;
-            acc[1] += mz * (1.0 / rb) * (double)G.f[VY][p] * (double)vc1[p];
-        }
-        if (xs && zs) {   // vz at (1,0,1)
-            const double b001 = (double)G.b[p + sz], b100 = (double)G.b[p + 1], b101 = (double)G.b[p + sz + 1];
-            const double rb = (b000 + b001 + b000 + b001 + b100 + b101 + b100 + b101) / 8;
-            acc[2] += my * (1.0 / rb) * (double)G.f[VZ][p] * (double)vc2[p];
-        }
-        if (medium == MED_GEN21) {
-            // terms 3..8 in stress order, trapezoid weights per position
-            if (xs) {
-                const double w = mz * my;
-                const T e1 = e1_at(GU, p), e2 = e2_at(GU, p);
-                const T e3 = e3_used(GU, Ext{nx, ny, nz}, flag && z == 0, x, y, z, p, e1, e2);
-                acc[3] += w * (double)e1 * (double)G.f[SXX][p];
-                acc[4] += w * (double)e2 * (double)G.f[SYY][p];
-                acc[5] += w * (double)e3 * (double)G.f[SZZ][p];
-            }
-            if (xs && ys && zs) acc[6] += (double)e4_at(GU, p) * (double)G.f[SYZ][p];
-            if (zs) acc[7] += my * mx * (double)e5_at(GU, p) * (double)G.f[SXZ][p];
-            if (ys) acc[8] += mz * mx * (double)e6_at(GU, p) * (double)G.f[SXY][p];
-            continue;
-        }
-        if (xs) {         // normal stresses at (1,0,0)
-            double k11, k22, k33, k23, k13, k12;
-            if (medium == MED_ISO5) {
-                const double s11 = (double)G.c[0][p], s13 = (double)G.c[1][p];
-                double base = s11 * s13 * s13 * 3 - s13 * s13 * s13 * 2 - s11 * s11 * s11;
-                base = 1.0 / base;
-                k11 = k22 = k33 = (s13 * s13 - s11 * s11) * base;
-                k23 = k13 = k12 = (s13 * s11 - s13 * s13) * base;
-            } else {
-                const double a = (double)G.c[0][p], e = (double)G.c[1][p], i = (double)G.c[2][p];
-                const double f = (double)G.c[3][p], c = (double)G.c[4][p], bb = (double)G.c[5][p];
-                // inverse of [[a,bb,c],[bb,e,f],[c,f,i]]
-                const double A = e * i - f * f, Bq = -(bb * i - f * c), Cq = bb * f - e * c;
-                const double det = a * A + bb * Bq + c * Cq;
-                const double id = 1.0 / det;
-                k11 = A * id;
-                k12 = Bq * id;
-                k13 = Cq * id;
-                k22 = (a * i - c * c) * id;
-                k23 = -(a * f - bb * c) * id;
-                k33 = (a * e - bb * bb) * id;
-            }
-            const double w = mz * my;
-            const double sxx = (double)G.f[SXX][p], syy = (double)G.f[SYY][p], szz = (double)G.f[SZZ][p];
-            acc[3] += w * k11 * sxx * sxx;
-            acc[4] += w * k22 * syy * syy;
-            acc[5] += w * k33 * szz * szz;
-            acc[6] += w * k23 * syy * szz;
-            acc[7] += w * k13 * sxx * szz;
-            acc[8] += w * k12 * sxx * syy;
-        }
-        const int s44 = medium == MED_ISO5 ? 2 : 6;
-        if (xs && ys && zs) {   // syz at (1,1,1)
-            const double s = (double)G.f[SYZ][p];
-            acc[9] += (1.0 / (double)G.c[s44][p]) * s * s;
-        }
-        if (zs) {               // sxz at (0,0,1)
-            const double s = (double)G.f[SXZ][p];
-            acc[10] += my * mx * (1.0 / (double)G.c[s44 + 1][p]) * s * s;
-        }
-        if (ys) {               // sxy at (0,1,0)
-            const double s = (double)G.f[SXY][p];
-            acc[11] += mz * mx * (1.0 / (double)G.c[s44 + 2][p]) * s * s;
-        }
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int tx = t % ntx, ty = (t / ntx) % nty, tz = t / (ntx * nty);
+        const int x = tx * ENERGY_TX + lx, y = ty * ENERGY_TY + ly;
+        if (x > nx || y > ny) continue;
+        const int z0 = tz * ENERGY_ZC, z1 = min(nz, z0 + ENERGY_ZC - 1);
+        int p = g.idx(x, y, z0);
+        for (int z = z0; z <= z1; z++, p += sz) energy_point<T, MED>(G, GU, vc0, vc1, vc2, flag, x, y, z, p, acc);
     }
     block_sums<12>(acc, partial, gridDim.x);
 }
@@ -372,11 +384,21 @@ cudaError_t launch_energy(const GridDev<T> &G, int medium, T *const vc[3], T *co
     for (int k = 0; k < 3; k++) GU.f[VX + k] = disp ? disp[k] : nullptr;
     if (medium == MED_GEN21 && !GU.f[VX]) return cudaErrorInvalidValue;
     // one wave: three CTAs per SM (the kernel's launch bounds), at most nblocks
+    // and at most one per tile
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const int eb = (sms > 0 && 3 * sms < nblocks) ? 3 * sms : nblocks;
-    energy_kernel<T><<<eb, RED_THREADS, 0, st>>>(G, medium, vc[0], vc[1], vc[2], GU, flag, partial);
+    const Geo &g = G.g;
+    const int64_t ntiles = (int64_t)((g.nx + ENERGY_TX) / ENERGY_TX) * ((g.ny + ENERGY_TY) / ENERGY_TY) *
+                           ((g.nz + ENERGY_ZC) / ENERGY_ZC);
+    int eb = (sms > 0 && 3 * sms < nblocks) ? 3 * sms : nblocks;
+    if (ntiles < eb) eb = (int)ntiles;
+    if (medium == MED_GEN21)
+        energy_kernel<T, MED_GEN21><<<eb, RED_THREADS, 0, st>>>(G, vc[0], vc[1], vc[2], GU, flag, partial);
+    else if (medium == MED_ISO5)
+        energy_kernel<T, MED_ISO5><<<eb, RED_THREADS, 0, st>>>(G, vc[0], vc[1], vc[2], GU, flag, partial);
+    else
+        energy_kernel<T, MED_ORTHO9><<<eb, RED_THREADS, 0, st>>>(G, vc[0], vc[1], vc[2], GU, flag, partial);
     energy_finalize_kernel<<<1, 32, 0, st>>>(partial, eb, h0, h1, h2, out, step, step0, first, status,
                                              medium == MED_GEN21);
     return cudaGetLastError();

@@ -107,6 +107,24 @@ struct SxzWork {
     int max_iter;
 };
 
+// Several sxz systems solved by one cooperative launch (interface.cu,
+// sxz_solve_multi_kernel): system i owns CTAs [cta0, cta0 + ncta).
+constexpr int kMaxSxzSys = 16;
+template <typename T>
+struct SxzSys {
+    GridDev<T> F, C;
+    SxzWork W;       // W.bar is not used: the list's barrier serves all systems
+    int cta0, ncta;
+};
+template <typename T>
+struct SxzSysList {
+    SxzSys<T> s[kMaxSxzSys];
+    int n;
+    int r;           // refinement ratio, the same for every system
+    unsigned *bar;   // kBarWords barrier words of the launch
+    int *status;     // ST_BARRIER_TIMEOUT
+};
+
 // Receivers and source of one run (diag.cu, src_rec_kernel).
 struct SrcRec {
     void *rec_base[kMaxGrids];   // receiver component per grid

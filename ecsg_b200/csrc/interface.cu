@@ -527,6 +527,209 @@ __global__ void __launch_bounds__(256, 4) sxz_solve_kernel(GridDev<T> F, GridDev
     }
 }
 
+// ---------------------------------------------------------------------------
+// Several independent sxz systems in one cooperative launch (the interfaces of
+// one step, or one interface of several shots).  System i owns CTAs
+// [cta0, cta0 + ncta) and maps its unknowns, its right-hand side and its
+// partial sums onto them exactly as its own launch with ncta CTAs would, so
+// its result is bitwise that of sxz_solve_kernel.  All CTAs share one grid
+// barrier per round; after it every CTA forms the totals of every system in
+// the same fixed order and takes the same stopping decisions, so a system
+// that has converged (or hit its cap) stops updating while the others go on,
+// and every CTA runs the same number of rounds.  The barrier's arrival count
+// and generation words are the list's; each system keeps its own partials,
+// status, sweep counts and warm start.
+// ---------------------------------------------------------------------------
+__device__ void grid_arrive_list(double v, double *slot, unsigned *bar, int *status, double *red, bool &ok)
+{
+    const double bs = block_sum(v, red);   // valid in thread 0; ends with a CTA barrier
+    __shared__ int s_ok;
+    if (threadIdx.x == 0) {
+        unsigned *gen_w = bar, *cnt_w = bar + 32;
+        const unsigned gen = *(volatile unsigned *)gen_w;
+        __stcg(slot, bs);
+        __threadfence();
+        int okv = 1;
+        if (atomicAdd(cnt_w, 1u) == gridDim.x - 1) {
+            *cnt_w = 0;
+            __threadfence();
+            atomicAdd(gen_w, 1u);
+        } else {
+            long long spin = 0;
+            while (*(volatile unsigned *)gen_w == gen) {
+                if (++spin > kSpinLimit) { atomicOr(status, ST_BARRIER_TIMEOUT); okv = 0; break; }
+                __nanosleep(32);
+            }
+        }
+        __threadfence();
+        s_ok = okv;
+    }
+    __syncthreads();
+    ok = s_ok != 0;
+}
+
+// total of one system's partials of a finished round: partial_share's strided
+// split over that system's CTAs, then share_total's tree
+__device__ __forceinline__ double system_total(const double *part, int ncta, double *red)
+{
+    double t = 0.0;
+    for (int i = threadIdx.x; i < ncta; i += blockDim.x) t += __ldcg(part + i);
+    return share_total(t, red);
+}
+
+template <typename T, int RR>
+__global__ void __launch_bounds__(256, 4) sxz_solve_multi_kernel(const __grid_constant__ SxzSysList<T> L)
+{
+    __shared__ double red[32];
+    __shared__ double s_tol[kMaxSxzSys];
+    __shared__ int s_it[kMaxSxzSys], s_act[kMaxSxzSys], s_cap[kMaxSxzSys];
+    int me = 0;
+    for (int i = 1; i < L.n; i++)
+        if ((int)blockIdx.x >= L.s[i].cta0) me = i;
+    const SxzSys<T> &S = L.s[me];
+    const GridDev<T> &F = S.F, &C = S.C;
+    const SxzWork &W = S.W;
+    const int r = L.r;
+    const int lb = blockIdx.x - S.cta0, ncta = S.ncta;
+    const int nx2 = C.g.nx, ny2 = C.g.ny, nz1 = F.g.nz;
+    const int n0 = nx2 - 1, n1 = ny2 - 1, ld = nx2 + 1;
+    const int nn = n0 * n1;
+    const int gtid = lb * blockDim.x + threadIdx.x;
+    const int gstride = ncta * blockDim.x;
+    bool ok = true;
+    int round = 0;
+    auto slot = [&](const SxzSys<T> &Y, int rd, int b) { return Y.W.partial + (size_t)(rd & 1) * Y.ncta + b; };
+
+    // B and avg|B| of this CTA's system
+    double sab = 0.0;
+    for (int q = gtid; q < nn; q += gstride) {
+        const double bq = sxz_rhs<T, RR>(F, C, r, q % n0 + 1, q / n0 + 1);
+        W.B[q] = bq;
+        sab += fabs(bq);
+    }
+    grid_arrive_list(sab, slot(S, round, lb), L.bar, L.status, red, ok);
+    round++;
+    for (int i = 0; i < L.n; i++) {
+        const SxzSys<T> &Y = L.s[i];
+        const double sumabs = system_total(slot(Y, round - 1, 0), Y.ncta, red);
+        if (threadIdx.x == 0) {
+            const int nni = (Y.C.g.nx - 1) * (Y.C.g.ny - 1);
+            double tol = 1e-5 * (sumabs / (double)nni);
+            if (tol > 1e-12) tol = 1e-12;
+            s_tol[i] = tol;
+            s_it[i] = 0;
+            s_act[i] = 1;
+            s_cap[i] = 0;
+        }
+    }
+    __syncthreads();
+
+    double *Xc = W.X0, *Xn = W.X1;
+    double a0[9] = {0, 0, 0, 0, 1, 0, 0, 0, 0}, b0 = 0.0;
+    if (gtid < nn) {
+#pragma unroll
+        for (int k = 0; k < 9; k++) a0[k] = W.A[(size_t)k * nn + gtid];
+        b0 = W.B[gtid];
+    }
+    auto update = [&](const double *Xo, double *Xw, int q, const double (&a)[9], double bq) {
+        const int i0 = q % n0 + 1, i1 = q / n0 + 1;
+        const double xn = (bq
+                           - a[0] * __ldcg(Xo + (i1 - 1) * ld + (i0 - 1))
+                           - a[1] * __ldcg(Xo + (i1) * ld + (i0 - 1))
+                           - a[2] * __ldcg(Xo + (i1 + 1) * ld + (i0 - 1))
+                           - a[3] * __ldcg(Xo + (i1 - 1) * ld + (i0))
+                           - a[5] * __ldcg(Xo + (i1 + 1) * ld + (i0))
+                           - a[6] * __ldcg(Xo + (i1 - 1) * ld + (i0 + 1))
+                           - a[7] * __ldcg(Xo + (i1) * ld + (i0 + 1))
+                           - a[8] * __ldcg(Xo + (i1 + 1) * ld + (i0 + 1))) / a[4];
+        const double d = xn - __ldcg(Xo + i1 * ld + i0);
+        __stcg(Xw + i1 * ld + i0, xn);
+        return d * d;
+    };
+    auto sweep = [&](const double *Xo, double *Xw) {
+        double s = 0.0;
+        if (gtid < nn) s += update(Xo, Xw, gtid, a0, b0);
+        for (int q = gtid + gstride; q < nn; q += gstride) {
+            double a[9];
+#pragma unroll
+            for (int k = 0; k < 9; k++) a[k] = W.A[(size_t)k * nn + q];
+            s += update(Xo, Xw, q, a, W.B[q]);
+        }
+        return s;
+    };
+    bool any = true;
+    while (ok && any) {
+        const bool mine = s_act[me] != 0;
+        const double s = mine ? sweep(Xc, Xn) : 0.0;
+        grid_arrive_list(s, slot(S, round, lb), L.bar, L.status, red, ok);
+        round++;
+        if (!ok) break;
+        for (int i = 0; i < L.n; i++) {
+            if (!s_act[i]) continue;   // uniform over the CTA (shared, set by thread 0 below a barrier)
+            const SxzSys<T> &Y = L.s[i];
+            const double tot = system_total(slot(Y, round - 1, 0), Y.ncta, red);
+            if (threadIdx.x == 0) {
+                s_it[i]++;
+                if (!(sqrt(tot) > s_tol[i])) s_act[i] = 0;
+                else if (s_it[i] >= Y.W.max_iter) { s_act[i] = 0; s_cap[i] = 1; }
+            }
+        }
+        __syncthreads();
+        if (mine) { double *tmp = Xc; Xc = Xn; Xn = tmp; }
+        any = false;
+        for (int i = 0; i < L.n; i++) any = any || s_act[i] != 0;
+        __syncthreads();   // every thread has read s_act before thread 0 changes it again
+    }
+    if (gtid == 0) {
+        *W.iters = s_it[me];
+        *W.iters_total += s_it[me];
+        *W.tol_out = s_tol[me];
+        if (s_cap[me]) atomicOr(W.status, ST_JACOBI_CAP);
+    }
+    // coarse ghost and fine ghosts (update_ghost_sxz.cpp:247-295)
+    T *sxz1 = F.f[SXZ];
+    T *sxz2 = C.f[SXZ];
+    const int csz = C.g.px * C.g.py, fsz = F.g.px * F.g.py;
+    for (int q = gtid; q < nn; q += gstride) {
+        const int j0 = q % n0 + 1, j1 = q / n0 + 1;
+        const double x = __ldcg(Xc + j1 * ld + j0);
+        sxz2[C.g.idx(j0, j1, 0) - csz] = (T)x;
+        if (Xc != W.X0) W.X0[j1 * ld + j0] = x;
+    }
+    const int nx1 = r * nx2, ny1 = r * ny2;
+    const int nf = (nx1 - 1) * (ny1 - 1);
+    constexpr int NB = 4;
+    for (int q0 = gtid; q0 < nf; q0 += NB * gstride) {
+        double val[NB];
+        int pfs[NB];
+#pragma unroll
+        for (int b = 0; b < NB; b++) {
+            const int q = q0 + b * gstride;
+            pfs[b] = -1;
+            val[b] = 0.0;
+            if (q >= nf) continue;
+            const int i0 = q % (nx1 - 1) + 1, i1 = q / (nx1 - 1) + 1;
+            const int jx = i0 / r, jy = i1 / r;
+            double acc = 0.0;
+            for (int ey = 0; ey < 2; ey++)
+                for (int ex = 0; ex < 2; ex++) {
+                    const int cx = jx + ex, cy = jy + ey;
+                    if (cx > nx2 || cy > ny2) continue;
+                    const double ww = pw_node_r<RR>(i0, cx, r, nx2) * pw_node_r<RR>(i1, cy, r, ny2);
+                    if (ww != 0.0) {
+                        const double xg = (double)(T)__ldcg(Xc + cy * ld + cx);
+                        acc += ww * (xg + (double)sxz2[C.g.idx(cx, cy, 0)]);
+                    }
+                }
+            pfs[b] = F.g.idx(i0, i1, nz1);
+            val[b] = -(double)sxz1[pfs[b] - fsz] + acc;
+        }
+#pragma unroll
+        for (int b = 0; b < NB; b++)
+            if (pfs[b] >= 0) sxz1[pfs[b]] = (T)val[b];
+    }
+}
+
 // ===========================================================================
 // Adjoints of the three interface solves (no reference counterpart).  Each
 // forward solve overwrites ghost entries with X = A^{-1} rhs(state) and the
@@ -1373,6 +1576,43 @@ cudaError_t launch_sxz_solve(const GridDev<T> &F, const GridDev<T> &C, int r, co
     return cudaLaunchKernelEx(&cfg, sxz_solve_kernel<T, 0>, F, C, r, W);
 }
 
+// CTAs of one multi-system launch that can be co-resident (the fewest per SM
+// of the three instantiations)
+template <typename T>
+int sxz_multi_capacity(int sms)
+{
+    int p0 = 0, p2 = 0, p3 = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p0, sxz_solve_multi_kernel<T, 0>, 256, 0) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p2, sxz_solve_multi_kernel<T, 2>, 256, 0) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&p3, sxz_solve_multi_kernel<T, 3>, 256, 0) != cudaSuccess)
+        return 0;
+    int per_sm = p0 < p2 ? p0 : p2;
+    per_sm = per_sm < p3 ? per_sm : p3;
+    return per_sm * sms;
+}
+
+// L.s[i].cta0 / ncta set by the caller (consecutive, from 0); the barrier words
+// L.bar start at zero and are left at zero count.
+template <typename T>
+cudaError_t launch_sxz_solve_multi(const SxzSysList<T> &L, cudaStream_t st)
+{
+    if (L.n < 1 || L.n > kMaxSxzSys) return cudaErrorInvalidValue;
+    const int nblocks = L.s[L.n - 1].cta0 + L.s[L.n - 1].ncta;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(nblocks);
+    cfg.blockDim = dim3(256);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    if (L.r == 2) return cudaLaunchKernelEx(&cfg, sxz_solve_multi_kernel<T, 2>, L);
+    if (L.r == 3) return cudaLaunchKernelEx(&cfg, sxz_solve_multi_kernel<T, 3>, L);
+    return cudaLaunchKernelEx(&cfg, sxz_solve_multi_kernel<T, 0>, L);
+}
+
 
 template <typename T>
 cudaError_t launch_ghost_vz_adj(const GridDev<T> &F, const GridDev<T> &C, const AdjDev<T> &AF, const AdjDev<T> &AC,
@@ -1445,7 +1685,9 @@ cudaError_t launch_ghost_sxz_adj(const GridDev<T> &F, const GridDev<T> &C, const
                                                 const AdjDev<T> &, cudaStream_t);                               \
     template cudaError_t launch_sxz_matrix<T>(const GridDev<T> &, const GridDev<T> &, int, double *, cudaStream_t); \
     template int sxz_solve_blocks<T>(int, int);                                                          \
-    template cudaError_t launch_sxz_solve<T>(const GridDev<T> &, const GridDev<T> &, int, const SxzWork &, int, cudaStream_t);
+    template cudaError_t launch_sxz_solve<T>(const GridDev<T> &, const GridDev<T> &, int, const SxzWork &, int, cudaStream_t); \
+    template int sxz_multi_capacity<T>(int);                                                              \
+    template cudaError_t launch_sxz_solve_multi<T>(const SxzSysList<T> &, cudaStream_t);
 INST(float)
 INST(double)
 #undef INST

@@ -282,3 +282,29 @@ def test_side_stream_grids_equal_one_stream(monkeypatch, medium, graph):
     assert np.array_equal(ra["energy"], rb["energy"], equal_nan=True)
     for a, b in zip(fa, fb):
         assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_fused_interface_solves_equal_one_launch_each(monkeypatch, prec):
+    """The sxz solves of both interfaces of a three-grid composite in one
+    cooperative launch (the default) against one launch per interface
+    (ECSG_SXZ_FUSED=0): bitwise equal traces, fields and sweep counts, over
+    enough steps for the wavefield to reach both interfaces (several sweeps
+    per solve)."""
+    from ecsg_b200.workloads import three_grid_case
+    case = three_grid_case(seed=5, grids=[((72, 54, 6), 5.0), ((24, 18, 4), 15.0), ((8, 6, 8), 45.0)],
+                           nsteps=160, medium="tti")
+    outs = []
+    for fused in ("0", "1"):
+        monkeypatch.setenv("ECSG_SXZ_FUSED", fused)
+        with Simulation(case, precision=prec, energy=True) as s:
+            r = s.run(160, energy_every=8)
+            totals = [s.sxz_state(i)[3] for i in (1, 2)]
+            outs.append((r, [s.field(g, k) for g in range(3) for k in range(9)], s.status(), totals))
+    (ra, fa, sa, ta), (rb, fb, sb, tb) = outs
+    assert sa == 0 and sb == 0
+    assert ta == tb and min(ta) > 160, ta   # both interfaces needed more than one sweep on some steps
+    assert np.array_equal(ra["rec"], rb["rec"])
+    assert np.array_equal(ra["energy"], rb["energy"], equal_nan=True)
+    for a, b in zip(fa, fb):
+        assert np.array_equal(a, b)

@@ -121,6 +121,8 @@ SIGNATURES = [
     ("ecsg_batch_misfit_gradient", ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_int,
                                                   ctypes.POINTER(c_fp), ctypes.c_int, c_dp]),
     ("ecsg_sum_gradients", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p), ctypes.c_int]),
+    ("ecsg_shots_misfit_gradient", ctypes.c_int, [ctypes.POINTER(ctypes.c_void_p), ctypes.c_int, ctypes.c_int,
+                                                  ctypes.POINTER(c_fp), ctypes.c_int, ctypes.c_int, c_dp]),
     ("ecsg_autotune", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int]),
     ("ecsg_get_tuning", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, c_ip]),
     ("ecsg_adjoint_reset", ctypes.c_int, [ctypes.c_void_p]),
@@ -507,6 +509,23 @@ def batch_misfit_gradient(sims, observed, ckpt_every=50):
                                           losses.ctypes.data_as(c_dp))
     if rc != ECSG_OK:
         raise EcsgError("ecsg_batch_misfit_gradient failed (%d): %s" % (rc, lib().ecsg_last_error(sims[0].h).decode()))
+    for s in sims:
+        s.step_index = nsteps
+    return losses
+
+
+def shots_misfit_gradient(sims, observed, ckpt_every=50, sub_every=0):
+    """The shots in lockstep (ecsg_shots_misfit_gradient): instances of one
+    model; returns the per-shot losses and leaves the gradient of their sum in
+    sims[0] (read with sims[0].gradient)."""
+    obs = [np.ascontiguousarray(o, dtype=np.float32) for o in observed]
+    nsteps = obs[0].shape[0]
+    ptrs = (c_fp * len(sims))(*[o.ctypes.data_as(c_fp) for o in obs])
+    losses = np.zeros(len(sims))
+    rc = lib().ecsg_shots_misfit_gradient(_handles(sims), len(sims), nsteps, ptrs, int(ckpt_every), int(sub_every),
+                                          losses.ctypes.data_as(c_dp))
+    if rc != ECSG_OK:
+        raise EcsgError("ecsg_shots_misfit_gradient failed (%d): %s" % (rc, lib().ecsg_last_error(sims[0].h).decode()))
     for s in sims:
         s.step_index = nsteps
     return losses

@@ -100,6 +100,78 @@ __global__ void vel_adj_kernel(GridDev<T> G, AdjDev<T> A, int zt, int bottom)
     }
 }
 
+// The velocity adjoint of every shot at each point: the buoyancy read once,
+// the buoyancy-gradient terms of all shots summed in registers and added with
+// one set of atomics (the shots' stress adjoints are scattered per shot).
+template <typename T>
+__global__ void vel_adj_shots_kernel(GridDev<T> G, T *gb, const __grid_constant__ AdjShots<T> S, int zt, int bottom)
+{
+    const Geo &g = G.g;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const int64_t n = (int64_t)nx * ny * (nz + 1);
+    const int sx = 1, sy = g.px, sz = g.px * g.py;
+    const T k0 = G.k[0], k1 = G.k[1], k2 = G.k[2], q = T(0.25);
+    const T *b = G.b;
+    const int64_t box = S.box;
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+        const int ix = (int)(t % nx), iy = (int)((t / nx) % ny), iz = (int)(t / ((int64_t)nx * ny));
+        const int p = g.idx(ix, iy, iz);
+        const bool zin = iz >= zt && iz <= nz - bottom;
+        const bool dx = ix >= 1 && iy >= 1 && zin, dy = zin, dz = iy >= 1 && iz <= nz - 1;
+        const T bx = dx ? b[p] : T(0);
+        const T bby = dy ? mul_(q, add_(add_(add_(b[p], b[p + sx]), b[p + sy]), b[p + sy + sx])) : T(0);
+        const T bbz = dz ? mul_(q, add_(add_(add_(b[p], b[p + sz]), b[p + sx]), b[p + sz + sx])) : T(0);
+        T gx = T(0), gy = T(0), gz = T(0);
+        for (int s = 0; s < S.ns; s++) {
+            const T *f = S.f[s];
+            T *l = S.l[s];
+            const T *sxx = f + SXX * box, *syy = f + SYY * box, *szz = f + SZZ * box;
+            const T *syz = f + SYZ * box, *sxz = f + SXZ * box, *sxy = f + SXY * box;
+            T *lsxx = l + SXX * box, *lsyy = l + SYY * box, *lszz = l + SZZ * box;
+            T *lsyz = l + SYZ * box, *lsxz = l + SXZ * box, *lsxy = l + SXY * box;
+            if (dx) {   // vx
+                const T a = l[VX * box + p];
+                if (a != T(0)) {
+                    const T d = add_(add_(mul_(k0, sub_(sxx[p], sxx[p - sx])), mul_(k1, sub_(sxy[p], sxy[p - sy]))),
+                                     mul_(k2, sub_(sxz[p], sxz[p - sz])));
+                    gx = add_(gx, mul_(a, d));
+                    const T u = mul_(a, bx);
+                    atom(lsxx + p, mul_(k0, u)); atom(lsxx + p - sx, -mul_(k0, u));
+                    atom(lsxy + p, mul_(k1, u)); atom(lsxy + p - sy, -mul_(k1, u));
+                    atom(lsxz + p, mul_(k2, u)); atom(lsxz + p - sz, -mul_(k2, u));
+                }
+            }
+            if (dy) {   // vy
+                const T a = l[VY * box + p];
+                if (a != T(0)) {
+                    const T d = add_(add_(mul_(k0, sub_(sxy[p + sx], sxy[p])), mul_(k2, sub_(syz[p], syz[p - sz]))),
+                                     mul_(k1, sub_(syy[p + sy], syy[p])));
+                    gy = add_(gy, mul_(q, mul_(a, d)));
+                    const T u = mul_(a, bby);
+                    atom(lsxy + p + sx, mul_(k0, u)); atom(lsxy + p, -mul_(k0, u));
+                    atom(lsyz + p, mul_(k2, u)); atom(lsyz + p - sz, -mul_(k2, u));
+                    atom(lsyy + p + sy, mul_(k1, u)); atom(lsyy + p, -mul_(k1, u));
+                }
+            }
+            if (dz) {   // vz
+                const T a = l[VZ * box + p];
+                if (a != T(0)) {
+                    const T d = add_(add_(mul_(k0, sub_(sxz[p + sx], sxz[p])), mul_(k2, sub_(szz[p + sz], szz[p]))),
+                                     mul_(k1, sub_(syz[p], syz[p - sy])));
+                    gz = add_(gz, mul_(q, mul_(a, d)));
+                    const T u = mul_(a, bbz);
+                    atom(lsxz + p + sx, mul_(k0, u)); atom(lsxz + p, -mul_(k0, u));
+                    atom(lszz + p + sz, mul_(k2, u)); atom(lszz + p, -mul_(k2, u));
+                    atom(lsyz + p, mul_(k1, u)); atom(lsyz + p - sy, -mul_(k1, u));
+                }
+            }
+        }
+        if (gx != T(0)) atom(gb + p, gx);
+        if (gy != T(0)) { atom(gb + p, gy); atom(gb + p + sx, gy); atom(gb + p + sy, gy); atom(gb + p + sy + sx, gy); }
+        if (gz != T(0)) { atom(gb + p, gz); atom(gb + p + sz, gz); atom(gb + p + sx, gz); atom(gb + p + sz + sx, gz); }
+    }
+}
+
 // ---------------------------------------------------------------------------
 // Velocity mirrors (stencil.cu vel_mirror_kernel): each assignment h = -v[i]
 // transposes to lambda[i] -= lambda[h], lambda[h] = 0, phase 1 before phase 0.
@@ -183,66 +255,323 @@ __device__ __forceinline__ T wgt(bool a0, bool a1, bool b0, bool b1, int i, int 
 __device__ __forceinline__ bool in_(int v, int lo, int hi) { return v >= lo && v <= hi; }
 
 template <typename T>
+__device__ __forceinline__ void g0_point(const GridDev<T> &G, const AdjDev<T> &A, int flag, const Ext &E, int x, int y, int z)
+{
+    const Geo &g = G.g;
+    const int nx = g.nx, ny = g.ny;
+    const int sz = g.px * g.py;
+    const T *const *c = G.c;
+    T *const *X = A.w;
+    const int p = g.idx(x, y, z);
+    // all loads and arithmetic of the point first, then its stores (the
+    // pointers may alias as far as the compiler knows: a load after a
+    // store could not be moved ahead of it and would wait for memory)
+    const bool in_n = E.n(x, y, z), in_4 = E.l4(x, y, z), in_5 = E.l5(x, y, z), in_6 = E.l6(x, y, z);
+    T en[3] = {}, le[3] = {}, ls[3] = {}, e4 = T(0), e5 = T(0), e6 = T(0);
+    if (in_n) {
+        const bool surf = flag && z == 0;
+        en[0] = e1_at(G, p);
+        en[1] = e2_at(G, p);
+        en[2] = e3_used(G, E, surf, x, y, z, p, en[0], en[1]);
+        const T a[3] = {A.l[SXX][p], A.l[SYY][p], surf ? T(0) : A.l[SZZ][p]};
+        const int rowc[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+#pragma unroll
+        for (int j = 0; j < 3; j++)
+#pragma unroll
+            for (int i = 0; i < 3; i++) {
+                le[j] = fma_(a[i], c[rowc[i][j]][p], le[j]);
+                ls[j] = fma_(a[i], c[6 + 3 * i + j][p], ls[j]);
+            }
+    }
+    // the surface mirrors of syz / sxz folded back: lambda(0) - lambda(-1)
+    const bool fold4 = in_4 && flag && z == 0;   // syz(-1) = -syz(0)
+    const bool fold5 = in_5 && flag && z == 0 && x >= 1 && x <= nx - 1 && y >= 1 && y <= ny - 1;
+    T f4 = T(0), f5 = T(0);
+    if (in_4) e4 = e4_at(G, p);
+    if (fold4) f4 = sub_(A.l[SYZ][p], A.l[SYZ][p - sz]);
+    if (in_5) e5 = e5_at(G, p);
+    if (fold5) f5 = sub_(A.l[SXZ][p], A.l[SXZ][p - sz]);
+    if (in_6) e6 = e6_at(G, p);
+    if (in_n) {
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            X[X_E + j][p] = en[j];
+            X[X_W + j][p] = le[j];
+            X[X_S + j][p] = ls[j];
+        }
+    }
+    if (in_4) X[X_E + 3][p] = e4;
+    if (fold4) {
+        A.l[SYZ][p] = f4;
+        A.l[SYZ][p - sz] = T(0);
+    }
+    if (in_5) X[X_E + 4][p] = e5;
+    if (fold5) {
+        A.l[SXZ][p] = f5;
+        A.l[SXZ][p - sz] = T(0);
+    }
+    if (in_6) X[X_E + 5][p] = e6;
+}
+
+template <typename T>
 __global__ void stress21_adj_g0(GridDev<T> G, AdjDev<T> A, int flag)
 {
     const Geo &g = G.g;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     const Ext E{nx, ny, nz};
     const int64_t n = (int64_t)(nx + 1) * (ny + 1) * (nz + 1);
-    const int sz = g.px * g.py;
-    const T *const *c = G.c;
-    T *const *X = A.w;
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
         const int x = (int)(t % (nx + 1)), y = (int)((t / (nx + 1)) % (ny + 1)), z = (int)(t / ((int64_t)(nx + 1) * (ny + 1)));
-        const int p = g.idx(x, y, z);
-        // all loads and arithmetic of the point first, then its stores (the
-        // pointers may alias as far as the compiler knows: a load after a
-        // store could not be moved ahead of it and would wait for memory)
-        const bool in_n = E.n(x, y, z), in_4 = E.l4(x, y, z), in_5 = E.l5(x, y, z), in_6 = E.l6(x, y, z);
-        T en[3] = {}, le[3] = {}, ls[3] = {}, e4 = T(0), e5 = T(0), e6 = T(0);
-        if (in_n) {
-            const bool surf = flag && z == 0;
-            en[0] = e1_at(G, p);
-            en[1] = e2_at(G, p);
-            en[2] = e3_used(G, E, surf, x, y, z, p, en[0], en[1]);
-            const T a[3] = {A.l[SXX][p], A.l[SYY][p], surf ? T(0) : A.l[SZZ][p]};
-            const int rowc[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
-#pragma unroll
-            for (int j = 0; j < 3; j++)
-#pragma unroll
-                for (int i = 0; i < 3; i++) {
-                    le[j] = fma_(a[i], c[rowc[i][j]][p], le[j]);
-                    ls[j] = fma_(a[i], c[6 + 3 * i + j][p], ls[j]);
-                }
+        g0_point(G, A, flag, E, x, y, z);
+    }
+}
+
+// G1, one shot's share at one point.  Each block (the position kinds N, L4,
+// L5, L6) takes the gradient slots of its position in registers (gk, loaded
+// and stored by the caller), adds this shot's terms to them and writes the
+// shot's strain adjoints W; a caller that holds the slots over several shots
+// reads and writes them once for all.
+template <typename T>
+__device__ __forceinline__ void g1_n_shot(const GridDev<T> &G, const AdjDev<T> &A, int flag, const Ext &E, int x, int y,
+                                          int z, T (&gk)[15])
+{
+    const Geo &g = G.g;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const T *const *c = G.c;
+    T *const *X = A.w;
+    const T *l4 = A.l[SYZ], *l5 = A.l[SXZ], *l6 = A.l[SXY];
+    auto I = [&](int xx, int yy, int zz) { return g.idx(xx, yy, zz); };
+    const int p = I(x, y, z);
+    T v[2][2];
+    bool oa[2], ob[2];
+    T zp[3] = {T(0), T(0), T(0)};
+    for (int i = 0; i < 2; i++)
+        for (int j = 0; j < 2; j++) {
+            int qx = x, qy = y - i, qz = z - j;   // L4 tp over N (x, y..y+1, z..z+1)
+            if (E.l4(qx, qy, qz))
+                zp[0] = fma_(wgt<T>(qy <= ny, qy + 1 <= ny, qz <= nz, qz + 1 <= nz, i, j), l4[I(qx, qy, qz)], zp[0]);
+            qx = x + 1 - i; qy = y; qz = z - j;   // L5 tp over N (x-1..x, y, z..z+1)
+            if (E.l5(qx, qy, qz))
+                zp[1] = fma_(wgt<T>(in_(qx - 1, 0, nx - 1), in_(qx, 0, nx - 1), qz <= nz, qz + 1 <= nz, i, j),
+                             l5[I(qx, qy, qz)], zp[1]);
+            qx = x + 1 - i; qy = y - j; qz = z;   // L6 P6 over N (x-1..x, y..y+1, z)
+            if (E.l6(qx, qy, qz))
+                zp[2] = fma_(wgt<T>(in_(qx - 1, 0, nx - 1), in_(qx, 0, nx - 1), qy <= ny, qy + 1 <= ny, i, j),
+                             l6[I(qx, qy, qz)], zp[2]);
         }
-        // the surface mirrors of syz / sxz folded back: lambda(0) - lambda(-1)
-        const bool fold4 = in_4 && flag && z == 0;   // syz(-1) = -syz(0)
-        const bool fold5 = in_5 && flag && z == 0 && x >= 1 && x <= nx - 1 && y >= 1 && y <= ny - 1;
-        T f4 = T(0), f5 = T(0);
-        if (in_4) e4 = e4_at(G, p);
-        if (fold4) f4 = sub_(A.l[SYZ][p], A.l[SYZ][p - sz]);
-        if (in_5) e5 = e5_at(G, p);
-        if (fold5) f5 = sub_(A.l[SXZ][p], A.l[SXZ][p - sz]);
-        if (in_6) e6 = e6_at(G, p);
-        if (in_n) {
+    const T e[3] = {X[X_E + 0][p], X[X_E + 1][p], X[X_E + 2][p]};
+    T ab[3];
+    for (int i = 0; i < 2; i++) { oa[i] = in_(y - 1 + i, 0, ny - 1); ob[i] = in_(z - 1 + i, 0, nz - 1); }
+    for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++) v[i][j] = (oa[i] && ob[j]) ? X[X_E + 3][I(x, y - 1 + i, z - 1 + j)] : T(0);
+    ab[0] = avg4<T>(v, oa, ob);
+    for (int i = 0; i < 2; i++) { oa[i] = (x + i) <= nx; ob[i] = in_(z - 1 + i, 0, nz - 1); }
+    for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++) v[i][j] = (oa[i] && ob[j]) ? X[X_E + 4][I(x + i, y, z - 1 + j)] : T(0);
+    ab[1] = avg4<T>(v, oa, ob);
+    for (int i = 0; i < 2; i++) { oa[i] = (x + i) <= nx; ob[i] = in_(y - 1 + i, 0, ny - 1); }
+    for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++) v[i][j] = (oa[i] && ob[j]) ? X[X_E + 5][I(x + i, y - 1 + j, z)] : T(0);
+    ab[2] = avg4<T>(v, oa, ob);
+    const bool surf = flag && z == 0;
+    const T a[3] = {A.l[SXX][p], A.l[SYY][p], surf ? T(0) : A.l[SZZ][p]};
+    T cs[9];
 #pragma unroll
-            for (int j = 0; j < 3; j++) {
-                X[X_E + j][p] = en[j];
-                X[X_W + j][p] = le[j];
-                X[X_S + j][p] = ls[j];
+    for (int k = 0; k < 9; k++) cs[k] = c[6 + k][p];
+    T le[3] = {X[X_W + 0][p], X[X_W + 1][p], X[X_W + 2][p]};
+    const int rowc[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+#pragma unroll
+    for (int i = 0; i < 3; i++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            gk[rowc[i][j]] = add_(gk[rowc[i][j]], mul_(a[i], e[j]));
+            gk[6 + 3 * i + j] = add_(gk[6 + 3 * i + j], mul_(a[i], ab[j]));
+        }
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+#pragma unroll
+        for (int j = 0; j < 3; j++) {
+            const int s = 6 + 3 * j + k;   // P(4+k) = C(1,4+k) e1 + C(2,4+k) e2 + C(3,4+k) e3
+            gk[s] = add_(gk[s], mul_(zp[k], e[j]));
+            le[j] = fma_(cs[s - 6], zp[k], le[j]);
+        }
+    X[X_W + 0][p] = le[0];
+    X[X_W + 1][p] = le[1];
+    X[X_W + 2][p] = le[2];
+}
+
+// L4 q: C44 a4 + C45 Z45 + C46 Z46 + Abar4 adjoints of N; slots 15..17
+template <typename T>
+__device__ __forceinline__ void g1_l4_shot(const GridDev<T> &G, const AdjDev<T> &A, const Ext &E, int x, int y, int z,
+                                           T &g15, T &g16, T &g17)
+{
+    const Geo &g = G.g;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const T *const *c = G.c;
+    T *const *X = A.w;
+    const T *l4 = A.l[SYZ], *l5 = A.l[SXZ], *l6 = A.l[SXY];
+    auto I = [&](int xx, int yy, int zz) { return g.idx(xx, yy, zz); };
+    const int p = I(x, y, z);
+    T v[2][2];
+    bool oa[2], ob[2];
+    const T a4 = l4[p], e4 = X[X_E + 3][p];
+    T z45 = T(0), z46 = T(0), sn = T(0);
+    for (int i = 0; i < 2; i++)
+        for (int j = 0; j < 2; j++) {
+            int sx = x + 1 - i, sy = y + 1 - j, sz_ = z;   // L5 t45 over L4 (x-1..x, y-1..y, z)
+            if (E.l5(sx, sy, sz_))
+                z45 = fma_(wgt<T>(in_(sx - 1, 0, nx - 1), in_(sx, 0, nx - 1), in_(sy - 1, 0, ny - 1), in_(sy, 0, ny - 1), i, j),
+                           l5[I(sx, sy, sz_)], z45);
+            sx = x + 1 - i; sy = y; sz_ = z + 1 - j;       // L6 t46 over L4 (x-1..x, y, z-1..z)
+            if (E.l6(sx, sy, sz_))
+                z46 = fma_(wgt<T>(in_(sx - 1, 0, nx - 1), in_(sx, 0, nx - 1), in_(sz_ - 1, 0, nz - 1), in_(sz_, 0, nz - 1), i, j),
+                           l6[I(sx, sy, sz_)], z46);
+            sx = x; sy = y + 1 - i; sz_ = z + 1 - j;       // N Abar4 over L4 (x, y-1..y, z-1..z)
+            if (E.n(sx, sy, sz_))
+                sn = fma_(wgt<T>(in_(sy - 1, 0, ny - 1), in_(sy, 0, ny - 1), in_(sz_ - 1, 0, nz - 1), in_(sz_, 0, nz - 1), i, j),
+                          X[X_S + 0][I(sx, sy, sz_)], sn);
+        }
+    // forward averages t5 (e5 over L5 (x..x+1, y..y+1, z)) and t6 (e6 over L6 (x..x+1, y, z..z+1))
+    for (int i = 0; i < 2; i++) { oa[i] = (x + i) <= nx; ob[i] = (y + i) <= ny; }
+    for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++) v[i][j] = (oa[i] && ob[j]) ? X[X_E + 4][I(x + i, y + j, z)] : T(0);
+    const T t5 = avg4<T>(v, oa, ob);
+    for (int i = 0; i < 2; i++) { oa[i] = (x + i) <= nx; ob[i] = (z + i) <= nz; }
+    for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++) v[i][j] = (oa[i] && ob[j]) ? X[X_E + 5][I(x + i, y, z + j)] : T(0);
+    const T t6 = avg4<T>(v, oa, ob);
+    const T c15 = c[15][p], c16 = c[16][p], c17 = c[17][p];
+    g15 = add_(g15, mul_(a4, e4));
+    g16 = add_(g16, add_(mul_(a4, t5), mul_(z45, e4)));
+    g17 = add_(g17, add_(mul_(a4, t6), mul_(z46, e4)));
+    X[X_W + 3][p] = add_(fma_(c15, a4, fma_(c16, z45, mul_(c17, z46))), sn);
+}
+
+// L5 s: C55 a5 + C56 Z56 + Abar5 adjoints of N + C45 a4 from L4's t5; slots 18, 19
+template <typename T>
+__device__ __forceinline__ void g1_l5_shot(const GridDev<T> &G, const AdjDev<T> &A, const Ext &E, int x, int y, int z,
+                                           T &g18, T &g19)
+{
+    const Geo &g = G.g;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const T *const *c = G.c;
+    T *const *X = A.w;
+    const T *l4 = A.l[SYZ], *l5 = A.l[SXZ], *l6 = A.l[SXY];
+    auto I = [&](int xx, int yy, int zz) { return g.idx(xx, yy, zz); };
+    const int p = I(x, y, z);
+    T v[2][2];
+    bool oa[2], ob[2];
+    const T a5 = l5[p], e5 = X[X_E + 4][p];
+    T z56 = T(0), sn = T(0), s4 = T(0);
+    for (int i = 0; i < 2; i++)
+        for (int j = 0; j < 2; j++) {
+            int qx = x, qy = y - i, qz = z + 1 - j;      // L6 t56 over L5 (x, y..y+1, z-1..z)
+            if (E.l6(qx, qy, qz))
+                z56 = fma_(wgt<T>(qy <= ny, qy + 1 <= ny, in_(qz - 1, 0, nz - 1), in_(qz, 0, nz - 1), i, j), l6[I(qx, qy, qz)], z56);
+            qx = x - i; qy = y; qz = z + 1 - j;          // N Abar5 over L5 (x..x+1, y, z-1..z)
+            if (E.n(qx, qy, qz))
+                sn = fma_(wgt<T>(qx <= nx, qx + 1 <= nx, in_(qz - 1, 0, nz - 1), in_(qz, 0, nz - 1), i, j),
+                          X[X_S + 1][I(qx, qy, qz)], sn);
+            qx = x - i; qy = y - j; qz = z;              // L4 t5 over L5 (x..x+1, y..y+1, z)
+            if (E.l4(qx, qy, qz)) {
+                const int q = I(qx, qy, qz);
+                s4 = fma_(wgt<T>(qx <= nx, qx + 1 <= nx, qy <= ny, qy + 1 <= ny, i, j), mul_(c[16][q], l4[q]), s4);
             }
         }
-        if (in_4) X[X_E + 3][p] = e4;
-        if (fold4) {
-            A.l[SYZ][p] = f4;
-            A.l[SYZ][p - sz] = T(0);
+    // forward average t6 (e6 over L6 (x, y-1..y, z..z+1))
+    for (int i = 0; i < 2; i++) { oa[i] = in_(y - 1 + i, 0, ny - 1); ob[i] = (z + i) <= nz; }
+    for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++) v[i][j] = (oa[i] && ob[j]) ? X[X_E + 5][I(x, y - 1 + i, z + j)] : T(0);
+    const T t6 = avg4<T>(v, oa, ob);
+    const T c18 = c[18][p], c19 = c[19][p];
+    g18 = add_(g18, mul_(a5, e5));
+    g19 = add_(g19, add_(mul_(a5, t6), mul_(z56, e5)));
+    X[X_W + 4][p] = add_(add_(fma_(c18, a5, mul_(c19, z56)), sn), s4);
+}
+
+// L6 t: C66 a6 + Abar6 adjoints of N + C46 a4 (L4 t6) + C56 a5 (L5 t6); slot 20
+template <typename T>
+__device__ __forceinline__ void g1_l6_shot(const GridDev<T> &G, const AdjDev<T> &A, const Ext &E, int x, int y, int z, T &g20)
+{
+    const Geo &g = G.g;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const T *const *c = G.c;
+    T *const *X = A.w;
+    const T *l4 = A.l[SYZ], *l5 = A.l[SXZ], *l6 = A.l[SXY];
+    auto I = [&](int xx, int yy, int zz) { return g.idx(xx, yy, zz); };
+    const int p = I(x, y, z);
+    const T a6 = l6[p];
+    T sn = T(0), s4 = T(0), s5 = T(0);
+    for (int i = 0; i < 2; i++)
+        for (int j = 0; j < 2; j++) {
+            int qx = x - i, qy = y + 1 - j, qz = z;      // N Abar6 over L6 (x..x+1, y-1..y, z)
+            if (E.n(qx, qy, qz))
+                sn = fma_(wgt<T>(qx <= nx, qx + 1 <= nx, in_(qy - 1, 0, ny - 1), in_(qy, 0, ny - 1), i, j),
+                          X[X_S + 2][I(qx, qy, qz)], sn);
+            qx = x - i; qy = y; qz = z - j;              // L4 t6 over L6 (x..x+1, y, z..z+1)
+            if (E.l4(qx, qy, qz)) {
+                const int q = I(qx, qy, qz);
+                s4 = fma_(wgt<T>(qx <= nx, qx + 1 <= nx, qz <= nz, qz + 1 <= nz, i, j), mul_(c[17][q], l4[q]), s4);
+            }
+            qx = x; qy = y + 1 - i; qz = z - j;          // L5 t6 over L6 (x, y-1..y, z..z+1)
+            if (E.l5(qx, qy, qz)) {
+                const int q = I(qx, qy, qz);
+                s5 = fma_(wgt<T>(in_(qy - 1, 0, ny - 1), in_(qy, 0, ny - 1), qz <= nz, qz + 1 <= nz, i, j),
+                          mul_(c[19][q], l5[q]), s5);
+            }
         }
-        if (in_5) X[X_E + 4][p] = e5;
-        if (fold5) {
-            A.l[SXZ][p] = f5;
-            A.l[SXZ][p - sz] = T(0);
+    const T e6 = X[X_E + 5][p], c20 = c[20][p];
+    g20 = add_(g20, mul_(a6, e6));
+    X[X_W + 5][p] = add_(add_(fma_(c20, a6, sn), s4), s5);
+}
+
+// One point of G1 for shots 0..ns-1: the gradient slots of each position
+// block are read once, take every shot's terms in shot order, and are written
+// once.  shot(s, Gs, As) gives shot s's forward-field and adjoint views.
+template <typename T, typename Shot>
+__device__ __forceinline__ void g1_point(const GridDev<T> &G, const AdjDev<T> &A0, int flag, const Ext &E, int x, int y,
+                                         int z, int ns, Shot shot)
+{
+    const int p = G.g.idx(x, y, z);
+    if (E.n(x, y, z)) {
+        T gk[15];
+#pragma unroll
+        for (int k = 0; k < 15; k++) gk[k] = A0.gc[k][p];
+        for (int s = 0; s < ns; s++) {
+            GridDev<T> Gs;
+            AdjDev<T> As;
+            shot(s, Gs, As);
+            g1_n_shot(Gs, As, flag, E, x, y, z, gk);
         }
-        if (in_6) X[X_E + 5][p] = e6;
+#pragma unroll
+        for (int k = 0; k < 15; k++) A0.gc[k][p] = gk[k];
+    }
+    if (E.l4(x, y, z)) {
+        T g15 = A0.gc[15][p], g16 = A0.gc[16][p], g17 = A0.gc[17][p];
+        for (int s = 0; s < ns; s++) {
+            GridDev<T> Gs;
+            AdjDev<T> As;
+            shot(s, Gs, As);
+            g1_l4_shot(Gs, As, E, x, y, z, g15, g16, g17);
+        }
+        A0.gc[15][p] = g15;
+        A0.gc[16][p] = g16;
+        A0.gc[17][p] = g17;
+    }
+    if (E.l5(x, y, z)) {
+        T g18 = A0.gc[18][p], g19 = A0.gc[19][p];
+        for (int s = 0; s < ns; s++) {
+            GridDev<T> Gs;
+            AdjDev<T> As;
+            shot(s, Gs, As);
+            g1_l5_shot(Gs, As, E, x, y, z, g18, g19);
+        }
+        A0.gc[18][p] = g18;
+        A0.gc[19][p] = g19;
+    }
+    if (E.l6(x, y, z)) {
+        T g20 = A0.gc[20][p];
+        for (int s = 0; s < ns; s++) {
+            GridDev<T> Gs;
+            AdjDev<T> As;
+            shot(s, Gs, As);
+            g1_l6_shot(Gs, As, E, x, y, z, g20);
+        }
+        A0.gc[20][p] = g20;
     }
 }
 
@@ -254,163 +583,62 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) stress21_adj_g1(G
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     const Ext E{nx, ny, nz};
     const int64_t n = (int64_t)(nx + 1) * (ny + 1) * (nz + 1);
-    const T *const *c = G.c;
-    T *const *X = A.w;
-    const T *l4 = A.l[SYZ], *l5 = A.l[SXZ], *l6 = A.l[SXY];
-    auto I = [&](int x, int y, int z) { return g.idx(x, y, z); };
+    auto one = [&](int, GridDev<T> &Gs, AdjDev<T> &As) { Gs = G; As = A; };
     for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
         const int x = (int)(t % (nx + 1)), y = (int)((t / (nx + 1)) % (ny + 1)), z = (int)(t / ((int64_t)(nx + 1) * (ny + 1)));
-        const int p = I(x, y, z);
-        T v[2][2];
-        bool oa[2], ob[2];
-        // ---- N: adjoints of P4..6 gathered from L4 / L5 / L6, forward averages, gradients
-        if (E.n(x, y, z)) {
-            T zp[3] = {T(0), T(0), T(0)};
-            for (int i = 0; i < 2; i++)
-                for (int j = 0; j < 2; j++) {
-                    int qx = x, qy = y - i, qz = z - j;   // L4 tp over N (x, y..y+1, z..z+1)
-                    if (E.l4(qx, qy, qz))
-                        zp[0] = fma_(wgt<T>(qy <= ny, qy + 1 <= ny, qz <= nz, qz + 1 <= nz, i, j), l4[I(qx, qy, qz)], zp[0]);
-                    qx = x + 1 - i; qy = y; qz = z - j;   // L5 tp over N (x-1..x, y, z..z+1)
-                    if (E.l5(qx, qy, qz))
-                        zp[1] = fma_(wgt<T>(in_(qx - 1, 0, nx - 1), in_(qx, 0, nx - 1), qz <= nz, qz + 1 <= nz, i, j),
-                                     l5[I(qx, qy, qz)], zp[1]);
-                    qx = x + 1 - i; qy = y - j; qz = z;   // L6 P6 over N (x-1..x, y..y+1, z)
-                    if (E.l6(qx, qy, qz))
-                        zp[2] = fma_(wgt<T>(in_(qx - 1, 0, nx - 1), in_(qx, 0, nx - 1), qy <= ny, qy + 1 <= ny, i, j),
-                                     l6[I(qx, qy, qz)], zp[2]);
-                }
-            const T e[3] = {X[X_E + 0][p], X[X_E + 1][p], X[X_E + 2][p]};
-            T ab[3];
-            for (int i = 0; i < 2; i++) { oa[i] = in_(y - 1 + i, 0, ny - 1); ob[i] = in_(z - 1 + i, 0, nz - 1); }
-            for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++) v[i][j] = (oa[i] && ob[j]) ? X[X_E + 3][I(x, y - 1 + i, z - 1 + j)] : T(0);
-            ab[0] = avg4<T>(v, oa, ob);
-            for (int i = 0; i < 2; i++) { oa[i] = (x + i) <= nx; ob[i] = in_(z - 1 + i, 0, nz - 1); }
-            for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++) v[i][j] = (oa[i] && ob[j]) ? X[X_E + 4][I(x + i, y, z - 1 + j)] : T(0);
-            ab[1] = avg4<T>(v, oa, ob);
-            for (int i = 0; i < 2; i++) { oa[i] = (x + i) <= nx; ob[i] = in_(y - 1 + i, 0, ny - 1); }
-            for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++) v[i][j] = (oa[i] && ob[j]) ? X[X_E + 5][I(x + i, y - 1 + j, z)] : T(0);
-            ab[2] = avg4<T>(v, oa, ob);
-            const bool surf = flag && z == 0;
-            const T a[3] = {A.l[SXX][p], A.l[SYY][p], surf ? T(0) : A.l[SZZ][p]};
-            // every load of the block before its first store (the pointers may
-            // alias as far as the compiler knows, so loads after a store would
-            // each wait for memory in turn); same updates in the same order
-            T gk[15], cs[9];
+        g1_point(G, A, flag, E, x, y, z, 1, one);
+    }
+}
+
+// Views of shot s: the common medium and gradients with the shot's fields,
+// adjoint fields and work boxes.
+template <typename T>
+__device__ __forceinline__ void shot_views(const GridDev<T> &G, const AdjDev<T> &A0, const AdjShots<T> &S, int s,
+                                           GridDev<T> &Gs, AdjDev<T> &As)
+{
+    Gs = G;
+    As = A0;
 #pragma unroll
-            for (int k = 0; k < 15; k++) gk[k] = A.gc[k][p];
+    for (int k = 0; k < 9; k++) {
+        Gs.f[k] = S.f[s] + k * S.box;
+        As.l[k] = S.l[s] + k * S.box;
+    }
 #pragma unroll
-            for (int k = 0; k < 9; k++) cs[k] = c[6 + k][p];
-            T le[3] = {X[X_W + 0][p], X[X_W + 1][p], X[X_W + 2][p]};
-            const int rowc[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
-#pragma unroll
-            for (int i = 0; i < 3; i++)
-#pragma unroll
-                for (int j = 0; j < 3; j++) {
-                    gk[rowc[i][j]] = add_(gk[rowc[i][j]], mul_(a[i], e[j]));
-                    gk[6 + 3 * i + j] = add_(gk[6 + 3 * i + j], mul_(a[i], ab[j]));
-                }
-#pragma unroll
-            for (int k = 0; k < 3; k++)
-#pragma unroll
-                for (int j = 0; j < 3; j++) {
-                    const int s = 6 + 3 * j + k;   // P(4+k) = C(1,4+k) e1 + C(2,4+k) e2 + C(3,4+k) e3
-                    gk[s] = add_(gk[s], mul_(zp[k], e[j]));
-                    le[j] = fma_(cs[s - 6], zp[k], le[j]);
-                }
-#pragma unroll
-            for (int k = 0; k < 15; k++) A.gc[k][p] = gk[k];
-            X[X_W + 0][p] = le[0];
-            X[X_W + 1][p] = le[1];
-            X[X_W + 2][p] = le[2];
+    for (int k = 0; k < 15; k++) As.w[k] = S.w[s] + k * S.wbox;
+}
+
+// G0 of every shot at each point (the medium read once from DRAM for all)
+template <typename T>
+__global__ void stress21_adj_g0_shots(GridDev<T> G, AdjDev<T> A0, const __grid_constant__ AdjShots<T> S, int flag)
+{
+    const Geo &g = G.g;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const Ext E{nx, ny, nz};
+    const int64_t n = (int64_t)(nx + 1) * (ny + 1) * (nz + 1);
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+        const int x = (int)(t % (nx + 1)), y = (int)((t / (nx + 1)) % (ny + 1)), z = (int)(t / ((int64_t)(nx + 1) * (ny + 1)));
+        for (int s = 0; s < S.ns; s++) {
+            GridDev<T> Gs;
+            AdjDev<T> As;
+            shot_views(G, A0, S, s, Gs, As);
+            g0_point(Gs, As, flag, E, x, y, z);
         }
-        // ---- L4 q: C44 a4 + C45 Z45 + C46 Z46 + Abar4 adjoints of N
-        if (E.l4(x, y, z)) {
-            const T a4 = l4[p], e4 = X[X_E + 3][p];
-            T z45 = T(0), z46 = T(0), sn = T(0);
-            for (int i = 0; i < 2; i++)
-                for (int j = 0; j < 2; j++) {
-                    int sx = x + 1 - i, sy = y + 1 - j, sz_ = z;   // L5 t45 over L4 (x-1..x, y-1..y, z)
-                    if (E.l5(sx, sy, sz_))
-                        z45 = fma_(wgt<T>(in_(sx - 1, 0, nx - 1), in_(sx, 0, nx - 1), in_(sy - 1, 0, ny - 1), in_(sy, 0, ny - 1), i, j),
-                                   l5[I(sx, sy, sz_)], z45);
-                    sx = x + 1 - i; sy = y; sz_ = z + 1 - j;       // L6 t46 over L4 (x-1..x, y, z-1..z)
-                    if (E.l6(sx, sy, sz_))
-                        z46 = fma_(wgt<T>(in_(sx - 1, 0, nx - 1), in_(sx, 0, nx - 1), in_(sz_ - 1, 0, nz - 1), in_(sz_, 0, nz - 1), i, j),
-                                   l6[I(sx, sy, sz_)], z46);
-                    sx = x; sy = y + 1 - i; sz_ = z + 1 - j;       // N Abar4 over L4 (x, y-1..y, z-1..z)
-                    if (E.n(sx, sy, sz_))
-                        sn = fma_(wgt<T>(in_(sy - 1, 0, ny - 1), in_(sy, 0, ny - 1), in_(sz_ - 1, 0, nz - 1), in_(sz_, 0, nz - 1), i, j),
-                                  X[X_S + 0][I(sx, sy, sz_)], sn);
-                }
-            // forward averages t5 (e5 over L5 (x..x+1, y..y+1, z)) and t6 (e6 over L6 (x..x+1, y, z..z+1))
-            for (int i = 0; i < 2; i++) { oa[i] = (x + i) <= nx; ob[i] = (y + i) <= ny; }
-            for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++) v[i][j] = (oa[i] && ob[j]) ? X[X_E + 4][I(x + i, y + j, z)] : T(0);
-            const T t5 = avg4<T>(v, oa, ob);
-            for (int i = 0; i < 2; i++) { oa[i] = (x + i) <= nx; ob[i] = (z + i) <= nz; }
-            for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++) v[i][j] = (oa[i] && ob[j]) ? X[X_E + 5][I(x + i, y, z + j)] : T(0);
-            const T t6 = avg4<T>(v, oa, ob);
-            const T g15 = A.gc[15][p], g16 = A.gc[16][p], g17 = A.gc[17][p];
-            const T c15 = c[15][p], c16 = c[16][p], c17 = c[17][p];
-            A.gc[15][p] = add_(g15, mul_(a4, e4));
-            A.gc[16][p] = add_(g16, add_(mul_(a4, t5), mul_(z45, e4)));
-            A.gc[17][p] = add_(g17, add_(mul_(a4, t6), mul_(z46, e4)));
-            X[X_W + 3][p] = add_(fma_(c15, a4, fma_(c16, z45, mul_(c17, z46))), sn);
-        }
-        // ---- L5 s: C55 a5 + C56 Z56 + Abar5 adjoints of N + C45 a4 from L4's t5
-        if (E.l5(x, y, z)) {
-            const T a5 = l5[p], e5 = X[X_E + 4][p];
-            T z56 = T(0), sn = T(0), s4 = T(0);
-            for (int i = 0; i < 2; i++)
-                for (int j = 0; j < 2; j++) {
-                    int qx = x, qy = y - i, qz = z + 1 - j;      // L6 t56 over L5 (x, y..y+1, z-1..z)
-                    if (E.l6(qx, qy, qz))
-                        z56 = fma_(wgt<T>(qy <= ny, qy + 1 <= ny, in_(qz - 1, 0, nz - 1), in_(qz, 0, nz - 1), i, j), l6[I(qx, qy, qz)], z56);
-                    qx = x - i; qy = y; qz = z + 1 - j;          // N Abar5 over L5 (x..x+1, y, z-1..z)
-                    if (E.n(qx, qy, qz))
-                        sn = fma_(wgt<T>(qx <= nx, qx + 1 <= nx, in_(qz - 1, 0, nz - 1), in_(qz, 0, nz - 1), i, j),
-                                  X[X_S + 1][I(qx, qy, qz)], sn);
-                    qx = x - i; qy = y - j; qz = z;              // L4 t5 over L5 (x..x+1, y..y+1, z)
-                    if (E.l4(qx, qy, qz)) {
-                        const int q = I(qx, qy, qz);
-                        s4 = fma_(wgt<T>(qx <= nx, qx + 1 <= nx, qy <= ny, qy + 1 <= ny, i, j), mul_(c[16][q], l4[q]), s4);
-                    }
-                }
-            // forward average t6 (e6 over L6 (x, y-1..y, z..z+1))
-            for (int i = 0; i < 2; i++) { oa[i] = in_(y - 1 + i, 0, ny - 1); ob[i] = (z + i) <= nz; }
-            for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++) v[i][j] = (oa[i] && ob[j]) ? X[X_E + 5][I(x, y - 1 + i, z + j)] : T(0);
-            const T t6 = avg4<T>(v, oa, ob);
-            const T g18 = A.gc[18][p], g19 = A.gc[19][p], c18 = c[18][p], c19 = c[19][p];
-            A.gc[18][p] = add_(g18, mul_(a5, e5));
-            A.gc[19][p] = add_(g19, add_(mul_(a5, t6), mul_(z56, e5)));
-            X[X_W + 4][p] = add_(add_(fma_(c18, a5, mul_(c19, z56)), sn), s4);
-        }
-        // ---- L6 t: C66 a6 + Abar6 adjoints of N + C46 a4 (L4 t6) + C56 a5 (L5 t6)
-        if (E.l6(x, y, z)) {
-            const T a6 = l6[p];
-            T sn = T(0), s4 = T(0), s5 = T(0);
-            for (int i = 0; i < 2; i++)
-                for (int j = 0; j < 2; j++) {
-                    int qx = x - i, qy = y + 1 - j, qz = z;      // N Abar6 over L6 (x..x+1, y-1..y, z)
-                    if (E.n(qx, qy, qz))
-                        sn = fma_(wgt<T>(qx <= nx, qx + 1 <= nx, in_(qy - 1, 0, ny - 1), in_(qy, 0, ny - 1), i, j),
-                                  X[X_S + 2][I(qx, qy, qz)], sn);
-                    qx = x - i; qy = y; qz = z - j;              // L4 t6 over L6 (x..x+1, y, z..z+1)
-                    if (E.l4(qx, qy, qz)) {
-                        const int q = I(qx, qy, qz);
-                        s4 = fma_(wgt<T>(qx <= nx, qx + 1 <= nx, qz <= nz, qz + 1 <= nz, i, j), mul_(c[17][q], l4[q]), s4);
-                    }
-                    qx = x; qy = y + 1 - i; qz = z - j;          // L5 t6 over L6 (x, y-1..y, z..z+1)
-                    if (E.l5(qx, qy, qz)) {
-                        const int q = I(qx, qy, qz);
-                        s5 = fma_(wgt<T>(in_(qy - 1, 0, ny - 1), in_(qy, 0, ny - 1), qz <= nz, qz + 1 <= nz, i, j),
-                                  mul_(c[19][q], l5[q]), s5);
-                    }
-                }
-            const T g20 = A.gc[20][p], e6 = X[X_E + 5][p], c20 = c[20][p];
-            A.gc[20][p] = add_(g20, mul_(a6, e6));
-            X[X_W + 5][p] = add_(add_(fma_(c20, a6, sn), s4), s5);
-        }
+    }
+}
+
+// G1 of every shot at each point: the gradient slots read and written once
+template <typename T>
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2)
+    stress21_adj_g1_shots(GridDev<T> G, AdjDev<T> A0, const __grid_constant__ AdjShots<T> S, int flag)
+{
+    const Geo &g = G.g;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const Ext E{nx, ny, nz};
+    const int64_t n = (int64_t)(nx + 1) * (ny + 1) * (nz + 1);
+    auto shot = [&](int s, GridDev<T> &Gs, AdjDev<T> &As) { shot_views(G, A0, S, s, Gs, As); };
+    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
+        const int x = (int)(t % (nx + 1)), y = (int)((t / (nx + 1)) % (ny + 1)), z = (int)(t / ((int64_t)(nx + 1) * (ny + 1)));
+        g1_point(G, A0, flag, E, x, y, z, S.ns, shot);
     }
 }
 
@@ -548,6 +776,52 @@ cudaError_t launch_stress21_adj(const GridDev<T> &G, const AdjDev<T> &A, int top
     return cudaGetLastError();
 }
 
+// The 21-Cij stress adjoint of every shot of one grid: G0 and G1 once for all
+// shots, then G2 (free surface) and G3 per shot; A0 holds the common gradients.
+template <typename T>
+cudaError_t launch_stress21_adj_shots(const GridDev<T> &G, const AdjDev<T> &A0, const AdjShots<T> &S, int top, int top_bc,
+                                      int sms, cudaStream_t st)
+{
+    const Geo &g = G.g;
+    const int flag = (top && top_bc) ? 1 : 0;
+    const int64_t n = (int64_t)(g.nx + 1) * (g.ny + 1) * (g.nz + 1);
+    const unsigned nb = blocks_for(n, sms);
+    stress21_adj_g0_shots<T><<<nb, 256, 0, st>>>(G, A0, S, flag);
+    stress21_adj_g1_shots<T><<<nb, 256, 0, st>>>(G, A0, S, flag);
+    for (int s = 0; s < S.ns; s++) {
+        GridDev<T> Gs = G;
+        AdjDev<T> As = A0;
+        for (int k = 0; k < 9; k++) {
+            Gs.f[k] = S.f[s] + k * S.box;
+            As.l[k] = S.l[s] + k * S.box;
+        }
+        for (int k = 0; k < 15; k++) As.w[k] = S.w[s] + k * S.wbox;
+        if (flag) stress21_adj_g2<T><<<(g.nx * (g.ny + 1) + 255) / 256, 256, 0, st>>>(Gs, As);
+        stress21_adj_g3<T><<<blocks_for((int64_t)(g.nx + 2) * (g.ny + 2) * (g.nz + 2), sms), 256, 0, st>>>(Gs, As);
+    }
+    return cudaGetLastError();
+}
+
+// The velocity adjoint of every shot of one grid: each shot's mirror
+// transposes, then the update's transpose for all shots at once.
+template <typename T>
+cudaError_t launch_vel_adj_shots(const GridDev<T> &G, T *gb, const AdjShots<T> &S, int top, int bottom, int top_bc,
+                                 int mirror_fix, int sms, cudaStream_t st)
+{
+    const Geo &g = G.g;
+    const int top_rigid = (top && top_bc != 1) ? 1 : 0;
+    const int64_t n0 = (int64_t)(top_rigid + bottom) * (g.ny + 1) * g.nx + 2LL * g.nz * (g.ny + 1)
+                     + 2LL * (g.nz + 1) * (g.ny + 1);
+    const int64_t n1 = 2LL * (g.nz + (mirror_fix ? 1 : 0)) * g.nx;
+    for (int s = 0; s < S.ns; s++) {
+        T *lvy = S.l[s] + VY * S.box, *lvz = S.l[s] + VZ * S.box;
+        vel_mirror_adj_kernel<T><<<(unsigned)((n1 + 255) / 256), 256, 0, st>>>(g, lvy, lvz, 1, top_rigid, bottom, mirror_fix);
+        vel_mirror_adj_kernel<T><<<(unsigned)((n0 + 255) / 256), 256, 0, st>>>(g, lvy, lvz, 0, top_rigid, bottom, mirror_fix);
+    }
+    vel_adj_shots_kernel<T><<<blocks_for((int64_t)g.nx * g.ny * (g.nz + 1), sms), 256, 0, st>>>(G, gb, S, top_rigid, bottom);
+    return cudaGetLastError();
+}
+
 template <typename T>
 cudaError_t launch_rec_adj(const RecAdj<T> &R, cudaStream_t st)
 {
@@ -561,7 +835,11 @@ cudaError_t launch_rec_adj(const RecAdj<T> &R, cudaStream_t st)
                                            cudaStream_t);                                                   \
     template cudaError_t launch_stress21_adj<T>(const GridDev<T> &, const AdjDev<T> &, int, int, int,          \
                                                 cudaStream_t);                                              \
-    template cudaError_t launch_rec_adj<T>(const RecAdj<T> &, cudaStream_t);
+    template cudaError_t launch_rec_adj<T>(const RecAdj<T> &, cudaStream_t);                                  \
+    template cudaError_t launch_stress21_adj_shots<T>(const GridDev<T> &, const AdjDev<T> &, const AdjShots<T> &,  \
+                                                      int, int, int, cudaStream_t);                              \
+    template cudaError_t launch_vel_adj_shots<T>(const GridDev<T> &, T *, const AdjShots<T> &, int, int, int, int,  \
+                                                 int, cudaStream_t);
 INST(float)
 INST(double)
 #undef INST

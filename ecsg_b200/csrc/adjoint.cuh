@@ -13,6 +13,20 @@ struct AdjDev {
     T *w[15];    // work boxes of the stress adjoint (strains, average adjoints, strain adjoints)
 };
 
+// Shots of one grid advanced together (shots sharing one medium): per shot
+// the block of the 9 forward fields the operator reads (field k at
+// f[s] + k * box), the block of its 9 adjoint fields (l[s] + k * box) and its
+// 15 work boxes (w[s] + k * wbox).  The medium and the gradient arrays are
+// the shots' common ones.
+template <typename T>
+struct AdjShots {
+    int ns;
+    T *f[kMaxShots];
+    T *l[kMaxShots];
+    T *w[kMaxShots];
+    int64_t box, wbox;
+};
+
 // Receiver adjoint sources of one step: lambda_{comp}[grid][off] += res[i].
 template <typename T>
 struct RecAdj {

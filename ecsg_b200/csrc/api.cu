@@ -87,6 +87,10 @@ cudaError_t launch_vel_adj(const GridDev<T> &, const AdjDev<T> &, int, int, int,
 template <typename T>
 cudaError_t launch_stress21_adj(const GridDev<T> &, const AdjDev<T> &, int, int, int, cudaStream_t);
 template <typename T>
+cudaError_t launch_stress21_adj_shots(const GridDev<T> &, const AdjDev<T> &, const AdjShots<T> &, int, int, int, cudaStream_t);
+template <typename T>
+cudaError_t launch_vel_adj_shots(const GridDev<T> &, T *, const AdjShots<T> &, int, int, int, int, int, cudaStream_t);
+template <typename T>
 cudaError_t launch_rec_adj(const RecAdj<T> &, cudaStream_t);
 template <typename T>
 cudaError_t launch_rec_sample(const SrcRec &, T *, cudaStream_t);
@@ -175,8 +179,8 @@ struct ecsg_sim {
     size_t wbox = 0;                                  // elements of one work box (the largest grid's box)
     double *adj_lx[kMaxGrids] = {}, *adj_y[kMaxGrids] = {}, *adj_Y0[kMaxGrids] = {}, *adj_Y1[kMaxGrids] = {};
     // misfit-gradient driver: checkpoints, segment states, samples, observations
-    char *ckpt = nullptr, *seg = nullptr;
-    size_t ckpt_cap = 0, seg_cap = 0;
+    char *ckpt = nullptr, *seg = nullptr, *seg2 = nullptr;   // seg2: sub-checkpoints of lockstep shots
+    size_t ckpt_cap = 0, seg_cap = 0, seg2_cap = 0;
     void *recT = nullptr;
     size_t recT_cap = 0;
     float *obs = nullptr;
@@ -475,7 +479,7 @@ int ecsg_destroy(ecsg_sim *s)
     cudaFree(s->partial); cudaFree(s->ints); cudaFree(s->iters_total); cudaFree(s->dscal); cudaFree(s->bar);
     cudaFree(s->src_trace); cudaFree(s->rec_grid); cudaFree(s->rec_off); cudaFree(s->traces);
     cudaFree(s->run_energy); cudaFree(s->run_res); cudaFree(s->snap);
-    cudaFree(s->wblk); cudaFree(s->ckpt); cudaFree(s->seg); cudaFree(s->recT); cudaFree(s->obs);
+    cudaFree(s->wblk); cudaFree(s->ckpt); cudaFree(s->seg); cudaFree(s->seg2); cudaFree(s->recT); cudaFree(s->obs);
     for (int v = 0; v < 2; v++)
         if (s->gx[v]) cudaGraphExecDestroy(s->gx[v]);
     for (int e = 0; e < 4; e++)
@@ -2232,6 +2236,344 @@ int ecsg_sum_gradients(ecsg_sim *dst, ecsg_sim *const *srcs, int n)
         }
     cudaFree(dptr);
     return ECSG_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Shots in lockstep (no reference counterpart): the misfit gradients of S
+// shots that share one medium (instances of one model made by
+// ecsg_create_shot), advanced together step by step on one stream.  Every
+// phase of a forward or adjoint step runs for all shots before the next
+// phase, so that the phases that read the medium (the stress and velocity
+// adjoints) or solve interface systems (the sxz solves) do so once for all
+// shots; the others run per shot.  Checkpoints: every k steps
+// (k = ckpt_every); the states inside a segment are recomputed from its
+// checkpoint, directly when the k + 1 states of every shot fit in device
+// memory, otherwise through sub-checkpoints every j steps (j ~ sqrt(k)) and
+// j + 1 states, for one more forward pass.  The gradient of the sum of the
+// shots' misfits is left in sims[0]: the stress and velocity adjoints add
+// every shot's terms to sims[0]'s gradient arrays directly (one read-modify-
+// write per point for all shots), the interface adjoints add to each shot's
+// own arrays, and the shots' arrays are summed in FP64 at the end.
+// losses[b] is shot b's misfit.
+// ---------------------------------------------------------------------------
+static int group_check(ecsg_sim *const *sims, int S)
+{
+    if (int rc = batch_check(sims, S)) return rc;
+    ecsg_sim *m = sims[0];
+    const ecsg_sim *model = m->share ? m->share : m;
+    for (int b = 0; b < S; b++) {
+        ecsg_sim *x = sims[b];
+        if (int rc = adj_check(x)) return rc;
+        const ecsg_sim *xm = x->share ? x->share : x;
+        if (xm != model) return fail(m, ECSG_ERR_INVALID, "shots: instance %d does not share the first instance's medium", b);
+        if (x->nrec != m->nrec || x->rec_comp != m->rec_comp)
+            return fail(m, ECSG_ERR_INVALID, "shots: instance %d has another receiver count or component", b);
+    }
+    return ECSG_OK;
+}
+
+// Runs f(x, b) for every shot with the shot's library stream set to the group's stream.
+template <typename F>
+static int each_shot(ecsg_sim *const *sims, int S, F f)
+{
+    cudaStream_t gs = sims[0]->st;
+    for (int b = 0; b < S; b++) {
+        ecsg_sim *x = sims[b];
+        cudaStream_t own = x->st;
+        x->st = gs;
+        const int rc = f(x, b);
+        x->st = own;
+        if (rc) return x == sims[0] ? rc : fail(sims[0], rc, "shot %d: %s", b, x->err.c_str());
+    }
+    return ECSG_OK;
+}
+
+// The sxz solves of every interface of every shot: one cooperative launch over
+// as many (shot, interface) systems as fit co-resident, each bitwise as in its
+// own launch.
+template <typename T>
+static int group_sxz_op(ecsg_sim *const *sims, int S)
+{
+    ecsg_sim *m = sims[0], *s = m;   // s: where CK reports
+    if (m->imode == ECSG_MODE_II || !m->sxz_fused)
+        return each_shot(sims, S, [&](ecsg_sim *x, int) { return sxz_all_op<T>(x); });
+    SxzSysList<T> L;
+    int cta = 0;
+    auto flush = [&]() -> int {
+        if (!L.n) return ECSG_OK;
+        L.r = m->itf[1].r;
+        L.bar = m->bar;
+        L.status = m->ints;
+        CK(launch_sxz_solve_multi<T>(L, m->st));
+        return ECSG_OK;
+    };
+    memset(&L, 0, sizeof L);
+    for (int b = 0; b < S; b++) {
+        ecsg_sim *x = sims[b];
+        for (int i = 1; i < x->ng; i++) {
+            const int nb = x->itf[i].nblocks;
+            if (x->itf[i].r != m->itf[1].r) return fail(m, ECSG_ERR_INVALID, "shots: interfaces of different ratios");
+            if (L.n == kMaxSxzSys || cta + nb > m->sxz_cap) {
+                if (int rc = flush()) return rc;
+                memset(&L, 0, sizeof L);
+                cta = 0;
+            }
+            SxzSys<T> &Y = L.s[L.n++];
+            Y.F = dev<T>(x, i - 1);
+            Y.C = dev<T>(x, i);
+            Y.W = sxz_work(x, i);
+            Y.cta0 = cta;
+            Y.ncta = nb;
+            cta += nb;
+        }
+    }
+    return flush();
+}
+
+// One forward step of every shot (the order of main.cpp:165-261 within each
+// shot); sample_rows[b]: shot b's receiver samples of this step, or null.
+template <typename T>
+static int group_step_op(ecsg_sim *const *sims, int S, T *const *sample_rows)
+{
+    ecsg_sim *s = sims[0];   // where CK reports
+    int rc;
+    if ((rc = each_shot(sims, S, [&](ecsg_sim *x, int) { return each_grid(x, [&](int g) { return vel_op<T>(x, g, false); }); })))
+        return rc;
+    if ((rc = each_shot(sims, S, [&](ecsg_sim *x, int b) -> int {
+             if (sample_rows && sample_rows[b]) CK(launch_rec_sample<T>(make_srcrec(x, 0), sample_rows[b], x->st));
+             CK(launch_src_rec<T>(make_srcrec(x, 3), x->st));
+             return each_vz_ghost<T>(x);
+         })))
+        return rc;
+    if ((rc = each_shot(sims, S, [&](ecsg_sim *x, int) { return each_grid(x, [&](int g) { return stress_op<T>(x, g); }); })))
+        return rc;
+    if ((rc = group_sxz_op<T>(sims, S))) return rc;
+    return each_shot(sims, S, [&](ecsg_sim *x, int) -> int {
+        for (int i = 1; i < x->ng; i++)
+            if (int r2 = syz_op<T>(x, i)) return r2;
+        return ECSG_OK;
+    });
+}
+
+// The shots' views of grid g for the multi-shot adjoint kernels: forward
+// fields from each shot's stored state `st[b]`, its adjoint fields and work boxes.
+template <typename T>
+static AdjShots<T> shot_set(ecsg_sim *const *sims, int S, int g, const char *const *st)
+{
+    AdjShots<T> A;
+    memset(&A, 0, sizeof A);
+    A.ns = S;
+    A.box = sims[0]->geo[g].size();
+    A.wbox = (int64_t)sims[0]->wbox;
+    for (int b = 0; b < S; b++) {
+        A.f[b] = dev_state<T>(sims[b], g, st[b]).f[0];
+        A.l[b] = (T *)sims[b]->lblk[g];
+        A.w[b] = (T *)sims[b]->wblk;
+    }
+    return A;
+}
+
+// One adjoint step of every shot: sa[b] / sb[b] are shot b's stored states
+// after / before the step.
+template <typename T>
+static int group_adjoint_step(ecsg_sim *const *sims, int S, const char *const *sa, const char *const *sbf, int n)
+{
+    ecsg_sim *m = sims[0], *s = m;   // s: where CK reports
+    const int ng = m->ng;
+    int rc;
+    auto states = [&](ecsg_sim *x, int b, const char *const *st, GridDev<T> *Gv) {
+        for (int g = 0; g < ng; g++) Gv[g] = dev_state<T>(x, g, st[b]);
+    };
+    if ((rc = each_shot(sims, S, [&](ecsg_sim *x, int b) -> int {
+             GridDev<T> Ga[kMaxGrids];
+             states(x, b, sa, Ga);
+             for (int i = ng - 1; i >= 1; i--) {
+                 if (int r2 = adj_op_impl<T>(x, ECSG_ADJ_GHOST_SYZ, i, Ga)) return r2;
+                 if (int r2 = adj_op_impl<T>(x, ECSG_ADJ_GHOST_SXZ, i, Ga)) return r2;
+             }
+             return ECSG_OK;
+         })))
+        return rc;
+    for (int g = 0; g < ng; g++)
+        CK(launch_stress21_adj_shots<T>(dev<T>(m, g), adj_dev<T>(m, g), shot_set<T>(sims, S, g, sa), g == 0, m->top_bc,
+                                        m->sms, m->st));
+    if ((rc = each_shot(sims, S, [&](ecsg_sim *x, int b) -> int {
+             GridDev<T> Ga[kMaxGrids];
+             states(x, b, sa, Ga);
+             for (int i = ng - 1; i >= 1; i--)
+                 if (int r2 = adj_op_impl<T>(x, ECSG_ADJ_GHOST_VZ, i, Ga)) return r2;
+             if (x->nrec) {
+                 RecAdj<T> R;
+                 memset(&R, 0, sizeof R);
+                 for (int g = 0; g < ng; g++) R.lbase[g] = adj_dev<T>(x, g).l[x->rec_comp];
+                 R.grid = x->rec_grid;
+                 R.off = x->rec_off;
+                 R.nrec = x->nrec;
+                 R.res = (T *)x->recT + (size_t)n * x->nrec;
+                 CK(launch_rec_adj<T>(R, x->st));
+             }
+             return ECSG_OK;
+         })))
+        return rc;
+    for (int g = ng - 1; g >= 0; g--)
+        CK(launch_vel_adj_shots<T>(dev<T>(m, g), (T *)m->gbblk[g], shot_set<T>(sims, S, g, sbf), g == 0, g == ng - 1,
+                                   m->top_bc, m->mirror_fix, m->sms, m->st));
+    return ECSG_OK;
+}
+
+template <typename T>
+static int group_gradient_op(ecsg_sim *const *sims, int S, int nsteps, const float *const *observed, int k,
+                             int sub_every, double *losses)
+{
+    int rc;
+    ecsg_sim *m = sims[0], *s = m;   // s: where CK reports
+    cudaStream_t gs = m->st;
+    const size_t sb = state_bytes(m);
+    const int ncp = (nsteps + k - 1) / k;
+    const size_t nrec = (size_t)m->nrec, nobs = (size_t)nsteps * nrec;
+    auto grow = [&](ecsg_sim *x, void **p, size_t &cap, size_t want) -> int {
+        if (cap >= want) return ECSG_OK;
+        cudaFree(*p);
+        *p = nullptr;
+        cap = 0;
+        if (cudaMalloc(p, want) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(m, ECSG_ERR_CUDA, "shots: %zu bytes of checkpoint memory for shot %p", want, (void *)x);
+        }
+        cap = want;
+        return ECSG_OK;
+    };
+    // checkpoints and observations first; then the segment buffers, one level
+    // (k + 1 states) if they fit, else two (sub-checkpoints every j steps)
+    for (int b = 0; b < S; b++) {
+        ecsg_sim *x = sims[b];
+        if ((rc = grow(x, (void **)&x->ckpt, x->ckpt_cap, sb * (ncp + 1)))) return rc;
+        if ((rc = grow(x, &x->recT, x->recT_cap, sizeof(T) * (nobs > 0 ? nobs : 1)))) return rc;
+        if ((rc = grow(x, (void **)&x->obs, x->obs_cap, sizeof(float) * (nobs > 0 ? nobs : 1)))) return rc;
+        if (nobs) CK(cudaMemcpyAsync(x->obs, observed[b], sizeof(float) * nobs, cudaMemcpyHostToDevice, gs));
+    }
+    int j = k;
+    if (sub_every > 0 && sub_every < k) j = sub_every;
+    {
+        size_t free_b = 0, total_b = 0;
+        CK(cudaMemGetInfo(&free_b, &total_b));
+        size_t have = free_b;
+        for (int b = 0; b < S; b++) have += sims[b]->seg_cap + sims[b]->seg2_cap;
+        const size_t margin = (size_t)1 << 30;
+        auto need = [&](int jj) { return (size_t)S * sb * ((size_t)(jj + 1) + (jj < k ? (size_t)((k + jj - 1) / jj) : 0)); };
+        if (j == k && need(k) + margin > have) {
+            j = 1;
+            while ((size_t)j * j < (size_t)k) j++;
+        }
+        if (need(j) + margin > have) return fail(m, ECSG_ERR_CUDA, "shots: %d shots do not fit in device memory", S);
+    }
+    const int nsub = (k + j - 1) / j;
+    for (int b = 0; b < S; b++) {
+        ecsg_sim *x = sims[b];
+        if ((rc = grow(x, (void **)&x->seg, x->seg_cap, sb * (j + 1)))) return rc;
+        if (j < k && (rc = grow(x, (void **)&x->seg2, x->seg2_cap, sb * nsub))) return rc;
+    }
+    if ((rc = each_shot(sims, S, [&](ecsg_sim *x, int) -> int {
+             for (int i = 1; i < x->ng; i++)
+                 if (int r2 = sxz_prepare<T>(x, i)) return r2;
+             if (int r2 = stress_prepare(x)) return r2;
+             return adj_zero(x, true, true);
+         })))
+        return rc;
+    auto set_clocks = [&](int n) -> int {
+        for (int b = 0; b < S; b++) {
+            ecsg_sim *x = sims[b];
+            x->run_n0 = n;
+            CK(cudaMemcpyAsync(x->ints + 1, &x->run_n0, sizeof(int), cudaMemcpyHostToDevice, gs));
+            CK(cudaMemcpyAsync(x->ints + 3, &x->run_n0, sizeof(int), cudaMemcpyHostToDevice, gs));
+        }
+        CK(cudaStreamSynchronize(gs));   // run_n0 is read by the copies above
+        return ECSG_OK;
+    };
+    auto save_all = [&](char *ecsg_sim::*buf, size_t idx) {
+        return each_shot(sims, S, [&](ecsg_sim *x, int) { return save_state(x, x->*buf + idx * sb); });
+    };
+    auto load_all = [&](char *ecsg_sim::*buf, size_t idx) {
+        return each_shot(sims, S, [&](ecsg_sim *x, int) { return load_state(x, x->*buf + idx * sb); });
+    };
+    std::vector<T *> rows(S);
+    // forward from rest with checkpoints every k steps
+    {
+        NvtxRange range("shots forward");
+        for (int b = 0; b < S; b++) {
+            ecsg_sim *x = sims[b];
+            for (int g = 0; g < x->ng; g++) CK(cudaMemsetAsync(x->fblk[g], 0, 9 * (size_t)x->geo[g].size() * x->tsize, gs));
+            for (int i = 1; i < x->ng; i++)
+                CK(cudaMemsetAsync(x->itf[i].X0, 0, sizeof(double) * (x->geo[i].nx + 1) * (x->geo[i].ny + 1), gs));
+        }
+        if ((rc = set_clocks(0))) return rc;
+        for (int n = 0; n < nsteps; n++) {
+            if (n % k == 0 && (rc = save_all(&ecsg_sim::ckpt, n / k))) return rc;
+            for (int b = 0; b < S; b++) rows[b] = nrec ? (T *)sims[b]->recT + (size_t)n * nrec : nullptr;
+            if ((rc = group_step_op<T>(sims, S, rows.data()))) return rc;
+        }
+        if ((rc = save_all(&ecsg_sim::ckpt, ncp))) return rc;
+    }
+    NvtxRange range("shots backward");
+    for (int b = 0; b < S; b++) {
+        ecsg_sim *x = sims[b];
+        CK(cudaMemsetAsync(x->dscal + 8, 0, sizeof(double), gs));
+        CK(launch_residual<T>((T *)x->recT, x->obs, (int64_t)nobs, x->dscal + 8, x->partial, 12 * x->red_blocks, gs));
+    }
+    std::vector<const char *> sa(S), sbf(S);
+    for (int c = ncp - 1; c >= 0; c--) {
+        const int n0 = c * k, n1 = (n0 + k < nsteps) ? n0 + k : nsteps;
+        if (j < k) {   // sub-checkpoints of this segment
+            if ((rc = load_all(&ecsg_sim::ckpt, c))) return rc;
+            if ((rc = set_clocks(n0))) return rc;
+            for (int n = n0; n < n1; n++) {
+                if ((n - n0) % j == 0 && (rc = save_all(&ecsg_sim::seg2, (n - n0) / j))) return rc;
+                if ((rc = group_step_op<T>(sims, S, nullptr))) return rc;
+            }
+        }
+        for (int d = (n1 - n0 - 1) / j; d >= 0; d--) {
+            const int m0 = n0 + d * j, m1 = (m0 + j < n1) ? m0 + j : n1;
+            if ((rc = j < k ? load_all(&ecsg_sim::seg2, d) : load_all(&ecsg_sim::ckpt, c))) return rc;
+            if ((rc = set_clocks(m0))) return rc;
+            if ((rc = save_all(&ecsg_sim::seg, 0))) return rc;
+            for (int n = m0; n < m1; n++) {
+                if ((rc = group_step_op<T>(sims, S, nullptr))) return rc;
+                if ((rc = save_all(&ecsg_sim::seg, n - m0 + 1))) return rc;
+            }
+            for (int n = m1 - 1; n >= m0; n--) {
+                for (int b = 0; b < S; b++) {
+                    sa[b] = sims[b]->seg + (size_t)(n - m0 + 1) * sb;
+                    sbf[b] = sims[b]->seg + (size_t)(n - m0) * sb;
+                }
+                if ((rc = group_adjoint_step<T>(sims, S, sa.data(), sbf.data(), n))) return rc;
+            }
+        }
+    }
+    // losses, then the shots' shares of the gradient summed (FP64) into sims[0]
+    std::vector<double> l(S, 0.0);
+    for (int b = 0; b < S; b++) CK(cudaMemcpyAsync(&l[b], sims[b]->dscal + 8, sizeof(double), cudaMemcpyDeviceToHost, gs));
+    CK(cudaStreamSynchronize(gs));
+    if (losses)
+        for (int b = 0; b < S; b++) losses[b] = l[b];
+    if (S > 1 && (rc = ecsg_sum_gradients(m, sims, S))) return rc;
+    // leave every shot at its final forward state, the step clock after the last step
+    if ((rc = load_all(&ecsg_sim::ckpt, ncp))) return rc;
+    return set_clocks(nsteps);
+}
+
+int ecsg_shots_misfit_gradient(ecsg_sim *const *sims, int n, int nsteps, const float *const *observed, int ckpt_every,
+                               int sub_every, double *losses)
+{
+    NvtxRange range("ecsg_shots_misfit_gradient");
+    if (!sims || !sims[0]) return ECSG_ERR_INVALID;
+    if (n < 1 || n > kMaxShots || nsteps < 1 || ckpt_every < 1)
+        return fail(sims[0], ECSG_ERR_INVALID, "shots_misfit_gradient: bad arguments (1 <= n <= %d shots)", kMaxShots);
+    if (int rc = group_check(sims, n)) return rc;
+    if (sims[0]->nrec > 0 && !observed) return fail(sims[0], ECSG_ERR_INVALID, "shots_misfit_gradient: observed data missing");
+    for (int b = 0; b < n && sims[0]->nrec > 0; b++)
+        if (!observed[b]) return fail(sims[0], ECSG_ERR_INVALID, "shots_misfit_gradient: observed data of shot %d missing", b);
+    return sims[0]->prec == ECSG_F32 ? group_gradient_op<float>(sims, n, nsteps, observed, ckpt_every, sub_every, losses)
+                                     : group_gradient_op<double>(sims, n, nsteps, observed, ckpt_every, sub_every, losses);
 }
 
 // ---------------------------------------------------------------------------

@@ -20,6 +20,7 @@ namespace ecsg {
 
 constexpr int XOFF = 32;
 constexpr int kMaxGrids = 8;
+constexpr int kMaxShots = 16;   // shots advanced in lockstep by one call
 
 struct Geo {
     int nx, ny, nz;   // cells

@@ -351,6 +351,25 @@ int ecsg_batch_misfit_gradient(ecsg_sim *const *sims, int n, int nsteps, const f
 /* dst's gradients = the sum of the instances' gradients, accumulated in FP64
  * (dst may be one of them; same geometry and precision). */
 int ecsg_sum_gradients(ecsg_sim *dst, ecsg_sim *const *srcs, int n);
+/* The misfit gradients of n shots (n <= 16) that share one medium (the
+ * instances of one model made by ecsg_create_shot, with the same receiver
+ * count and component), advanced in lockstep on sims[0]'s stream: each phase
+ * of a forward or adjoint step runs for all shots before the next, so the
+ * phases that read the medium or solve the interface systems do so once for
+ * all of them.  No reference counterpart: it batches the time loop of
+ * main.cpp:165-261 (a shot = one pass of it) and the adjoint of
+ * ecsg_misfit_gradient.  Checkpoints every ckpt_every steps; inside a
+ * segment the states are recomputed from its checkpoint, through
+ * sub-checkpoints every sub_every steps when 0 < sub_every < ckpt_every, or
+ * when the segment's states of all n shots do not fit in device memory
+ * (sub_every <= 0: chosen, about sqrt(ckpt_every)).  Leaves in sims[0]'s
+ * gradient arrays the gradient of the sum of the n misfits (the medium
+ * adjoints accumulate every shot's terms in the field precision; the
+ * interface adjoints' shares are summed in FP64 at the end); losses[b] (may
+ * be NULL) receives shot b's misfit; every instance is left at its final
+ * forward state. */
+int ecsg_shots_misfit_gradient(ecsg_sim *const *sims, int n, int nsteps, const float *const *observed, int ckpt_every,
+                               int sub_every, double *losses);
 /* Autotuner: for each grid, time the FP32 velocity and stress sweeps over
  * candidate z-march depths (chunks per column) on the simulation's own state
  * (restored afterwards) and keep the fastest; reps timed repetitions each.

@@ -144,19 +144,20 @@ def run_reference(args):
 
 
 def shot_gradients(args, local, world, max_over_ranks, barrier):
-    """Plain (one shot at a time) misfit gradients on the two-grid adjoint
-    workload: 361x361x61 @ 10 m over 121x121x81 @ 30 m (9,135,502 points),
-    smooth orthorhombic model, 121 x 121 surface vz receivers, checkpoints
-    every 50 steps; observed data from the same model with a 3 % vs blob.
-    One shot per GPU; device time (CUDA events on the library's stream)
-    around ecsg_misfit_gradient (forward with checkpoints, recomputation and
-    adjoint) and, on several GPUs, the FP64 all-reduce of the gradient volumes
-    (NCCL, on the same stream).
+    """Misfit gradients on the two-grid adjoint workload: 361x361x61 @ 10 m
+    over 121x121x81 @ 30 m (9,135,502 points), smooth orthorhombic model,
+    121 x 121 surface vz receivers, checkpoints every 50 steps; observed data
+    from the same model with a 3 % vs blob.
 
-    Batched leg (--grad-batch B > 1): B shots of the same model sharing one
-    medium allocation (ecsg_create_shot) run at once (ecsg_batch_misfit_gradient,
-    one stream per shot); host wall clock around that synchronous call against
-    the same clock around one plain ecsg_misfit_gradient call."""
+    Plain: one shot at a time (ecsg_misfit_gradient: forward with
+    checkpoints, recomputation, adjoint) on each GPU.  Batched (--grad-batch
+    B > 1): B shots of the same model sharing one medium allocation
+    (ecsg_create_shot), advanced in lockstep (ecsg_shots_misfit_gradient: the
+    medium adjoints and the interface solves once for all shots, the gradient
+    of the shots' summed misfit).  Both legs are device-timed with CUDA events
+    on the library stream (the lockstep call runs on the first instance's
+    stream); on several GPUs the plain leg includes the FP64 all-reduce of the
+    gradient volumes (NCCL, on the same stream)."""
     import ecsg_b200
     from ecsg_b200.workloads import two_grid_adjoint_case
     n = args.grad_steps
@@ -177,9 +178,6 @@ def shot_gradients(args, local, world, max_over_ranks, barrier):
         ms = s.timer_stop()
         gmax = float(np.abs(s.gradient(0, 0)).max())
         status = s.status()
-        t0 = time.perf_counter()
-        s.misfit_gradient(obs, ckpt_every=50)
-        plain_wall = time.perf_counter() - t0
     ms = max_over_ranks(ms)
     batched = None
     nb = args.grad_batch
@@ -192,22 +190,23 @@ def shot_gradients(args, local, world, max_over_ranks, barrier):
         model = ecsg_b200.Simulation(two_grid_adjoint_case(0, shots[0], n, blob=False), precision="f32", device=local)
         sims = [model] + [ecsg_b200.Simulation.shot(model, two_grid_adjoint_case(0, k, n, blob=False)) for k in shots[1:]]
         try:
-            ecsg_b200.batch_misfit_gradient(sims, [o[: min(n, 60)] for o in obs_b], ckpt_every=50)   # warm-up
+            ecsg_b200.shots_misfit_gradient(sims, [o[: min(n, 60)] for o in obs_b], ckpt_every=50)   # warm-up
             barrier()
-            t0 = time.perf_counter()
-            losses = ecsg_b200.batch_misfit_gradient(sims, obs_b, ckpt_every=50)
-            wall = time.perf_counter() - t0
+            model.timer_start()
+            losses = ecsg_b200.shots_misfit_gradient(sims, obs_b, ckpt_every=50)
+            bms = model.timer_stop()
             bstatus = max(x.status() for x in sims)
+            bgmax = float(np.abs(model.gradient(0, 0)).max())
         finally:
             for x in sims[1:]:
                 x.close()
             model.close()
-        wall = max_over_ranks(wall)
-        plain_wall = max_over_ranks(plain_wall)
-        batched = {"shots": nb, "value": world * nb / wall, "plain_value_wall_clock": world / plain_wall,
-                   "speedup_vs_plain": (nb / wall) / (1.0 / plain_wall), "s_per_batch": wall,
-                   "finite": bool(np.isfinite(losses).all()), "status": bstatus,
-                   "timing": "host wall clock around the synchronous calls (batched and one plain call)"}
+        bms = max_over_ranks(bms)
+        batched = {"shots": nb, "value": world * nb / (bms * 1e-3), "ms_per_batch": bms,
+                   "ms_per_shot_gradient": bms / nb, "speedup_vs_plain": (nb / bms) / (1.0 / ms),
+                   "finite": bool(np.isfinite(losses).all() and np.isfinite(bgmax)), "status": bstatus,
+                   "mode": "lockstep shots sharing the medium (ecsg_shots_misfit_gradient), gradient of the summed "
+                           "misfit", "timing": "CUDA events on the library stream, both legs"}
     return {"metric": "shot-gradients/s", "value": world / (ms * 1e-3), "unit": "shot-gradients/s",
             "mode": "plain (one shot per GPU at a time)" + (", FP64 NCCL all-reduce of the gradients" if world > 1 else ""),
             "ms_per_shot_gradient": ms, "steps": n,
@@ -215,6 +214,40 @@ def shot_gradients(args, local, world, max_over_ranks, barrier):
             "loss": loss, "finite": bool(np.isfinite(loss) and np.isfinite(gmax)), "status": status,
             "workload": "two-grid 361x361x61@10m / 121x121x81@30m, smooth orthorhombic, shot %d of 4x4" % shot,
             "batched": batched}
+
+
+def accuracy(args, local):
+    """FP32 production path against an FP64 shadow run of a reduced copy of the
+    benchmark case (three grids at ratio 3, 181x181x25 @ 5 m / 61x61x19 @ 15 m
+    / 21x21x13 @ 45 m, the same seeded tilted-VTI construction, free surface,
+    vz source and surface vz receivers), over args.accuracy_steps steps with
+    energy every 10 steps: rel-L2 of the traces and of the final fields (the
+    largest over the 27 components), and the energy: the largest relative
+    difference FP32 / FP64, and the drift (max - min) / mean of each after the
+    source has stopped."""
+    import ecsg_b200
+    from ecsg_b200.workloads import three_grid_case
+    n = args.accuracy_steps
+    grids = [((180, 180, 24), 5.0), ((60, 60, 18), 15.0), ((20, 20, 12), 45.0)]
+    case = three_grid_case(seed=0, grids=grids, nsteps=n, medium="tti")
+    runs = {}
+    for prec in ("f64", "f32"):
+        with ecsg_b200.Simulation(case, precision=prec, energy=True, device=local) as s:
+            out = s.run(n, energy_every=10)
+            runs[prec] = (out["rec"].astype(np.float64), out["energy"][9::10],
+                          [s.field(g, k)[1:-1, 1:-1, 1:-1] for g in range(3) for k in range(9)])
+    (r64, e64, f64), (r32, e32, f32) = runs["f64"], runs["f32"]
+    rel = lambda a, b: float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+    src_end = len(case.src["trace"])
+    post = [i for i in range(len(e64)) if 10 * (i + 1) > src_end + 10]
+    drift = lambda e: float((e.max() - e.min()) / e.mean()) if len(e) > 1 else None
+    return {"workload": "three-grid ratio-3 tilted VTI 181x181x25@5m / 61x61x19@15m / 21x21x13@45m, %d steps" % n,
+            "reference": "FP64 device path (bitwise equal to the FP64 CPU oracle per operator)",
+            "traces_rel_l2": rel(r32, r64), "final_fields_rel_l2_max": max(rel(a, b) for a, b in zip(f32, f64)),
+            "energy_rel_diff_max": float(np.abs(e32 - e64).max() / np.abs(e64).max()),
+            "energy_drift_post_source_f32": drift(e32[post]) if post else None,
+            "energy_drift_post_source_f64": drift(e64[post]) if post else None,
+            "mirror_fix": False}
 
 
 def batched_forward(args, local, world, max_over_ranks, barrier):
@@ -263,10 +296,12 @@ def main():
     ap.add_argument("--energy-every", type=int, default=100)
     ap.add_argument("--medium", default="tti", choices=["tti", "iso"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--grad-batch", type=int, default=4,
+    ap.add_argument("--grad-batch", type=int, default=8,
                     help="shots per batched shot-gradient run (0 or 1: no batched leg)")
     ap.add_argument("--grad-steps", type=int, default=1500,
                     help="steps of the shot-gradient measurement (0: skip it)")
+    ap.add_argument("--accuracy-steps", type=int, default=600,
+                    help="steps of the FP32-vs-FP64 accuracy run (0: skip it)")
     ap.add_argument("--batch-steps", type=int, default=200,
                     help="steps of the batched-forward measurement (0: skip it)")
     args = ap.parse_args()
@@ -390,6 +425,7 @@ def main():
     sim.close()
     grad = shot_gradients(args, local, world, max_over_ranks, barrier) if args.grad_steps > 0 else None
     batched = batched_forward(args, local, world, max_over_ranks, barrier) if args.batch_steps > 0 else None
+    acc_line = accuracy(args, local) if (rank == 0 and args.accuracy_steps > 0) else None
     if rank == 0:
         line = {
             "metric": "Gcell-updates/s", "value": value, "unit": "Gcell/s", "n_gpus": world,
@@ -421,6 +457,7 @@ def main():
             "gpu_launches": launches,
             "shot_gradients": grad,
             "batched_forward": batched,
+            "accuracy": acc_line,
         }
         print(json.dumps(line))
     if pg is not None:

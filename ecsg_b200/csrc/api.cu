@@ -36,10 +36,14 @@ size_t s21_maps_bytes();
 bool s21_encode_maps(void *, const GridDev<float> &, float *const[3]);
 cudaError_t s21_set_attributes();
 cudaError_t launch_stress21_tma(const void *, const GridDev<float> &, int, int, float *const[3], int *, int, cudaStream_t, int);
+cudaError_t launch_stress21_tma_shots(const void *const *, int, const GridDev<float> &, int, int, bool, int *, int,
+                                      cudaStream_t, int);
 size_t vel_maps_bytes();
 bool vel_encode_maps(void *, const GridDev<float> &);
 cudaError_t vel_tma_set_attributes();
 cudaError_t launch_vel_tma(const void *, const GridDev<float> &, int, int, int, float *const[3], int *, int, cudaStream_t, int);
+cudaError_t launch_vel_tma_shots(const void *const *, int, const GridDev<float> &, int, int, int, int *, int, cudaStream_t,
+                                 int);
 // interface.cu
 template <typename T>
 cudaError_t launch_ghost_vz(const GridDev<T> &, const GridDev<T> &, int, int, double *, cudaStream_t);
@@ -55,6 +59,14 @@ template <typename T>
 cudaError_t launch_sxz_solve(const GridDev<T> &, const GridDev<T> &, int, const SxzWork &, int, cudaStream_t);
 template <typename T>
 int sxz_multi_capacity(int);
+int sxz_adj_multi_capacity(int);
+cudaError_t launch_sxz_adj_solve_multi(const SxzAdjList &, cudaStream_t);
+template <typename T>
+cudaError_t launch_sxz_adj_collect(const GridDev<T> &, const GridDev<T> &, const AdjDev<T> &, const AdjDev<T> &, int,
+                                   double *, cudaStream_t);
+template <typename T>
+cudaError_t launch_sxz_adj_scatter(const GridDev<T> &, const GridDev<T> &, const AdjDev<T> &, const AdjDev<T> &, int,
+                                   const double *, cudaStream_t);
 template <typename T>
 cudaError_t launch_sxz_solve_multi(const SxzSysList<T> &, cudaStream_t);
 // diag.cu
@@ -169,7 +181,7 @@ struct ecsg_sim {
     // (each interface bitwise as in its own launch), when their CTAs fit
     // co-resident (sxz_cap); otherwise one launch per interface.
     bool sxz_fused = true;
-    int sxz_cap = 0;
+    int sxz_cap = 0, sxz_adj_cap = 0;   // co-resident CTAs of the multi-system forward / adjoint solves
     cudaStream_t side[kMaxGrids] = {};
     cudaEvent_t fork_ev = nullptr, join_ev[kMaxGrids] = {};
     // adjoint state (allocated on first use): adjoint fields, gradients, work boxes
@@ -426,8 +438,10 @@ static int create_impl(const ecsg_grid_desc *grids, const ecsg_config *cfg, ecsg
         if ((rc = dmalloc(s, (void **)&I.X0, sizeof(double) * nxy))) return bail(rc);
         if ((rc = dmalloc(s, (void **)&I.X1, sizeof(double) * nxy))) return bail(rc);
         I.nblocks = s->prec == ECSG_F32 ? sxz_solve_blocks<float>((int)nn, s->sms) : sxz_solve_blocks<double>((int)nn, s->sms);
-        if (i == 1)
+        if (i == 1) {
             s->sxz_cap = s->prec == ECSG_F32 ? sxz_multi_capacity<float>(s->sms) : sxz_multi_capacity<double>(s->sms);
+            s->sxz_adj_cap = sxz_adj_multi_capacity(s->sms);
+        }
         // two halves: the solve's reduction rounds alternate between them
         if ((rc = dmalloc(s, (void **)&I.partial, sizeof(double) * 2 * (size_t)I.nblocks))) return bail(rc);
     }
@@ -2332,12 +2346,35 @@ static int group_sxz_op(ecsg_sim *const *sims, int S)
 
 // One forward step of every shot (the order of main.cpp:165-261 within each
 // shot); sample_rows[b]: shot b's receiver samples of this step, or null.
+// The FP32 TMA sweeps of every shot of grid g in one launch (the shots' CTAs
+// of a tile column adjacent, so the medium planes one stages are L2 hits for
+// the others); false where the shots take the per-shot operators.
+template <typename T>
+static bool group_tma(ecsg_sim *const *sims, int S, bool stress)
+{
+    if (!std::is_same<T, float>::value || S < 2) return false;
+    for (int b = 0; b < S; b++)
+        if (!(stress ? use_s21_tma(sims[b]) : use_vel_tma(sims[b])) || (stress && sims[b]->energy)) return false;
+    return true;
+}
+
 template <typename T>
 static int group_step_op(ecsg_sim *const *sims, int S, T *const *sample_rows)
 {
     ecsg_sim *s = sims[0];   // where CK reports
+    ecsg_sim *m = s;
     int rc;
-    if ((rc = each_shot(sims, S, [&](ecsg_sim *x, int) { return each_grid(x, [&](int g) { return vel_op<T>(x, g, false); }); })))
+    std::vector<const void *> maps(S);
+    if (group_tma<T>(sims, S, false)) {
+        for (int g = 0; g < m->ng; g++) {
+            for (int b = 0; b < S; b++) maps[b] = sims[b]->velmaps[g].data();
+            CK(launch_vel_tma_shots(maps.data(), S, dev<float>(m, g), top_of(m, g, -1), bottom_of(m, g, -1), m->top_bc,
+                                    m->ints, m->sms, m->st, 0));
+            if ((rc = each_shot(sims, S, [&](ecsg_sim *x, int) { return vel_mirror_op<T>(x, g); }))) return rc;
+        }
+    } else if ((rc = each_shot(sims, S, [&](ecsg_sim *x, int) {
+                    return each_grid(x, [&](int g) { return vel_op<T>(x, g, false); });
+                })))
         return rc;
     if ((rc = each_shot(sims, S, [&](ecsg_sim *x, int b) -> int {
              if (sample_rows && sample_rows[b]) CK(launch_rec_sample<T>(make_srcrec(x, 0), sample_rows[b], x->st));
@@ -2345,7 +2382,15 @@ static int group_step_op(ecsg_sim *const *sims, int S, T *const *sample_rows)
              return each_vz_ghost<T>(x);
          })))
         return rc;
-    if ((rc = each_shot(sims, S, [&](ecsg_sim *x, int) { return each_grid(x, [&](int g) { return stress_op<T>(x, g); }); })))
+    if (group_tma<T>(sims, S, true)) {
+        for (int g = 0; g < m->ng; g++) {
+            for (int b = 0; b < S; b++) maps[b] = sims[b]->s21maps[g].data();
+            CK(launch_stress21_tma_shots(maps.data(), S, dev<float>(m, g), top_of(m, g, -1), m->top_bc, false, m->ints,
+                                         m->sms, m->st, 0));
+        }
+    } else if ((rc = each_shot(sims, S, [&](ecsg_sim *x, int) {
+                    return each_grid(x, [&](int g) { return stress_op<T>(x, g); });
+                })))
         return rc;
     if ((rc = group_sxz_op<T>(sims, S))) return rc;
     return each_shot(sims, S, [&](ecsg_sim *x, int) -> int {
@@ -2384,16 +2429,59 @@ static int group_adjoint_step(ecsg_sim *const *sims, int S, const char *const *s
     auto states = [&](ecsg_sim *x, int b, const char *const *st, GridDev<T> *Gv) {
         for (int g = 0; g < ng; g++) Gv[g] = dev_state<T>(x, g, st[b]);
     };
-    if ((rc = each_shot(sims, S, [&](ecsg_sim *x, int b) -> int {
-             GridDev<T> Ga[kMaxGrids];
-             states(x, b, sa, Ga);
-             for (int i = ng - 1; i >= 1; i--) {
+    // interfaces from the deepest: per shot the syz adjoint and the collection
+    // of the sxz adjoint's right-hand side, the sxz adjoint solves of all shots
+    // in shared cooperative launches, then per shot their scatter
+    for (int i = ng - 1; i >= 1; i--) {
+        if ((rc = each_shot(sims, S, [&](ecsg_sim *x, int b) -> int {
+                 GridDev<T> Ga[kMaxGrids];
+                 states(x, b, sa, Ga);
                  if (int r2 = adj_op_impl<T>(x, ECSG_ADJ_GHOST_SYZ, i, Ga)) return r2;
-                 if (int r2 = adj_op_impl<T>(x, ECSG_ADJ_GHOST_SXZ, i, Ga)) return r2;
-             }
-             return ECSG_OK;
-         })))
-        return rc;
+                 if (x->imode == ECSG_MODE_II) return adj_op_impl<T>(x, ECSG_ADJ_GHOST_SXZ, i, Ga);
+                 CK(launch_sxz_adj_collect<T>(Ga[i - 1], Ga[i], adj_dev<T>(x, i - 1), adj_dev<T>(x, i), x->itf[i].r,
+                                              x->adj_lx[i], x->st));
+                 return ECSG_OK;
+             })))
+            return rc;
+        if (m->imode == ECSG_MODE_II) continue;
+        SxzAdjList L;
+        memset(&L, 0, sizeof L);
+        int cta = 0;
+        auto flush = [&]() -> int {
+            if (!L.n) return ECSG_OK;
+            L.bar = m->bar;
+            L.status = m->ints;
+            CK(launch_sxz_adj_solve_multi(L, m->st));
+            memset(&L, 0, sizeof L);
+            cta = 0;
+            return ECSG_OK;
+        };
+        for (int b = 0; b < S; b++) {
+            ecsg_sim *x = sims[b];
+            const int nb = x->itf[i].nblocks;
+            if (L.n == kMaxSxzSys || cta + nb > m->sxz_adj_cap)
+                if ((rc = flush())) return rc;
+            SxzAdjSys &Y = L.s[L.n++];
+            Y.W = sxz_work(x, i);
+            Y.W.X0 = x->adj_Y0[i];
+            Y.W.X1 = x->adj_Y1[i];
+            Y.lx = x->adj_lx[i];
+            Y.nx2 = x->geo[i].nx;
+            Y.ny2 = x->geo[i].ny;
+            Y.cta0 = cta;
+            Y.ncta = nb;
+            cta += nb;
+        }
+        if ((rc = flush())) return rc;
+        if ((rc = each_shot(sims, S, [&](ecsg_sim *x, int b) -> int {
+                 GridDev<T> Ga[kMaxGrids];
+                 states(x, b, sa, Ga);
+                 CK(launch_sxz_adj_scatter<T>(Ga[i - 1], Ga[i], adj_dev<T>(x, i - 1), adj_dev<T>(x, i), x->itf[i].r,
+                                              x->adj_Y0[i], x->st));
+                 return ECSG_OK;
+             })))
+            return rc;
+    }
     for (int g = 0; g < ng; g++)
         CK(launch_stress21_adj_shots<T>(dev<T>(m, g), adj_dev<T>(m, g), shot_set<T>(sims, S, g, sa), g == 0, m->top_bc,
                                         m->sms, m->st));

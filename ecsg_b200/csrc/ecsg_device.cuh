@@ -126,6 +126,22 @@ struct SxzSysList {
     int *status;     // ST_BARRIER_TIMEOUT
 };
 
+// Several adjoint sxz systems (A^T y = lambda_X) in one cooperative launch
+// (interface.cu, sxz_adj_solve_multi_kernel): system i owns CTAs
+// [cta0, cta0 + ncta); W.X0 / W.X1 are its iterates, lx its right-hand side.
+struct SxzAdjSys {
+    SxzWork W;
+    const double *lx;
+    int nx2, ny2;
+    int cta0, ncta;
+};
+struct SxzAdjList {
+    SxzAdjSys s[kMaxSxzSys];
+    int n;
+    unsigned *bar;   // kBarWords barrier words of the launch
+    int *status;
+};
+
 // Receivers and source of one run (diag.cu, src_rec_kernel).
 struct SrcRec {
     void *rec_base[kMaxGrids];   // receiver component per grid

@@ -1103,6 +1103,100 @@ __global__ void __launch_bounds__(256) sxz_adj_solve_kernel(int nx2, int ny2, Sx
     if (gtid == 0) *W.iters = it;
 }
 
+// The adjoint solves of several systems in one cooperative launch, each
+// bitwise as sxz_adj_solve_kernel with its ncta CTAs (the same mapping of
+// unknowns and partial sums), sharing one barrier per round; every CTA forms
+// every system's totals and takes the same stopping decisions, so systems
+// that have converged (or have no adjoint yet) idle at the barriers while the
+// others sweep.
+__global__ void __launch_bounds__(256) sxz_adj_solve_multi_kernel(const __grid_constant__ SxzAdjList L)
+{
+    __shared__ double red[32];
+    __shared__ double s_tol[kMaxSxzSys];
+    __shared__ int s_it[kMaxSxzSys], s_act[kMaxSxzSys], s_cap[kMaxSxzSys], s_zero[kMaxSxzSys];
+    int me = 0;
+    for (int i = 1; i < L.n; i++)
+        if ((int)blockIdx.x >= L.s[i].cta0) me = i;
+    const SxzAdjSys &S = L.s[me];
+    const SxzWork &W = S.W;
+    const double *lx = S.lx;
+    const int lb = blockIdx.x - S.cta0, ncta = S.ncta;
+    const int n0 = S.nx2 - 1, n1 = S.ny2 - 1, ld = S.nx2 + 1, nn = n0 * n1;
+    const int gtid = lb * blockDim.x + threadIdx.x, gstride = ncta * blockDim.x;
+    bool ok = true;
+    int round = 0;
+    auto slot = [&](const SxzAdjSys &Y, int rd, int b) { return Y.W.partial + (size_t)(rd & 1) * Y.ncta + b; };
+    double sab = 0.0;
+    for (int q = gtid; q < nn; q += gstride) sab += fabs(lx[q]);
+    grid_arrive_list(sab, slot(S, round, lb), L.bar, L.status, red, ok);
+    round++;
+    for (int i = 0; i < L.n; i++) {
+        const double sum = system_total(slot(L.s[i], round - 1, 0), L.s[i].ncta, red);
+        if (threadIdx.x == 0) {
+            s_zero[i] = !(sum > 0.0);
+            s_tol[i] = 1e-13 * sum;
+            s_it[i] = 0;
+            s_act[i] = s_zero[i] ? 0 : 1;
+            s_cap[i] = 0;
+        }
+    }
+    __syncthreads();
+    if (s_zero[me]) {   // no adjoint at this interface yet: y = 0
+        for (int q = gtid; q < nn; q += gstride) W.X0[(q / n0 + 1) * ld + q % n0 + 1] = 0.0;
+    }
+    double *Xc = W.X0, *Xn = W.X1;
+    bool any = false;
+    for (int i = 0; i < L.n; i++) any = any || s_act[i] != 0;
+    while (ok && any) {
+        const bool mine = s_act[me] != 0;
+        double s = 0.0;
+        if (mine)
+            for (int q = gtid; q < nn; q += gstride) {
+                const int i0 = q % n0 + 1, i1 = q / n0 + 1;
+                const double *a = W.A + q;
+                const double xn = (lx[q]
+                                   - a[0 * nn] * __ldcg(Xc + (i1 - 1) * ld + (i0 - 1))
+                                   - a[1 * nn] * __ldcg(Xc + (i1) * ld + (i0 - 1))
+                                   - a[2 * nn] * __ldcg(Xc + (i1 + 1) * ld + (i0 - 1))
+                                   - a[3 * nn] * __ldcg(Xc + (i1 - 1) * ld + (i0))
+                                   - a[5 * nn] * __ldcg(Xc + (i1 + 1) * ld + (i0))
+                                   - a[6 * nn] * __ldcg(Xc + (i1 - 1) * ld + (i0 + 1))
+                                   - a[7 * nn] * __ldcg(Xc + (i1) * ld + (i0 + 1))
+                                   - a[8 * nn] * __ldcg(Xc + (i1 + 1) * ld + (i0 + 1))) / a[4 * nn];
+                const double d = xn - __ldcg(Xc + i1 * ld + i0);
+                __stcg(Xn + i1 * ld + i0, xn);
+                s += d * d;
+            }
+        grid_arrive_list(s, slot(S, round, lb), L.bar, L.status, red, ok);
+        round++;
+        if (!ok) break;
+        for (int i = 0; i < L.n; i++) {
+            if (!s_act[i]) continue;   // uniform over the CTA
+            const SxzAdjSys &Y = L.s[i];
+            const double tot = system_total(slot(Y, round - 1, 0), Y.ncta, red);
+            if (threadIdx.x == 0) {
+                s_it[i]++;
+                if (!(sqrt(tot) > s_tol[i])) s_act[i] = 0;
+                else if (s_it[i] >= Y.W.max_iter) { s_act[i] = 0; s_cap[i] = 1; }
+            }
+        }
+        __syncthreads();
+        if (mine) { double *tmp = Xc; Xc = Xn; Xn = tmp; }
+        any = false;
+        for (int i = 0; i < L.n; i++) any = any || s_act[i] != 0;
+        __syncthreads();
+    }
+    if (Xc != W.X0)
+        for (int q = gtid; q < nn; q += gstride) {
+            const int i0 = q % n0 + 1, i1 = q / n0 + 1;
+            W.X0[i1 * ld + i0] = __ldcg(Xc + i1 * ld + i0);
+        }
+    if (gtid == 0) {
+        *W.iters = s_it[me];
+        if (s_cap[me]) atomicOr(W.status, ST_JACOBI_CAP);
+    }
+}
+
 // rhs^T y (B = r^4 pc - r^2 fsum) and buoyancy gradients, coarse rows
 template <typename T>
 __global__ void sxz_adj_coarse(GridDev<T> C, AdjDev<T> AC, int r, const double *y)
@@ -1670,6 +1764,56 @@ cudaError_t launch_ghost_sxz_adj(const GridDev<T> &F, const GridDev<T> &C, const
     return cudaGetLastError();
 }
 
+// The adjoint sxz solve in three parts, for solving several systems in one
+// launch: collect lambda_X (and zero the ghosts) ...
+template <typename T>
+cudaError_t launch_sxz_adj_collect(const GridDev<T> &F, const GridDev<T> &C, const AdjDev<T> &AF, const AdjDev<T> &AC,
+                                   int r, double *lx, cudaStream_t st)
+{
+    const int nx2 = C.g.nx, ny2 = C.g.ny, nn = (nx2 - 1) * (ny2 - 1);
+    const int nx1 = r * nx2, ny1 = r * ny2;
+    sxz_adj_collect_coarse<T><<<(nn + 255) / 256, 256, 0, st>>>(C, AC, lx);
+    dim3 bf(64, 4), gf((nx1 - 1 + 63) / 64, (ny1 - 1 + 3) / 4);
+    sxz_adj_collect_fine<T><<<gf, bf, 0, st>>>(F, C, AF, AC, r, lx);
+    return cudaGetLastError();
+}
+
+// ... solve the systems of a list (cta0 / ncta set by the caller) ...
+cudaError_t launch_sxz_adj_solve_multi(const SxzAdjList &L, cudaStream_t st)
+{
+    if (L.n < 1 || L.n > kMaxSxzSys) return cudaErrorInvalidValue;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(L.s[L.n - 1].cta0 + L.s[L.n - 1].ncta);
+    cfg.blockDim = dim3(256);
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, sxz_adj_solve_multi_kernel, L);
+}
+
+int sxz_adj_multi_capacity(int sms)
+{
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, sxz_adj_solve_multi_kernel, 256, 0) != cudaSuccess) return 0;
+    return per_sm * sms;
+}
+
+// ... and add rhs^T y and the buoyancy gradients
+template <typename T>
+cudaError_t launch_sxz_adj_scatter(const GridDev<T> &F, const GridDev<T> &C, const AdjDev<T> &AF, const AdjDev<T> &AC,
+                                   int r, const double *y, cudaStream_t st)
+{
+    const int nx2 = C.g.nx, ny2 = C.g.ny, nn = (nx2 - 1) * (ny2 - 1);
+    const int nx1 = r * nx2, ny1 = r * ny2;
+    dim3 bf(64, 4), gf((nx1 - 1 + 63) / 64, (ny1 - 1 + 3) / 4);
+    sxz_adj_coarse<T><<<(nn + 255) / 256, 256, 0, st>>>(C, AC, r, y);
+    sxz_adj_fine<T><<<gf, bf, 0, st>>>(F, C, AF, AC, r, y);
+    return cudaGetLastError();
+}
+
 #define INST(T)                                                                                         \
     template cudaError_t launch_ghost_vz_adj<T>(const GridDev<T> &, const GridDev<T> &, const AdjDev<T> &,         \
                                                 const AdjDev<T> &, int, double *, double *, double *, cudaStream_t); \
@@ -1687,6 +1831,10 @@ cudaError_t launch_ghost_sxz_adj(const GridDev<T> &F, const GridDev<T> &C, const
     template int sxz_solve_blocks<T>(int, int);                                                          \
     template cudaError_t launch_sxz_solve<T>(const GridDev<T> &, const GridDev<T> &, int, const SxzWork &, int, cudaStream_t); \
     template int sxz_multi_capacity<T>(int);                                                              \
+    template cudaError_t launch_sxz_adj_collect<T>(const GridDev<T> &, const GridDev<T> &, const AdjDev<T> &,     \
+                                                   const AdjDev<T> &, int, double *, cudaStream_t);            \
+    template cudaError_t launch_sxz_adj_scatter<T>(const GridDev<T> &, const GridDev<T> &, const AdjDev<T> &,     \
+                                                   const AdjDev<T> &, int, const double *, cudaStream_t);                                                              \
     template cudaError_t launch_sxz_solve_multi<T>(const SxzSysList<T> &, cudaStream_t);
 INST(float)
 INST(double)

@@ -73,16 +73,22 @@ __host__ __device__ constexpr int ch_slot(int k) { return k < 9 ? 6 + k : (k == 
 __host__ __device__ constexpr int ci_slot(int k) { return k < 6 ? k : (k == 6 ? 15 : (k == 7 ? 18 : 20)); }
 } // namespace s21t
 
+// The maps of one sweep over NSH shots of one grid that share the medium:
+// the coefficient maps are common, the field maps and output blocks per shot.
+template <int NSH>
 struct S21Maps {
-    CUtensorMap v;    // vx vy vz: haloed boxes
-    CUtensorMap cha;  // c6..c14: boxes x-4 .. x+31, y .. y+8
-    CUtensorMap chb;  // c16, c17: boxes x-4 .. x+31, y-1 .. y+7
-    CUtensorMap chc;  // c19: box x .. x+35, y .. y+8
-    CUtensorMap ci;   // c0..c5, c15, c18, c20: interior boxes
-    CUtensorMap sg;   // sxx syy szz syz sxz sxy: interior boxes
-    CUtensorMap ep;   // displacement sums: interior boxes
-    CUtensorMap epx;  // displacement sums: x = -4..-1 face boxes (tiles at x0 = 0)
-    CUtensorMap epy;  // displacement sums: y = -1 face rows (tiles at y0 = 0)
+    CUtensorMap cha;       // c6..c14: boxes x-4 .. x+31, y .. y+8
+    CUtensorMap chb;       // c16, c17: boxes x-4 .. x+31, y-1 .. y+7
+    CUtensorMap chc;       // c19: box x .. x+35, y .. y+8
+    CUtensorMap ci;        // c0..c5, c15, c18, c20: interior boxes
+    CUtensorMap v[NSH];    // vx vy vz: haloed boxes
+    CUtensorMap sg[NSH];   // sxx syy szz syz sxz sxy: interior boxes
+    CUtensorMap ep[NSH];   // displacement sums: interior boxes
+    CUtensorMap epx[NSH];  // displacement sums: x = -4..-1 face boxes (tiles at x0 = 0)
+    CUtensorMap epy[NSH];  // displacement sums: y = -1 face rows (tiles at y0 = 0)
+    float *sg_out[NSH][6]; // the shot's stresses sxx syy szz syz sxz sxy
+    float *u[NSH][3];      // the shot's displacement sums (null: none)
+    int ns;
 };
 
 // the two closure weights of a neighbour pair (w2 of gen21_device.cuh)
@@ -90,10 +96,12 @@ __device__ __forceinline__ void closure_w2(bool a, bool b, float (&w)[2]) { w2<f
 
 __device__ __forceinline__ void consumer_sync() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
 
-template <bool ACC>
+// NSH > 1: maps.ns shots of the grid in one launch, the CTAs of one tile
+// column adjacent (shot fastest), so that the coefficient planes one of them
+// stages are still in L2 when the others stage them.
+template <bool ACC, int NSH>
 __global__ void __launch_bounds__(s21t::NTHREADS, 2)
-    stress21_tma_kernel(const __grid_constant__ S21Maps maps, GridDev<float> G, int flag, int zchunk, float *u0,
-                        float *u1, float *u2, int *status)
+    stress21_tma_kernel(const __grid_constant__ S21Maps<NSH> maps, GridDev<float> G, int flag, int zchunk, int *status)
 {
     using namespace s21t;
     extern __shared__ __align__(128) unsigned char sm[];
@@ -101,9 +109,11 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 2)
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     const Ext E{nx, ny, nz};
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+    const int shot = NSH == 1 ? 0 : (int)(blockIdx.x % (unsigned)maps.ns);
+    const int x0 = (NSH == 1 ? (int)blockIdx.x : (int)(blockIdx.x / (unsigned)maps.ns)) * TX, y0 = blockIdx.y * TY;
     const int z0 = blockIdx.z * zchunk, z1 = min(nz, z0 + zchunk - 1);
     const int qstart = z0 - 1, n = z1 - z0 + 3;   // planes z0-1 .. z1+1
+    float *const u0 = maps.u[shot][0], *const u1 = maps.u[shot][1], *const u2 = maps.u[shot][2];
     const int sz = g.px * g.py;
     const unsigned bar0 = smem_u32(sm + OFF_BAR);
     auto fullP = [&](int s) { return bar0 + 8u * s; };
@@ -138,7 +148,7 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 2)
                 const unsigned dst = smem_u32(sm + OFF_V + s * VSLOT);
                 mbar_expect_tx(fullV(s), 3 * HBOX);
                 const int zc = g.R + qstart - 1 + j;
-                tma_load4(dst, &maps.v, hx0, hy0, zc, fullV(s));
+                tma_load4(dst, &maps.v[shot], hx0, hy0, zc, fullV(s));
                 return true;
             };
             auto issueP = [&](int i) -> bool {
@@ -159,11 +169,11 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 2)
                 tma_load4(dst + P_CHC, &maps.chc, ix0, iy0, zc, fullP(s));
                 if (inner) {
                     tma_load4(dst + P_CI, &maps.ci, ix0, iy0, zc, fullP(s));
-                    tma_load4(dst + P_SG, &maps.sg, ix0, iy0, zc, fullP(s));
+                    tma_load4(dst + P_SG, &maps.sg[shot], ix0, iy0, zc, fullP(s));
                 }
-                if (uin) tma_load4(dst + P_EP, &maps.ep, ix0, iy0, zc, fullP(s));
-                if (ux) tma_load4(dst + P_EX, &maps.epx, XOFF - XFW, iy0, zc, fullP(s));
-                if (uy) tma_load4(dst + P_EY, &maps.epy, ix0, g.R - 1, zc, fullP(s));
+                if (uin) tma_load4(dst + P_EP, &maps.ep[shot], ix0, iy0, zc, fullP(s));
+                if (ux) tma_load4(dst + P_EX, &maps.epx[shot], XOFF - XFW, iy0, zc, fullP(s));
+                if (uy) tma_load4(dst + P_EY, &maps.epy[shot], ix0, g.R - 1, zc, fullP(s));
                 return true;
             };
             bool ok = true;
@@ -189,7 +199,8 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 2)
         const int ox = x0 + tx, oy = y0 + ty;
         const int vb = (ty + 1) * BW + tx + 4, ib = ty * TX + tx, hx = tx + 1, hy = ty + 1;
         const float k0 = G.k[0], k1 = G.k[1], k2 = G.k[2];
-        float *sxx = G.f[SXX], *syy = G.f[SYY], *szz = G.f[SZZ], *syz = G.f[SYZ], *sxz = G.f[SXZ], *sxy = G.f[SXY];
+        float *sxx = maps.sg_out[shot][0], *syy = maps.sg_out[shot][1], *szz = maps.sg_out[shot][2],
+              *syz = maps.sg_out[shot][3], *sxz = maps.sg_out[shot][4], *sxy = maps.sg_out[shot][5];
         // carries from plane pm = p-1 for the syz / sxz outputs
         float c15p = 0.f, c16p = 0.f, c17p = 0.f, c18p = 0.f, c19p = 0.f, s3p = 0.f, s4p = 0.f;
         // the halo job of this warp: kind (0 L4, 1 L5, 2 L6, 3 N) and point
@@ -495,7 +506,7 @@ static bool strided(const Geo &g, int count, F ptr)
 }
 
 // Opaque storage for the maps of one grid (allocated by the caller, s21_maps_bytes()).
-size_t s21_maps_bytes() { return sizeof(S21Maps); }
+size_t s21_maps_bytes() { return sizeof(S21Maps<1>); }
 
 // Fills the maps of one grid; false if the driver entry point is missing, a
 // group is not laid out at a fixed stride, or an address / pitch is not
@@ -503,20 +514,23 @@ size_t s21_maps_bytes() { return sizeof(S21Maps); }
 bool s21_encode_maps(void *out, const GridDev<float> &G, float *const disp[3])
 {
     using namespace s21t;
-    S21Maps M;
+    S21Maps<1> M;
     memset(&M, 0, sizeof M);
+    M.ns = 1;
+    for (int k = 0; k < 6; k++) M.sg_out[0][k] = G.f[SXX + k];
+    for (int k = 0; k < 3; k++) M.u[0][k] = disp ? disp[k] : nullptr;
     const Geo &g = G.g;
     if ((g.px * 4) % 16 != 0 || (XOFF - 4) % 4 != 0) return false;
     bool ok = strided(g, 3, [&](int k) { return (const float *)G.f[k]; }) &&
               strided(g, NCH, [&](int k) { return G.c[ch_slot(k)]; }) &&
               strided(g, NCI, [&](int k) { return G.c[ci_slot(k)]; }) &&
               strided(g, 6, [&](int k) { return (const float *)G.f[SXX + k]; });
-    ok = ok && encode(&M.v, g, G.f[0], 3, BW, BH) && encode(&M.cha, g, G.c[ch_slot(0)], NCA, CW, CHH) &&
+    ok = ok && encode(&M.v[0], g, G.f[0], 3, BW, BH) && encode(&M.cha, g, G.c[ch_slot(0)], NCA, CW, CHH) &&
          encode(&M.chb, g, G.c[ch_slot(NCA)], NCB, CW, CHH) && encode(&M.chc, g, G.c[ch_slot(NCA + NCB)], 1, CW, CHH) &&
-         encode(&M.ci, g, G.c[ci_slot(0)], NCI, TX, TY) && encode(&M.sg, g, G.f[SXX], 6, TX, TY);
+         encode(&M.ci, g, G.c[ci_slot(0)], NCI, TX, TY) && encode(&M.sg[0], g, G.f[SXX], 6, TX, TY);
     if (ok && disp && disp[0])
-        ok = strided(g, 3, [&](int k) { return (const float *)disp[k]; }) && encode(&M.ep, g, disp[0], 3, TX, TY) &&
-             encode(&M.epx, g, disp[0], 3, XFW, TY) && encode(&M.epy, g, disp[0], 3, TX, 1);
+        ok = strided(g, 3, [&](int k) { return (const float *)disp[k]; }) && encode(&M.ep[0], g, disp[0], 3, TX, TY) &&
+             encode(&M.epx[0], g, disp[0], 3, XFW, TY) && encode(&M.epy[0], g, disp[0], 3, TX, 1);
     if (ok) memcpy(out, &M, sizeof M);
     return ok;
 }
@@ -524,9 +538,13 @@ bool s21_encode_maps(void *out, const GridDev<float> &G, float *const disp[3])
 // Opt-in to the kernel's shared memory; call outside stream capture.
 cudaError_t s21_set_attributes()
 {
-    cudaError_t e = cudaFuncSetAttribute(stress21_tma_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s21t::SMEM);
+    cudaError_t e = cudaFuncSetAttribute(stress21_tma_kernel<true, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, s21t::SMEM);
     if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(stress21_tma_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s21t::SMEM);
+        e = cudaFuncSetAttribute(stress21_tma_kernel<false, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, s21t::SMEM);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(stress21_tma_kernel<true, kMaxShots>, cudaFuncAttributeMaxDynamicSharedMemorySize, s21t::SMEM);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(stress21_tma_kernel<false, kMaxShots>, cudaFuncAttributeMaxDynamicSharedMemorySize, s21t::SMEM);
     return e;
 }
 
@@ -546,12 +564,58 @@ cudaError_t launch_stress21_tma(const void *maps, const GridDev<float> &G, int t
     if (nchunk_req > 0) nchunk = nchunk_req < g.nz + 1 ? nchunk_req : g.nz + 1;   // tuned
     const int zc = (g.nz + 1 + nchunk - 1) / nchunk;
     dim3 grd(bx, by, (g.nz + 1 + zc - 1) / zc);
-    const S21Maps &M = *(const S21Maps *)maps;
+    const S21Maps<1> &M = *(const S21Maps<1> *)maps;
     if (disp && disp[0]) {
-        stress21_tma_kernel<true><<<grd, NTHREADS, SMEM, st>>>(M, G, flag, zc, disp[0], disp[1], disp[2], status);
+        stress21_tma_kernel<true, 1><<<grd, NTHREADS, SMEM, st>>>(M, G, flag, zc, status);
     } else {
-        stress21_tma_kernel<false><<<grd, NTHREADS, SMEM, st>>>(M, G, flag, zc, nullptr, nullptr, nullptr, status);
+        stress21_tma_kernel<false, 1><<<grd, NTHREADS, SMEM, st>>>(M, G, flag, zc, status);
     }
+    return cudaGetLastError();
+}
+
+// The sweep of ns shots of one grid sharing the medium (same geometry, same
+// coefficients): maps[s] is shot s's opaque map block (s21_encode_maps); the
+// coefficient maps are taken from shot 0's.  Same launch shape as one shot
+// per tile column, with the shots' CTAs of a column adjacent.
+cudaError_t launch_stress21_tma_shots(const void *const *maps, int ns, const GridDev<float> &G, int top, int top_bc,
+                                      bool acc, int *status, int sms, cudaStream_t st, int nchunk_req)
+{
+    using namespace s21t;
+    if (ns < 1 || ns > kMaxShots) return cudaErrorInvalidValue;
+    static thread_local S21Maps<kMaxShots> M;   // host staging of the kernel parameter (2 KB of maps per shot)
+    memset(&M, 0, sizeof M);
+    const S21Maps<1> &M0 = *(const S21Maps<1> *)maps[0];
+    M.cha = M0.cha;
+    M.chb = M0.chb;
+    M.chc = M0.chc;
+    M.ci = M0.ci;
+    M.ns = ns;
+    for (int s = 0; s < ns; s++) {
+        const S21Maps<1> &Ms = *(const S21Maps<1> *)maps[s];
+        M.v[s] = Ms.v[0];
+        M.sg[s] = Ms.sg[0];
+        M.ep[s] = Ms.ep[0];
+        M.epx[s] = Ms.epx[0];
+        M.epy[s] = Ms.epy[0];
+        for (int k = 0; k < 6; k++) M.sg_out[s][k] = Ms.sg_out[0][k];
+        for (int k = 0; k < 3; k++) M.u[s][k] = Ms.u[0][k];
+        if (acc && !Ms.u[0][0]) return cudaErrorInvalidValue;
+    }
+    const Geo &g = G.g;
+    const int flag = (top && top_bc) ? 1 : 0;
+    const int bx = (g.nx + 1 + TX - 1) / TX, by = (g.ny + 1 + TY - 1) / TY;
+    const int64_t cols = (int64_t)bx * by * ns;
+    int nchunk = (int)(((int64_t)sms * 4 + cols - 1) / cols);
+    if (nchunk < 1) nchunk = 1;
+    const int maxc = (g.nz + 1) / 24 > 0 ? (g.nz + 1) / 24 : 1;
+    if (nchunk > maxc) nchunk = maxc;
+    if (nchunk_req > 0) nchunk = nchunk_req < g.nz + 1 ? nchunk_req : g.nz + 1;
+    const int zc = (g.nz + 1 + nchunk - 1) / nchunk;
+    dim3 grd(bx * ns, by, (g.nz + 1 + zc - 1) / zc);
+    if (acc)
+        stress21_tma_kernel<true, kMaxShots><<<grd, NTHREADS, SMEM, st>>>(M, G, flag, zc, status);
+    else
+        stress21_tma_kernel<false, kMaxShots><<<grd, NTHREADS, SMEM, st>>>(M, G, flag, zc, status);
     return cudaGetLastError();
 }
 

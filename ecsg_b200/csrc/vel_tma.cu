@@ -51,14 +51,24 @@ constexpr int TX_IN = bytes(B_SXX) + bytes(B_SXY) + bytes(B_SXZ) + bytes(B_SYY) 
                       bytes(B_B) + 3 * bytes(B_V);
 } // namespace vtma
 
+// The maps of one sweep over NSH shots of one grid that share the medium: the
+// buoyancy map is common, the field maps and the velocity outputs per shot.
+template <int NSH>
 struct VelMaps {
-    CUtensorMap sxx, sxy, sxz, syy, syz, szz, b, v;
+    CUtensorMap b;
+    CUtensorMap sxx[NSH], sxy[NSH], sxz[NSH], syy[NSH], syz[NSH], szz[NSH], v[NSH];
+    float *vout[NSH][3];   // the shot's vx vy vz
+    int ns;
 };
 
 __device__ __forceinline__ void vel_consumer_sync() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
 
+// NSH > 1: maps.ns shots of the grid in one launch, the CTAs of one tile
+// column adjacent (shot fastest), so the buoyancy planes one of them stages
+// are still in L2 for the others.
+template <int NSH>
 __global__ void __launch_bounds__(vtma::NTHREADS, 2)
-    vel_tma_kernel(const __grid_constant__ VelMaps maps, GridDev<float> G, int zt, int bottom, int zchunk, float *vc0,
+    vel_tma_kernel(const __grid_constant__ VelMaps<NSH> maps, GridDev<float> G, int zt, int bottom, int zchunk, float *vc0,
                    float *vc1, float *vc2, int *status)
 {
     using namespace vtma;
@@ -66,7 +76,8 @@ __global__ void __launch_bounds__(vtma::NTHREADS, 2)
     const Geo &g = G.g;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+    const int shot = NSH == 1 ? 0 : (int)(blockIdx.x % (unsigned)maps.ns);
+    const int x0 = (NSH == 1 ? (int)blockIdx.x : (int)(blockIdx.x / (unsigned)maps.ns)) * TX, y0 = blockIdx.y * TY;
     const int z0 = blockIdx.z * zchunk, z1 = min(nz, z0 + zchunk - 1);
     const int n = z1 - z0 + 3;   // planes z0-1 .. z1+1
     const unsigned bar0 = smem_u32(sm + OFF_BAR);
@@ -97,18 +108,18 @@ __global__ void __launch_bounds__(vtma::NTHREADS, 2)
                 const bool lo = q < z0, hi = q > z1;
                 mbar_expect_tx(full(s), lo ? TX_LO : (hi ? TX_HI : TX_IN));
                 if (!hi) {
-                    tma_load4(d + O_SXZ, &maps.sxz, xa + B_SXZ.ox, ya + B_SXZ.oy, zc, full(s));
-                    tma_load4(d + O_SYZ, &maps.syz, xa + B_SYZ.ox, ya + B_SYZ.oy, zc, full(s));
+                    tma_load4(d + O_SXZ, &maps.sxz[shot], xa + B_SXZ.ox, ya + B_SXZ.oy, zc, full(s));
+                    tma_load4(d + O_SYZ, &maps.syz[shot], xa + B_SYZ.ox, ya + B_SYZ.oy, zc, full(s));
                 }
                 if (!lo) {
-                    tma_load4(d + O_SZZ, &maps.szz, xa + B_SZZ.ox, ya + B_SZZ.oy, zc, full(s));
+                    tma_load4(d + O_SZZ, &maps.szz[shot], xa + B_SZZ.ox, ya + B_SZZ.oy, zc, full(s));
                     tma_load4(d + O_B, &maps.b, xa + B_B.ox, ya + B_B.oy, zc, full(s));
                 }
                 if (!lo && !hi) {
-                    tma_load4(d + O_SXX, &maps.sxx, xa + B_SXX.ox, ya + B_SXX.oy, zc, full(s));
-                    tma_load4(d + O_SXY, &maps.sxy, xa + B_SXY.ox, ya + B_SXY.oy, zc, full(s));
-                    tma_load4(d + O_SYY, &maps.syy, xa + B_SYY.ox, ya + B_SYY.oy, zc, full(s));
-                    tma_load4(d + O_V, &maps.v, xa + B_V.ox, ya + B_V.oy, zc, full(s));
+                    tma_load4(d + O_SXX, &maps.sxx[shot], xa + B_SXX.ox, ya + B_SXX.oy, zc, full(s));
+                    tma_load4(d + O_SXY, &maps.sxy[shot], xa + B_SXY.ox, ya + B_SXY.oy, zc, full(s));
+                    tma_load4(d + O_SYY, &maps.syy[shot], xa + B_SYY.ox, ya + B_SYY.oy, zc, full(s));
+                    tma_load4(d + O_V, &maps.v[shot], xa + B_V.ox, ya + B_V.oy, zc, full(s));
                 }
                 issued = i + 1;
                 if (flags[3]) break;
@@ -123,7 +134,7 @@ __global__ void __launch_bounds__(vtma::NTHREADS, 2)
         const int ty = warp, iy = y0 + ty;
         const float k0 = G.k[0], k1 = G.k[1], k2 = G.k[2];
         const float qq = 0.25f;
-        float *vxg = G.f[VX], *vyg = G.f[VY], *vzg = G.f[VZ];
+        float *vxg = maps.vout[shot][0], *vyg = maps.vout[shot][1], *vzg = maps.vout[shot][2];
         const bool vc = vc0 != nullptr;
         const bool yrow = iy <= ny - 1;                  // rows the velocity update touches (vy: 0 .. ny-1)
         const bool yin = iy >= 1 && iy <= ny - 1;        // vx, vz: y walls excluded
@@ -211,31 +222,36 @@ __global__ void __launch_bounds__(vtma::NTHREADS, 2)
 // ---------------------------------------------------------------------------
 // Host side
 // ---------------------------------------------------------------------------
-size_t vel_maps_bytes() { return sizeof(VelMaps); }
+size_t vel_maps_bytes() { return sizeof(VelMaps<1>); }
 
 // Maps of one grid's velocity sweep; false if the driver entry point is missing
 // or an address / pitch is not encodable.
 bool vel_encode_maps(void *out, const GridDev<float> &G)
 {
     using namespace vtma;
-    VelMaps M;
+    VelMaps<1> M;
     memset(&M, 0, sizeof M);
+    M.ns = 1;
+    for (int k = 0; k < 3; k++) M.vout[0][k] = G.f[VX + k];
     const Geo &g = G.g;
     if ((g.px * 4) % 16 != 0) return false;
     // velocities: one allocation at a fixed stride
     for (int k = 1; k < 3; k++)
         if (G.f[k] != G.f[0] + (size_t)k * g.size()) return false;
-    bool ok = encode(&M.sxx, g, G.f[SXX], 1, B_SXX.w, B_SXX.h) && encode(&M.sxy, g, G.f[SXY], 1, B_SXY.w, B_SXY.h) &&
-              encode(&M.sxz, g, G.f[SXZ], 1, B_SXZ.w, B_SXZ.h) && encode(&M.syy, g, G.f[SYY], 1, B_SYY.w, B_SYY.h) &&
-              encode(&M.syz, g, G.f[SYZ], 1, B_SYZ.w, B_SYZ.h) && encode(&M.szz, g, G.f[SZZ], 1, B_SZZ.w, B_SZZ.h) &&
-              encode(&M.b, g, G.b, 1, B_B.w, B_B.h) && encode(&M.v, g, G.f[VX], 3, B_V.w, B_V.h);
+    bool ok = encode(&M.sxx[0], g, G.f[SXX], 1, B_SXX.w, B_SXX.h) && encode(&M.sxy[0], g, G.f[SXY], 1, B_SXY.w, B_SXY.h) &&
+              encode(&M.sxz[0], g, G.f[SXZ], 1, B_SXZ.w, B_SXZ.h) && encode(&M.syy[0], g, G.f[SYY], 1, B_SYY.w, B_SYY.h) &&
+              encode(&M.syz[0], g, G.f[SYZ], 1, B_SYZ.w, B_SYZ.h) && encode(&M.szz[0], g, G.f[SZZ], 1, B_SZZ.w, B_SZZ.h) &&
+              encode(&M.b, g, G.b, 1, B_B.w, B_B.h) && encode(&M.v[0], g, G.f[VX], 3, B_V.w, B_V.h);
     if (ok) memcpy(out, &M, sizeof M);
     return ok;
 }
 
 cudaError_t vel_tma_set_attributes()
 {
-    return cudaFuncSetAttribute(vel_tma_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, vtma::SMEM);
+    cudaError_t e = cudaFuncSetAttribute(vel_tma_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, vtma::SMEM);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(vel_tma_kernel<kMaxShots>, cudaFuncAttributeMaxDynamicSharedMemorySize, vtma::SMEM);
+    return e;
 }
 
 cudaError_t launch_vel_tma(const void *maps, const GridDev<float> &G, int top, int bottom, int top_bc,
@@ -254,8 +270,47 @@ cudaError_t launch_vel_tma(const void *maps, const GridDev<float> &G, int top, i
     if (nchunk_req > 0) nchunk = nchunk_req < g.nz + 1 ? nchunk_req : g.nz + 1;   // tuned
     const int zc = (g.nz + 1 + nchunk - 1) / nchunk;
     dim3 grd(bx, by, (g.nz + 1 + zc - 1) / zc);
-    vel_tma_kernel<<<grd, NTHREADS, SMEM, st>>>(*(const VelMaps *)maps, G, zt, bottom, zc, vcopy ? vcopy[0] : nullptr,
-                                                vcopy ? vcopy[1] : nullptr, vcopy ? vcopy[2] : nullptr, status);
+    vel_tma_kernel<1><<<grd, NTHREADS, SMEM, st>>>(*(const VelMaps<1> *)maps, G, zt, bottom, zc, vcopy ? vcopy[0] : nullptr,
+                                                   vcopy ? vcopy[1] : nullptr, vcopy ? vcopy[2] : nullptr, status);
+    return cudaGetLastError();
+}
+
+// The sweep of ns shots of one grid sharing the medium (no velocity copies):
+// maps[s] is shot s's opaque map block (vel_encode_maps); the buoyancy map
+// is shot 0's.  Same launch shape as one shot per tile column, the shots'
+// CTAs of a column adjacent.
+cudaError_t launch_vel_tma_shots(const void *const *maps, int ns, const GridDev<float> &G, int top, int bottom,
+                                 int top_bc, int *status, int sms, cudaStream_t st, int nchunk_req)
+{
+    using namespace vtma;
+    if (ns < 1 || ns > kMaxShots) return cudaErrorInvalidValue;
+    static thread_local VelMaps<kMaxShots> M;   // host staging of the kernel parameter
+    memset(&M, 0, sizeof M);
+    M.b = ((const VelMaps<1> *)maps[0])->b;
+    M.ns = ns;
+    for (int s = 0; s < ns; s++) {
+        const VelMaps<1> &Ms = *(const VelMaps<1> *)maps[s];
+        M.sxx[s] = Ms.sxx[0];
+        M.sxy[s] = Ms.sxy[0];
+        M.sxz[s] = Ms.sxz[0];
+        M.syy[s] = Ms.syy[0];
+        M.syz[s] = Ms.syz[0];
+        M.szz[s] = Ms.szz[0];
+        M.v[s] = Ms.v[0];
+        for (int k = 0; k < 3; k++) M.vout[s][k] = Ms.vout[0][k];
+    }
+    const Geo &g = G.g;
+    const int zt = (top && top_bc != 1) ? 1 : 0;
+    const int bx = (g.nx + 1 + TX - 1) / TX, by = (g.ny + TY - 1) / TY;
+    const int64_t cols = (int64_t)bx * by * ns;
+    int nchunk = (int)(((int64_t)sms * 8 + cols - 1) / cols);
+    if (nchunk < 1) nchunk = 1;
+    const int maxc = (g.nz + 1) / 24 > 0 ? (g.nz + 1) / 24 : 1;
+    if (nchunk > maxc) nchunk = maxc;
+    if (nchunk_req > 0) nchunk = nchunk_req < g.nz + 1 ? nchunk_req : g.nz + 1;
+    const int zc = (g.nz + 1 + nchunk - 1) / nchunk;
+    dim3 grd(bx * ns, by, (g.nz + 1 + zc - 1) / zc);
+    vel_tma_kernel<kMaxShots><<<grd, NTHREADS, SMEM, st>>>(M, G, zt, bottom, zc, nullptr, nullptr, nullptr, status);
     return cudaGetLastError();
 }
 

@@ -15,7 +15,9 @@
   by 1000 and vx receivers, as the reference's main.cpp injects and records)
   against the reference's own FP32 build (oracle/_ref/libecsg_ref32.so,
   whose Jacobi loop is capped at 20000 sweeps because the unmodified FP32
-  loop does not terminate on test1), 1500 steps: traces within 1e-5 rel-L2.
+  loop does not terminate on test1), 1500 steps: traces within 1e-5 rel-L2,
+  all receivers together and each one that records a signal (the two on
+  the rigid x walls record vx = 0 on both sides).
 * The reference's experiment test1 (tests/test1-cmp-eci-ii/eci, ECI, ratio
   2) against the same FP32 build over its first 212 steps, which include
   Jacobi solves where the FP32 reference stops at its 20000-sweep cap:
@@ -95,7 +97,9 @@ def test_config1_ratio2_twin_against_reference_fp32_build():
         out = s.run(case.nsteps)
         assert s.status() == 0
     assert _rel(out["rec"], ref) <= 1e-5
-    per = np.linalg.norm(out["rec"] - ref, axis=1) / np.linalg.norm(ref, axis=1)
+    live = np.linalg.norm(ref, axis=1) > 0   # the receivers on the rigid x walls record vx = 0 exactly
+    assert live.sum() >= 89 and np.array_equal(out["rec"][~live], ref[~live])
+    per = np.linalg.norm(out["rec"][live] - ref[live], axis=1) / np.linalg.norm(ref[live], axis=1)
     assert per.max() <= 1e-5, per.max()
 
 
@@ -125,5 +129,7 @@ def test_tilted_vti_three_grid_fp32_against_fp64_over_1000_steps():
     for g in range(3):
         for k in range(9):
             assert _rel(f32[g][k], f64[g][k]) <= 1e-5, (g, k)
-    e64, e32 = o64["energy"][49::50], o32["energy"][49::50]
+    on = ~np.isnan(o64["energy"])   # the steps with an energy evaluation
+    e64, e32 = o64["energy"][on], o32["energy"][on]
+    assert len(e64) == n // 50 and np.isfinite(e32).all()
     assert np.abs(e32 - e64).max() <= 1e-5 * np.abs(e64).max()

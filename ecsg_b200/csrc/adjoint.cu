@@ -185,7 +185,8 @@ __device__ __forceinline__ void mirror_adj(T *l, int h, int i)
 }
 
 template <typename T>
-__global__ void vel_mirror_adj_kernel(Geo g, T *lvy, T *lvz, int phase, int top_rigid, int bottom, int mirror_fix)
+__device__ __forceinline__ void vel_mirror_adj_body(const Geo &g, T *lvy, T *lvz, int phase, int top_rigid, int bottom,
+                                                    int mirror_fix)
 {
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -211,6 +212,12 @@ __global__ void vel_mirror_adj_kernel(Geo g, T *lvy, T *lvz, int phase, int top_
         t -= nG;
         if (t < nG) { int ix = t % nx, iz = t / nx; mirror_adj(lvy, g.idx(ix, ny, iz), g.idx(ix, ny - 1, iz)); return; }
     }
+}
+
+template <typename T>
+__global__ void vel_mirror_adj_kernel(Geo g, T *lvy, T *lvz, int phase, int top_rigid, int bottom, int mirror_fix)
+{
+    vel_mirror_adj_body(g, lvy, lvz, phase, top_rigid, bottom, mirror_fix);
 }
 
 // Receiver sampling: lambda_v[rec] += residual (a receiver samples a velocity).
@@ -701,7 +708,7 @@ __global__ void stress21_adj_g2(GridDev<T> G, AdjDev<T> A)
 // transpose of the strain differences: every velocity entry gathers the W of
 // the strains that read it
 template <typename T>
-__global__ void stress21_adj_g3(GridDev<T> G, AdjDev<T> A)
+__device__ __forceinline__ void g3_body(const GridDev<T> &G, const AdjDev<T> &A)
 {
     const Geo &g = G.g;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
@@ -733,6 +740,31 @@ __global__ void stress21_adj_g3(GridDev<T> G, AdjDev<T> A)
         if (gy != T(0)) A.l[VY][p] = add_(ly, gy);
         if (gz != T(0)) A.l[VZ][p] = add_(lz, gz);
     }
+}
+
+template <typename T>
+__global__ void stress21_adj_g3(GridDev<T> G, AdjDev<T> A)
+{
+    g3_body(G, A);
+}
+
+// G3 of every shot: shot blockIdx.y
+template <typename T>
+__global__ void stress21_adj_g3_shots(GridDev<T> G, AdjDev<T> A0, const __grid_constant__ AdjShots<T> S)
+{
+    GridDev<T> Gs;
+    AdjDev<T> As;
+    shot_views(G, A0, S, blockIdx.y, Gs, As);
+    g3_body(Gs, As);
+}
+
+// velocity mirror transposes of every shot: shot blockIdx.y
+template <typename T>
+__global__ void vel_mirror_adj_shots_kernel(Geo g, const __grid_constant__ AdjShots<T> S, int phase, int top_rigid,
+                                            int bottom, int mirror_fix)
+{
+    T *l = S.l[blockIdx.y];
+    vel_mirror_adj_body(g, l + VY * S.box, l + VZ * S.box, phase, top_rigid, bottom, mirror_fix);
 }
 
 // ---------------------------------------------------------------------------
@@ -788,17 +820,20 @@ cudaError_t launch_stress21_adj_shots(const GridDev<T> &G, const AdjDev<T> &A0, 
     const unsigned nb = blocks_for(n, sms);
     stress21_adj_g0_shots<T><<<nb, 256, 0, st>>>(G, A0, S, flag);
     stress21_adj_g1_shots<T><<<nb, 256, 0, st>>>(G, A0, S, flag);
-    for (int s = 0; s < S.ns; s++) {
-        GridDev<T> Gs = G;
-        AdjDev<T> As = A0;
-        for (int k = 0; k < 9; k++) {
-            Gs.f[k] = S.f[s] + k * S.box;
-            As.l[k] = S.l[s] + k * S.box;
+    if (flag)   // the free surface adds to the common gradient without atomics: one shot at a time
+        for (int s = 0; s < S.ns; s++) {
+            GridDev<T> Gs = G;
+            AdjDev<T> As = A0;
+            for (int k = 0; k < 9; k++) {
+                Gs.f[k] = S.f[s] + k * S.box;
+                As.l[k] = S.l[s] + k * S.box;
+            }
+            for (int k = 0; k < 15; k++) As.w[k] = S.w[s] + k * S.wbox;
+            stress21_adj_g2<T><<<(g.nx * (g.ny + 1) + 255) / 256, 256, 0, st>>>(Gs, As);
         }
-        for (int k = 0; k < 15; k++) As.w[k] = S.w[s] + k * S.wbox;
-        if (flag) stress21_adj_g2<T><<<(g.nx * (g.ny + 1) + 255) / 256, 256, 0, st>>>(Gs, As);
-        stress21_adj_g3<T><<<blocks_for((int64_t)(g.nx + 2) * (g.ny + 2) * (g.nz + 2), sms), 256, 0, st>>>(Gs, As);
-    }
+    const unsigned nb3 = blocks_for((int64_t)(g.nx + 2) * (g.ny + 2) * (g.nz + 2), sms);
+    const unsigned per = (nb3 + S.ns - 1) / S.ns;   // about the one-shot launch's CTAs in all
+    stress21_adj_g3_shots<T><<<dim3(per, S.ns), 256, 0, st>>>(G, A0, S);
     return cudaGetLastError();
 }
 
@@ -813,11 +848,10 @@ cudaError_t launch_vel_adj_shots(const GridDev<T> &G, T *gb, const AdjShots<T> &
     const int64_t n0 = (int64_t)(top_rigid + bottom) * (g.ny + 1) * g.nx + 2LL * g.nz * (g.ny + 1)
                      + 2LL * (g.nz + 1) * (g.ny + 1);
     const int64_t n1 = 2LL * (g.nz + (mirror_fix ? 1 : 0)) * g.nx;
-    for (int s = 0; s < S.ns; s++) {
-        T *lvy = S.l[s] + VY * S.box, *lvz = S.l[s] + VZ * S.box;
-        vel_mirror_adj_kernel<T><<<(unsigned)((n1 + 255) / 256), 256, 0, st>>>(g, lvy, lvz, 1, top_rigid, bottom, mirror_fix);
-        vel_mirror_adj_kernel<T><<<(unsigned)((n0 + 255) / 256), 256, 0, st>>>(g, lvy, lvz, 0, top_rigid, bottom, mirror_fix);
-    }
+    vel_mirror_adj_shots_kernel<T><<<dim3((unsigned)((n1 + 255) / 256), S.ns), 256, 0, st>>>(g, S, 1, top_rigid, bottom,
+                                                                                             mirror_fix);
+    vel_mirror_adj_shots_kernel<T><<<dim3((unsigned)((n0 + 255) / 256), S.ns), 256, 0, st>>>(g, S, 0, top_rigid, bottom,
+                                                                                             mirror_fix);
     vel_adj_shots_kernel<T><<<blocks_for((int64_t)g.nx * g.ny * (g.nz + 1), sms), 256, 0, st>>>(G, gb, S, top_rigid, bottom);
     return cudaGetLastError();
 }

@@ -216,6 +216,62 @@ def shot_gradients(args, local, world, max_over_ranks, barrier):
             "batched": batched}
 
 
+def config5_subset(args, local, world, max_over_ranks, barrier):
+    """Batched shot gradients with the structure of the benchmark's batched
+    configuration (shots on an 8 x 8 surface grid of the three-grid tilted-VTI
+    model, 8 shots per lockstep call sharing the medium, 2000 steps,
+    checkpoints every 100 steps) on the 1/27-volume copy of the model
+    (361x361x41 @ 5 m / 121x121x55 @ 15 m / 41x41x35 @ 45 m): at full size one
+    shot's 21 checkpoints alone (6.5 GB each) exceed a GPU's memory.  Observed
+    data: the model built from seed 1 (other perturbations, dips and
+    azimuths).  The first args.c5_shots shots of the 8 x 8 grid in lockstep
+    against plain runs of the first args.c5_plain of them, device-timed."""
+    import ecsg_b200
+    from ecsg_b200.workloads import three_grid_case
+    n, k = args.c5_steps, 100
+    grids = [((360, 360, 40), 5.0), ((120, 120, 54), 15.0), ((40, 40, 34), 45.0)]
+
+    def shot_case(j, seed):
+        c = three_grid_case(seed=seed, grids=grids, nsteps=n, medium="tti")
+        n0, h0 = grids[0]
+        c.src = dict(c.src, xyz=((j % 8 + 0.5) / 8 * n0[0] * h0, (j // 8 + 0.5) / 8 * n0[1] * h0, 0.0))
+        return c
+    S = args.c5_shots
+    obs = []
+    for j in range(S):
+        with ecsg_b200.Simulation(shot_case(j, 1), precision="f32", device=local) as s:
+            obs.append(s.run(n)["rec"].T.copy())
+    plain_ms = []
+    for j in range(args.c5_plain):
+        with ecsg_b200.Simulation(shot_case(j, 0), precision="f32", device=local) as s:
+            s.misfit_gradient(obs[j][:min(n, 120)], ckpt_every=k)
+            s.timer_start()
+            s.misfit_gradient(obs[j], ckpt_every=k)
+            plain_ms.append(s.timer_stop())
+    model = ecsg_b200.Simulation(shot_case(0, 0), precision="f32", device=local)
+    sims = [model] + [ecsg_b200.Simulation.shot(model, shot_case(j, 0)) for j in range(1, S)]
+    try:
+        ecsg_b200.shots_misfit_gradient(sims, [o[:min(n, 120)] for o in obs], ckpt_every=k)
+        barrier()
+        model.timer_start()
+        losses = ecsg_b200.shots_misfit_gradient(sims, obs, ckpt_every=k)
+        bms = model.timer_stop()
+        status = max(x.status() for x in sims)
+    finally:
+        for x in sims[1:]:
+            x.close()
+        model.close()
+    bms = max_over_ranks(bms)
+    pms = max_over_ranks(float(np.mean(plain_ms)))
+    return {"metric": "shot-gradients/s", "workload": "batched-configuration subset: %d shots of the 8 x 8 surface "
+                                                      "grid, three-grid tilted VTI at 1/27 volume (6,207,251 points), "
+                                                      "%d steps, checkpoints every %d" % (S, n, k),
+            "shots": S, "value": world * S / (bms * 1e-3), "ms_per_batch": bms,
+            "plain_value": world / (pms * 1e-3), "plain_ms_per_shot_gradient": pms, "plain_shots_timed": args.c5_plain,
+            "speedup_vs_plain": (S / bms) / (1.0 / pms), "finite": bool(np.isfinite(losses).all()), "status": status,
+            "timing": "CUDA events on the library stream"}
+
+
 def accuracy(args, local):
     """FP32 production path against an FP64 shadow run of a reduced copy of the
     benchmark case (three grids at ratio 3, 181x181x25 @ 5 m / 61x61x19 @ 15 m
@@ -300,6 +356,10 @@ def main():
                     help="shots per batched shot-gradient run (0 or 1: no batched leg)")
     ap.add_argument("--grad-steps", type=int, default=1500,
                     help="steps of the shot-gradient measurement (0: skip it)")
+    ap.add_argument("--c5-steps", type=int, default=2000,
+                    help="steps of the batched-configuration subset (0: skip it)")
+    ap.add_argument("--c5-shots", type=int, default=8)
+    ap.add_argument("--c5-plain", type=int, default=1, help="plain shots timed for the subset's comparison")
     ap.add_argument("--accuracy-steps", type=int, default=600,
                     help="steps of the FP32-vs-FP64 accuracy run (0: skip it)")
     ap.add_argument("--batch-steps", type=int, default=200,
@@ -425,6 +485,7 @@ def main():
     sim.close()
     grad = shot_gradients(args, local, world, max_over_ranks, barrier) if args.grad_steps > 0 else None
     batched = batched_forward(args, local, world, max_over_ranks, barrier) if args.batch_steps > 0 else None
+    c5 = config5_subset(args, local, world, max_over_ranks, barrier) if args.c5_steps > 0 else None
     acc_line = accuracy(args, local) if (rank == 0 and args.accuracy_steps > 0) else None
     if rank == 0:
         line = {
@@ -457,6 +518,7 @@ def main():
             "gpu_launches": launches,
             "shot_gradients": grad,
             "batched_forward": batched,
+            "shot_gradients_batched_config_subset": c5,
             "accuracy": acc_line,
         }
         print(json.dumps(line))

@@ -37,6 +37,16 @@ __device__ __forceinline__ void weights4(const bool (&a)[2], const bool (&b)[2],
     w[1][0] = mul_(wa1, wb0); w[1][1] = mul_(wa1, wb1);
 }
 
+// The point kernels below run one thread per point on a 3-D launch: 256
+// threads cover a 32 x 8 (x, y) tile, blockIdx.z the plane (no index
+// division).
+__device__ __forceinline__ void tile_xy(int &x, int &y)
+{
+    x = (int)blockIdx.x * 32 + (int)(threadIdx.x & 31);
+    y = (int)blockIdx.y * 8 + (int)(threadIdx.x >> 5);
+}
+static inline dim3 grid3(int nx, int ny, int nz) { return dim3((unsigned)(nx + 31) / 32, (unsigned)(ny + 7) / 8, (unsigned)nz); }
+
 // ---------------------------------------------------------------------------
 // Velocity update: v += b * (k . D sigma) on the forward ranges.
 // lambda_sigma += (b D)^T lambda_v; g_b += lambda_v * (k . D sigma), the vy
@@ -47,14 +57,16 @@ __global__ void vel_adj_kernel(GridDev<T> G, AdjDev<T> A, int zt, int bottom)
 {
     const Geo &g = G.g;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
-    const int64_t n = (int64_t)nx * ny * (nz + 1);   // x < nx, y < ny cover every updated point
     const int sx = 1, sy = g.px, sz = g.px * g.py;
     const T k0 = G.k[0], k1 = G.k[1], k2 = G.k[2], q = T(0.25);
     const T *b = G.b;
     const T *sxx = G.f[SXX], *syy = G.f[SYY], *szz = G.f[SZZ], *syz = G.f[SYZ], *sxz = G.f[SXZ], *sxy = G.f[SXY];
     T *lsxx = A.l[SXX], *lsyy = A.l[SYY], *lszz = A.l[SZZ], *lsyz = A.l[SYZ], *lsxz = A.l[SXZ], *lsxy = A.l[SXY];
-    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
-        const int ix = (int)(t % nx), iy = (int)((t / nx) % ny), iz = (int)(t / ((int64_t)nx * ny));
+    {
+        int ix, iy;
+        tile_xy(ix, iy);
+        const int iz = blockIdx.z;
+        if (ix >= nx || iy >= ny) return;
         const int p = g.idx(ix, iy, iz);
         const bool zin = iz >= zt && iz <= nz - bottom;
         if (ix >= 1 && iy >= 1 && zin) {   // vx
@@ -108,13 +120,15 @@ __global__ void vel_adj_shots_kernel(GridDev<T> G, T *gb, const __grid_constant_
 {
     const Geo &g = G.g;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
-    const int64_t n = (int64_t)nx * ny * (nz + 1);
     const int sx = 1, sy = g.px, sz = g.px * g.py;
     const T k0 = G.k[0], k1 = G.k[1], k2 = G.k[2], q = T(0.25);
     const T *b = G.b;
     const int64_t box = S.box;
-    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
-        const int ix = (int)(t % nx), iy = (int)((t / nx) % ny), iz = (int)(t / ((int64_t)nx * ny));
+    {
+        int ix, iy;
+        tile_xy(ix, iy);
+        const int iz = blockIdx.z;
+        if (ix >= nx || iy >= ny) return;
         const int p = g.idx(ix, iy, iz);
         const bool zin = iz >= zt && iz <= nz - bottom;
         const bool dx = ix >= 1 && iy >= 1 && zin, dy = zin, dz = iy >= 1 && iz <= nz - 1;
@@ -326,9 +340,11 @@ __global__ void stress21_adj_g0(GridDev<T> G, AdjDev<T> A, int flag)
     const Geo &g = G.g;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     const Ext E{nx, ny, nz};
-    const int64_t n = (int64_t)(nx + 1) * (ny + 1) * (nz + 1);
-    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
-        const int x = (int)(t % (nx + 1)), y = (int)((t / (nx + 1)) % (ny + 1)), z = (int)(t / ((int64_t)(nx + 1) * (ny + 1)));
+    {
+        int x, y;
+        tile_xy(x, y);
+        const int z = blockIdx.z;
+        if (x > nx || y > ny) return;
         g0_point(G, A, flag, E, x, y, z);
     }
 }
@@ -589,10 +605,12 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2) stress21_adj_g1(G
     const Geo &g = G.g;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     const Ext E{nx, ny, nz};
-    const int64_t n = (int64_t)(nx + 1) * (ny + 1) * (nz + 1);
     auto one = [&](int, GridDev<T> &Gs, AdjDev<T> &As) { Gs = G; As = A; };
-    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
-        const int x = (int)(t % (nx + 1)), y = (int)((t / (nx + 1)) % (ny + 1)), z = (int)(t / ((int64_t)(nx + 1) * (ny + 1)));
+    {
+        int x, y;
+        tile_xy(x, y);
+        const int z = blockIdx.z;
+        if (x > nx || y > ny) return;
         g1_point(G, A, flag, E, x, y, z, 1, one);
     }
 }
@@ -621,9 +639,11 @@ __global__ void stress21_adj_g0_shots(GridDev<T> G, AdjDev<T> A0, const __grid_c
     const Geo &g = G.g;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     const Ext E{nx, ny, nz};
-    const int64_t n = (int64_t)(nx + 1) * (ny + 1) * (nz + 1);
-    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
-        const int x = (int)(t % (nx + 1)), y = (int)((t / (nx + 1)) % (ny + 1)), z = (int)(t / ((int64_t)(nx + 1) * (ny + 1)));
+    {
+        int x, y;
+        tile_xy(x, y);
+        const int z = blockIdx.z;
+        if (x > nx || y > ny) return;
         for (int s = 0; s < S.ns; s++) {
             GridDev<T> Gs;
             AdjDev<T> As;
@@ -641,10 +661,12 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2)
     const Geo &g = G.g;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     const Ext E{nx, ny, nz};
-    const int64_t n = (int64_t)(nx + 1) * (ny + 1) * (nz + 1);
     auto shot = [&](int s, GridDev<T> &Gs, AdjDev<T> &As) { shot_views(G, A0, S, s, Gs, As); };
-    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
-        const int x = (int)(t % (nx + 1)), y = (int)((t / (nx + 1)) % (ny + 1)), z = (int)(t / ((int64_t)(nx + 1) * (ny + 1)));
+    {
+        int x, y;
+        tile_xy(x, y);
+        const int z = blockIdx.z;
+        if (x > nx || y > ny) return;
         g1_point(G, A0, flag, E, x, y, z, S.ns, shot);
     }
 }
@@ -708,18 +730,22 @@ __global__ void stress21_adj_g2(GridDev<T> G, AdjDev<T> A)
 // transpose of the strain differences: every velocity entry gathers the W of
 // the strains that read it
 template <typename T>
-__device__ __forceinline__ void g3_body(const GridDev<T> &G, const AdjDev<T> &A)
+__device__ __forceinline__ void g3_body(const GridDev<T> &G, const AdjDev<T> &A, int zb)
 {
     const Geo &g = G.g;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     const Ext E{nx, ny, nz};
-    const int64_t n = (int64_t)(nx + 2) * (ny + 2) * (nz + 2);   // x, y, z in [-1, n]
     const T k0 = G.k[0], k1 = G.k[1], k2 = G.k[2];
     T *const *X = A.w;
     auto I = [&](int x, int y, int z) { return g.idx(x, y, z); };
     auto W = [&](int k, bool ok, int x, int y, int z) -> T { return ok ? X[X_W + k][I(x, y, z)] : T(0); };
-    for (int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; t < n; t += (int64_t)gridDim.x * blockDim.x) {
-        const int x = (int)(t % (nx + 2)) - 1, y = (int)((t / (nx + 2)) % (ny + 2)) - 1, z = (int)(t / ((int64_t)(nx + 2) * (ny + 2))) - 1;
+    {
+        int x, y;
+        tile_xy(x, y);
+        x -= 1;
+        y -= 1;
+        const int z = zb - 1;
+        if (x > nx || y > ny) return;
         const int p = I(x, y, z);
         // vx: e1(N x-1) - e1(N x), e5(L5 z-1) - e5(L5 z), e6(L6 y-1) - e6(L6 y)
         const T gx = add_(add_(mul_(k0, sub_(W(0, E.n(x - 1, y, z), x - 1, y, z), W(0, E.n(x, y, z), x, y, z))),
@@ -745,17 +771,18 @@ __device__ __forceinline__ void g3_body(const GridDev<T> &G, const AdjDev<T> &A)
 template <typename T>
 __global__ void stress21_adj_g3(GridDev<T> G, AdjDev<T> A)
 {
-    g3_body(G, A);
+    g3_body(G, A, blockIdx.z);
 }
 
-// G3 of every shot: shot blockIdx.y
+// G3 of every shot: blockIdx.z = plane + (nz + 2) * shot
 template <typename T>
 __global__ void stress21_adj_g3_shots(GridDev<T> G, AdjDev<T> A0, const __grid_constant__ AdjShots<T> S)
 {
+    const int nzb = G.g.nz + 2;
     GridDev<T> Gs;
     AdjDev<T> As;
-    shot_views(G, A0, S, blockIdx.y, Gs, As);
-    g3_body(Gs, As);
+    shot_views(G, A0, S, blockIdx.z / nzb, Gs, As);
+    g3_body(Gs, As, blockIdx.z % nzb);
 }
 
 // velocity mirror transposes of every shot: shot blockIdx.y
@@ -770,13 +797,6 @@ __global__ void vel_mirror_adj_shots_kernel(Geo g, const __grid_constant__ AdjSh
 // ---------------------------------------------------------------------------
 // Launchers
 // ---------------------------------------------------------------------------
-static unsigned blocks_for(int64_t n, int sms)
-{
-    int64_t b = (n + 255) / 256;
-    const int64_t cap = (int64_t)sms * 16;
-    return (unsigned)(b < 1 ? 1 : (b > cap ? cap : b));
-}
-
 template <typename T>
 cudaError_t launch_vel_adj(const GridDev<T> &G, const AdjDev<T> &A, int top, int bottom, int top_bc, int mirror_fix,
                            int sms, cudaStream_t st)
@@ -790,7 +810,7 @@ cudaError_t launch_vel_adj(const GridDev<T> &G, const AdjDev<T> &A, int top, int
     vel_mirror_adj_kernel<T><<<(unsigned)((n1 + 255) / 256), 256, 0, st>>>(g, A.l[VY], A.l[VZ], 1, top_rigid, bottom, mirror_fix);
     vel_mirror_adj_kernel<T><<<(unsigned)((n0 + 255) / 256), 256, 0, st>>>(g, A.l[VY], A.l[VZ], 0, top_rigid, bottom, mirror_fix);
     const int zt = top_rigid;
-    vel_adj_kernel<T><<<blocks_for((int64_t)g.nx * g.ny * (g.nz + 1), sms), 256, 0, st>>>(G, A, zt, bottom);
+    vel_adj_kernel<T><<<grid3(g.nx, g.ny, g.nz + 1), 256, 0, st>>>(G, A, zt, bottom);
     return cudaGetLastError();
 }
 
@@ -799,12 +819,11 @@ cudaError_t launch_stress21_adj(const GridDev<T> &G, const AdjDev<T> &A, int top
 {
     const Geo &g = G.g;
     const int flag = (top && top_bc) ? 1 : 0;
-    const int64_t n = (int64_t)(g.nx + 1) * (g.ny + 1) * (g.nz + 1);
-    const unsigned nb = blocks_for(n, sms);
+    const dim3 nb = grid3(g.nx + 1, g.ny + 1, g.nz + 1);
     stress21_adj_g0<T><<<nb, 256, 0, st>>>(G, A, flag);
     stress21_adj_g1<T><<<nb, 256, 0, st>>>(G, A, flag);
     if (flag) stress21_adj_g2<T><<<(g.nx * (g.ny + 1) + 255) / 256, 256, 0, st>>>(G, A);
-    stress21_adj_g3<T><<<blocks_for((int64_t)(g.nx + 2) * (g.ny + 2) * (g.nz + 2), sms), 256, 0, st>>>(G, A);
+    stress21_adj_g3<T><<<grid3(g.nx + 2, g.ny + 2, g.nz + 2), 256, 0, st>>>(G, A);
     return cudaGetLastError();
 }
 
@@ -816,8 +835,7 @@ cudaError_t launch_stress21_adj_shots(const GridDev<T> &G, const AdjDev<T> &A0, 
 {
     const Geo &g = G.g;
     const int flag = (top && top_bc) ? 1 : 0;
-    const int64_t n = (int64_t)(g.nx + 1) * (g.ny + 1) * (g.nz + 1);
-    const unsigned nb = blocks_for(n, sms);
+    const dim3 nb = grid3(g.nx + 1, g.ny + 1, g.nz + 1);
     stress21_adj_g0_shots<T><<<nb, 256, 0, st>>>(G, A0, S, flag);
     stress21_adj_g1_shots<T><<<nb, 256, 0, st>>>(G, A0, S, flag);
     if (flag)   // the free surface adds to the common gradient without atomics: one shot at a time
@@ -831,9 +849,7 @@ cudaError_t launch_stress21_adj_shots(const GridDev<T> &G, const AdjDev<T> &A0, 
             for (int k = 0; k < 15; k++) As.w[k] = S.w[s] + k * S.wbox;
             stress21_adj_g2<T><<<(g.nx * (g.ny + 1) + 255) / 256, 256, 0, st>>>(Gs, As);
         }
-    const unsigned nb3 = blocks_for((int64_t)(g.nx + 2) * (g.ny + 2) * (g.nz + 2), sms);
-    const unsigned per = (nb3 + S.ns - 1) / S.ns;   // about the one-shot launch's CTAs in all
-    stress21_adj_g3_shots<T><<<dim3(per, S.ns), 256, 0, st>>>(G, A0, S);
+    stress21_adj_g3_shots<T><<<grid3(g.nx + 2, g.ny + 2, (g.nz + 2) * S.ns), 256, 0, st>>>(G, A0, S);
     return cudaGetLastError();
 }
 
@@ -852,7 +868,7 @@ cudaError_t launch_vel_adj_shots(const GridDev<T> &G, T *gb, const AdjShots<T> &
                                                                                              mirror_fix);
     vel_mirror_adj_shots_kernel<T><<<dim3((unsigned)((n0 + 255) / 256), S.ns), 256, 0, st>>>(g, S, 0, top_rigid, bottom,
                                                                                              mirror_fix);
-    vel_adj_shots_kernel<T><<<blocks_for((int64_t)g.nx * g.ny * (g.nz + 1), sms), 256, 0, st>>>(G, gb, S, top_rigid, bottom);
+    vel_adj_shots_kernel<T><<<grid3(g.nx, g.ny, g.nz + 1), 256, 0, st>>>(G, gb, S, top_rigid, bottom);
     return cudaGetLastError();
 }
 

@@ -2611,12 +2611,13 @@ static int group_gradient_op(ecsg_sim *const *sims, int S, int nsteps, const flo
     std::vector<const char *> sa(S), sbf(S);
     for (int c = ncp - 1; c >= 0; c--) {
         const int n0 = c * k, n1 = (n0 + k < nsteps) ? n0 + k : nsteps;
-        if (j < k) {   // sub-checkpoints of this segment
+        if (j < k) {   // sub-checkpoints of this segment, up to the start of its last sub-segment
             if ((rc = load_all(&ecsg_sim::ckpt, c))) return rc;
             if ((rc = set_clocks(n0))) return rc;
-            for (int n = n0; n < n1; n++) {
+            const int last = n0 + ((n1 - n0 - 1) / j) * j;
+            for (int n = n0; n <= last; n++) {
                 if ((n - n0) % j == 0 && (rc = save_all(&ecsg_sim::seg2, (n - n0) / j))) return rc;
-                if ((rc = group_step_op<T>(sims, S, nullptr))) return rc;
+                if (n < last && (rc = group_step_op<T>(sims, S, nullptr))) return rc;
             }
         }
         for (int d = (n1 - n0 - 1) / j; d >= 0; d--) {

@@ -53,3 +53,12 @@ def test_product_does_not_import_the_oracle():
                 text = open(os.path.join(dirpath, f)).read()
                 assert "import oracle" not in text and "from oracle" not in text, f
                 assert "ecsg_oracle" not in text, f
+
+
+def test_shots_entry_rejects_bad_arguments_without_a_device():
+    """ecsg_shots_misfit_gradient checks its arguments before touching a
+    device: no instances, or more than 16 shots, is ECSG_ERR_INVALID."""
+    L = ecsg_b200.lib()
+    assert L.ecsg_shots_misfit_gradient(None, 1, 10, None, 5, 0, None) == -1
+    handles = (ctypes.c_void_p * 1)(None)
+    assert L.ecsg_shots_misfit_gradient(handles, 1, 10, None, 5, 0, None) == -1

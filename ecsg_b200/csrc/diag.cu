@@ -7,6 +7,8 @@
 #include "ecsg_device.cuh"
 #include "gen21_device.cuh"
 
+#include <type_traits>
+
 namespace ecsg {
 
 constexpr int RED_THREADS = 256;
@@ -50,10 +52,50 @@ __device__ __forceinline__ void block_sums(double (&v)[N], double *partial, int 
 // fixed by the launch shape, so the result is the same on every run.
 constexpr int ENERGY_TX = 32, ENERGY_TY = 8, ENERGY_ZC = 16;
 
+// FP32 fields: each point's terms in FP32 (the precision of the fields they
+// multiply), accumulated in FP64; the 21-Cij medium only (the production path).
+__device__ __forceinline__ void energy_point_f32_gen21(const GridDev<float> &G, const GridDev<float> &GU, const float *vc0,
+                                                       const float *vc1, const float *vc2, int flag, int x, int y, int z,
+                                                       int p, double (&acc)[12])
+{
+    const Geo &g = G.g;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const int sy = g.px, sz = g.px * g.py;
+    const float mx = (x == 0 || x == nx) ? 0.5f : 1.0f;
+    const float my = (y == 0 || y == ny) ? 0.5f : 1.0f;
+    const float mz = (z == 0 || z == nz) ? 0.5f : 1.0f;
+    const bool xs = x < nx, ys = y < ny, zs = z < nz;
+    const float b000 = G.b[p];
+    acc[0] += (double)(mz * my * mx * (G.f[VX][p] * vc0[p]) / b000);
+    if (xs && ys) {
+        const float rb = 0.25f * (b000 + G.b[p + sy] + G.b[p + 1] + G.b[p + sy + 1]);
+        acc[1] += (double)(mz * (G.f[VY][p] * vc1[p]) / rb);
+    }
+    if (xs && zs) {
+        const float rb = 0.25f * (b000 + G.b[p + sz] + G.b[p + 1] + G.b[p + sz + 1]);
+        acc[2] += (double)(my * (G.f[VZ][p] * vc2[p]) / rb);
+    }
+    if (xs) {
+        const float w = mz * my;
+        const float e1 = e1_at(GU, p), e2 = e2_at(GU, p);
+        const float e3 = (flag && z == 0) ? e3_used(GU, Ext{nx, ny, nz}, true, x, y, z, p, e1, e2) : e3_at(GU, p);
+        acc[3] += (double)(w * e1 * G.f[SXX][p]);
+        acc[4] += (double)(w * e2 * G.f[SYY][p]);
+        acc[5] += (double)(w * e3 * G.f[SZZ][p]);
+    }
+    if (xs && ys && zs) acc[6] += (double)(e4_at(GU, p) * G.f[SYZ][p]);
+    if (zs) acc[7] += (double)(my * mx * e5_at(GU, p) * G.f[SXZ][p]);
+    if (ys) acc[8] += (double)(mz * mx * e6_at(GU, p) * G.f[SXY][p]);
+}
+
 template <typename T, int MED>
 __device__ __forceinline__ void energy_point(const GridDev<T> &G, const GridDev<T> &GU, const T *vc0, const T *vc1,
                                              const T *vc2, int flag, int x, int y, int z, int p, double (&acc)[12])
 {
+    if constexpr (std::is_same<T, float>::value && MED == MED_GEN21) {
+        energy_point_f32_gen21(G, GU, vc0, vc1, vc2, flag, x, y, z, p, acc);
+        return;
+    }
     const Geo &g = G.g;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     const int sy = g.px, sz = g.px * g.py;

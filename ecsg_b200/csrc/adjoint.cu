@@ -52,138 +52,146 @@ static inline dim3 grid3(int nx, int ny, int nz) { return dim3((unsigned)(nx + 3
 // lambda_sigma += (b D)^T lambda_v; g_b += lambda_v * (k . D sigma), the vy
 // and vz buoyancies being 4-node means (1/4 to each node).
 // ---------------------------------------------------------------------------
+// As gathers: the stress adjoints at q collect the transposed differences of
+// the velocity points that read them, u = lambda_v * (the buoyancy mean of
+// that velocity), zero outside each velocity's update range (the scatter
+//   vx: lsxx[p] += k0 u, lsxx[p-1] -= k0 u, lsxy[p] += k1 u, lsxy[p-sy] -= k1 u,
+//       lsxz[p] += k2 u, lsxz[p-sz] -= k2 u;
+//   vy: lsxy[p+1] += k0 u, lsxy[p] -= k0 u, lsyz[p] += k2 u, lsyz[p-sz] -= k2 u,
+//       lsyy[p+sy] += k1 u, lsyy[p] -= k1 u;
+//   vz: lsxz[p+1] += k0 u, lsxz[p] -= k0 u, lszz[p+sz] += k2 u, lszz[p] -= k2 u,
+//       lsyz[p] += k1 u, lsyz[p-sy] -= k1 u
+// read backwards), so no atomics and a fixed order.  The buoyancy-gradient
+// terms of the velocity point q are returned in gx (vx, node q) and gy, gz
+// (vy, vz: a quarter to each of the four nodes of the mean).
+template <typename T>
+__device__ __forceinline__ void vel_adj_point(const GridDev<T> &G, const T *const lv[3], const T *const *f, T *const *ls,
+                                              int zt, int bottom, int x, int y, int z, T &gx, T &gy, T &gz)
+{
+    const Geo &g = G.g;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const int sy = g.px, sz = g.px * g.py;
+    const T k0 = G.k[0], k1 = G.k[1], k2 = G.k[2], qq = T(0.25);
+    const T *b = G.b;
+    auto zin = [&](int zz) { return zz >= zt && zz <= nz - bottom; };
+    auto rx = [&](int xx, int yy, int zz) { return xx >= 1 && xx <= nx - 1 && yy >= 1 && yy <= ny - 1 && zin(zz); };
+    auto ry = [&](int xx, int yy, int zz) { return xx >= 0 && xx <= nx - 1 && yy >= 0 && yy <= ny - 1 && zin(zz); };
+    auto rz = [&](int xx, int yy, int zz) { return xx >= 0 && xx <= nx - 1 && yy >= 1 && yy <= ny - 1 && zz >= 0 && zz <= nz - 1; };
+    auto ux = [&](int xx, int yy, int zz) -> T {
+        if (!rx(xx, yy, zz)) return T(0);
+        const int i = g.idx(xx, yy, zz);
+        return mul_(lv[0][i], b[i]);
+    };
+    auto uy = [&](int xx, int yy, int zz) -> T {
+        if (!ry(xx, yy, zz)) return T(0);
+        const int i = g.idx(xx, yy, zz);
+        return mul_(lv[1][i], mul_(qq, add_(add_(add_(b[i], b[i + 1]), b[i + sy]), b[i + sy + 1])));
+    };
+    auto uz = [&](int xx, int yy, int zz) -> T {
+        if (!rz(xx, yy, zz)) return T(0);
+        const int i = g.idx(xx, yy, zz);
+        return mul_(lv[2][i], mul_(qq, add_(add_(add_(b[i], b[i + sz]), b[i + 1]), b[i + sz + 1])));
+    };
+    const T ux0 = ux(x, y, z), uy0 = uy(x, y, z), uz0 = uz(x, y, z);
+    const T dsxx = mul_(k0, sub_(ux0, ux(x + 1, y, z)));
+    const T dsxy = add_(mul_(k1, sub_(ux0, ux(x, y + 1, z))), mul_(k0, sub_(uy(x - 1, y, z), uy0)));
+    const T dsxz = add_(mul_(k2, sub_(ux0, ux(x, y, z + 1))), mul_(k0, sub_(uz(x - 1, y, z), uz0)));
+    const T dsyy = mul_(k1, sub_(uy(x, y - 1, z), uy0));
+    const T dsyz = add_(mul_(k2, sub_(uy0, uy(x, y, z + 1))), mul_(k1, sub_(uz0, uz(x, y + 1, z))));
+    const T dszz = mul_(k2, sub_(uz(x, y, z - 1), uz0));
+    const int p = g.idx(x, y, z);
+    // buoyancy-gradient terms of the velocity point p (its own update ranges)
+    gx = T(0);
+    gy = T(0);
+    gz = T(0);
+    if (rx(x, y, z)) {
+        const T a = lv[0][p];
+        const T d = add_(add_(mul_(k0, sub_(f[SXX][p], f[SXX][p - 1])), mul_(k1, sub_(f[SXY][p], f[SXY][p - sy]))),
+                         mul_(k2, sub_(f[SXZ][p], f[SXZ][p - sz])));
+        gx = mul_(a, d);
+    }
+    if (ry(x, y, z)) {
+        const T a = lv[1][p];
+        const T d = add_(add_(mul_(k0, sub_(f[SXY][p + 1], f[SXY][p])), mul_(k2, sub_(f[SYZ][p], f[SYZ][p - sz]))),
+                         mul_(k1, sub_(f[SYY][p + sy], f[SYY][p])));
+        gy = mul_(qq, mul_(a, d));
+    }
+    if (rz(x, y, z)) {
+        const T a = lv[2][p];
+        const T d = add_(add_(mul_(k0, sub_(f[SXZ][p + 1], f[SXZ][p])), mul_(k2, sub_(f[SZZ][p + sz], f[SZZ][p]))),
+                         mul_(k1, sub_(f[SYZ][p], f[SYZ][p - sy])));
+        gz = mul_(qq, mul_(a, d));
+    }
+    // every load above before the stores
+    if (dsxx != T(0)) ls[SXX][p] = add_(ls[SXX][p], dsxx);
+    if (dsxy != T(0)) ls[SXY][p] = add_(ls[SXY][p], dsxy);
+    if (dsxz != T(0)) ls[SXZ][p] = add_(ls[SXZ][p], dsxz);
+    if (dsyy != T(0)) ls[SYY][p] = add_(ls[SYY][p], dsyy);
+    if (dsyz != T(0)) ls[SYZ][p] = add_(ls[SYZ][p], dsyz);
+    if (dszz != T(0)) ls[SZZ][p] = add_(ls[SZZ][p], dszz);
+}
+
+// the buoyancy-gradient terms of velocity point p into the node gradient
+template <typename T>
+__device__ __forceinline__ void vel_adj_gb(const Geo &g, T *gb, int p, T gx, T gy, T gz)
+{
+    const int sy = g.px, sz = g.px * g.py;
+    if (gx != T(0)) atom(gb + p, gx);
+    if (gy != T(0)) { atom(gb + p, gy); atom(gb + p + 1, gy); atom(gb + p + sy, gy); atom(gb + p + sy + 1, gy); }
+    if (gz != T(0)) { atom(gb + p, gz); atom(gb + p + sz, gz); atom(gb + p + 1, gz); atom(gb + p + sz + 1, gz); }
+}
+
+// x, y, z in [-1, n]: every stress entry a velocity update reads
 template <typename T>
 __global__ void vel_adj_kernel(GridDev<T> G, AdjDev<T> A, int zt, int bottom)
 {
     const Geo &g = G.g;
-    const int nx = g.nx, ny = g.ny, nz = g.nz;
-    const int sx = 1, sy = g.px, sz = g.px * g.py;
-    const T k0 = G.k[0], k1 = G.k[1], k2 = G.k[2], q = T(0.25);
-    const T *b = G.b;
-    const T *sxx = G.f[SXX], *syy = G.f[SYY], *szz = G.f[SZZ], *syz = G.f[SYZ], *sxz = G.f[SXZ], *sxy = G.f[SXY];
-    T *lsxx = A.l[SXX], *lsyy = A.l[SYY], *lszz = A.l[SZZ], *lsyz = A.l[SYZ], *lsxz = A.l[SXZ], *lsxy = A.l[SXY];
-    {
-        int ix, iy;
-        tile_xy(ix, iy);
-        const int iz = blockIdx.z;
-        if (ix >= nx || iy >= ny) return;
-        const int p = g.idx(ix, iy, iz);
-        const bool zin = iz >= zt && iz <= nz - bottom;
-        if (ix >= 1 && iy >= 1 && zin) {   // vx
-            const T a = A.l[VX][p];
-            if (a != T(0)) {
-                const T d = add_(add_(mul_(k0, sub_(sxx[p], sxx[p - sx])), mul_(k1, sub_(sxy[p], sxy[p - sy]))),
-                                 mul_(k2, sub_(sxz[p], sxz[p - sz])));
-                atom(A.gb + p, mul_(a, d));
-                const T u = mul_(a, b[p]);
-                atom(lsxx + p, mul_(k0, u)); atom(lsxx + p - sx, -mul_(k0, u));
-                atom(lsxy + p, mul_(k1, u)); atom(lsxy + p - sy, -mul_(k1, u));
-                atom(lsxz + p, mul_(k2, u)); atom(lsxz + p - sz, -mul_(k2, u));
-            }
-        }
-        if (zin) {   // vy
-            const T a = A.l[VY][p];
-            if (a != T(0)) {
-                const T bb = mul_(q, add_(add_(add_(b[p], b[p + sx]), b[p + sy]), b[p + sy + sx]));
-                const T d = add_(add_(mul_(k0, sub_(sxy[p + sx], sxy[p])), mul_(k2, sub_(syz[p], syz[p - sz]))),
-                                 mul_(k1, sub_(syy[p + sy], syy[p])));
-                const T gq = mul_(q, mul_(a, d));
-                atom(A.gb + p, gq); atom(A.gb + p + sx, gq); atom(A.gb + p + sy, gq); atom(A.gb + p + sy + sx, gq);
-                const T u = mul_(a, bb);
-                atom(lsxy + p + sx, mul_(k0, u)); atom(lsxy + p, -mul_(k0, u));
-                atom(lsyz + p, mul_(k2, u)); atom(lsyz + p - sz, -mul_(k2, u));
-                atom(lsyy + p + sy, mul_(k1, u)); atom(lsyy + p, -mul_(k1, u));
-            }
-        }
-        if (iy >= 1 && iz <= nz - 1) {   // vz
-            const T a = A.l[VZ][p];
-            if (a != T(0)) {
-                const T bb = mul_(q, add_(add_(add_(b[p], b[p + sz]), b[p + sx]), b[p + sz + sx]));
-                const T d = add_(add_(mul_(k0, sub_(sxz[p + sx], sxz[p])), mul_(k2, sub_(szz[p + sz], szz[p]))),
-                                 mul_(k1, sub_(syz[p], syz[p - sy])));
-                const T gq = mul_(q, mul_(a, d));
-                atom(A.gb + p, gq); atom(A.gb + p + sz, gq); atom(A.gb + p + sx, gq); atom(A.gb + p + sz + sx, gq);
-                const T u = mul_(a, bb);
-                atom(lsxz + p + sx, mul_(k0, u)); atom(lsxz + p, -mul_(k0, u));
-                atom(lszz + p + sz, mul_(k2, u)); atom(lszz + p, -mul_(k2, u));
-                atom(lsyz + p, mul_(k1, u)); atom(lsyz + p - sy, -mul_(k1, u));
-            }
-        }
-    }
+    int x, y;
+    tile_xy(x, y);
+    x -= 1;
+    y -= 1;
+    const int z = (int)blockIdx.z - 1;
+    if (x > g.nx || y > g.ny) return;
+    const T *lv[3] = {A.l[VX], A.l[VY], A.l[VZ]};
+    T gx, gy, gz;
+    vel_adj_point(G, lv, G.f, A.l, zt, bottom, x, y, z, gx, gy, gz);
+    vel_adj_gb(g, A.gb, g.idx(x, y, z), gx, gy, gz);
 }
 
-// The velocity adjoint of every shot at each point: the buoyancy read once,
-// the buoyancy-gradient terms of all shots summed in registers and added with
-// one set of atomics (the shots' stress adjoints are scattered per shot).
+// The velocity adjoint of every shot at each point: the buoyancy read once
+// (cached) for all shots, their buoyancy-gradient terms summed in registers
+// and added with one set of atomics.
 template <typename T>
-__global__ void vel_adj_shots_kernel(GridDev<T> G, T *gb, const __grid_constant__ AdjShots<T> S, int zt, int bottom)
+__global__ void __launch_bounds__(256, 3)
+    vel_adj_shots_kernel(GridDev<T> G, T *gb, const __grid_constant__ AdjShots<T> S, int zt, int bottom)
 {
     const Geo &g = G.g;
-    const int nx = g.nx, ny = g.ny, nz = g.nz;
-    const int sx = 1, sy = g.px, sz = g.px * g.py;
-    const T k0 = G.k[0], k1 = G.k[1], k2 = G.k[2], q = T(0.25);
-    const T *b = G.b;
+    int x, y;
+    tile_xy(x, y);
+    x -= 1;
+    y -= 1;
+    const int z = (int)blockIdx.z - 1;
+    if (x > g.nx || y > g.ny) return;
     const int64_t box = S.box;
-    {
-        int ix, iy;
-        tile_xy(ix, iy);
-        const int iz = blockIdx.z;
-        if (ix >= nx || iy >= ny) return;
-        const int p = g.idx(ix, iy, iz);
-        const bool zin = iz >= zt && iz <= nz - bottom;
-        const bool dx = ix >= 1 && iy >= 1 && zin, dy = zin, dz = iy >= 1 && iz <= nz - 1;
-        const T bx = dx ? b[p] : T(0);
-        const T bby = dy ? mul_(q, add_(add_(add_(b[p], b[p + sx]), b[p + sy]), b[p + sy + sx])) : T(0);
-        const T bbz = dz ? mul_(q, add_(add_(add_(b[p], b[p + sz]), b[p + sx]), b[p + sz + sx])) : T(0);
-        T gx = T(0), gy = T(0), gz = T(0);
-        for (int s = 0; s < S.ns; s++) {
-            const T *f = S.f[s];
-            T *l = S.l[s];
-            const T *sxx = f + SXX * box, *syy = f + SYY * box, *szz = f + SZZ * box;
-            const T *syz = f + SYZ * box, *sxz = f + SXZ * box, *sxy = f + SXY * box;
-            T *lsxx = l + SXX * box, *lsyy = l + SYY * box, *lszz = l + SZZ * box;
-            T *lsyz = l + SYZ * box, *lsxz = l + SXZ * box, *lsxy = l + SXY * box;
-            if (dx) {   // vx
-                const T a = l[VX * box + p];
-                if (a != T(0)) {
-                    const T d = add_(add_(mul_(k0, sub_(sxx[p], sxx[p - sx])), mul_(k1, sub_(sxy[p], sxy[p - sy]))),
-                                     mul_(k2, sub_(sxz[p], sxz[p - sz])));
-                    gx = add_(gx, mul_(a, d));
-                    const T u = mul_(a, bx);
-                    atom(lsxx + p, mul_(k0, u)); atom(lsxx + p - sx, -mul_(k0, u));
-                    atom(lsxy + p, mul_(k1, u)); atom(lsxy + p - sy, -mul_(k1, u));
-                    atom(lsxz + p, mul_(k2, u)); atom(lsxz + p - sz, -mul_(k2, u));
-                }
-            }
-            if (dy) {   // vy
-                const T a = l[VY * box + p];
-                if (a != T(0)) {
-                    const T d = add_(add_(mul_(k0, sub_(sxy[p + sx], sxy[p])), mul_(k2, sub_(syz[p], syz[p - sz]))),
-                                     mul_(k1, sub_(syy[p + sy], syy[p])));
-                    gy = add_(gy, mul_(q, mul_(a, d)));
-                    const T u = mul_(a, bby);
-                    atom(lsxy + p + sx, mul_(k0, u)); atom(lsxy + p, -mul_(k0, u));
-                    atom(lsyz + p, mul_(k2, u)); atom(lsyz + p - sz, -mul_(k2, u));
-                    atom(lsyy + p + sy, mul_(k1, u)); atom(lsyy + p, -mul_(k1, u));
-                }
-            }
-            if (dz) {   // vz
-                const T a = l[VZ * box + p];
-                if (a != T(0)) {
-                    const T d = add_(add_(mul_(k0, sub_(sxz[p + sx], sxz[p])), mul_(k2, sub_(szz[p + sz], szz[p]))),
-                                     mul_(k1, sub_(syz[p], syz[p - sy])));
-                    gz = add_(gz, mul_(q, mul_(a, d)));
-                    const T u = mul_(a, bbz);
-                    atom(lsxz + p + sx, mul_(k0, u)); atom(lsxz + p, -mul_(k0, u));
-                    atom(lszz + p + sz, mul_(k2, u)); atom(lszz + p, -mul_(k2, u));
-                    atom(lsyz + p, mul_(k1, u)); atom(lsyz + p - sy, -mul_(k1, u));
-                }
-            }
+    T sx = T(0), sy = T(0), sz = T(0);
+    for (int s = 0; s < S.ns; s++) {
+        T *l = S.l[s];
+        const T *fs = S.f[s];
+        const T *lv[3] = {l + VX * box, l + VY * box, l + VZ * box};
+        const T *f[9];
+        T *ls[9];
+#pragma unroll
+        for (int k = 0; k < 9; k++) {
+            f[k] = fs + k * box;
+            ls[k] = l + k * box;
         }
-        if (gx != T(0)) atom(gb + p, gx);
-        if (gy != T(0)) { atom(gb + p, gy); atom(gb + p + sx, gy); atom(gb + p + sy, gy); atom(gb + p + sy + sx, gy); }
-        if (gz != T(0)) { atom(gb + p, gz); atom(gb + p + sz, gz); atom(gb + p + sx, gz); atom(gb + p + sz + sx, gz); }
+        T gx, gy, gz;
+        vel_adj_point(G, lv, f, ls, zt, bottom, x, y, z, gx, gy, gz);
+        sx = add_(sx, gx);
+        sy = add_(sy, gy);
+        sz = add_(sz, gz);
     }
+    vel_adj_gb(g, gb, g.idx(x, y, z), sx, sy, sz);
 }
 
 // ---------------------------------------------------------------------------
@@ -810,7 +818,7 @@ cudaError_t launch_vel_adj(const GridDev<T> &G, const AdjDev<T> &A, int top, int
     vel_mirror_adj_kernel<T><<<(unsigned)((n1 + 255) / 256), 256, 0, st>>>(g, A.l[VY], A.l[VZ], 1, top_rigid, bottom, mirror_fix);
     vel_mirror_adj_kernel<T><<<(unsigned)((n0 + 255) / 256), 256, 0, st>>>(g, A.l[VY], A.l[VZ], 0, top_rigid, bottom, mirror_fix);
     const int zt = top_rigid;
-    vel_adj_kernel<T><<<grid3(g.nx, g.ny, g.nz + 1), 256, 0, st>>>(G, A, zt, bottom);
+    vel_adj_kernel<T><<<grid3(g.nx + 2, g.ny + 2, g.nz + 2), 256, 0, st>>>(G, A, zt, bottom);
     return cudaGetLastError();
 }
 
@@ -868,7 +876,7 @@ cudaError_t launch_vel_adj_shots(const GridDev<T> &G, T *gb, const AdjShots<T> &
                                                                                              mirror_fix);
     vel_mirror_adj_shots_kernel<T><<<dim3((unsigned)((n0 + 255) / 256), S.ns), 256, 0, st>>>(g, S, 0, top_rigid, bottom,
                                                                                              mirror_fix);
-    vel_adj_shots_kernel<T><<<grid3(g.nx, g.ny, g.nz + 1), 256, 0, st>>>(G, gb, S, top_rigid, bottom);
+    vel_adj_shots_kernel<T><<<grid3(g.nx + 2, g.ny + 2, g.nz + 2), 256, 0, st>>>(G, gb, S, top_rigid, bottom);
     return cudaGetLastError();
 }
 

@@ -24,6 +24,8 @@ cudaError_t launch_vel(const GridDev<T> &, int, int, int, T *const[3], int, cuda
 template <typename T>
 cudaError_t launch_vel_mirror(const GridDev<T> &, int, int, int, int, cudaStream_t);
 template <typename T>
+cudaError_t launch_vel_mirror_shots(const Geo &, T *const *, T *const *, int, int, int, int, int, cudaStream_t);
+template <typename T>
 cudaError_t launch_stress(const GridDev<T> &, int, int, int, int, cudaStream_t);
 // stencil_v4.cu (FP32 production sweeps)
 cudaError_t launch_vel_v4(const GridDev<float> &, int, int, int, float *const[3], int, cudaStream_t, int);
@@ -2370,7 +2372,13 @@ static int group_step_op(ecsg_sim *const *sims, int S, T *const *sample_rows)
             for (int b = 0; b < S; b++) maps[b] = sims[b]->velmaps[g].data();
             CK(launch_vel_tma_shots(maps.data(), S, dev<float>(m, g), top_of(m, g, -1), bottom_of(m, g, -1), m->top_bc,
                                     m->ints, m->sms, m->st, 0));
-            if ((rc = each_shot(sims, S, [&](ecsg_sim *x, int) { return vel_mirror_op<T>(x, g); }))) return rc;
+            std::vector<T *> vy(S), vz(S);
+            for (int b = 0; b < S; b++) {
+                vy[b] = (T *)sims[b]->f[g][VY];
+                vz[b] = (T *)sims[b]->f[g][VZ];
+            }
+            CK(launch_vel_mirror_shots<T>(m->geo[g], vy.data(), vz.data(), S, top_of(m, g, -1), bottom_of(m, g, -1),
+                                          m->top_bc, m->mirror_fix, m->st));
         }
     } else if ((rc = each_shot(sims, S, [&](ecsg_sim *x, int) {
                     return each_grid(x, [&](int g) { return vel_op<T>(x, g, false); });

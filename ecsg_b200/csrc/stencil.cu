@@ -119,12 +119,10 @@ __global__ void __launch_bounds__(TX *TY) vel_kernel(GridDev<T> G, int zt, int b
 //            energy is conserved exactly)
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void vel_mirror_kernel(GridDev<T> G, int phase, int top_rigid, int bottom, int mirror_fix)
+__device__ __forceinline__ void vel_mirror_body(const Geo &g, T *vy, T *vz, int phase, int top_rigid, int bottom,
+                                                int mirror_fix)
 {
-    const Geo &g = G.g;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
-    T *vy = G.f[VY];
-    T *vz = G.f[VZ];
     int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (phase == 0) {
         const int64_t nA = top_rigid ? (int64_t)(ny + 1) * nx : 0;
@@ -148,6 +146,24 @@ __global__ void vel_mirror_kernel(GridDev<T> G, int phase, int top_rigid, int bo
         t -= nG;
         if (t < nG) { int ix = t % nx, iz = t / nx; vy[g.idx(ix, ny, iz)] = -vy[g.idx(ix, ny - 1, iz)]; return; }
     }
+}
+
+template <typename T>
+__global__ void vel_mirror_kernel(GridDev<T> G, int phase, int top_rigid, int bottom, int mirror_fix)
+{
+    vel_mirror_body(G.g, G.f[VY], G.f[VZ], phase, top_rigid, bottom, mirror_fix);
+}
+
+// the mirrors of several shots of one grid (shot blockIdx.y)
+template <typename T>
+struct ShotVel {
+    T *vy[kMaxShots], *vz[kMaxShots];
+};
+template <typename T>
+__global__ void vel_mirror_shots_kernel(Geo g, const __grid_constant__ ShotVel<T> P, int phase, int top_rigid, int bottom,
+                                        int mirror_fix)
+{
+    vel_mirror_body(g, P.vy[blockIdx.y], P.vz[blockIdx.y], phase, top_rigid, bottom, mirror_fix);
 }
 
 // ---------------------------------------------------------------------------
@@ -311,6 +327,26 @@ cudaError_t launch_vel_mirror(const GridDev<T> &G, int top, int bottom, int top_
     return cudaGetLastError();
 }
 
+// launch_vel_mirror for ns shots of one grid (vy[s], vz[s] the shot's fields)
+template <typename T>
+cudaError_t launch_vel_mirror_shots(const Geo &g, T *const *vy, T *const *vz, int ns, int top, int bottom, int top_bc,
+                                    int mirror_fix, cudaStream_t st)
+{
+    if (ns < 1 || ns > kMaxShots) return cudaErrorInvalidValue;
+    ShotVel<T> P;
+    for (int s = 0; s < ns; s++) {
+        P.vy[s] = vy[s];
+        P.vz[s] = vz[s];
+    }
+    const int top_rigid = (top && top_bc != 1) ? 1 : 0;
+    const int64_t n0 = (int64_t)(top_rigid + bottom) * (g.ny + 1) * g.nx + 2LL * g.nz * (g.ny + 1)
+                     + 2LL * (g.nz + 1) * (g.ny + 1);
+    const int64_t n1 = 2LL * (g.nz + (mirror_fix ? 1 : 0)) * g.nx;
+    vel_mirror_shots_kernel<T><<<dim3((unsigned)((n0 + 255) / 256), ns), 256, 0, st>>>(g, P, 0, top_rigid, bottom, mirror_fix);
+    vel_mirror_shots_kernel<T><<<dim3((unsigned)((n1 + 255) / 256), ns), 256, 0, st>>>(g, P, 1, top_rigid, bottom, mirror_fix);
+    return cudaGetLastError();
+}
+
 template <typename T>
 cudaError_t launch_stress(const GridDev<T> &G, int medium, int top, int top_bc, int sms, cudaStream_t st)
 {
@@ -331,6 +367,10 @@ template cudaError_t launch_vel<float>(const GridDev<float> &, int, int, int, fl
 template cudaError_t launch_vel<double>(const GridDev<double> &, int, int, int, double *const[3], int, cudaStream_t);
 template cudaError_t launch_vel_mirror<float>(const GridDev<float> &, int, int, int, int, cudaStream_t);
 template cudaError_t launch_vel_mirror<double>(const GridDev<double> &, int, int, int, int, cudaStream_t);
+template cudaError_t launch_vel_mirror_shots<float>(const Geo &, float *const *, float *const *, int, int, int, int, int,
+                                                    cudaStream_t);
+template cudaError_t launch_vel_mirror_shots<double>(const Geo &, double *const *, double *const *, int, int, int, int,
+                                                     int, cudaStream_t);
 template cudaError_t launch_stress<float>(const GridDev<float> &, int, int, int, int, cudaStream_t);
 template cudaError_t launch_stress<double>(const GridDev<double> &, int, int, int, int, cudaStream_t);
 

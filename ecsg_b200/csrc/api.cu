@@ -2355,6 +2355,8 @@ template <typename T>
 static bool group_tma(ecsg_sim *const *sims, int S, bool stress)
 {
     if (!std::is_same<T, float>::value || S < 2) return false;
+    const char *env = getenv("ECSG_SHOTS_TMA");   // "0": the shots' sweeps launched one shot at a time
+    if (env && env[0] == '0') return false;
     for (int b = 0; b < S; b++)
         if (!(stress ? use_s21_tma(sims[b]) : use_vel_tma(sims[b])) || (stress && sims[b]->energy)) return false;
     return true;

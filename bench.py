@@ -290,12 +290,13 @@ def accuracy(args, local):
     for prec in ("f64", "f32"):
         with ecsg_b200.Simulation(case, precision=prec, energy=True, device=local) as s:
             out = s.run(n, energy_every=10)
-            runs[prec] = (out["rec"].astype(np.float64), out["energy"][9::10],
+            e = out["energy"]
+            runs[prec] = (out["rec"].astype(np.float64), e[~np.isnan(e)],
                           [s.field(g, k)[1:-1, 1:-1, 1:-1] for g in range(3) for k in range(9)])
     (r64, e64, f64), (r32, e32, f32) = runs["f64"], runs["f32"]
     rel = lambda a, b: float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
     src_end = len(case.src["trace"])
-    post = [i for i in range(len(e64)) if 10 * (i + 1) > src_end + 10]
+    post = [i for i in range(len(e64)) if 10 * i > src_end + 10]   # energy on steps 0, 10, 20, ...
     drift = lambda e: float((e.max() - e.min()) / e.mean()) if len(e) > 1 else None
     return {"workload": "three-grid ratio-3 tilted VTI 181x181x25@5m / 61x61x19@15m / 21x21x13@45m, %d steps" % n,
             "reference": "FP64 device path (bitwise equal to the FP64 CPU oracle per operator)",

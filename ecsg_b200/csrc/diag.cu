@@ -52,11 +52,13 @@ __device__ __forceinline__ void block_sums(double (&v)[N], double *partial, int 
 // fixed by the launch shape, so the result is the same on every run.
 constexpr int ENERGY_TX = 32, ENERGY_TY = 8, ENERGY_ZC = 16;
 
-// FP32 fields: each point's terms in FP32 (the precision of the fields they
-// multiply), accumulated in FP64; the 21-Cij medium only (the production path).
+// FP32 fields, 21-Cij medium (the production path): each point's terms in
+// FP32 (the precision of the fields they multiply), the point's kinetic and
+// potential parts added to two FP64 sums (the finalize of this medium only
+// adds the terms up, so the per-term split is not kept).
 __device__ __forceinline__ void energy_point_f32_gen21(const GridDev<float> &G, const GridDev<float> &GU, const float *vc0,
                                                        const float *vc1, const float *vc2, int flag, int x, int y, int z,
-                                                       int p, double (&acc)[12])
+                                                       int p, double &kin, double &pot)
 {
     const Geo &g = G.g;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
@@ -66,36 +68,61 @@ __device__ __forceinline__ void energy_point_f32_gen21(const GridDev<float> &G, 
     const float mz = (z == 0 || z == nz) ? 0.5f : 1.0f;
     const bool xs = x < nx, ys = y < ny, zs = z < nz;
     const float b000 = G.b[p];
-    acc[0] += (double)(mz * my * mx * (G.f[VX][p] * vc0[p]) / b000);
+    float k = mz * my * mx * (G.f[VX][p] * vc0[p]) / b000;
     if (xs && ys) {
         const float rb = 0.25f * (b000 + G.b[p + sy] + G.b[p + 1] + G.b[p + sy + 1]);
-        acc[1] += (double)(mz * (G.f[VY][p] * vc1[p]) / rb);
+        k += mz * (G.f[VY][p] * vc1[p]) / rb;
     }
     if (xs && zs) {
         const float rb = 0.25f * (b000 + G.b[p + sz] + G.b[p + 1] + G.b[p + sz + 1]);
-        acc[2] += (double)(my * (G.f[VZ][p] * vc2[p]) / rb);
+        k += my * (G.f[VZ][p] * vc2[p]) / rb;
     }
+    float e = 0.0f;
     if (xs) {
         const float w = mz * my;
         const float e1 = e1_at(GU, p), e2 = e2_at(GU, p);
         const float e3 = (flag && z == 0) ? e3_used(GU, Ext{nx, ny, nz}, true, x, y, z, p, e1, e2) : e3_at(GU, p);
-        acc[3] += (double)(w * e1 * G.f[SXX][p]);
-        acc[4] += (double)(w * e2 * G.f[SYY][p]);
-        acc[5] += (double)(w * e3 * G.f[SZZ][p]);
+        e += w * (e1 * G.f[SXX][p] + e2 * G.f[SYY][p] + e3 * G.f[SZZ][p]);
     }
-    if (xs && ys && zs) acc[6] += (double)(e4_at(GU, p) * G.f[SYZ][p]);
-    if (zs) acc[7] += (double)(my * mx * e5_at(GU, p) * G.f[SXZ][p]);
-    if (ys) acc[8] += (double)(mz * mx * e6_at(GU, p) * G.f[SXY][p]);
+    if (xs && ys && zs) e += e4_at(GU, p) * G.f[SYZ][p];
+    if (zs) e += my * mx * e5_at(GU, p) * G.f[SXZ][p];
+    if (ys) e += mz * mx * e6_at(GU, p) * G.f[SXY][p];
+    kin += (double)k;
+    pot += (double)e;
+}
+
+// The FP32 21-Cij energy: 4 CTAs per SM, two planes of loads in flight per
+// thread (the kernel is bound by memory latency, not bytes).
+__global__ void __launch_bounds__(RED_THREADS, 4)
+    energy_f32_gen21_kernel(GridDev<float> G, const float *vc0, const float *vc1, const float *vc2, GridDev<float> GU,
+                            int flag, double *partial)
+{
+    const Geo &g = G.g;
+    const int nx = g.nx, ny = g.ny, nz = g.nz;
+    const int sz = g.px * g.py;
+    const int ntx = (nx + ENERGY_TX) / ENERGY_TX, nty = (ny + ENERGY_TY) / ENERGY_TY;
+    const int ntz = (nz + ENERGY_ZC) / ENERGY_ZC;
+    const int ntiles = ntx * nty * ntz;
+    const int lx = threadIdx.x % ENERGY_TX, ly = threadIdx.x / ENERGY_TX;
+    double kin = 0.0, pot = 0.0;
+    for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+        const int tx = t % ntx, ty = (t / ntx) % nty, tz = t / (ntx * nty);
+        const int x = tx * ENERGY_TX + lx, y = ty * ENERGY_TY + ly;
+        if (x > nx || y > ny) continue;
+        const int z0 = tz * ENERGY_ZC, z1 = min(nz, z0 + ENERGY_ZC - 1);
+        int p = g.idx(x, y, z0);
+#pragma unroll 2
+        for (int z = z0; z <= z1; z++, p += sz) energy_point_f32_gen21(G, GU, vc0, vc1, vc2, flag, x, y, z, p, kin, pot);
+    }
+    double acc[12] = {kin, 0.0, 0.0, pot, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    block_sums<12>(acc, partial, gridDim.x);
 }
 
 template <typename T, int MED>
 __device__ __forceinline__ void energy_point(const GridDev<T> &G, const GridDev<T> &GU, const T *vc0, const T *vc1,
                                              const T *vc2, int flag, int x, int y, int z, int p, double (&acc)[12])
 {
-    if constexpr (std::is_same<T, float>::value && MED == MED_GEN21) {
-        energy_point_f32_gen21(G, GU, vc0, vc1, vc2, flag, x, y, z, p, acc);
-        return;
-    }
+
     const Geo &g = G.g;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     const int sy = g.px, sz = g.px * g.py;
@@ -435,7 +462,18 @@ cudaError_t launch_energy(const GridDev<T> &G, int medium, T *const vc[3], T *co
                            ((g.nz + ENERGY_ZC) / ENERGY_ZC);
     int eb = (sms > 0 && 3 * sms < nblocks) ? 3 * sms : nblocks;
     if (ntiles < eb) eb = (int)ntiles;
-    if (medium == MED_GEN21)
+    bool done = false;
+    if constexpr (std::is_same<T, float>::value) {
+        if (medium == MED_GEN21) {   // the FP32 production path: its own kernel, 4 CTAs per SM
+            int eb4 = (sms > 0 && 4 * sms < nblocks) ? 4 * sms : nblocks;
+            if (ntiles < eb4) eb4 = (int)ntiles;
+            eb = eb4;
+            energy_f32_gen21_kernel<<<eb, RED_THREADS, 0, st>>>(G, vc[0], vc[1], vc[2], GU, flag, partial);
+            done = true;
+        }
+    }
+    if (done) {
+    } else if (medium == MED_GEN21)
         energy_kernel<T, MED_GEN21><<<eb, RED_THREADS, 0, st>>>(G, vc[0], vc[1], vc[2], GU, flag, partial);
     else if (medium == MED_ISO5)
         energy_kernel<T, MED_ISO5><<<eb, RED_THREADS, 0, st>>>(G, vc[0], vc[1], vc[2], GU, flag, partial);

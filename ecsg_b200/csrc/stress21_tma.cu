@@ -87,6 +87,7 @@ struct S21Maps {
     CUtensorMap epx[NSH];  // displacement sums: x = -4..-1 face boxes (tiles at x0 = 0)
     CUtensorMap epy[NSH];  // displacement sums: y = -1 face rows (tiles at y0 = 0)
     float *sg_out[NSH][6]; // the shot's stresses sxx syy szz syz sxz sxy
+    float *vin[NSH][3];    // the shot's velocities (read from memory by the free-surface condensation)
     float *u[NSH][3];      // the shot's displacement sums (null: none)
     int ns;
 };
@@ -199,6 +200,16 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 2)
         const int ox = x0 + tx, oy = y0 + ty;
         const int vb = (ty + 1) * BW + tx + 4, ib = ty * TX + tx, hx = tx + 1, hy = ty + 1;
         const float k0 = G.k[0], k1 = G.k[1], k2 = G.k[2];
+        // the free-surface e3 (gen21_device.cuh e3_used) reads the averaged
+        // strains around the point from memory: this shot's velocities
+        auto e3_surface = [&](int xs, int ys, int ps, int pidx, float a1, float a2) -> float {
+            if (NSH == 1) return e3_used(G, E, true, xs, ys, ps, pidx, a1, a2);
+            GridDev<float> Gs = G;
+            Gs.f[VX] = maps.vin[shot][0];
+            Gs.f[VY] = maps.vin[shot][1];
+            Gs.f[VZ] = maps.vin[shot][2];
+            return e3_used(Gs, E, true, xs, ys, ps, pidx, a1, a2);
+        };
         float *sxx = maps.sg_out[shot][0], *syy = maps.sg_out[shot][1], *szz = maps.sg_out[shot][2],
               *syz = maps.sg_out[shot][3], *sxz = maps.sg_out[shot][4], *sxy = maps.sg_out[shot][5];
         // carries from plane pm = p-1 for the syz / sxz outputs
@@ -317,7 +328,7 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 2)
                         e1 = mul_(k0, sub_(Vp[vb + 1], Vp[vb]));
                         e2 = mul_(k1, sub_(Vp[HS + vb], Vp[HS + vb - BW]));
                         if (!FAST && surf)
-                            e3 = e3_used(G, E, true, ox, oy, p, pbase + p * sz, e1, e2);
+                            e3 = e3_surface(ox, oy, p, pbase + p * sz, e1, e2);
                         else
                             e3 = mul_(k2, sub_(Vp[2 * HS + vb], Vm[2 * HS + vb]));
                         p4 = fma_(cho(6), e3, fma_(cho(3), e2, mul_(cho(0), e1)));
@@ -355,7 +366,7 @@ __global__ void __launch_bounds__(s21t::NTHREADS, 2)
                         if (FAST || E.n(x, y, p)) {
                             const float f1 = mul_(k0, sub_(Vp[b + 1], Vp[b]));
                             const float f2 = mul_(k1, sub_(Vp[HS + b], Vp[HS + b - BW]));
-                            const float f3 = (!FAST && surf) ? e3_used(G, E, true, x, y, p, g.idx(x, y, p), f1, f2)
+                            const float f3 = (!FAST && surf) ? e3_surface(x, y, p, g.idx(x, y, p), f1, f2)
                                                              : mul_(k2, sub_(Vp[2 * HS + b], Vm[2 * HS + b]));
                             p4 = fma_(chh(6), f3, fma_(chh(3), f2, mul_(chh(0), f1)));
                             p5 = fma_(chh(7), f3, fma_(chh(4), f2, mul_(chh(1), f1)));
@@ -518,6 +529,7 @@ bool s21_encode_maps(void *out, const GridDev<float> &G, float *const disp[3])
     memset(&M, 0, sizeof M);
     M.ns = 1;
     for (int k = 0; k < 6; k++) M.sg_out[0][k] = G.f[SXX + k];
+    for (int k = 0; k < 3; k++) M.vin[0][k] = G.f[VX + k];
     for (int k = 0; k < 3; k++) M.u[0][k] = disp ? disp[k] : nullptr;
     const Geo &g = G.g;
     if ((g.px * 4) % 16 != 0 || (XOFF - 4) % 4 != 0) return false;
@@ -598,6 +610,7 @@ cudaError_t launch_stress21_tma_shots(const void *const *maps, int ns, const Gri
         M.epx[s] = Ms.epx[0];
         M.epy[s] = Ms.epy[0];
         for (int k = 0; k < 6; k++) M.sg_out[s][k] = Ms.sg_out[0][k];
+        for (int k = 0; k < 3; k++) M.vin[s][k] = Ms.vin[0][k];
         for (int k = 0; k < 3; k++) M.u[s][k] = Ms.u[0][k];
         if (acc && !Ms.u[0][0]) return cudaErrorInvalidValue;
     }

@@ -47,6 +47,29 @@ __device__ __forceinline__ void tile_xy(int &x, int &y)
 }
 static inline dim3 grid3(int nx, int ny, int nz) { return dim3((unsigned)(nx + 31) / 32, (unsigned)(ny + 7) / 8, (unsigned)nz); }
 
+// A load through the read-only path, for data that no thread of the kernel
+// writes: the compiler may then issue it ahead of the kernel's stores (which
+// it must otherwise assume could alias it), so the loads of consecutive
+// position blocks and shots overlap.
+template <typename T>
+__device__ __forceinline__ T ro(const T *a, int i)
+{
+    return __ldg(a + i);
+}
+
+// a point in [2, n - 3] in every dimension: every neighbour range test of the
+// velocity and G1 adjoints holds there
+__device__ __forceinline__ bool inner_pt(const Geo &g, int x, int y, int z)
+{
+    return x >= 2 && x <= g.nx - 3 && y >= 2 && y <= g.ny - 3 && z >= 2 && z <= g.nz - 3;
+}
+
+// Multi-shot point kernels run the shots of a point in turn in one thread when
+// the shots add to a common gradient (G1, the velocity adjoint: the terms are
+// summed in registers in shot order and the gradient is read and written
+// once), or put the shots of a tile in adjacent CTAs when they do not (G0:
+// the medium planes are then shared through L2).
+
 // ---------------------------------------------------------------------------
 // Velocity update: v += b * (k . D sigma) on the forward ranges.
 // lambda_sigma += (b D)^T lambda_v; g_b += lambda_v * (k . D sigma), the vy
@@ -63,8 +86,10 @@ static inline dim3 grid3(int nx, int ny, int nz) { return dim3((unsigned)(nx + 3
 //       lsyz[p] += k1 u, lsyz[p-sy] -= k1 u
 // read backwards), so no atomics and a fixed order.  The buoyancy-gradient
 // terms of the velocity point q are returned in gx (vx, node q) and gy, gz
-// (vy, vz: a quarter to each of the four nodes of the mean).
-template <typename T>
+// (vy, vz: a quarter to each of the four nodes of the mean).  IN: the point
+// lies in [2, n - 3] in every dimension, where every range test below holds
+// (the same arithmetic without the tests).
+template <typename T, bool IN>
 __device__ __forceinline__ void vel_adj_point(const GridDev<T> &G, const T *const lv[3], const T *const *f, T *const *ls,
                                               int zt, int bottom, int x, int y, int z, T &gx, T &gy, T &gz)
 {
@@ -73,24 +98,27 @@ __device__ __forceinline__ void vel_adj_point(const GridDev<T> &G, const T *cons
     const int sy = g.px, sz = g.px * g.py;
     const T k0 = G.k[0], k1 = G.k[1], k2 = G.k[2], qq = T(0.25);
     const T *b = G.b;
+    const int p = g.idx(x, y, z);
     auto zin = [&](int zz) { return zz >= zt && zz <= nz - bottom; };
-    auto rx = [&](int xx, int yy, int zz) { return xx >= 1 && xx <= nx - 1 && yy >= 1 && yy <= ny - 1 && zin(zz); };
-    auto ry = [&](int xx, int yy, int zz) { return xx >= 0 && xx <= nx - 1 && yy >= 0 && yy <= ny - 1 && zin(zz); };
-    auto rz = [&](int xx, int yy, int zz) { return xx >= 0 && xx <= nx - 1 && yy >= 1 && yy <= ny - 1 && zz >= 0 && zz <= nz - 1; };
+    auto rx = [&](int xx, int yy, int zz) { return IN || (xx >= 1 && xx <= nx - 1 && yy >= 1 && yy <= ny - 1 && zin(zz)); };
+    auto ry = [&](int xx, int yy, int zz) { return IN || (xx >= 0 && xx <= nx - 1 && yy >= 0 && yy <= ny - 1 && zin(zz)); };
+    auto rz = [&](int xx, int yy, int zz) {
+        return IN || (xx >= 0 && xx <= nx - 1 && yy >= 1 && yy <= ny - 1 && zz >= 0 && zz <= nz - 1);
+    };
     auto ux = [&](int xx, int yy, int zz) -> T {
         if (!rx(xx, yy, zz)) return T(0);
-        const int i = g.idx(xx, yy, zz);
-        return mul_(lv[0][i], b[i]);
+        const int i = p + (xx - x) + (yy - y) * sy + (zz - z) * sz;
+        return mul_(ro(lv[0], i), ro(b, i));
     };
     auto uy = [&](int xx, int yy, int zz) -> T {
         if (!ry(xx, yy, zz)) return T(0);
-        const int i = g.idx(xx, yy, zz);
-        return mul_(lv[1][i], mul_(qq, add_(add_(add_(b[i], b[i + 1]), b[i + sy]), b[i + sy + 1])));
+        const int i = p + (xx - x) + (yy - y) * sy + (zz - z) * sz;
+        return mul_(ro(lv[1], i), mul_(qq, add_(add_(add_(ro(b, i), ro(b, i + 1)), ro(b, i + sy)), ro(b, i + sy + 1))));
     };
     auto uz = [&](int xx, int yy, int zz) -> T {
         if (!rz(xx, yy, zz)) return T(0);
-        const int i = g.idx(xx, yy, zz);
-        return mul_(lv[2][i], mul_(qq, add_(add_(add_(b[i], b[i + sz]), b[i + 1]), b[i + sz + 1])));
+        const int i = p + (xx - x) + (yy - y) * sy + (zz - z) * sz;
+        return mul_(ro(lv[2], i), mul_(qq, add_(add_(add_(ro(b, i), ro(b, i + sz)), ro(b, i + 1)), ro(b, i + sz + 1))));
     };
     const T ux0 = ux(x, y, z), uy0 = uy(x, y, z), uz0 = uz(x, y, z);
     const T dsxx = mul_(k0, sub_(ux0, ux(x + 1, y, z)));
@@ -99,27 +127,26 @@ __device__ __forceinline__ void vel_adj_point(const GridDev<T> &G, const T *cons
     const T dsyy = mul_(k1, sub_(uy(x, y - 1, z), uy0));
     const T dsyz = add_(mul_(k2, sub_(uy0, uy(x, y, z + 1))), mul_(k1, sub_(uz0, uz(x, y + 1, z))));
     const T dszz = mul_(k2, sub_(uz(x, y, z - 1), uz0));
-    const int p = g.idx(x, y, z);
     // buoyancy-gradient terms of the velocity point p (its own update ranges)
     gx = T(0);
     gy = T(0);
     gz = T(0);
     if (rx(x, y, z)) {
-        const T a = lv[0][p];
-        const T d = add_(add_(mul_(k0, sub_(f[SXX][p], f[SXX][p - 1])), mul_(k1, sub_(f[SXY][p], f[SXY][p - sy]))),
-                         mul_(k2, sub_(f[SXZ][p], f[SXZ][p - sz])));
+        const T a = ro(lv[0], p);
+        const T d = add_(add_(mul_(k0, sub_(ro(f[SXX], p), ro(f[SXX], p - 1))), mul_(k1, sub_(ro(f[SXY], p), ro(f[SXY], p - sy)))),
+                         mul_(k2, sub_(ro(f[SXZ], p), ro(f[SXZ], p - sz))));
         gx = mul_(a, d);
     }
     if (ry(x, y, z)) {
-        const T a = lv[1][p];
-        const T d = add_(add_(mul_(k0, sub_(f[SXY][p + 1], f[SXY][p])), mul_(k2, sub_(f[SYZ][p], f[SYZ][p - sz]))),
-                         mul_(k1, sub_(f[SYY][p + sy], f[SYY][p])));
+        const T a = ro(lv[1], p);
+        const T d = add_(add_(mul_(k0, sub_(ro(f[SXY], p + 1), ro(f[SXY], p))), mul_(k2, sub_(ro(f[SYZ], p), ro(f[SYZ], p - sz)))),
+                         mul_(k1, sub_(ro(f[SYY], p + sy), ro(f[SYY], p))));
         gy = mul_(qq, mul_(a, d));
     }
     if (rz(x, y, z)) {
-        const T a = lv[2][p];
-        const T d = add_(add_(mul_(k0, sub_(f[SXZ][p + 1], f[SXZ][p])), mul_(k2, sub_(f[SZZ][p + sz], f[SZZ][p]))),
-                         mul_(k1, sub_(f[SYZ][p], f[SYZ][p - sy])));
+        const T a = ro(lv[2], p);
+        const T d = add_(add_(mul_(k0, sub_(ro(f[SXZ], p + 1), ro(f[SXZ], p))), mul_(k2, sub_(ro(f[SZZ], p + sz), ro(f[SZZ], p)))),
+                         mul_(k1, sub_(ro(f[SYZ], p), ro(f[SYZ], p - sy))));
         gz = mul_(qq, mul_(a, d));
     }
     // every load above before the stores
@@ -154,16 +181,19 @@ __global__ void vel_adj_kernel(GridDev<T> G, AdjDev<T> A, int zt, int bottom)
     if (x > g.nx || y > g.ny) return;
     const T *lv[3] = {A.l[VX], A.l[VY], A.l[VZ]};
     T gx, gy, gz;
-    vel_adj_point(G, lv, G.f, A.l, zt, bottom, x, y, z, gx, gy, gz);
+    if (inner_pt(g, x, y, z))
+        vel_adj_point<T, true>(G, lv, G.f, A.l, zt, bottom, x, y, z, gx, gy, gz);
+    else
+        vel_adj_point<T, false>(G, lv, G.f, A.l, zt, bottom, x, y, z, gx, gy, gz);
     vel_adj_gb(g, A.gb, g.idx(x, y, z), gx, gy, gz);
 }
 
-// The velocity adjoint of every shot at each point: the buoyancy read once
-// (cached) for all shots, their buoyancy-gradient terms summed in registers
-// and added with one set of atomics.
+// The velocity adjoint of shots 0 .. ns - 1 (points x, y, z in [-1, n]): a
+// thread per point runs each shot's gather in turn and sums the shots'
+// buoyancy-gradient terms, in shot order, before one set of atomics.
 template <typename T>
-__global__ void __launch_bounds__(256, 3)
-    vel_adj_shots_kernel(GridDev<T> G, T *gb, const __grid_constant__ AdjShots<T> S, int zt, int bottom)
+__global__ void __launch_bounds__(256) vel_adj_shots_kernel(GridDev<T> G, T *gb, const __grid_constant__ AdjShots<T> S,
+                                                             int zt, int bottom)
 {
     const Geo &g = G.g;
     int x, y;
@@ -172,6 +202,7 @@ __global__ void __launch_bounds__(256, 3)
     y -= 1;
     const int z = (int)blockIdx.z - 1;
     if (x > g.nx || y > g.ny) return;
+    const bool inner = inner_pt(g, x, y, z);
     const int64_t box = S.box;
     T sx = T(0), sy = T(0), sz = T(0);
     for (int s = 0; s < S.ns; s++) {
@@ -186,7 +217,10 @@ __global__ void __launch_bounds__(256, 3)
             ls[k] = l + k * box;
         }
         T gx, gy, gz;
-        vel_adj_point(G, lv, f, ls, zt, bottom, x, y, z, gx, gy, gz);
+        if (inner)
+            vel_adj_point<T, true>(G, lv, f, ls, zt, bottom, x, y, z, gx, gy, gz);
+        else
+            vel_adj_point<T, false>(G, lv, f, ls, zt, bottom, x, y, z, gx, gy, gz);
         sx = add_(sx, gx);
         sy = add_(sy, gy);
         sz = add_(sz, gz);
@@ -302,14 +336,14 @@ __device__ __forceinline__ void g0_point(const GridDev<T> &G, const AdjDev<T> &A
         en[0] = e1_at(G, p);
         en[1] = e2_at(G, p);
         en[2] = e3_used(G, E, surf, x, y, z, p, en[0], en[1]);
-        const T a[3] = {A.l[SXX][p], A.l[SYY][p], surf ? T(0) : A.l[SZZ][p]};
+        const T a[3] = {ro(A.l[SXX], p), ro(A.l[SYY], p), surf ? T(0) : ro(A.l[SZZ], p)};
         const int rowc[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
 #pragma unroll
         for (int j = 0; j < 3; j++)
 #pragma unroll
             for (int i = 0; i < 3; i++) {
                 le[j] = fma_(a[i], c[rowc[i][j]][p], le[j]);
-                ls[j] = fma_(a[i], c[6 + 3 * i + j][p], ls[j]);
+                ls[j] = fma_(a[i], ro(c[6 + 3 * i + j], p), ls[j]);
             }
     }
     // the surface mirrors of syz / sxz folded back: lambda(0) - lambda(-1)
@@ -362,7 +396,7 @@ __global__ void stress21_adj_g0(GridDev<T> G, AdjDev<T> A, int flag)
 // and stored by the caller), adds this shot's terms to them and writes the
 // shot's strain adjoints W; a caller that holds the slots over several shots
 // reads and writes them once for all.
-template <typename T>
+template <typename T, bool IN>
 __device__ __forceinline__ void g1_n_shot(const GridDev<T> &G, const AdjDev<T> &A, int flag, const Ext &E, int x, int y,
                                           int z, T (&gk)[15])
 {
@@ -371,41 +405,47 @@ __device__ __forceinline__ void g1_n_shot(const GridDev<T> &G, const AdjDev<T> &
     const T *const *c = G.c;
     T *const *X = A.w;
     const T *l4 = A.l[SYZ], *l5 = A.l[SXZ], *l6 = A.l[SXY];
-    auto I = [&](int xx, int yy, int zz) { return g.idx(xx, yy, zz); };
-    const int p = I(x, y, z);
+    const int p = g.idx(x, y, z), PY = g.px, PZ = g.px * g.py;
+    auto I = [&](int xx, int yy, int zz) { return p + (xx - x) + (yy - y) * PY + (zz - z) * PZ; };
+    auto L4 = [&](int xx, int yy, int zz) { return IN || E.l4(xx, yy, zz); };
+    auto L5 = [&](int xx, int yy, int zz) { return IN || E.l5(xx, yy, zz); };
+    auto L6 = [&](int xx, int yy, int zz) { return IN || E.l6(xx, yy, zz); };
+    auto LN = [&](int xx, int yy, int zz) { return IN || E.n(xx, yy, zz); };
+    auto inr = [&](int v, int lo, int hi) { return IN || in_(v, lo, hi); };
+    auto lq = [&](int v, int hi) { return IN || v <= hi; };
     T v[2][2];
     bool oa[2], ob[2];
     T zp[3] = {T(0), T(0), T(0)};
     for (int i = 0; i < 2; i++)
         for (int j = 0; j < 2; j++) {
             int qx = x, qy = y - i, qz = z - j;   // L4 tp over N (x, y..y+1, z..z+1)
-            if (E.l4(qx, qy, qz))
-                zp[0] = fma_(wgt<T>(qy <= ny, qy + 1 <= ny, qz <= nz, qz + 1 <= nz, i, j), l4[I(qx, qy, qz)], zp[0]);
+            if (L4(qx, qy, qz))
+                zp[0] = fma_(wgt<T>(lq(qy, ny), lq(qy + 1, ny), lq(qz, nz), lq(qz + 1, nz), i, j), ro(l4, I(qx, qy, qz)), zp[0]);
             qx = x + 1 - i; qy = y; qz = z - j;   // L5 tp over N (x-1..x, y, z..z+1)
-            if (E.l5(qx, qy, qz))
-                zp[1] = fma_(wgt<T>(in_(qx - 1, 0, nx - 1), in_(qx, 0, nx - 1), qz <= nz, qz + 1 <= nz, i, j),
-                             l5[I(qx, qy, qz)], zp[1]);
+            if (L5(qx, qy, qz))
+                zp[1] = fma_(wgt<T>(inr(qx - 1, 0, nx - 1), inr(qx, 0, nx - 1), lq(qz, nz), lq(qz + 1, nz), i, j),
+                             ro(l5, I(qx, qy, qz)), zp[1]);
             qx = x + 1 - i; qy = y - j; qz = z;   // L6 P6 over N (x-1..x, y..y+1, z)
-            if (E.l6(qx, qy, qz))
-                zp[2] = fma_(wgt<T>(in_(qx - 1, 0, nx - 1), in_(qx, 0, nx - 1), qy <= ny, qy + 1 <= ny, i, j),
-                             l6[I(qx, qy, qz)], zp[2]);
+            if (L6(qx, qy, qz))
+                zp[2] = fma_(wgt<T>(inr(qx - 1, 0, nx - 1), inr(qx, 0, nx - 1), lq(qy, ny), lq(qy + 1, ny), i, j),
+                             ro(l6, I(qx, qy, qz)), zp[2]);
         }
-    const T e[3] = {X[X_E + 0][p], X[X_E + 1][p], X[X_E + 2][p]};
+    const T e[3] = {ro(X[X_E + 0], p), ro(X[X_E + 1], p), ro(X[X_E + 2], p)};
     T ab[3];
-    for (int i = 0; i < 2; i++) { oa[i] = in_(y - 1 + i, 0, ny - 1); ob[i] = in_(z - 1 + i, 0, nz - 1); }
-    for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++) v[i][j] = (oa[i] && ob[j]) ? X[X_E + 3][I(x, y - 1 + i, z - 1 + j)] : T(0);
+    for (int i = 0; i < 2; i++) { oa[i] = inr(y - 1 + i, 0, ny - 1); ob[i] = inr(z - 1 + i, 0, nz - 1); }
+    for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++) v[i][j] = (oa[i] && ob[j]) ? ro(X[X_E + 3], I(x, y - 1 + i, z - 1 + j)) : T(0);
     ab[0] = avg4<T>(v, oa, ob);
-    for (int i = 0; i < 2; i++) { oa[i] = (x + i) <= nx; ob[i] = in_(z - 1 + i, 0, nz - 1); }
-    for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++) v[i][j] = (oa[i] && ob[j]) ? X[X_E + 4][I(x + i, y, z - 1 + j)] : T(0);
+    for (int i = 0; i < 2; i++) { oa[i] = lq((x + i), nx); ob[i] = inr(z - 1 + i, 0, nz - 1); }
+    for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++) v[i][j] = (oa[i] && ob[j]) ? ro(X[X_E + 4], I(x + i, y, z - 1 + j)) : T(0);
     ab[1] = avg4<T>(v, oa, ob);
-    for (int i = 0; i < 2; i++) { oa[i] = (x + i) <= nx; ob[i] = in_(y - 1 + i, 0, ny - 1); }
-    for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++) v[i][j] = (oa[i] && ob[j]) ? X[X_E + 5][I(x + i, y - 1 + j, z)] : T(0);
+    for (int i = 0; i < 2; i++) { oa[i] = lq((x + i), nx); ob[i] = inr(y - 1 + i, 0, ny - 1); }
+    for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++) v[i][j] = (oa[i] && ob[j]) ? ro(X[X_E + 5], I(x + i, y - 1 + j, z)) : T(0);
     ab[2] = avg4<T>(v, oa, ob);
-    const bool surf = flag && z == 0;
-    const T a[3] = {A.l[SXX][p], A.l[SYY][p], surf ? T(0) : A.l[SZZ][p]};
+    const bool surf = !IN && flag && z == 0;
+    const T a[3] = {ro(A.l[SXX], p), ro(A.l[SYY], p), surf ? T(0) : ro(A.l[SZZ], p)};
     T cs[9];
 #pragma unroll
-    for (int k = 0; k < 9; k++) cs[k] = c[6 + k][p];
+    for (int k = 0; k < 9; k++) cs[k] = ro(c[6 + k], p);
     T le[3] = {X[X_W + 0][p], X[X_W + 1][p], X[X_W + 2][p]};
     const int rowc[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
 #pragma unroll
@@ -429,7 +469,7 @@ __device__ __forceinline__ void g1_n_shot(const GridDev<T> &G, const AdjDev<T> &
 }
 
 // L4 q: C44 a4 + C45 Z45 + C46 Z46 + Abar4 adjoints of N; slots 15..17
-template <typename T>
+template <typename T, bool IN>
 __device__ __forceinline__ void g1_l4_shot(const GridDev<T> &G, const AdjDev<T> &A, const Ext &E, int x, int y, int z,
                                            T &g15, T &g16, T &g17)
 {
@@ -438,35 +478,41 @@ __device__ __forceinline__ void g1_l4_shot(const GridDev<T> &G, const AdjDev<T> 
     const T *const *c = G.c;
     T *const *X = A.w;
     const T *l4 = A.l[SYZ], *l5 = A.l[SXZ], *l6 = A.l[SXY];
-    auto I = [&](int xx, int yy, int zz) { return g.idx(xx, yy, zz); };
-    const int p = I(x, y, z);
+    const int p = g.idx(x, y, z), PY = g.px, PZ = g.px * g.py;
+    auto I = [&](int xx, int yy, int zz) { return p + (xx - x) + (yy - y) * PY + (zz - z) * PZ; };
+    auto L4 = [&](int xx, int yy, int zz) { return IN || E.l4(xx, yy, zz); };
+    auto L5 = [&](int xx, int yy, int zz) { return IN || E.l5(xx, yy, zz); };
+    auto L6 = [&](int xx, int yy, int zz) { return IN || E.l6(xx, yy, zz); };
+    auto LN = [&](int xx, int yy, int zz) { return IN || E.n(xx, yy, zz); };
+    auto inr = [&](int v, int lo, int hi) { return IN || in_(v, lo, hi); };
+    auto lq = [&](int v, int hi) { return IN || v <= hi; };
     T v[2][2];
     bool oa[2], ob[2];
-    const T a4 = l4[p], e4 = X[X_E + 3][p];
+    const T a4 = ro(l4, p), e4 = ro(X[X_E + 3], p);
     T z45 = T(0), z46 = T(0), sn = T(0);
     for (int i = 0; i < 2; i++)
         for (int j = 0; j < 2; j++) {
             int sx = x + 1 - i, sy = y + 1 - j, sz_ = z;   // L5 t45 over L4 (x-1..x, y-1..y, z)
-            if (E.l5(sx, sy, sz_))
-                z45 = fma_(wgt<T>(in_(sx - 1, 0, nx - 1), in_(sx, 0, nx - 1), in_(sy - 1, 0, ny - 1), in_(sy, 0, ny - 1), i, j),
-                           l5[I(sx, sy, sz_)], z45);
+            if (L5(sx, sy, sz_))
+                z45 = fma_(wgt<T>(inr(sx - 1, 0, nx - 1), inr(sx, 0, nx - 1), inr(sy - 1, 0, ny - 1), inr(sy, 0, ny - 1), i, j),
+                           ro(l5, I(sx, sy, sz_)), z45);
             sx = x + 1 - i; sy = y; sz_ = z + 1 - j;       // L6 t46 over L4 (x-1..x, y, z-1..z)
-            if (E.l6(sx, sy, sz_))
-                z46 = fma_(wgt<T>(in_(sx - 1, 0, nx - 1), in_(sx, 0, nx - 1), in_(sz_ - 1, 0, nz - 1), in_(sz_, 0, nz - 1), i, j),
-                           l6[I(sx, sy, sz_)], z46);
+            if (L6(sx, sy, sz_))
+                z46 = fma_(wgt<T>(inr(sx - 1, 0, nx - 1), inr(sx, 0, nx - 1), inr(sz_ - 1, 0, nz - 1), inr(sz_, 0, nz - 1), i, j),
+                           ro(l6, I(sx, sy, sz_)), z46);
             sx = x; sy = y + 1 - i; sz_ = z + 1 - j;       // N Abar4 over L4 (x, y-1..y, z-1..z)
-            if (E.n(sx, sy, sz_))
-                sn = fma_(wgt<T>(in_(sy - 1, 0, ny - 1), in_(sy, 0, ny - 1), in_(sz_ - 1, 0, nz - 1), in_(sz_, 0, nz - 1), i, j),
-                          X[X_S + 0][I(sx, sy, sz_)], sn);
+            if (LN(sx, sy, sz_))
+                sn = fma_(wgt<T>(inr(sy - 1, 0, ny - 1), inr(sy, 0, ny - 1), inr(sz_ - 1, 0, nz - 1), inr(sz_, 0, nz - 1), i, j),
+                          ro(X[X_S + 0], I(sx, sy, sz_)), sn);
         }
     // forward averages t5 (e5 over L5 (x..x+1, y..y+1, z)) and t6 (e6 over L6 (x..x+1, y, z..z+1))
-    for (int i = 0; i < 2; i++) { oa[i] = (x + i) <= nx; ob[i] = (y + i) <= ny; }
-    for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++) v[i][j] = (oa[i] && ob[j]) ? X[X_E + 4][I(x + i, y + j, z)] : T(0);
+    for (int i = 0; i < 2; i++) { oa[i] = lq((x + i), nx); ob[i] = lq((y + i), ny); }
+    for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++) v[i][j] = (oa[i] && ob[j]) ? ro(X[X_E + 4], I(x + i, y + j, z)) : T(0);
     const T t5 = avg4<T>(v, oa, ob);
-    for (int i = 0; i < 2; i++) { oa[i] = (x + i) <= nx; ob[i] = (z + i) <= nz; }
-    for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++) v[i][j] = (oa[i] && ob[j]) ? X[X_E + 5][I(x + i, y, z + j)] : T(0);
+    for (int i = 0; i < 2; i++) { oa[i] = lq((x + i), nx); ob[i] = lq((z + i), nz); }
+    for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++) v[i][j] = (oa[i] && ob[j]) ? ro(X[X_E + 5], I(x + i, y, z + j)) : T(0);
     const T t6 = avg4<T>(v, oa, ob);
-    const T c15 = c[15][p], c16 = c[16][p], c17 = c[17][p];
+    const T c15 = ro(c[15], p), c16 = ro(c[16], p), c17 = ro(c[17], p);
     g15 = add_(g15, mul_(a4, e4));
     g16 = add_(g16, add_(mul_(a4, t5), mul_(z45, e4)));
     g17 = add_(g17, add_(mul_(a4, t6), mul_(z46, e4)));
@@ -474,7 +520,7 @@ __device__ __forceinline__ void g1_l4_shot(const GridDev<T> &G, const AdjDev<T> 
 }
 
 // L5 s: C55 a5 + C56 Z56 + Abar5 adjoints of N + C45 a4 from L4's t5; slots 18, 19
-template <typename T>
+template <typename T, bool IN>
 __device__ __forceinline__ void g1_l5_shot(const GridDev<T> &G, const AdjDev<T> &A, const Ext &E, int x, int y, int z,
                                            T &g18, T &g19)
 {
@@ -483,39 +529,45 @@ __device__ __forceinline__ void g1_l5_shot(const GridDev<T> &G, const AdjDev<T> 
     const T *const *c = G.c;
     T *const *X = A.w;
     const T *l4 = A.l[SYZ], *l5 = A.l[SXZ], *l6 = A.l[SXY];
-    auto I = [&](int xx, int yy, int zz) { return g.idx(xx, yy, zz); };
-    const int p = I(x, y, z);
+    const int p = g.idx(x, y, z), PY = g.px, PZ = g.px * g.py;
+    auto I = [&](int xx, int yy, int zz) { return p + (xx - x) + (yy - y) * PY + (zz - z) * PZ; };
+    auto L4 = [&](int xx, int yy, int zz) { return IN || E.l4(xx, yy, zz); };
+    auto L5 = [&](int xx, int yy, int zz) { return IN || E.l5(xx, yy, zz); };
+    auto L6 = [&](int xx, int yy, int zz) { return IN || E.l6(xx, yy, zz); };
+    auto LN = [&](int xx, int yy, int zz) { return IN || E.n(xx, yy, zz); };
+    auto inr = [&](int v, int lo, int hi) { return IN || in_(v, lo, hi); };
+    auto lq = [&](int v, int hi) { return IN || v <= hi; };
     T v[2][2];
     bool oa[2], ob[2];
-    const T a5 = l5[p], e5 = X[X_E + 4][p];
+    const T a5 = ro(l5, p), e5 = ro(X[X_E + 4], p);
     T z56 = T(0), sn = T(0), s4 = T(0);
     for (int i = 0; i < 2; i++)
         for (int j = 0; j < 2; j++) {
             int qx = x, qy = y - i, qz = z + 1 - j;      // L6 t56 over L5 (x, y..y+1, z-1..z)
-            if (E.l6(qx, qy, qz))
-                z56 = fma_(wgt<T>(qy <= ny, qy + 1 <= ny, in_(qz - 1, 0, nz - 1), in_(qz, 0, nz - 1), i, j), l6[I(qx, qy, qz)], z56);
+            if (L6(qx, qy, qz))
+                z56 = fma_(wgt<T>(lq(qy, ny), lq(qy + 1, ny), inr(qz - 1, 0, nz - 1), inr(qz, 0, nz - 1), i, j), ro(l6, I(qx, qy, qz)), z56);
             qx = x - i; qy = y; qz = z + 1 - j;          // N Abar5 over L5 (x..x+1, y, z-1..z)
-            if (E.n(qx, qy, qz))
-                sn = fma_(wgt<T>(qx <= nx, qx + 1 <= nx, in_(qz - 1, 0, nz - 1), in_(qz, 0, nz - 1), i, j),
-                          X[X_S + 1][I(qx, qy, qz)], sn);
+            if (LN(qx, qy, qz))
+                sn = fma_(wgt<T>(lq(qx, nx), lq(qx + 1, nx), inr(qz - 1, 0, nz - 1), inr(qz, 0, nz - 1), i, j),
+                          ro(X[X_S + 1], I(qx, qy, qz)), sn);
             qx = x - i; qy = y - j; qz = z;              // L4 t5 over L5 (x..x+1, y..y+1, z)
-            if (E.l4(qx, qy, qz)) {
+            if (L4(qx, qy, qz)) {
                 const int q = I(qx, qy, qz);
-                s4 = fma_(wgt<T>(qx <= nx, qx + 1 <= nx, qy <= ny, qy + 1 <= ny, i, j), mul_(c[16][q], l4[q]), s4);
+                s4 = fma_(wgt<T>(lq(qx, nx), lq(qx + 1, nx), lq(qy, ny), lq(qy + 1, ny), i, j), mul_(ro(c[16], q), ro(l4, q)), s4);
             }
         }
     // forward average t6 (e6 over L6 (x, y-1..y, z..z+1))
-    for (int i = 0; i < 2; i++) { oa[i] = in_(y - 1 + i, 0, ny - 1); ob[i] = (z + i) <= nz; }
-    for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++) v[i][j] = (oa[i] && ob[j]) ? X[X_E + 5][I(x, y - 1 + i, z + j)] : T(0);
+    for (int i = 0; i < 2; i++) { oa[i] = inr(y - 1 + i, 0, ny - 1); ob[i] = lq((z + i), nz); }
+    for (int i = 0; i < 2; i++) for (int j = 0; j < 2; j++) v[i][j] = (oa[i] && ob[j]) ? ro(X[X_E + 5], I(x, y - 1 + i, z + j)) : T(0);
     const T t6 = avg4<T>(v, oa, ob);
-    const T c18 = c[18][p], c19 = c[19][p];
+    const T c18 = ro(c[18], p), c19 = ro(c[19], p);
     g18 = add_(g18, mul_(a5, e5));
     g19 = add_(g19, add_(mul_(a5, t6), mul_(z56, e5)));
     X[X_W + 4][p] = add_(add_(fma_(c18, a5, mul_(c19, z56)), sn), s4);
 }
 
 // L6 t: C66 a6 + Abar6 adjoints of N + C46 a4 (L4 t6) + C56 a5 (L5 t6); slot 20
-template <typename T>
+template <typename T, bool IN>
 __device__ __forceinline__ void g1_l6_shot(const GridDev<T> &G, const AdjDev<T> &A, const Ext &E, int x, int y, int z, T &g20)
 {
     const Geo &g = G.g;
@@ -523,29 +575,35 @@ __device__ __forceinline__ void g1_l6_shot(const GridDev<T> &G, const AdjDev<T> 
     const T *const *c = G.c;
     T *const *X = A.w;
     const T *l4 = A.l[SYZ], *l5 = A.l[SXZ], *l6 = A.l[SXY];
-    auto I = [&](int xx, int yy, int zz) { return g.idx(xx, yy, zz); };
-    const int p = I(x, y, z);
-    const T a6 = l6[p];
+    const int p = g.idx(x, y, z), PY = g.px, PZ = g.px * g.py;
+    auto I = [&](int xx, int yy, int zz) { return p + (xx - x) + (yy - y) * PY + (zz - z) * PZ; };
+    auto L4 = [&](int xx, int yy, int zz) { return IN || E.l4(xx, yy, zz); };
+    auto L5 = [&](int xx, int yy, int zz) { return IN || E.l5(xx, yy, zz); };
+    auto L6 = [&](int xx, int yy, int zz) { return IN || E.l6(xx, yy, zz); };
+    auto LN = [&](int xx, int yy, int zz) { return IN || E.n(xx, yy, zz); };
+    auto inr = [&](int v, int lo, int hi) { return IN || in_(v, lo, hi); };
+    auto lq = [&](int v, int hi) { return IN || v <= hi; };
+    const T a6 = ro(l6, p);
     T sn = T(0), s4 = T(0), s5 = T(0);
     for (int i = 0; i < 2; i++)
         for (int j = 0; j < 2; j++) {
             int qx = x - i, qy = y + 1 - j, qz = z;      // N Abar6 over L6 (x..x+1, y-1..y, z)
-            if (E.n(qx, qy, qz))
-                sn = fma_(wgt<T>(qx <= nx, qx + 1 <= nx, in_(qy - 1, 0, ny - 1), in_(qy, 0, ny - 1), i, j),
-                          X[X_S + 2][I(qx, qy, qz)], sn);
+            if (LN(qx, qy, qz))
+                sn = fma_(wgt<T>(lq(qx, nx), lq(qx + 1, nx), inr(qy - 1, 0, ny - 1), inr(qy, 0, ny - 1), i, j),
+                          ro(X[X_S + 2], I(qx, qy, qz)), sn);
             qx = x - i; qy = y; qz = z - j;              // L4 t6 over L6 (x..x+1, y, z..z+1)
-            if (E.l4(qx, qy, qz)) {
+            if (L4(qx, qy, qz)) {
                 const int q = I(qx, qy, qz);
-                s4 = fma_(wgt<T>(qx <= nx, qx + 1 <= nx, qz <= nz, qz + 1 <= nz, i, j), mul_(c[17][q], l4[q]), s4);
+                s4 = fma_(wgt<T>(lq(qx, nx), lq(qx + 1, nx), lq(qz, nz), lq(qz + 1, nz), i, j), mul_(ro(c[17], q), ro(l4, q)), s4);
             }
             qx = x; qy = y + 1 - i; qz = z - j;          // L5 t6 over L6 (x, y-1..y, z..z+1)
-            if (E.l5(qx, qy, qz)) {
+            if (L5(qx, qy, qz)) {
                 const int q = I(qx, qy, qz);
-                s5 = fma_(wgt<T>(in_(qy - 1, 0, ny - 1), in_(qy, 0, ny - 1), qz <= nz, qz + 1 <= nz, i, j),
-                          mul_(c[19][q], l5[q]), s5);
+                s5 = fma_(wgt<T>(inr(qy - 1, 0, ny - 1), inr(qy, 0, ny - 1), lq(qz, nz), lq(qz + 1, nz), i, j),
+                          mul_(ro(c[19], q), ro(l5, q)), s5);
             }
         }
-    const T e6 = X[X_E + 5][p], c20 = c[20][p];
+    const T e6 = ro(X[X_E + 5], p), c20 = ro(c[20], p);
     g20 = add_(g20, mul_(a6, e6));
     X[X_W + 5][p] = add_(add_(fma_(c20, a6, sn), s4), s5);
 }
@@ -553,12 +611,12 @@ __device__ __forceinline__ void g1_l6_shot(const GridDev<T> &G, const AdjDev<T> 
 // One point of G1 for shots 0..ns-1: the gradient slots of each position
 // block are read once, take every shot's terms in shot order, and are written
 // once.  shot(s, Gs, As) gives shot s's forward-field and adjoint views.
-template <typename T, typename Shot>
-__device__ __forceinline__ void g1_point(const GridDev<T> &G, const AdjDev<T> &A0, int flag, const Ext &E, int x, int y,
+template <typename T, bool IN, typename Shot>
+__device__ __forceinline__ void g1_point_k(const GridDev<T> &G, const AdjDev<T> &A0, int flag, const Ext &E, int x, int y,
                                          int z, int ns, Shot shot)
 {
     const int p = G.g.idx(x, y, z);
-    if (E.n(x, y, z)) {
+    if (IN || E.n(x, y, z)) {
         T gk[15];
 #pragma unroll
         for (int k = 0; k < 15; k++) gk[k] = A0.gc[k][p];
@@ -566,44 +624,54 @@ __device__ __forceinline__ void g1_point(const GridDev<T> &G, const AdjDev<T> &A
             GridDev<T> Gs;
             AdjDev<T> As;
             shot(s, Gs, As);
-            g1_n_shot(Gs, As, flag, E, x, y, z, gk);
+            g1_n_shot<T, IN>(Gs, As, flag, E, x, y, z, gk);
         }
 #pragma unroll
         for (int k = 0; k < 15; k++) A0.gc[k][p] = gk[k];
     }
-    if (E.l4(x, y, z)) {
+    if (IN || E.l4(x, y, z)) {
         T g15 = A0.gc[15][p], g16 = A0.gc[16][p], g17 = A0.gc[17][p];
         for (int s = 0; s < ns; s++) {
             GridDev<T> Gs;
             AdjDev<T> As;
             shot(s, Gs, As);
-            g1_l4_shot(Gs, As, E, x, y, z, g15, g16, g17);
+            g1_l4_shot<T, IN>(Gs, As, E, x, y, z, g15, g16, g17);
         }
         A0.gc[15][p] = g15;
         A0.gc[16][p] = g16;
         A0.gc[17][p] = g17;
     }
-    if (E.l5(x, y, z)) {
+    if (IN || E.l5(x, y, z)) {
         T g18 = A0.gc[18][p], g19 = A0.gc[19][p];
         for (int s = 0; s < ns; s++) {
             GridDev<T> Gs;
             AdjDev<T> As;
             shot(s, Gs, As);
-            g1_l5_shot(Gs, As, E, x, y, z, g18, g19);
+            g1_l5_shot<T, IN>(Gs, As, E, x, y, z, g18, g19);
         }
         A0.gc[18][p] = g18;
         A0.gc[19][p] = g19;
     }
-    if (E.l6(x, y, z)) {
+    if (IN || E.l6(x, y, z)) {
         T g20 = A0.gc[20][p];
         for (int s = 0; s < ns; s++) {
             GridDev<T> Gs;
             AdjDev<T> As;
             shot(s, Gs, As);
-            g1_l6_shot(Gs, As, E, x, y, z, g20);
+            g1_l6_shot<T, IN>(Gs, As, E, x, y, z, g20);
         }
         A0.gc[20][p] = g20;
     }
+}
+
+template <typename T, typename Shot>
+__device__ __forceinline__ void g1_point(const GridDev<T> &G, const AdjDev<T> &A0, int flag, const Ext &E, int x, int y,
+                                         int z, int ns, Shot shot)
+{
+    if (inner_pt(G.g, x, y, z))
+        g1_point_k<T, true>(G, A0, flag, E, x, y, z, ns, shot);
+    else
+        g1_point_k<T, false>(G, A0, flag, E, x, y, z, ns, shot);
 }
 
 // FP32: 4 CTAs per SM (64 registers, no spills) for latency hiding
@@ -640,43 +708,40 @@ __device__ __forceinline__ void shot_views(const GridDev<T> &G, const AdjDev<T> 
     for (int k = 0; k < 15; k++) As.w[k] = S.w[s] + k * S.wbox;
 }
 
-// G0 of every shot at each point (the medium read once from DRAM for all)
+// G0 of shots 0 .. ns - 1: CTA blockIdx.x runs shot blockIdx.x % ns on x tile
+// blockIdx.x / ns, so the shots of a tile run side by side and share its
+// medium through L2.
 template <typename T>
-__global__ void stress21_adj_g0_shots(GridDev<T> G, AdjDev<T> A0, const __grid_constant__ AdjShots<T> S, int flag)
+__global__ void __launch_bounds__(256) stress21_adj_g0_shots(GridDev<T> G, AdjDev<T> A0, const __grid_constant__ AdjShots<T> S,
+                                                              int flag)
 {
     const Geo &g = G.g;
-    const int nx = g.nx, ny = g.ny, nz = g.nz;
-    const Ext E{nx, ny, nz};
-    {
-        int x, y;
-        tile_xy(x, y);
-        const int z = blockIdx.z;
-        if (x > nx || y > ny) return;
-        for (int s = 0; s < S.ns; s++) {
-            GridDev<T> Gs;
-            AdjDev<T> As;
-            shot_views(G, A0, S, s, Gs, As);
-            g0_point(Gs, As, flag, E, x, y, z);
-        }
-    }
+    const Ext E{g.nx, g.ny, g.nz};
+    const int s = (int)blockIdx.x % S.ns;
+    const int x = (int)blockIdx.x / S.ns * 32 + (int)(threadIdx.x & 31);
+    const int y = (int)blockIdx.y * 8 + (int)(threadIdx.x >> 5);
+    const int z = blockIdx.z;
+    if (x > g.nx || y > g.ny) return;
+    GridDev<T> Gs;
+    AdjDev<T> As;
+    shot_views(G, A0, S, s, Gs, As);
+    g0_point(Gs, As, flag, E, x, y, z);
 }
 
-// G1 of every shot at each point: the gradient slots read and written once
+// G1 of shots 0 .. ns - 1: a thread per point runs the shots in turn, the
+// point's gradient slots and medium read once for all of them (g1_point).
 template <typename T>
-__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 2)
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 4 : 2)
     stress21_adj_g1_shots(GridDev<T> G, AdjDev<T> A0, const __grid_constant__ AdjShots<T> S, int flag)
 {
     const Geo &g = G.g;
-    const int nx = g.nx, ny = g.ny, nz = g.nz;
-    const Ext E{nx, ny, nz};
+    const Ext E{g.nx, g.ny, g.nz};
+    int x, y;
+    tile_xy(x, y);
+    const int z = blockIdx.z;
+    if (x > g.nx || y > g.ny) return;
     auto shot = [&](int s, GridDev<T> &Gs, AdjDev<T> &As) { shot_views(G, A0, S, s, Gs, As); };
-    {
-        int x, y;
-        tile_xy(x, y);
-        const int z = blockIdx.z;
-        if (x > nx || y > ny) return;
-        g1_point(G, A0, flag, E, x, y, z, S.ns, shot);
-    }
+    g1_point(G, A0, flag, E, x, y, z, S.ns, shot);
 }
 
 // free surface: e3 = -(C13 e1 + C23 e2 + C34 A4 + C35 A5 + C36 A6) / C33 at z = 0
@@ -843,9 +908,10 @@ cudaError_t launch_stress21_adj_shots(const GridDev<T> &G, const AdjDev<T> &A0, 
 {
     const Geo &g = G.g;
     const int flag = (top && top_bc) ? 1 : 0;
-    const dim3 nb = grid3(g.nx + 1, g.ny + 1, g.nz + 1);
+    dim3 nb = grid3(g.nx + 1, g.ny + 1, g.nz + 1);
+    nb.x *= (unsigned)S.ns;
     stress21_adj_g0_shots<T><<<nb, 256, 0, st>>>(G, A0, S, flag);
-    stress21_adj_g1_shots<T><<<nb, 256, 0, st>>>(G, A0, S, flag);
+    stress21_adj_g1_shots<T><<<grid3(g.nx + 1, g.ny + 1, g.nz + 1), 256, 0, st>>>(G, A0, S, flag);
     if (flag)   // the free surface adds to the common gradient without atomics: one shot at a time
         for (int s = 0; s < S.ns; s++) {
             GridDev<T> Gs = G;

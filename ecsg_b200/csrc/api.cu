@@ -2520,13 +2520,46 @@ static int group_adjoint_step(ecsg_sim *const *sims, int S, const char *const *s
 }
 
 template <typename T>
-static int group_gradient_op(ecsg_sim *const *sims, int S, int nsteps, const float *const *observed, int k,
+static int group_gradient_op(ecsg_sim *const *sims, int S, int nsteps, const float *const *observed, int k_req,
                              int sub_every, double *losses)
 {
     int rc;
     ecsg_sim *m = sims[0], *s = m;   // s: where CK reports
     cudaStream_t gs = m->st;
     const size_t sb = state_bytes(m);
+    // Memory plan, per shot: checkpoints every k steps (ncp + 1 states) and
+    // one segment of k + 1 states.  When the requested interval does not fit,
+    // a shorter one that does is taken first (the same single recomputation
+    // of each segment, only more checkpoints); only when none fits is the
+    // segment split again by sub-checkpoints every j steps (two levels, one
+    // more forward pass of each segment).
+    const size_t margin = (size_t)1 << 30;
+    size_t have = 0;
+    {
+        size_t free_b = 0, total_b = 0;
+        CK(cudaMemGetInfo(&free_b, &total_b));
+        have = free_b;
+        for (int b = 0; b < S; b++) have += sims[b]->ckpt_cap + sims[b]->seg_cap + sims[b]->seg2_cap;
+    }
+    auto states = [&](int kk, int jj) {   // per shot, checkpoint interval kk, sub-checkpoints every jj
+        const size_t ncp_ = (size_t)(nsteps + kk - 1) / kk;
+        return (ncp_ + 1) + (size_t)(jj + 1) + (jj < kk ? (size_t)((kk + jj - 1) / jj) : 0);
+    };
+    auto fits = [&](int kk, int jj) { return (size_t)S * sb * states(kk, jj) + margin <= have; };
+    int k = k_req, j = k_req;
+    if (sub_every > 0 && sub_every < k) {
+        j = sub_every;
+    } else if (!fits(k, k)) {
+        int kk = k - 1;
+        while (kk >= 1 && !fits(kk, kk)) kk--;
+        if (kk >= 1) {
+            k = j = kk;
+        } else {
+            j = 1;
+            while ((size_t)j * j < (size_t)k) j++;
+        }
+    }
+    if (!fits(k, j)) return fail(m, ECSG_ERR_CUDA, "shots: %d shots do not fit in device memory", S);
     const int ncp = (nsteps + k - 1) / k;
     const size_t nrec = (size_t)m->nrec, nobs = (size_t)nsteps * nrec;
     auto grow = [&](ecsg_sim *x, void **p, size_t &cap, size_t want) -> int {
@@ -2541,29 +2574,21 @@ static int group_gradient_op(ecsg_sim *const *sims, int S, int nsteps, const flo
         cap = want;
         return ECSG_OK;
     };
-    // checkpoints and observations first; then the segment buffers, one level
-    // (k + 1 states) if they fit, else two (sub-checkpoints every j steps)
+    // checkpoints and observations first, then the segment buffers (k + 1
+    // states, or j + 1 and the sub-checkpoints); a shot whose buffers must
+    // grow releases its old segment buffers first, as the plan counted them
     for (int b = 0; b < S; b++) {
         ecsg_sim *x = sims[b];
+        if (x->ckpt_cap < sb * (ncp + 1) || x->seg_cap < sb * (j + 1)) {
+            cudaFree(x->seg);
+            cudaFree(x->seg2);
+            x->seg = x->seg2 = nullptr;
+            x->seg_cap = x->seg2_cap = 0;
+        }
         if ((rc = grow(x, (void **)&x->ckpt, x->ckpt_cap, sb * (ncp + 1)))) return rc;
         if ((rc = grow(x, &x->recT, x->recT_cap, sizeof(T) * (nobs > 0 ? nobs : 1)))) return rc;
         if ((rc = grow(x, (void **)&x->obs, x->obs_cap, sizeof(float) * (nobs > 0 ? nobs : 1)))) return rc;
         if (nobs) CK(cudaMemcpyAsync(x->obs, observed[b], sizeof(float) * nobs, cudaMemcpyHostToDevice, gs));
-    }
-    int j = k;
-    if (sub_every > 0 && sub_every < k) j = sub_every;
-    {
-        size_t free_b = 0, total_b = 0;
-        CK(cudaMemGetInfo(&free_b, &total_b));
-        size_t have = free_b;
-        for (int b = 0; b < S; b++) have += sims[b]->seg_cap + sims[b]->seg2_cap;
-        const size_t margin = (size_t)1 << 30;
-        auto need = [&](int jj) { return (size_t)S * sb * ((size_t)(jj + 1) + (jj < k ? (size_t)((k + jj - 1) / jj) : 0)); };
-        if (j == k && need(k) + margin > have) {
-            j = 1;
-            while ((size_t)j * j < (size_t)k) j++;
-        }
-        if (need(j) + margin > have) return fail(m, ECSG_ERR_CUDA, "shots: %d shots do not fit in device memory", S);
     }
     const int nsub = (k + j - 1) / j;
     for (int b = 0; b < S; b++) {

@@ -55,7 +55,12 @@ constexpr int ENERGY_TX = 32, ENERGY_TY = 8, ENERGY_ZC = 16;
 // FP32 fields, 21-Cij medium (the production path): each point's terms in
 // FP32 (the precision of the fields they multiply), the point's kinetic and
 // potential parts added to two FP64 sums (the finalize of this medium only
-// adds the terms up, so the per-term split is not kept).
+// adds the terms up, so the per-term split is not kept).  Every load of the
+// point is issued first and unconditionally (the neighbours at n + 1 and
+// -1 lie in the halo of every box), the terms outside the point's position
+// sets are dropped by selects afterwards: a load inside a branch, or after a
+// division's slow path, could not be started before the branch and the
+// kernel would wait on each in turn.
 __device__ __forceinline__ void energy_point_f32_gen21(const GridDev<float> &G, const GridDev<float> &GU, const float *vc0,
                                                        const float *vc1, const float *vc2, int flag, int x, int y, int z,
                                                        int p, double &kin, double &pot)
@@ -63,30 +68,41 @@ __device__ __forceinline__ void energy_point_f32_gen21(const GridDev<float> &G, 
     const Geo &g = G.g;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     const int sy = g.px, sz = g.px * g.py;
+    const float *b = G.b;
+    const float b000 = b[p], b010 = b[p + sy], b100 = b[p + 1], b110 = b[p + sy + 1], b001 = b[p + sz],
+                b101 = b[p + sz + 1];
+    const float vx = G.f[VX][p], vy = G.f[VY][p], vz = G.f[VZ][p], c0 = vc0[p], c1 = vc1[p], c2 = vc2[p];
+    const float sxx = G.f[SXX][p], syy = G.f[SYY][p], szz = G.f[SZZ][p];
+    const float syz = G.f[SYZ][p], sxz = G.f[SXZ][p], sxy = G.f[SXY][p];
+    const float *ux = GU.f[VX], *uy = GU.f[VY], *uz = GU.f[VZ];
+    const float ux0 = ux[p], ux1 = ux[p + 1], uxy = ux[p + sy], uxz = ux[p + sz];
+    const float uy0 = uy[p], uym = uy[p - sy], uyx = uy[p - 1], uyz = uy[p + sz];
+    const float uz0 = uz[p], uzm = uz[p - sz], uzx = uz[p - 1], uzy = uz[p + sy];
+    const float k0 = GU.k[0], k1 = GU.k[1], k2 = GU.k[2];
     const float mx = (x == 0 || x == nx) ? 0.5f : 1.0f;
     const float my = (y == 0 || y == ny) ? 0.5f : 1.0f;
     const float mz = (z == 0 || z == nz) ? 0.5f : 1.0f;
     const bool xs = x < nx, ys = y < ny, zs = z < nz;
-    const float b000 = G.b[p];
-    float k = mz * my * mx * (G.f[VX][p] * vc0[p]) / b000;
-    if (xs && ys) {
-        const float rb = 0.25f * (b000 + G.b[p + sy] + G.b[p + 1] + G.b[p + sy + 1]);
-        k += mz * (G.f[VY][p] * vc1[p]) / rb;
-    }
-    if (xs && zs) {
-        const float rb = 0.25f * (b000 + G.b[p + sz] + G.b[p + 1] + G.b[p + sz + 1]);
-        k += my * (G.f[VZ][p] * vc2[p]) / rb;
-    }
+    // the strain functions of the stress update (e1_at .. e6_at), same operations
+    const float e1 = k0 * (ux1 - ux0), e2 = k1 * (uy0 - uym);
+    float e3 = k2 * (uz0 - uzm);
+    const float e4 = __fmaf_rn(k1, uzy - uz0, k2 * (uyz - uy0));
+    const float e5 = __fmaf_rn(k0, uz0 - uzx, k2 * (uxz - ux0));
+    const float e6 = __fmaf_rn(k0, uy0 - uyx, k1 * (uxy - ux0));
+    float k = mz * my * mx * (vx * c0) / b000;
+    const float ky = mz * (vy * c1) / (0.25f * (b000 + b010 + b100 + b110));
+    const float kz = my * (vz * c2) / (0.25f * (b000 + b001 + b100 + b101));
+    if (xs && ys) k += ky;
+    if (xs && zs) k += kz;
+    if (flag && z == 0 && xs) e3 = e3_used(GU, Ext{nx, ny, nz}, true, x, y, z, p, e1, e2);
     float e = 0.0f;
-    if (xs) {
-        const float w = mz * my;
-        const float e1 = e1_at(GU, p), e2 = e2_at(GU, p);
-        const float e3 = (flag && z == 0) ? e3_used(GU, Ext{nx, ny, nz}, true, x, y, z, p, e1, e2) : e3_at(GU, p);
-        e += w * (e1 * G.f[SXX][p] + e2 * G.f[SYY][p] + e3 * G.f[SZZ][p]);
-    }
-    if (xs && ys && zs) e += e4_at(GU, p) * G.f[SYZ][p];
-    if (zs) e += my * mx * e5_at(GU, p) * G.f[SXZ][p];
-    if (ys) e += mz * mx * e6_at(GU, p) * G.f[SXY][p];
+    const float w = mz * my;
+    const float en = w * (e1 * sxx + e2 * syy + e3 * szz);
+    const float e44 = e4 * syz, e55 = my * mx * e5 * sxz, e66 = mz * mx * e6 * sxy;
+    if (xs) e += en;
+    if (xs && ys && zs) e += e44;
+    if (zs) e += e55;
+    if (ys) e += e66;
     kin += (double)k;
     pot += (double)e;
 }

@@ -143,6 +143,12 @@ def run_reference(args):
     print(json.dumps(line))
 
 
+# geometries of the shot-gradient leg: the benchmark's (None: the workload
+# default, 361x361x61 @ 10 m over 121x121x81 @ 30 m) and a medium one for
+# profiling captures (1/8 of the volume: 181x181x31 over 61x61x41)
+GRAD_GRIDS = {"full": None, "medium": [((180, 180, 30), 10.0), ((60, 60, 40), 30.0)]}
+
+
 def shot_gradients(args, local, world, max_over_ranks, barrier):
     """Misfit gradients on the two-grid adjoint workload: 361x361x61 @ 10 m
     over 121x121x81 @ 30 m (9,135,502 points), smooth orthorhombic model,
@@ -162,9 +168,10 @@ def shot_gradients(args, local, world, max_over_ranks, barrier):
     from ecsg_b200.workloads import two_grid_adjoint_case
     n = args.grad_steps
     shot = local % 16
-    with ecsg_b200.Simulation(two_grid_adjoint_case(0, shot, n, blob=True), precision="f32", device=local) as s:
+    G = GRAD_GRIDS[args.grad_size]
+    with ecsg_b200.Simulation(two_grid_adjoint_case(0, shot, n, blob=True, grids=G), precision="f32", device=local) as s:
         obs = s.run(n)["rec"].T.copy()
-    case = two_grid_adjoint_case(0, shot, n, blob=False)
+    case = two_grid_adjoint_case(0, shot, n, blob=False, grids=G)
     with ecsg_b200.Simulation(case, precision="f32", device=local) as s:
         s.misfit_gradient(obs[: min(n, 60)], ckpt_every=50)   # warm-up (allocations, tensor maps)
         if world > 1:
@@ -185,10 +192,10 @@ def shot_gradients(args, local, world, max_over_ranks, barrier):
         shots = [(local * nb + k) % 16 for k in range(nb)]
         obs_b = []
         for k in shots:
-            with ecsg_b200.Simulation(two_grid_adjoint_case(0, k, n, blob=True), precision="f32", device=local) as s:
+            with ecsg_b200.Simulation(two_grid_adjoint_case(0, k, n, blob=True, grids=G), precision="f32", device=local) as s:
                 obs_b.append(s.run(n)["rec"].T.copy())
-        model = ecsg_b200.Simulation(two_grid_adjoint_case(0, shots[0], n, blob=False), precision="f32", device=local)
-        sims = [model] + [ecsg_b200.Simulation.shot(model, two_grid_adjoint_case(0, k, n, blob=False)) for k in shots[1:]]
+        model = ecsg_b200.Simulation(two_grid_adjoint_case(0, shots[0], n, blob=False, grids=G), precision="f32", device=local)
+        sims = [model] + [ecsg_b200.Simulation.shot(model, two_grid_adjoint_case(0, k, n, blob=False, grids=G)) for k in shots[1:]]
         try:
             ecsg_b200.shots_misfit_gradient(sims, [o[: min(n, 60)] for o in obs_b], ckpt_every=50)   # warm-up
             barrier()
@@ -212,7 +219,8 @@ def shot_gradients(args, local, world, max_over_ranks, barrier):
             "ms_per_shot_gradient": ms, "steps": n,
             "ckpt_every": 50, "points": case.points(), "receivers": len(case.rec), "dtype": "f32",
             "loss": loss, "finite": bool(np.isfinite(loss) and np.isfinite(gmax)), "status": status,
-            "workload": "two-grid 361x361x61@10m / 121x121x81@30m, smooth orthorhombic, shot %d of 4x4" % shot,
+            "workload": "two-grid %s, smooth orthorhombic, shot %d of 4x4" % (
+                " / ".join("%dx%dx%d@%gm" % (g["n"][0] + 1, g["n"][1] + 1, g["n"][2] + 1, g["h"][0]) for g in case.grids), shot),
             "batched": batched}
 
 
@@ -355,6 +363,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grad-batch", type=int, default=8,
                     help="shots per batched shot-gradient run (0 or 1: no batched leg)")
+    ap.add_argument("--grad-size", choices=sorted(GRAD_GRIDS), default="full",
+                    help="geometry of the shot-gradient leg (medium: for profiling captures)")
     ap.add_argument("--grad-steps", type=int, default=1500,
                     help="steps of the shot-gradient measurement (0: skip it)")
     ap.add_argument("--c5-steps", type=int, default=2000,

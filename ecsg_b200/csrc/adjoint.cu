@@ -57,6 +57,17 @@ __device__ __forceinline__ T ro(const T *a, int i)
     return __ldg(a + i);
 }
 
+// ro() when RO, else an ordinary load (the plain velocity adjoint measured
+// faster with ordinary loads, the multi-shot one with read-only loads)
+template <bool RO, typename T>
+__device__ __forceinline__ T ld_(const T *a, int i)
+{
+    if constexpr (RO)
+        return ro(a, i);
+    else
+        return a[i];
+}
+
 // a point in [2, n - 3] in every dimension: every neighbour range test of the
 // velocity and G1 adjoints holds there
 __device__ __forceinline__ bool inner_pt(const Geo &g, int x, int y, int z)
@@ -89,7 +100,7 @@ __device__ __forceinline__ bool inner_pt(const Geo &g, int x, int y, int z)
 // (vy, vz: a quarter to each of the four nodes of the mean).  IN: the point
 // lies in [2, n - 3] in every dimension, where every range test below holds
 // (the same arithmetic without the tests).
-template <typename T, bool IN>
+template <typename T, bool IN, bool RO>
 __device__ __forceinline__ void vel_adj_point(const GridDev<T> &G, const T *const lv[3], const T *const *f, T *const *ls,
                                               int zt, int bottom, int x, int y, int z, T &gx, T &gy, T &gz)
 {
@@ -108,17 +119,17 @@ __device__ __forceinline__ void vel_adj_point(const GridDev<T> &G, const T *cons
     auto ux = [&](int xx, int yy, int zz) -> T {
         if (!rx(xx, yy, zz)) return T(0);
         const int i = p + (xx - x) + (yy - y) * sy + (zz - z) * sz;
-        return mul_(ro(lv[0], i), ro(b, i));
+        return mul_(ld_<RO>(lv[0], i), ld_<RO>(b, i));
     };
     auto uy = [&](int xx, int yy, int zz) -> T {
         if (!ry(xx, yy, zz)) return T(0);
         const int i = p + (xx - x) + (yy - y) * sy + (zz - z) * sz;
-        return mul_(ro(lv[1], i), mul_(qq, add_(add_(add_(ro(b, i), ro(b, i + 1)), ro(b, i + sy)), ro(b, i + sy + 1))));
+        return mul_(ld_<RO>(lv[1], i), mul_(qq, add_(add_(add_(ld_<RO>(b, i), ld_<RO>(b, i + 1)), ld_<RO>(b, i + sy)), ld_<RO>(b, i + sy + 1))));
     };
     auto uz = [&](int xx, int yy, int zz) -> T {
         if (!rz(xx, yy, zz)) return T(0);
         const int i = p + (xx - x) + (yy - y) * sy + (zz - z) * sz;
-        return mul_(ro(lv[2], i), mul_(qq, add_(add_(add_(ro(b, i), ro(b, i + sz)), ro(b, i + 1)), ro(b, i + sz + 1))));
+        return mul_(ld_<RO>(lv[2], i), mul_(qq, add_(add_(add_(ld_<RO>(b, i), ld_<RO>(b, i + sz)), ld_<RO>(b, i + 1)), ld_<RO>(b, i + sz + 1))));
     };
     const T ux0 = ux(x, y, z), uy0 = uy(x, y, z), uz0 = uz(x, y, z);
     const T dsxx = mul_(k0, sub_(ux0, ux(x + 1, y, z)));
@@ -132,21 +143,21 @@ __device__ __forceinline__ void vel_adj_point(const GridDev<T> &G, const T *cons
     gy = T(0);
     gz = T(0);
     if (rx(x, y, z)) {
-        const T a = ro(lv[0], p);
-        const T d = add_(add_(mul_(k0, sub_(ro(f[SXX], p), ro(f[SXX], p - 1))), mul_(k1, sub_(ro(f[SXY], p), ro(f[SXY], p - sy)))),
-                         mul_(k2, sub_(ro(f[SXZ], p), ro(f[SXZ], p - sz))));
+        const T a = ld_<RO>(lv[0], p);
+        const T d = add_(add_(mul_(k0, sub_(ld_<RO>(f[SXX], p), ld_<RO>(f[SXX], p - 1))), mul_(k1, sub_(ld_<RO>(f[SXY], p), ld_<RO>(f[SXY], p - sy)))),
+                         mul_(k2, sub_(ld_<RO>(f[SXZ], p), ld_<RO>(f[SXZ], p - sz))));
         gx = mul_(a, d);
     }
     if (ry(x, y, z)) {
-        const T a = ro(lv[1], p);
-        const T d = add_(add_(mul_(k0, sub_(ro(f[SXY], p + 1), ro(f[SXY], p))), mul_(k2, sub_(ro(f[SYZ], p), ro(f[SYZ], p - sz)))),
-                         mul_(k1, sub_(ro(f[SYY], p + sy), ro(f[SYY], p))));
+        const T a = ld_<RO>(lv[1], p);
+        const T d = add_(add_(mul_(k0, sub_(ld_<RO>(f[SXY], p + 1), ld_<RO>(f[SXY], p))), mul_(k2, sub_(ld_<RO>(f[SYZ], p), ld_<RO>(f[SYZ], p - sz)))),
+                         mul_(k1, sub_(ld_<RO>(f[SYY], p + sy), ld_<RO>(f[SYY], p))));
         gy = mul_(qq, mul_(a, d));
     }
     if (rz(x, y, z)) {
-        const T a = ro(lv[2], p);
-        const T d = add_(add_(mul_(k0, sub_(ro(f[SXZ], p + 1), ro(f[SXZ], p))), mul_(k2, sub_(ro(f[SZZ], p + sz), ro(f[SZZ], p)))),
-                         mul_(k1, sub_(ro(f[SYZ], p), ro(f[SYZ], p - sy))));
+        const T a = ld_<RO>(lv[2], p);
+        const T d = add_(add_(mul_(k0, sub_(ld_<RO>(f[SXZ], p + 1), ld_<RO>(f[SXZ], p))), mul_(k2, sub_(ld_<RO>(f[SZZ], p + sz), ld_<RO>(f[SZZ], p)))),
+                         mul_(k1, sub_(ld_<RO>(f[SYZ], p), ld_<RO>(f[SYZ], p - sy))));
         gz = mul_(qq, mul_(a, d));
     }
     // every load above before the stores
@@ -182,9 +193,9 @@ __global__ void vel_adj_kernel(GridDev<T> G, AdjDev<T> A, int zt, int bottom)
     const T *lv[3] = {A.l[VX], A.l[VY], A.l[VZ]};
     T gx, gy, gz;
     if (inner_pt(g, x, y, z))
-        vel_adj_point<T, true>(G, lv, G.f, A.l, zt, bottom, x, y, z, gx, gy, gz);
+        vel_adj_point<T, true, false>(G, lv, G.f, A.l, zt, bottom, x, y, z, gx, gy, gz);
     else
-        vel_adj_point<T, false>(G, lv, G.f, A.l, zt, bottom, x, y, z, gx, gy, gz);
+        vel_adj_point<T, false, false>(G, lv, G.f, A.l, zt, bottom, x, y, z, gx, gy, gz);
     vel_adj_gb(g, A.gb, g.idx(x, y, z), gx, gy, gz);
 }
 
@@ -218,9 +229,9 @@ __global__ void __launch_bounds__(256) vel_adj_shots_kernel(GridDev<T> G, T *gb,
         }
         T gx, gy, gz;
         if (inner)
-            vel_adj_point<T, true>(G, lv, f, ls, zt, bottom, x, y, z, gx, gy, gz);
+            vel_adj_point<T, true, true>(G, lv, f, ls, zt, bottom, x, y, z, gx, gy, gz);
         else
-            vel_adj_point<T, false>(G, lv, f, ls, zt, bottom, x, y, z, gx, gy, gz);
+            vel_adj_point<T, false, true>(G, lv, f, ls, zt, bottom, x, y, z, gx, gy, gz);
         sx = add_(sx, gx);
         sy = add_(sy, gy);
         sz = add_(sz, gz);

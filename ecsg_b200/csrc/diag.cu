@@ -55,29 +55,49 @@ constexpr int ENERGY_TX = 32, ENERGY_TY = 8, ENERGY_ZC = 16;
 // FP32 fields, 21-Cij medium (the production path): each point's terms in
 // FP32 (the precision of the fields they multiply), the point's kinetic and
 // potential parts added to two FP64 sums (the finalize of this medium only
-// adds the terms up, so the per-term split is not kept).  Every load of the
-// point is issued first and unconditionally (the neighbours at n + 1 and
-// -1 lie in the halo of every box), the terms outside the point's position
-// sets are dropped by selects afterwards: a load inside a branch, or after a
-// division's slow path, could not be started before the branch and the
-// kernel would wait on each in turn.
+// adds the terms up, so the per-term split is not kept).  A thread marches z
+// down its column: the values a plane shares with the one before (the
+// buoyancy and the displacement sums at p, which the plane before read at
+// p + sz, and uz at p - sz) come along in registers, and every other load of
+// the point is issued first and unconditionally (the neighbours at n + 1
+// and -1 lie in the halo of every box); the terms outside the point's
+// position sets are dropped by selects afterwards.  The kinetic terms divide
+// by the buoyancy means with __fdividef (within 2 ulp).
+struct EnergyCarry {
+    float b0, b1, ux0, uy0, uzm;   // b(p), b(p+1), ux(p), uy(p), uz(p - sz)
+};
+
+__device__ __forceinline__ void energy_carry_init(const GridDev<float> &G, const GridDev<float> &GU, int p, EnergyCarry &c)
+{
+    const int sz = G.g.px * G.g.py;
+    c.b0 = G.b[p];
+    c.b1 = G.b[p + 1];
+    c.ux0 = GU.f[VX][p];
+    c.uy0 = GU.f[VY][p];
+    c.uzm = GU.f[VZ][p - sz];
+}
+
 __device__ __forceinline__ void energy_point_f32_gen21(const GridDev<float> &G, const GridDev<float> &GU, const float *vc0,
                                                        const float *vc1, const float *vc2, int flag, int x, int y, int z,
-                                                       int p, double &kin, double &pot)
+                                                       int p, EnergyCarry &cr, double &kin, double &pot)
 {
     const Geo &g = G.g;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
     const int sy = g.px, sz = g.px * g.py;
     const float *b = G.b;
-    const float b000 = b[p], b010 = b[p + sy], b100 = b[p + 1], b110 = b[p + sy + 1], b001 = b[p + sz],
-                b101 = b[p + sz + 1];
+    const float b000 = cr.b0, b100 = cr.b1, b010 = b[p + sy], b110 = b[p + sy + 1], b001 = b[p + sz], b101 = b[p + sz + 1];
     const float vx = G.f[VX][p], vy = G.f[VY][p], vz = G.f[VZ][p], c0 = vc0[p], c1 = vc1[p], c2 = vc2[p];
     const float sxx = G.f[SXX][p], syy = G.f[SYY][p], szz = G.f[SZZ][p];
     const float syz = G.f[SYZ][p], sxz = G.f[SXZ][p], sxy = G.f[SXY][p];
     const float *ux = GU.f[VX], *uy = GU.f[VY], *uz = GU.f[VZ];
-    const float ux0 = ux[p], ux1 = ux[p + 1], uxy = ux[p + sy], uxz = ux[p + sz];
-    const float uy0 = uy[p], uym = uy[p - sy], uyx = uy[p - 1], uyz = uy[p + sz];
-    const float uz0 = uz[p], uzm = uz[p - sz], uzx = uz[p - 1], uzy = uz[p + sy];
+    const float ux0 = cr.ux0, ux1 = ux[p + 1], uxy = ux[p + sy], uxz = ux[p + sz];
+    const float uy0 = cr.uy0, uym = uy[p - sy], uyx = uy[p - 1], uyz = uy[p + sz];
+    const float uz0 = uz[p], uzm = cr.uzm, uzx = uz[p - 1], uzy = uz[p + sy];
+    cr.b0 = b001;
+    cr.b1 = b101;
+    cr.ux0 = uxz;
+    cr.uy0 = uyz;
+    cr.uzm = uz0;
     const float k0 = GU.k[0], k1 = GU.k[1], k2 = GU.k[2];
     const float mx = (x == 0 || x == nx) ? 0.5f : 1.0f;
     const float my = (y == 0 || y == ny) ? 0.5f : 1.0f;
@@ -89,9 +109,9 @@ __device__ __forceinline__ void energy_point_f32_gen21(const GridDev<float> &G, 
     const float e4 = __fmaf_rn(k1, uzy - uz0, k2 * (uyz - uy0));
     const float e5 = __fmaf_rn(k0, uz0 - uzx, k2 * (uxz - ux0));
     const float e6 = __fmaf_rn(k0, uy0 - uyx, k1 * (uxy - ux0));
-    float k = mz * my * mx * (vx * c0) / b000;
-    const float ky = mz * (vy * c1) / (0.25f * (b000 + b010 + b100 + b110));
-    const float kz = my * (vz * c2) / (0.25f * (b000 + b001 + b100 + b101));
+    float k = __fdividef(mz * my * mx * (vx * c0), b000);
+    const float ky = __fdividef(mz * (vy * c1), 0.25f * (b000 + b010 + b100 + b110));
+    const float kz = __fdividef(my * (vz * c2), 0.25f * (b000 + b001 + b100 + b101));
     if (xs && ys) k += ky;
     if (xs && zs) k += kz;
     if (flag && z == 0 && xs) e3 = e3_used(GU, Ext{nx, ny, nz}, true, x, y, z, p, e1, e2);
@@ -107,8 +127,8 @@ __device__ __forceinline__ void energy_point_f32_gen21(const GridDev<float> &G, 
     pot += (double)e;
 }
 
-// The FP32 21-Cij energy: 4 CTAs per SM, two planes of loads in flight per
-// thread (the kernel is bound by memory latency, not bytes).
+// The FP32 21-Cij energy: 4 CTAs per SM, one plane per thread at a time (64
+// registers, no spills; two planes in flight spilled and measured 4 % slower).
 __global__ void __launch_bounds__(RED_THREADS, 4)
     energy_f32_gen21_kernel(GridDev<float> G, const float *vc0, const float *vc1, const float *vc2, GridDev<float> GU,
                             int flag, double *partial)
@@ -127,8 +147,9 @@ __global__ void __launch_bounds__(RED_THREADS, 4)
         if (x > nx || y > ny) continue;
         const int z0 = tz * ENERGY_ZC, z1 = min(nz, z0 + ENERGY_ZC - 1);
         int p = g.idx(x, y, z0);
-#pragma unroll 2
-        for (int z = z0; z <= z1; z++, p += sz) energy_point_f32_gen21(G, GU, vc0, vc1, vc2, flag, x, y, z, p, kin, pot);
+        EnergyCarry cr;
+        energy_carry_init(G, GU, p, cr);
+        for (int z = z0; z <= z1; z++, p += sz) energy_point_f32_gen21(G, GU, vc0, vc1, vc2, flag, x, y, z, p, cr, kin, pot);
     }
     double acc[12] = {kin, 0.0, 0.0, pot, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     block_sums<12>(acc, partial, gridDim.x);

@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <type_traits>
@@ -2533,28 +2534,66 @@ static int group_gradient_op(ecsg_sim *const *sims, int S, int nsteps, const flo
     // of each segment, only more checkpoints); only when none fits is the
     // segment split again by sub-checkpoints every j steps (two levels, one
     // more forward pass of each segment).
-    const size_t margin = (size_t)1 << 30;
+    size_t margin = (size_t)1 << 30;
     size_t have = 0;
     {
         size_t free_b = 0, total_b = 0;
         CK(cudaMemGetInfo(&free_b, &total_b));
         have = free_b;
         for (int b = 0; b < S; b++) have += sims[b]->ckpt_cap + sims[b]->seg_cap + sims[b]->seg2_cap;
+        // ECSG_SHOTS_MEMORY: the bytes the plan may give checkpoints and
+        // segments, no margin (to exercise the plans on small cases)
+        if (const char *env = getenv("ECSG_SHOTS_MEMORY")) {
+            const size_t cap = (size_t)strtoull(env, nullptr, 10);
+            if (cap > 0 && cap < have) have = cap;
+            margin = 0;
+        }
     }
     auto states = [&](int kk, int jj) {   // per shot, checkpoint interval kk, sub-checkpoints every jj
         const size_t ncp_ = (size_t)(nsteps + kk - 1) / kk;
         return (ncp_ + 1) + (size_t)(jj + 1) + (jj < kk ? (size_t)((kk + jj - 1) / jj) : 0);
     };
-    auto fits = [&](int kk, int jj) { return (size_t)S * sb * states(kk, jj) + margin <= have; };
+    auto fits_n = [&](int n, int kk, int jj) { return (size_t)n * sb * states(kk, jj) + margin <= have; };
+    auto fits = [&](int kk, int jj) { return fits_n(S, kk, jj); };
+    auto one_level = [&](int n) {   // the longest interval <= k_req at which n shots fit one level (0: none)
+        int kk = k_req;
+        while (kk >= 1 && !fits_n(n, kk, kk)) kk--;
+        return kk;
+    };
+    auto release = [&](ecsg_sim *x) {
+        cudaFree(x->ckpt);
+        cudaFree(x->seg);
+        cudaFree(x->seg2);
+        x->ckpt = x->seg = x->seg2 = nullptr;
+        x->ckpt_cap = x->seg_cap = x->seg2_cap = 0;
+    };
     int k = k_req, j = k_req;
     if (sub_every > 0 && sub_every < k) {
         j = sub_every;
     } else if (!fits(k, k)) {
-        int kk = k - 1;
-        while (kk >= 1 && !fits(kk, kk)) kk--;
+        const int kk = one_level(S);
         if (kk >= 1) {
             k = j = kk;
         } else {
+            // groups of fewer shots that fit one level run in turn (each group
+            // shares the medium; a two-level plan would cost one more forward
+            // pass of every segment); their gradients are summed at the end
+            int S1 = S;
+            while (S1 > 1 && one_level(S1) < 1) S1 = (S1 + 1) / 2;
+            if (S1 < S && one_level(S1) >= 1) {
+                CK(cudaStreamSynchronize(gs));
+                std::vector<ecsg_sim *> heads;
+                for (int b0 = 0; b0 < S; b0 += S1) {
+                    const int n = S - b0 < S1 ? S - b0 : S1;
+                    for (int b = 0; b < S; b++) release(sims[b]);
+                    if ((rc = group_gradient_op<T>(sims + b0, n, nsteps, observed ? observed + b0 : nullptr, k_req, 0,
+                                                   losses ? losses + b0 : nullptr)))
+                        return rc;
+                    heads.push_back(sims[b0]);
+                }
+                for (int b = 0; b < S; b++) release(sims[b]);
+                return heads.size() > 1 ? ecsg_sum_gradients(m, heads.data(), (int)heads.size()) : ECSG_OK;
+            }
             j = 1;
             while ((size_t)j * j < (size_t)k) j++;
         }

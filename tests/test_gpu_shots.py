@@ -14,7 +14,7 @@ atomics, in no fixed order)."""
 import numpy as np
 import pytest
 
-from ecsg_b200 import Simulation, shots_misfit_gradient
+from ecsg_b200 import Simulation, device_layout, shots_misfit_gradient
 from ecsg_b200.workloads import random_case_gen21, ricker
 
 pytestmark = pytest.mark.gpu
@@ -79,6 +79,61 @@ def test_shots_in_lockstep_equal_one_at_a_time(prec, ratio):
         with Simulation(c, precision=prec) as s:
             s.run(nsteps, graph=False)
             assert np.array_equal(fa, s.field(0, 2)) and np.array_equal(fb, fa)
+
+
+def _state_bytes(case, prec):
+    """Bytes of one saved state: the nine fields of every grid's box and the
+    sxz warm starts of every interface (the plan's unit)."""
+    tsize = 8 if prec == "f64" else 4
+    b = 0
+    for g in case.grids:
+        px, py, pz = device_layout(g["n"], case.radius)["pitch"]
+        b += 9 * px * py * pz * tsize
+    for g in case.grids[1:]:
+        b += 8 * (g["n"][0] + 1) * (g["n"][1] + 1)
+    return b
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+def test_shots_in_groups_when_one_level_does_not_fit(monkeypatch, prec):
+    """A checkpoint budget (ECSG_SHOTS_MEMORY) of 30 states in all:
+    three shots need at least 36 states for one level at any interval up to
+    the requested 8 steps (22 steps), two shots 26 at 8, so the call runs the
+    shots as a group of two and a group of one, one level each, and sums the
+    groups' gradients.  Losses bitwise and gradient to the one-at-a-time
+    tolerance, as in the unconstrained call."""
+    nsteps, k, ratio = 22, 8, 3
+    cases = [_shot_case(93, ratio, shift, nsteps) for shift in (-2, 0, 3)]
+    rng = np.random.default_rng(7)
+    obs = [(0.05 * rng.standard_normal((nsteps, len(c.rec)))).astype(np.float32) for c in cases]
+    want_loss, want_grad = [], []
+    for c, o in zip(cases, obs):
+        with Simulation(c, precision=prec) as s:
+            want_loss.append(s.misfit_gradient(o, ckpt_every=k))
+            want_grad.append([s.gradient(g, w) for g in range(2) for w in range(22)])
+    monkeypatch.setenv("ECSG_SHOTS_MEMORY", str(30 * _state_bytes(cases[0], prec)))
+    model = Simulation(cases[0], precision=prec)
+    sims = [model] + [Simulation.shot(model, c) for c in cases[1:]]
+    try:
+        losses = shots_misfit_gradient(sims, obs, ckpt_every=k)
+        grad = [model.gradient(g, w) for g in range(2) for w in range(22)]
+        status = [x.status() for x in sims]
+        final = [x.field(0, 2) for x in sims]
+    finally:
+        for x in sims[1:]:
+            x.close()
+        model.close()
+    assert status == [0, 0, 0]
+    assert np.array_equal(losses, np.array(want_loss)), (losses, want_loss)
+    tol = 1e-12 if prec == "f64" else 1e-6
+    scale = max(max(float(np.abs(gs[v]).max()) for v in range(44)) for gs in want_grad)
+    for w in range(44):
+        ref = sum(gs[w] for gs in want_grad)
+        assert _close(grad[w], ref, tol, scale), (w, float(np.abs(grad[w] - ref).max()) / scale)
+    for c, f in zip(cases, final):
+        with Simulation(c, precision=prec) as s:
+            s.run(nsteps, graph=False)
+            assert np.array_equal(f, s.field(0, 2))
 
 
 def test_shots_reject_instances_of_another_model():

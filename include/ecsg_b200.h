@@ -359,10 +359,13 @@ int ecsg_sum_gradients(ecsg_sim *dst, ecsg_sim *const *srcs, int n);
  * all of them.  No reference counterpart: it batches the time loop of
  * main.cpp:165-261 (a shot = one pass of it) and the adjoint of
  * ecsg_misfit_gradient.  Checkpoints every ckpt_every steps; inside a
- * segment the states are recomputed from its checkpoint, through
- * sub-checkpoints every sub_every steps when 0 < sub_every < ckpt_every, or
- * when the segment's states of all n shots do not fit in device memory
- * (sub_every <= 0: chosen, about sqrt(ckpt_every)).  Leaves in sims[0]'s
+ * segment the states are recomputed from its checkpoint.  With
+ * 0 < sub_every < ckpt_every, through sub-checkpoints every sub_every steps.
+ * With sub_every <= 0, when the checkpoints and a segment's states of all n
+ * shots do not fit in device memory: a shorter checkpoint interval that fits;
+ * else groups of fewer shots that fit, run one after the other (their
+ * gradients summed); else sub-checkpoints every ~sqrt(ckpt_every) steps (one
+ * more forward pass of each segment).  Leaves in sims[0]'s
  * gradient arrays the gradient of the sum of the n misfits (the medium
  * adjoints accumulate every shot's terms in the field precision; the
  * interface adjoints' shares are summed in FP64 at the end); losses[b] (may

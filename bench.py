@@ -373,7 +373,7 @@ def main():
     ap.add_argument("--c5-plain", type=int, default=1, help="plain shots timed for the subset's comparison")
     ap.add_argument("--accuracy-steps", type=int, default=600,
                     help="steps of the FP32-vs-FP64 accuracy run (0: skip it)")
-    ap.add_argument("--batch-steps", type=int, default=200,
+    ap.add_argument("--batch-steps", type=int, default=1000,
                     help="steps of the batched-forward measurement (0: skip it)")
     args = ap.parse_args()
     if args.impl == "reference":

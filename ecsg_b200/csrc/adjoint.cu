@@ -719,24 +719,25 @@ __device__ __forceinline__ void shot_views(const GridDev<T> &G, const AdjDev<T> 
     for (int k = 0; k < 15; k++) As.w[k] = S.w[s] + k * S.wbox;
 }
 
-// G0 of shots 0 .. ns - 1: CTA blockIdx.x runs shot blockIdx.x % ns on x tile
-// blockIdx.x / ns, so the shots of a tile run side by side and share its
-// medium through L2.
+// G0 of shots 0 .. ns - 1, the shots in turn in one thread per point (the
+// coefficients' loads of the next shot hit L1; 8 % faster than putting the
+// shots of a tile in side-by-side CTAs)
 template <typename T>
-__global__ void __launch_bounds__(256) stress21_adj_g0_shots(GridDev<T> G, AdjDev<T> A0, const __grid_constant__ AdjShots<T> S,
-                                                              int flag)
+__global__ void __launch_bounds__(256) stress21_adj_g0_shots(GridDev<T> G, AdjDev<T> A0,
+                                                                   const __grid_constant__ AdjShots<T> S, int flag)
 {
     const Geo &g = G.g;
     const Ext E{g.nx, g.ny, g.nz};
-    const int s = (int)blockIdx.x % S.ns;
-    const int x = (int)blockIdx.x / S.ns * 32 + (int)(threadIdx.x & 31);
-    const int y = (int)blockIdx.y * 8 + (int)(threadIdx.x >> 5);
+    int x, y;
+    tile_xy(x, y);
     const int z = blockIdx.z;
     if (x > g.nx || y > g.ny) return;
-    GridDev<T> Gs;
-    AdjDev<T> As;
-    shot_views(G, A0, S, s, Gs, As);
-    g0_point(Gs, As, flag, E, x, y, z);
+    for (int s = 0; s < S.ns; s++) {
+        GridDev<T> Gs;
+        AdjDev<T> As;
+        shot_views(G, A0, S, s, Gs, As);
+        g0_point(Gs, As, flag, E, x, y, z);
+    }
 }
 
 // G1 of shots 0 .. ns - 1: a thread per point runs the shots in turn, the
@@ -813,43 +814,51 @@ __global__ void stress21_adj_g2(GridDev<T> G, AdjDev<T> A)
 
 // transpose of the strain differences: every velocity entry gathers the W of
 // the strains that read it
+// G3 at one point: IN: every neighbour range test holds (points in [2, n - 3])
+template <typename T, bool IN>
+__device__ __forceinline__ void g3_point(const GridDev<T> &G, const AdjDev<T> &A, int x, int y, int z)
+{
+    const Geo &g = G.g;
+    const Ext E{g.nx, g.ny, g.nz};
+    const T k0 = G.k[0], k1 = G.k[1], k2 = G.k[2];
+    T *const *X = A.w;
+    auto I = [&](int xx, int yy, int zz) { return g.idx(xx, yy, zz); };
+    auto W = [&](int k, bool ok, int xx, int yy, int zz) -> T { return (IN || ok) ? X[X_W + k][I(xx, yy, zz)] : T(0); };
+    const int p = I(x, y, z);
+    // vx: e1(N x-1) - e1(N x), e5(L5 z-1) - e5(L5 z), e6(L6 y-1) - e6(L6 y)
+    const T gx = add_(add_(mul_(k0, sub_(W(0, E.n(x - 1, y, z), x - 1, y, z), W(0, E.n(x, y, z), x, y, z))),
+                           mul_(k2, sub_(W(4, E.l5(x, y, z - 1), x, y, z - 1), W(4, E.l5(x, y, z), x, y, z)))),
+                      mul_(k1, sub_(W(5, E.l6(x, y - 1, z), x, y - 1, z), W(5, E.l6(x, y, z), x, y, z))));
+    // vy: e2(N y) - e2(N y+1), e4(L4 z-1) - e4(L4 z), e6(L6 x) - e6(L6 x+1)
+    const T gy = add_(add_(mul_(k1, sub_(W(1, E.n(x, y, z), x, y, z), W(1, E.n(x, y + 1, z), x, y + 1, z))),
+                           mul_(k2, sub_(W(3, E.l4(x, y, z - 1), x, y, z - 1), W(3, E.l4(x, y, z), x, y, z)))),
+                      mul_(k0, sub_(W(5, E.l6(x, y, z), x, y, z), W(5, E.l6(x + 1, y, z), x + 1, y, z))));
+    // vz: e3(N z) - e3(N z+1), e4(L4 y-1) - e4(L4 y), e5(L5 x) - e5(L5 x+1)
+    const T gz = add_(add_(mul_(k2, sub_(W(2, E.n(x, y, z), x, y, z), W(2, E.n(x, y, z + 1), x, y, z + 1))),
+                           mul_(k1, sub_(W(3, E.l4(x, y - 1, z), x, y - 1, z), W(3, E.l4(x, y, z), x, y, z)))),
+                      mul_(k0, sub_(W(4, E.l5(x, y, z), x, y, z), W(4, E.l5(x + 1, y, z), x + 1, y, z))));
+    // the three loads before the first store (they are in the box for every
+    // x, y, z in [-1, n])
+    const T lx = A.l[VX][p], ly = A.l[VY][p], lz = A.l[VZ][p];
+    if (gx != T(0)) A.l[VX][p] = add_(lx, gx);
+    if (gy != T(0)) A.l[VY][p] = add_(ly, gy);
+    if (gz != T(0)) A.l[VZ][p] = add_(lz, gz);
+}
+
 template <typename T>
 __device__ __forceinline__ void g3_body(const GridDev<T> &G, const AdjDev<T> &A, int zb)
 {
     const Geo &g = G.g;
-    const int nx = g.nx, ny = g.ny, nz = g.nz;
-    const Ext E{nx, ny, nz};
-    const T k0 = G.k[0], k1 = G.k[1], k2 = G.k[2];
-    T *const *X = A.w;
-    auto I = [&](int x, int y, int z) { return g.idx(x, y, z); };
-    auto W = [&](int k, bool ok, int x, int y, int z) -> T { return ok ? X[X_W + k][I(x, y, z)] : T(0); };
-    {
-        int x, y;
-        tile_xy(x, y);
-        x -= 1;
-        y -= 1;
-        const int z = zb - 1;
-        if (x > nx || y > ny) return;
-        const int p = I(x, y, z);
-        // vx: e1(N x-1) - e1(N x), e5(L5 z-1) - e5(L5 z), e6(L6 y-1) - e6(L6 y)
-        const T gx = add_(add_(mul_(k0, sub_(W(0, E.n(x - 1, y, z), x - 1, y, z), W(0, E.n(x, y, z), x, y, z))),
-                               mul_(k2, sub_(W(4, E.l5(x, y, z - 1), x, y, z - 1), W(4, E.l5(x, y, z), x, y, z)))),
-                          mul_(k1, sub_(W(5, E.l6(x, y - 1, z), x, y - 1, z), W(5, E.l6(x, y, z), x, y, z))));
-        // vy: e2(N y) - e2(N y+1), e4(L4 z-1) - e4(L4 z), e6(L6 x) - e6(L6 x+1)
-        const T gy = add_(add_(mul_(k1, sub_(W(1, E.n(x, y, z), x, y, z), W(1, E.n(x, y + 1, z), x, y + 1, z))),
-                               mul_(k2, sub_(W(3, E.l4(x, y, z - 1), x, y, z - 1), W(3, E.l4(x, y, z), x, y, z)))),
-                          mul_(k0, sub_(W(5, E.l6(x, y, z), x, y, z), W(5, E.l6(x + 1, y, z), x + 1, y, z))));
-        // vz: e3(N z) - e3(N z+1), e4(L4 y-1) - e4(L4 y), e5(L5 x) - e5(L5 x+1)
-        const T gz = add_(add_(mul_(k2, sub_(W(2, E.n(x, y, z), x, y, z), W(2, E.n(x, y, z + 1), x, y, z + 1))),
-                               mul_(k1, sub_(W(3, E.l4(x, y - 1, z), x, y - 1, z), W(3, E.l4(x, y, z), x, y, z)))),
-                          mul_(k0, sub_(W(4, E.l5(x, y, z), x, y, z), W(4, E.l5(x + 1, y, z), x + 1, y, z))));
-        // the three loads before the first store (they are in the box for every
-        // x, y, z in [-1, n])
-        const T lx = A.l[VX][p], ly = A.l[VY][p], lz = A.l[VZ][p];
-        if (gx != T(0)) A.l[VX][p] = add_(lx, gx);
-        if (gy != T(0)) A.l[VY][p] = add_(ly, gy);
-        if (gz != T(0)) A.l[VZ][p] = add_(lz, gz);
-    }
+    int x, y;
+    tile_xy(x, y);
+    x -= 1;
+    y -= 1;
+    const int z = zb - 1;
+    if (x > g.nx || y > g.ny) return;
+    if (inner_pt(g, x, y, z))
+        g3_point<T, true>(G, A, x, y, z);
+    else
+        g3_point<T, false>(G, A, x, y, z);
 }
 
 template <typename T>
@@ -919,9 +928,7 @@ cudaError_t launch_stress21_adj_shots(const GridDev<T> &G, const AdjDev<T> &A0, 
 {
     const Geo &g = G.g;
     const int flag = (top && top_bc) ? 1 : 0;
-    dim3 nb = grid3(g.nx + 1, g.ny + 1, g.nz + 1);
-    nb.x *= (unsigned)S.ns;
-    stress21_adj_g0_shots<T><<<nb, 256, 0, st>>>(G, A0, S, flag);
+    stress21_adj_g0_shots<T><<<grid3(g.nx + 1, g.ny + 1, g.nz + 1), 256, 0, st>>>(G, A0, S, flag);
     stress21_adj_g1_shots<T><<<grid3(g.nx + 1, g.ny + 1, g.nz + 1), 256, 0, st>>>(G, A0, S, flag);
     if (flag)   // the free surface adds to the common gradient without atomics: one shot at a time
         for (int s = 0; s < S.ns; s++) {

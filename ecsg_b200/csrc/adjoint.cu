@@ -204,8 +204,9 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 5 : 1) vel_adj_kernel(Gr
 // The velocity adjoint of shots 0 .. ns - 1 (points x, y, z in [-1, n]): a
 // thread per point runs each shot's gather in turn and sums the shots'
 // buoyancy-gradient terms, in shot order, before one set of atomics.
+// FP32: 5 CTAs per SM (48 registers; 5 % faster than 4 at 64)
 template <typename T>
-__global__ void __launch_bounds__(256) vel_adj_shots_kernel(GridDev<T> G, T *gb, const __grid_constant__ AdjShots<T> S,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 5 : 2) vel_adj_shots_kernel(GridDev<T> G, T *gb, const __grid_constant__ AdjShots<T> S,
                                                              int zt, int bottom)
 {
     const Geo &g = G.g;
@@ -389,8 +390,9 @@ __device__ __forceinline__ void g0_point(const GridDev<T> &G, const AdjDev<T> &A
     if (in_6) X[X_E + 5][p] = e6;
 }
 
+// FP32: 8 CTAs per SM (32 registers; 21 % faster than 4 CTAs at 64)
 template <typename T>
-__global__ void stress21_adj_g0(GridDev<T> G, AdjDev<T> A, int flag)
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 8 : 2) stress21_adj_g0(GridDev<T> G, AdjDev<T> A, int flag)
 {
     const Geo &g = G.g;
     const int nx = g.nx, ny = g.ny, nz = g.nz;
@@ -725,8 +727,9 @@ __device__ __forceinline__ void shot_views(const GridDev<T> &G, const AdjDev<T> 
 // G0 of shots 0 .. ns - 1, the shots in turn in one thread per point (the
 // coefficients' loads of the next shot hit L1; 8 % faster than putting the
 // shots of a tile in side-by-side CTAs)
+// FP32: 6 CTAs per SM (40 registers; 11 % faster than 4 at 64)
 template <typename T>
-__global__ void __launch_bounds__(256) stress21_adj_g0_shots(GridDev<T> G, AdjDev<T> A0,
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 6 : 2) stress21_adj_g0_shots(GridDev<T> G, AdjDev<T> A0,
                                                                    const __grid_constant__ AdjShots<T> S, int flag)
 {
     const Geo &g = G.g;

@@ -7,8 +7,8 @@
 //   lambda_in = Op^T lambda_out                  (in place on lambda), and
 //   g_m      += d<lambda_out, Op_m(s_in)>/dm     (gradient accumulators),
 // reading the forward fields the operator used.  They are written as reverse
-// mode of the forward code, term for term, scattering with atomics; the
-// operator order is reversed by the caller.
+// mode of the forward code, term for term; the operator order is reversed by
+// the caller.
 //
 // Operators here (one grid each):
 //   velocity update (update_vel.cpp:20-69 ranges, radius 1) and its odd halo
@@ -18,8 +18,11 @@
 //
 // Adjoint state of a grid: lambda of the 9 fields in the grid's box layout;
 // gradients: g_b at the nodes (buoyancy) and g_c[21] at the slot positions.
-// The grid operators gather where the forward gathers (no atomics) except on
-// the free-surface plane; the velocity update scatters with atomics.
+// The grid operators are gathers (each adjoint value written by one thread)
+// except the buoyancy gradient of the velocity update (the 4-node means of vy
+// and vz: atomics) and the free-surface plane.  Multi-shot variants (*_shots)
+// run the shots of a point in one thread where the shots add to a common
+// gradient, so that gradient and the medium are read once for all of them.
 // Work boxes of the stress adjoint: see the stage description below.
 #include "adjoint.cuh"
 #include "gen21_device.cuh"

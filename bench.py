@@ -359,6 +359,8 @@ def main():
     ap.add_argument("--size", default="full", choices=["full", "medium", "small"],
                     help="medium: 541x541x61 / 181x181x55 / 61x61x35 (2.9 GB, for ncu captures)")
     ap.add_argument("--energy-every", type=int, default=100)
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the sweeps' built-in z-march depth (default: ecsg_autotune before the warm-up)")
     ap.add_argument("--medium", default="tti", choices=["tti", "iso"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--grad-batch", type=int, default=8,
@@ -420,6 +422,9 @@ def main():
         pg.all_reduce(t, op=pg.ReduceOp.MAX)
         return float(t.item())
 
+    # the library's own autotuner picks the z-march depth of the FP32 sweeps of
+    # each grid (ecsg_autotune: trial sweeps, state restored), before the warm-up
+    tuned = None if args.no_autotune else sim.autotune()
     # warm-up (untimed), then the device-timed region (inputs resident in HBM,
     # 20 GB of fields and media >> 126 MB L2)
     sim.run(max(args.warmup, 3), energy_every=ev)
@@ -511,7 +516,9 @@ def main():
                                   "azimuth (Thomsen eps 0.10, delta 0.05, gamma 0.08)" if medium == "tti" else
                                   "isotropic stiffness from the seeded vp/vs/rho model (5 distinct moduli)"),
                        "points": pts, "parallelism": "replicas" if world > 1 else "single",
-                       "l2": "inputs larger than L2: %.1f GB of fields and media resident" % (dev_bytes / 1e9)},
+                       "l2": "inputs larger than L2: %.1f GB of fields and media resident" % (dev_bytes / 1e9),
+                       "z_march_chunks": ({"autotuned": True, "per_grid_vel_stress": [list(t) for t in tuned]}
+                                          if tuned is not None else {"autotuned": False})},
             "e2e": {"value": e2e, "unit": "Gcell/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "traces_finite": ok_traces},
             "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",

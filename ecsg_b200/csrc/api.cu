@@ -2315,6 +2315,7 @@ static int group_sxz_op(ecsg_sim *const *sims, int S)
     if (m->imode == ECSG_MODE_II || !m->sxz_fused)
         return each_shot(sims, S, [&](ecsg_sim *x, int) { return sxz_all_op<T>(x); });
     SxzSysList<T> L;
+    memset(&L, 0, sizeof L);
     int cta = 0;
     auto flush = [&]() -> int {
         if (!L.n) return ECSG_OK;
@@ -2324,7 +2325,6 @@ static int group_sxz_op(ecsg_sim *const *sims, int S)
         CK(launch_sxz_solve_multi<T>(L, m->st));
         return ECSG_OK;
     };
-    memset(&L, 0, sizeof L);
     for (int b = 0; b < S; b++) {
         ecsg_sim *x = sims[b];
         for (int i = 1; i < x->ng; i++) {

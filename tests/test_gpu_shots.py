@@ -10,7 +10,9 @@ shot).  Checkpointing with one level (the segment's states stored) and with
 two (sub-checkpoints every 3 steps, the form used when the segment's states
 of all shots do not fit in device memory) gives the same losses bitwise and
 the same gradient to the same tolerance (the velocity adjoint adds with
-atomics, in no fixed order)."""
+atomics, in no fixed order).  Under a checkpoint budget that three shots do
+not fit at one level, the call runs them as groups that do and sums the
+groups' gradients: the same losses bitwise and the same gradient."""
 import numpy as np
 import pytest
 

@@ -128,7 +128,8 @@ __device__ __forceinline__ void energy_point_f32_gen21(const GridDev<float> &G, 
 }
 
 // The FP32 21-Cij energy: 4 CTAs per SM, one plane per thread at a time (64
-// registers, no spills; two planes in flight spilled and measured 4 % slower).
+// registers, no spills; two planes in flight spilled and measured 4 % slower,
+// 5 and 6 CTAs per SM spilled and measured 32 % and 44 % slower).
 __global__ void __launch_bounds__(RED_THREADS, 4)
     energy_f32_gen21_kernel(GridDev<float> G, const float *vc0, const float *vc1, const float *vc2, GridDev<float> GU,
                             int flag, double *partial)
